@@ -1,0 +1,481 @@
+// Sum-factorized matrix-free cell kernels for sm_100a.
+//
+// Semantics follow Grico.jl's accumulator cell apply for TestChannels(mass*u, kappa*k(x)*∇u)
+// on axis-aligned affine cells (accumulators.jl:1003-1020, 1955-2013): gather the local
+// coefficients through the cell's term map (assembly.jl:1751-1771), interpolate value and
+// gradient at the tensor Gauss points, weight by ŵ·det J, project back and scatter
+// (assembly.jl:1788-1803).
+//
+// Schedule (differs from the reference's D + D² contractions, same result up to rounding):
+// interpolate modes -> points with the 1-D basis table B (n x q) once per axis, take
+// reference derivatives at the points with the q x q collocation matrix D of the Gauss
+// points (exact because q >= p+1), apply the pointwise flux, and run the transposed
+// sequence.  That is 2·D contractions each way instead of D + D².
+//
+// Thread layout, 3-D: one thread per (x, y) point column, the z column held in registers;
+// contractions along z are register-only, along x and y through shared memory.  CPB cells
+// share a block.  Accumulation into the global result uses atomicAdd (the reference's
+// colouring only makes its CPU scatter race-free; the GPU sums in arbitrary order, which
+// changes results at the rounding level only).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace grico {
+
+struct BatchView {
+  int32_t n_cells;
+  const int32_t* map;        // [n_cells*nbox]
+  const double* coef;        // nullable
+  const int64_t* tail_off;
+  const int32_t* tail_idx;
+  const double* tail_coef;
+  const double* h;           // [n_cells*dim]
+  const double* kappa_pts;   // nullable [n_cells*nq]
+  const double* B;           // [n*q]   B[i*q+p] = psi_i(xi_p)
+  const double* D;           // [q*q]   D[p*q+l] = L_l'(xi_p)
+  const double* W;           // [q]     reference Gauss weights
+  const double* G;           // [n*q]   reference derivative table psi_i'(xi_p)
+};
+
+template <typename T>
+__device__ __forceinline__ T gather_entry(const BatchView& b, int64_t e, const T* __restrict__ x) {
+  int v = __ldg(b.map + e);
+  if (v >= 0) return b.coef ? T(__ldg(b.coef + e)) * x[v] : x[v];
+  if (v == -1) return T(0);
+  int64_t k = -(int64_t(v) + 2);
+  T s = T(0);
+  for (int64_t t = b.tail_off[k]; t < b.tail_off[k + 1]; ++t) s += T(b.tail_coef[t]) * x[b.tail_idx[t]];
+  return s;
+}
+
+template <typename T>
+__device__ __forceinline__ void scatter_entry(const BatchView& b, int64_t e, T val, T* __restrict__ y) {
+  int v = __ldg(b.map + e);
+  if (v >= 0) {
+    atomicAdd(y + v, b.coef ? T(__ldg(b.coef + e)) * val : val);
+    return;
+  }
+  if (v == -1) return;
+  int64_t k = -(int64_t(v) + 2);
+  for (int64_t t = b.tail_off[k]; t < b.tail_off[k + 1]; ++t) atomicAdd(y + b.tail_idx[t], T(b.tail_coef[t]) * val);
+}
+
+// mode: 0 = operator apply, 1 = load (rhs) from src points, 2 = operator apply without scatter
+// masks (same as 0).
+template <int N, int Q, int CPB, typename T>
+__global__ void __launch_bounds__(Q* Q* CPB) cell_apply_3d(BatchView b, const T* __restrict__ x, T* __restrict__ y,
+                                                           int64_t n_vec, T mass, T kappa, int mode,
+                                                           const double* __restrict__ src) {
+  constexpr int Q3 = Q * Q * Q;
+  constexpr int NB = N * N * N;
+  __shared__ T sB[N * Q], sD[Q * Q], sW[Q];
+  __shared__ T S0[CPB][Q3], S1[CPB][Q3];
+  const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+  for (int i = tid; i < N * Q; i += blockDim.x * blockDim.y) sB[i] = T(b.B[i]);
+  for (int i = tid; i < Q * Q; i += blockDim.x * blockDim.y) sD[i] = T(b.D[i]);
+  for (int i = tid; i < Q; i += blockDim.x * blockDim.y) sW[i] = T(b.W[i]);
+  const int tx = threadIdx.x % Q, ty = threadIdx.x / Q, c = threadIdx.y;
+  const int64_t cell = int64_t(blockIdx.x) * CPB + c;
+  const bool act = cell < b.n_cells;
+  const int rhs = blockIdx.y;
+  x += rhs * n_vec;
+  y += rhs * n_vec;
+  T* s0 = S0[c];
+  T* s1 = S1[c];
+  __syncthreads();
+
+  T u[Q];
+  T dx[Q], dy[Q], dz[Q];
+  T h0 = 1, h1 = 1, h2 = 1;
+  if (act) {
+    h0 = T(b.h[cell * 3 + 0]);
+    h1 = T(b.h[cell * 3 + 1]);
+    h2 = T(b.h[cell * 3 + 2]);
+  }
+  const T sx = T(2) / h0, sy = T(2) / h1, sz = T(2) / h2;
+  const T detJ = h0 * h1 * h2 * T(0.125);
+
+  if (mode != 1) {
+    // ---- gather + interpolate along z (registers) ----
+    T reg[N];
+    if (act && tx < N && ty < N) {
+#pragma unroll
+      for (int k = 0; k < N; ++k) reg[k] = gather_entry<T>(b, cell * NB + tx + N * (ty + N * k), x);
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        T s = T(0);
+#pragma unroll
+        for (int k = 0; k < N; ++k) s += sB[k * Q + q] * reg[k];
+        s0[tx + Q * (ty + Q * q)] = s;
+      }
+    }
+    __syncthreads();
+    // ---- y ----
+    T col[Q];
+    if (tx < N) {
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        T s = T(0);
+#pragma unroll
+        for (int j = 0; j < N; ++j) s += sB[j * Q + ty] * s0[tx + Q * (j + Q * q)];
+        col[q] = s;
+      }
+    }
+    __syncthreads();
+    if (tx < N) {
+#pragma unroll
+      for (int q = 0; q < Q; ++q) s0[tx + Q * (ty + Q * q)] = col[q];
+    }
+    __syncthreads();
+    // ---- x ----
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      T s = T(0);
+#pragma unroll
+      for (int i = 0; i < N; ++i) s += sB[i * Q + tx] * s0[i + Q * (ty + Q * q)];
+      u[q] = s;
+    }
+    // ---- collocation derivatives ----
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      T s = T(0);
+#pragma unroll
+      for (int l = 0; l < Q; ++l) s += sD[q * Q + l] * u[l];
+      dz[q] = s;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < Q; ++q) s0[tx + Q * (ty + Q * q)] = u[q];
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      T a = T(0), bb = T(0);
+#pragma unroll
+      for (int l = 0; l < Q; ++l) {
+        a += sD[tx * Q + l] * s0[l + Q * (ty + Q * q)];
+        bb += sD[ty * Q + l] * s0[tx + Q * (l + Q * q)];
+      }
+      dx[q] = a;
+      dy[q] = bb;
+    }
+  }
+  // ---- pointwise flux ----
+  T r[Q];
+  {
+    const T wxy = sW[tx] * sW[ty] * detJ;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const T w = wxy * sW[q];
+      if (mode == 1) {
+        T f = act && src ? T(src[cell * Q3 + tx + Q * (ty + Q * q)]) : T(0);
+        r[q] = w * f;
+        dx[q] = dy[q] = dz[q] = T(0);
+      } else {
+        T k = kappa;
+        if (b.kappa_pts && act) k *= T(b.kappa_pts[cell * Q3 + tx + Q * (ty + Q * q)]);
+        const T wk = w * k;
+        r[q] = w * mass * u[q];
+        dx[q] *= wk * sx * sx;
+        dy[q] *= wk * sy * sy;
+        dz[q] *= wk * sz * sz;
+      }
+    }
+  }
+  if (mode != 1) {
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      s0[tx + Q * (ty + Q * q)] = dx[q];
+      s1[tx + Q * (ty + Q * q)] = dy[q];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int l = 0; l < Q; ++l) {
+      T s = r[l];
+#pragma unroll
+      for (int q = 0; q < Q; ++q) s += sD[q * Q + l] * dz[q];
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        s += sD[q * Q + tx] * s0[q + Q * (ty + Q * l)];
+        s += sD[q * Q + ty] * s1[tx + Q * (q + Q * l)];
+      }
+      u[l] = s;
+    }
+  } else {
+#pragma unroll
+    for (int l = 0; l < Q; ++l) u[l] = r[l];
+  }
+  // ---- transposed interpolation ----
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < Q; ++q) s0[tx + Q * (ty + Q * q)] = u[q];
+  __syncthreads();
+  T t[Q];
+  if (tx < N) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      T s = T(0);
+#pragma unroll
+      for (int p = 0; p < Q; ++p) s += sB[tx * Q + p] * s0[p + Q * (ty + Q * q)];
+      t[q] = s;
+    }
+  }
+  __syncthreads();
+  if (tx < N) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) s0[tx + Q * (ty + Q * q)] = t[q];
+  }
+  __syncthreads();
+  if (act && tx < N && ty < N) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      T s = T(0);
+#pragma unroll
+      for (int p = 0; p < Q; ++p) s += sB[ty * Q + p] * s0[tx + Q * (p + Q * q)];
+      t[q] = s;
+    }
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      T s = T(0);
+#pragma unroll
+      for (int q = 0; q < Q; ++q) s += sB[k * Q + q] * t[q];
+      scatter_entry<T>(b, cell * NB + tx + N * (ty + N * k), s, y);
+    }
+  }
+}
+
+template <int N, int Q, int CPB, typename T>
+__global__ void __launch_bounds__(Q* CPB) cell_apply_2d(BatchView b, const T* __restrict__ x, T* __restrict__ y,
+                                                        int64_t n_vec, T mass, T kappa, int mode,
+                                                        const double* __restrict__ src) {
+  constexpr int Q2 = Q * Q;
+  constexpr int NB = N * N;
+  __shared__ T sB[N * Q], sD[Q * Q], sW[Q];
+  __shared__ T S0[CPB][Q2];
+  const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+  for (int i = tid; i < N * Q; i += blockDim.x * blockDim.y) sB[i] = T(b.B[i]);
+  for (int i = tid; i < Q * Q; i += blockDim.x * blockDim.y) sD[i] = T(b.D[i]);
+  for (int i = tid; i < Q; i += blockDim.x * blockDim.y) sW[i] = T(b.W[i]);
+  const int tx = threadIdx.x, c = threadIdx.y;
+  const int64_t cell = int64_t(blockIdx.x) * CPB + c;
+  const bool act = cell < b.n_cells;
+  const int rhs = blockIdx.y;
+  x += rhs * n_vec;
+  y += rhs * n_vec;
+  T* s0 = S0[c];
+  __syncthreads();
+  T h0 = 1, h1 = 1;
+  if (act) {
+    h0 = T(b.h[cell * 2 + 0]);
+    h1 = T(b.h[cell * 2 + 1]);
+  }
+  const T sx = T(2) / h0, sy = T(2) / h1;
+  const T detJ = h0 * h1 * T(0.25);
+  T u[Q], dx[Q], dy[Q];
+  if (mode != 1) {
+    if (act && tx < N) {
+      T reg[N];
+#pragma unroll
+      for (int k = 0; k < N; ++k) reg[k] = gather_entry<T>(b, cell * NB + tx + N * k, x);
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        T s = T(0);
+#pragma unroll
+        for (int k = 0; k < N; ++k) s += sB[k * Q + q] * reg[k];
+        s0[tx + Q * q] = s;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      T s = T(0);
+#pragma unroll
+      for (int i = 0; i < N; ++i) s += sB[i * Q + tx] * s0[i + Q * q];
+      u[q] = s;
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      T s = T(0);
+#pragma unroll
+      for (int l = 0; l < Q; ++l) s += sD[q * Q + l] * u[l];
+      dy[q] = s;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < Q; ++q) s0[tx + Q * q] = u[q];
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      T s = T(0);
+#pragma unroll
+      for (int l = 0; l < Q; ++l) s += sD[tx * Q + l] * s0[l + Q * q];
+      dx[q] = s;
+    }
+  }
+  T r[Q];
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const T w = sW[tx] * sW[q] * detJ;
+    if (mode == 1) {
+      T f = act && src ? T(src[cell * Q2 + tx + Q * q]) : T(0);
+      r[q] = w * f;
+    } else {
+      T k = kappa;
+      if (b.kappa_pts && act) k *= T(b.kappa_pts[cell * Q2 + tx + Q * q]);
+      r[q] = w * mass * u[q];
+      dx[q] *= w * k * sx * sx;
+      dy[q] *= w * k * sy * sy;
+    }
+  }
+  if (mode != 1) {
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < Q; ++q) s0[tx + Q * q] = dx[q];
+    __syncthreads();
+#pragma unroll
+    for (int l = 0; l < Q; ++l) {
+      T s = r[l];
+#pragma unroll
+      for (int q = 0; q < Q; ++q) s += sD[q * Q + l] * dy[q] + sD[q * Q + tx] * s0[q + Q * l];
+      r[l] = s;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < Q; ++q) s0[tx + Q * q] = r[q];
+  __syncthreads();
+  if (act && tx < N) {
+    T t[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      T s = T(0);
+#pragma unroll
+      for (int p = 0; p < Q; ++p) s += sB[tx * Q + p] * s0[p + Q * q];
+      t[q] = s;
+    }
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      T s = T(0);
+#pragma unroll
+      for (int q = 0; q < Q; ++q) s += sB[k * Q + q] * t[q];
+      scatter_entry<T>(b, cell * NB + tx + N * k, s, y);
+    }
+  }
+}
+
+// Generic tensor-table kernel for any dimension 1..3 and any (n, q) — one block per cell,
+// threads over points then over modes; O(n^D q^D D) per cell.  Used for 1-D, q < p+1 and as
+// the diagonal kernel (mode 3: local diagonal sum of squared shape products).
+template <typename T>
+__global__ void cell_apply_generic(BatchView b, int dim, int n0, int n1, int n2, int q0, int q1, int q2,
+                                   const T* __restrict__ x, T* __restrict__ y, int64_t n_vec, T mass, T kappa,
+                                   int mode, const double* __restrict__ src) {
+  extern __shared__ unsigned char smem_raw[];
+  T* sm = reinterpret_cast<T*>(smem_raw);
+  const int q[3] = {q0, q1, q2};
+  const int nb = n0 * n1 * n2, nq = q0 * q1 * q2;
+  T* xl = sm;            // nb
+  T* flux = xl + nb;     // (dim+1)*nq
+  const int64_t cell = blockIdx.x;
+  const int rhs = blockIdx.y;
+  x += rhs * n_vec;
+  y += rhs * n_vec;
+  const int nmax = max(n0, max(n1, n2)), qmax = max(q0, max(q1, q2));
+  // tables are stored with per-axis stride nmax*qmax: B[a][i*q[a]+p]
+  T hs[3] = {1, 1, 1};
+  T detJ = 1;
+  for (int a = 0; a < dim; ++a) {
+    hs[a] = T(b.h[cell * dim + a]);
+    detJ *= hs[a] * T(0.5);
+  }
+  auto Bv = [&](int a, int i, int p) { return T(b.B[a * nmax * qmax + i * q[a] + p]); };
+  auto Gv = [&](int a, int i, int p) { return T(b.G[a * nmax * qmax + i * q[a] + p]) * (T(2) / hs[a]); };
+  auto Wv = [&](int a, int p) { return T(b.W[a * qmax + p]); };
+  if (mode == 0) {
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) xl[i] = gather_entry<T>(b, cell * nb + i, x);
+    __syncthreads();
+  }
+  if (mode != 3) {
+    for (int p = threadIdx.x; p < nq; p += blockDim.x) {
+      int pi[3] = {p % q0, (p / q0) % q1, p / (q0 * q1)};
+      T w = detJ;
+      for (int a = 0; a < dim; ++a) w *= Wv(a, pi[a]);
+      if (mode == 1) {
+        flux[p] = w * (src ? T(src[cell * nq + p]) : T(0));
+        for (int a = 0; a < dim; ++a) flux[(a + 1) * nq + p] = T(0);
+        continue;
+      }
+      T uval = 0, g[3] = {0, 0, 0};
+      for (int i = 0; i < nb; ++i) {
+        int mi[3] = {i % n0, (i / n0) % n1, i / (n0 * n1)};
+        T bv[3] = {1, 1, 1};
+        for (int a = 0; a < dim; ++a) bv[a] = Bv(a, mi[a], pi[a]);
+        T prod = bv[0] * bv[1] * bv[2];
+        uval += xl[i] * prod;
+        for (int a = 0; a < dim; ++a) {
+          T gg = Gv(a, mi[a], pi[a]);
+          for (int e = 0; e < dim; ++e)
+            if (e != a) gg *= bv[e];
+          g[a] += xl[i] * gg;
+        }
+      }
+      T k = kappa;
+      if (b.kappa_pts) k *= T(b.kappa_pts[cell * nq + p]);
+      flux[p] = w * mass * uval;
+      for (int a = 0; a < dim; ++a) flux[(a + 1) * nq + p] = w * k * g[a];
+    }
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+    int mi[3] = {i % n0, (i / n0) % n1, i / (n0 * n1)};
+    T acc = 0;
+    for (int p = 0; p < nq; ++p) {
+      int pi[3] = {p % q0, (p / q0) % q1, p / (q0 * q1)};
+      T bv[3] = {1, 1, 1};
+      for (int a = 0; a < dim; ++a) bv[a] = Bv(a, mi[a], pi[a]);
+      T prod = bv[0] * bv[1] * bv[2];
+      if (mode == 3) {
+        T w = detJ;
+        for (int a = 0; a < dim; ++a) w *= Wv(a, pi[a]);
+        T k = kappa;
+        if (b.kappa_pts) k *= T(b.kappa_pts[cell * nq + p]);
+        T s = mass * prod * prod;
+        for (int a = 0; a < dim; ++a) {
+          T gg = Gv(a, mi[a], pi[a]);
+          for (int e = 0; e < dim; ++e)
+            if (e != a) gg *= bv[e];
+          s += k * gg * gg;
+        }
+        acc += w * s;
+        continue;
+      }
+      acc += flux[p] * prod;
+      for (int a = 0; a < dim; ++a) {
+        T gg = Gv(a, mi[a], pi[a]);
+        for (int e = 0; e < dim; ++e)
+          if (e != a) gg *= bv[e];
+        acc += flux[(a + 1) * nq + p] * gg;
+      }
+    }
+    if (mode == 3) {
+      // diagonal: coefficient squared scatter (assembly.jl:1811-1825)
+      int v = b.map[cell * nb + i];
+      if (v >= 0) {
+        T cc = b.coef ? T(b.coef[cell * nb + i]) : T(1);
+        atomicAdd(y + v, cc * cc * acc);
+      } else if (v <= -2) {
+        int64_t kk = -(int64_t(v) + 2);
+        for (int64_t t = b.tail_off[kk]; t < b.tail_off[kk + 1]; ++t) {
+          T cc = T(b.tail_coef[t]);
+          atomicAdd(y + b.tail_idx[t], cc * cc * acc);
+        }
+      }
+    } else {
+      scatter_entry<T>(b, cell * nb + i, acc, y);
+    }
+  }
+}
+
+}  // namespace grico

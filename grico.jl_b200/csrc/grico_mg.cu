@@ -1,0 +1,380 @@
+// hp geometric multigrid V-cycle on the device (multigrid.jl:858-1087).
+//
+// Levels are device plans (coarse -> fine).  Transfers are the reduced-space prolongations
+// P_l (coarse -> fine, CSR over fine rows); restriction uses the explicit transpose (CSR over
+// coarse rows) so both directions are gathers without atomics.  Smoothers:
+//   * damped Jacobi x += w D^-1 (b - A x)   — the reference's SPD smoother (multigrid.jl:943-956)
+//   * Chebyshev-Jacobi of a given degree on [lambda_max*lower, 1.2*lambda_max] of D^-1 A, with
+//     lambda_max from a power iteration at set-up — no reference counterpart.
+// The coarsest level is solved in FP64 with the dense Cholesky factor of its reduced matrix
+// (common.jl:272-330); the factor is inverted once on the host and applied as a dense
+// matrix-vector product.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <memory>
+#include <vector>
+
+#include "grico_host.h"
+#include "grico_mg_internal.h"
+#include "grico_plan_internal.h"
+#include "vector_kernels.cuh"
+
+struct GricoMultigrid {
+  struct Transfer {
+    int64_t nf = 0, nc = 0;
+    grico::DevBuf p_off, p_idx, p_val;  // fine rows
+    grico::DevBuf r_off, r_idx, r_val;  // coarse rows (transpose)
+  };
+  std::vector<GricoPlan*> levels;
+  std::vector<Transfer> xfer;
+  std::vector<grico::DevBuf> dinv, b, x, r, t, d;
+  std::vector<double> lmax;
+  grico::DevBuf coarse_inv;
+  int64_t n0 = 0;
+  GricoMGOptions opts{};
+  cudaStream_t stream = nullptr;
+  grico::DevBuf io_r, io_z;
+};
+
+namespace grico {
+
+namespace {
+
+__global__ void csr_gather(const int64_t* __restrict__ off, const int64_t* __restrict__ idx,
+                           const double* __restrict__ val, const double* __restrict__ x, double* __restrict__ y,
+                           int64_t nrows, int accumulate) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nrows; i += int64_t(gridDim.x) * blockDim.x) {
+    double s = 0.0;
+    for (int64_t t = off[i]; t < off[i + 1]; ++t) s += val[t] * x[idx[t]];
+    y[i] = accumulate ? y[i] + s : s;
+  }
+}
+
+// x += w * dinv * (b - ax)
+__global__ void jacobi_smooth(double* __restrict__ x, const double* __restrict__ b, const double* __restrict__ ax,
+                              const double* __restrict__ dinv, double w, int64_t n) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    x[i] += w * dinv[i] * (b[i] - ax[i]);
+}
+
+// d = c1*d + c2*dinv*(b - ax); x += d
+__global__ void chebyshev_step(double* __restrict__ x, double* __restrict__ d, const double* __restrict__ b,
+                               const double* __restrict__ ax, const double* __restrict__ dinv, double c1, double c2,
+                               int64_t n) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    double di = c1 * d[i] + c2 * dinv[i] * (b[i] - ax[i]);
+    d[i] = di;
+    x[i] += di;
+  }
+}
+
+// r = b - ax
+__global__ void residual_kernel(double* __restrict__ r, const double* __restrict__ b, const double* __restrict__ ax,
+                                int64_t n) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    r[i] = b[i] - ax[i];
+}
+
+// y = M x for a dense row-major n x n matrix (one warp per row)
+__global__ void dense_matvec(const double* __restrict__ M, const double* __restrict__ x, double* __restrict__ y, int64_t n) {
+  const int lane = threadIdx.x & 31;
+  const int64_t row = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
+  if (row >= n) return;
+  double s = 0.0;
+  for (int64_t j = lane; j < n; j += 32) s += M[row * n + j] * x[j];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0) y[row] = s;
+}
+
+int blocks(int64_t n) { return int(std::min<int64_t>((n + 255) / 256, 148 * 8)); }
+
+// Dense Cholesky A = L L^T in place (lower triangle), restating common.jl:272-300.
+bool cholesky(std::vector<double>& a, int64_t n) {
+  for (int64_t j = 0; j < n; ++j) {
+    double s = a[j * n + j];
+    for (int64_t k = 0; k < j; ++k) s -= a[j * n + k] * a[j * n + k];
+    if (!(s > 0.0) || !std::isfinite(s)) return false;
+    double ljj = std::sqrt(s);
+    a[j * n + j] = ljj;
+    for (int64_t i = j + 1; i < n; ++i) {
+      double v = a[i * n + j];
+      for (int64_t k = 0; k < j; ++k) v -= a[i * n + k] * a[j * n + k];
+      a[i * n + j] = v / ljj;
+    }
+  }
+  return true;
+}
+
+// Solve L L^T x = b on the host (common.jl:302-330)
+void cholesky_solve(const std::vector<double>& l, int64_t n, std::vector<double>& x) {
+  for (int64_t i = 0; i < n; ++i) {
+    double v = x[i];
+    for (int64_t k = 0; k < i; ++k) v -= l[i * n + k] * x[k];
+    x[i] = v / l[i * n + i];
+  }
+  for (int64_t i = n - 1; i >= 0; --i) {
+    double v = x[i];
+    for (int64_t k = i + 1; k < n; ++k) v -= l[k * n + i] * x[k];
+    x[i] = v / l[i * n + i];
+  }
+}
+
+void level_apply(GricoMultigrid* mg, int l, const double* x, double* y, cudaStream_t st) {
+  run_apply<double>(mg->levels[l], true, x, y, 1, st);
+}
+
+void smooth(GricoMultigrid* mg, int l, double* x, const double* b, int steps, cudaStream_t st) {
+  const int64_t n = mg->levels[l]->n_red;
+  double* t = mg->t[l].get<double>();
+  const double* dinv = mg->dinv[l].get<double>();
+  if (steps <= 0) return;
+  if (mg->opts.smoother == GRICO_SMOOTHER_JACOBI) {
+    for (int s = 0; s < steps; ++s) {
+      level_apply(mg, l, x, t, st);
+      jacobi_smooth<<<blocks(n), 256, 0, st>>>(x, b, t, dinv, mg->opts.jacobi_omega, n);
+    }
+    return;
+  }
+  const double lmax = 1.2 * mg->lmax[l];
+  const double lmin = lmax * mg->opts.chebyshev_lower;
+  const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin);
+  const double sigma = theta / delta;
+  double* d = mg->d[l].get<double>();
+  for (int s = 0; s < steps; ++s) {
+    double rho_old = 1.0 / sigma;
+    for (int k = 0; k < mg->opts.chebyshev_degree; ++k) {
+      level_apply(mg, l, x, t, st);
+      if (k == 0) {
+        chebyshev_step<<<blocks(n), 256, 0, st>>>(x, d, b, t, dinv, 0.0, 1.0 / theta, n);
+      } else {
+        const double rho = 1.0 / (2.0 * sigma - rho_old);
+        chebyshev_step<<<blocks(n), 256, 0, st>>>(x, d, b, t, dinv, rho * rho_old, 2.0 * rho / delta, n);
+        rho_old = rho;
+      }
+    }
+  }
+}
+
+void vcycle(GricoMultigrid* mg, int l, double* x, const double* b, cudaStream_t st) {
+  const int64_t n = mg->levels[l]->n_red;
+  cudaMemsetAsync(x, 0, sizeof(double) * n, st);
+  if (l == 0) {
+    if (n > 0) dense_matvec<<<int((n * 32 + 255) / 256), 256, 0, st>>>(mg->coarse_inv.get<double>(), b, x, n);
+    return;
+  }
+  smooth(mg, l, x, b, mg->opts.pre_steps, st);
+  double* t = mg->t[l].get<double>();
+  double* r = mg->r[l].get<double>();
+  level_apply(mg, l, x, t, st);
+  residual_kernel<<<blocks(n), 256, 0, st>>>(r, b, t, n);
+  auto& X = mg->xfer[l - 1];
+  double* bc = mg->b[l - 1].get<double>();
+  double* xc = mg->x[l - 1].get<double>();
+  csr_gather<<<blocks(X.nc), 256, 0, st>>>(X.r_off.get<int64_t>(), X.r_idx.get<int64_t>(), X.r_val.get<double>(), r,
+                                           bc, X.nc, 0);
+  vcycle(mg, l - 1, xc, bc, st);
+  csr_gather<<<blocks(X.nf), 256, 0, st>>>(X.p_off.get<int64_t>(), X.p_idx.get<int64_t>(), X.p_val.get<double>(), xc,
+                                           x, X.nf, 1);
+  smooth(mg, l, x, b, mg->opts.post_steps, st);
+}
+
+}  // namespace
+
+int mg_vcycle_device(GricoMultigrid* mg, const double* r, double* z, cudaStream_t st) {
+  if (!mg) return GRICO_ERR_INVALID;
+  const int L = int(mg->levels.size());
+  vcycle(mg, L - 1, z, r, st);
+  return cuda_ok(cudaGetLastError(), "vcycle") ? GRICO_OK : GRICO_ERR_CUDA;
+}
+
+int prepare_jacobi(GricoPlan* P, cudaStream_t st);
+
+}  // namespace grico
+
+using namespace grico;
+
+extern "C" {
+
+int grico_mg_create(GricoPlan* const* levels, int nlevels, const GricoTransferDesc* transfers,
+                    const double* coarse_matrix, const GricoMGOptions* opts, GricoMultigrid** out) {
+  if (!levels || nlevels < 1 || !opts || !out || (nlevels > 1 && !transfers)) {
+    set_error("grico_mg_create: invalid argument");
+    return GRICO_ERR_INVALID;
+  }
+  if (opts->smoother != GRICO_SMOOTHER_JACOBI && opts->smoother != GRICO_SMOOTHER_CHEBYSHEV) {
+    set_error("grico_mg_create: unknown smoother");
+    return GRICO_ERR_INVALID;
+  }
+  if (opts->smoother == GRICO_SMOOTHER_CHEBYSHEV && (opts->chebyshev_degree < 1 || !(opts->chebyshev_lower > 0.0 && opts->chebyshev_lower < 1.0))) {
+    set_error("grico_mg_create: Chebyshev degree must be >= 1 and the lower bound fraction in (0,1)");
+    return GRICO_ERR_INVALID;
+  }
+  std::unique_ptr<GricoMultigrid> mg(new GricoMultigrid());
+  mg->opts = *opts;
+  mg->stream = levels[nlevels - 1]->stream;
+  cudaStream_t st = mg->stream;
+  for (int l = 0; l < nlevels; ++l) {
+    if (!levels[l]) { set_error("grico_mg_create: null level"); return GRICO_ERR_INVALID; }
+    mg->levels.push_back(levels[l]);
+  }
+  mg->dinv.resize(nlevels);
+  mg->b.resize(nlevels);
+  mg->x.resize(nlevels);
+  mg->r.resize(nlevels);
+  mg->t.resize(nlevels);
+  mg->d.resize(nlevels);
+  mg->lmax.assign(nlevels, 0.0);
+  for (int l = 0; l < nlevels; ++l) {
+    const int64_t n = std::max<int64_t>(levels[l]->n_red, 1);
+    if (!mg->b[l].alloc(8 * n) || !mg->x[l].alloc(8 * n) || !mg->r[l].alloc(8 * n) || !mg->t[l].alloc(8 * n) ||
+        !mg->d[l].alloc(8 * n))
+      return GRICO_ERR_CUDA;
+    if (l > 0) {
+      int rc = prepare_jacobi(levels[l], st);
+      if (rc) return rc;
+      if (!mg->dinv[l].alloc(8 * n)) return GRICO_ERR_CUDA;
+      cudaMemcpyAsync(mg->dinv[l].ptr, levels[l]->w_dinv.ptr, 8 * levels[l]->n_red, cudaMemcpyDeviceToDevice, st);
+    }
+  }
+  for (int l = 0; l + 1 < nlevels; ++l) {
+    const GricoTransferDesc& T = transfers[l];
+    if (T.n_fine != levels[l + 1]->n_red || T.n_coarse != levels[l]->n_red) {
+      set_error("grico_mg_create: transfer sizes do not match the level plans");
+      return GRICO_ERR_INVALID;
+    }
+    GricoMultigrid::Transfer X;
+    X.nf = T.n_fine;
+    X.nc = T.n_coarse;
+    const int64_t nnz = T.row_offsets[T.n_fine];
+    for (int64_t k = 0; k < nnz; ++k)
+      if (T.col_index[k] < 0 || T.col_index[k] >= T.n_coarse) { set_error("transfer column out of range"); return GRICO_ERR_INVALID; }
+    // transpose on the host (coarse rows), keeping fine-row order inside each coarse row
+    std::vector<int64_t> roff(T.n_coarse + 1, 0), ridx(nnz);
+    std::vector<double> rval(nnz);
+    for (int64_t k = 0; k < nnz; ++k) roff[T.col_index[k] + 1]++;
+    for (int64_t c = 0; c < T.n_coarse; ++c) roff[c + 1] += roff[c];
+    std::vector<int64_t> fill(roff.begin(), roff.end() - 1);
+    for (int64_t f = 0; f < T.n_fine; ++f)
+      for (int64_t k = T.row_offsets[f]; k < T.row_offsets[f + 1]; ++k) {
+        int64_t pos = fill[T.col_index[k]]++;
+        ridx[pos] = f;
+        rval[pos] = T.values[k];
+      }
+    bool ok = X.p_off.upload(T.row_offsets, size_t(T.n_fine + 1)) && X.p_idx.upload(T.col_index, size_t(nnz)) &&
+              X.p_val.upload(T.values, size_t(nnz)) && X.r_off.upload(roff) && X.r_idx.upload(ridx) &&
+              X.r_val.upload(rval);
+    if (!ok) return GRICO_ERR_CUDA;
+    mg->xfer.push_back(std::move(X));
+  }
+  // coarse matrix: given, or assembled by probing the coarsest reduced operator
+  const int64_t n0 = levels[0]->n_red;
+  mg->n0 = n0;
+  if (n0 > 4096) { set_error("coarse level too large for the dense Cholesky solve (n > 4096)"); return GRICO_ERR_INVALID; }
+  std::vector<double> A(n0 * n0, 0.0);
+  if (coarse_matrix) {
+    std::copy(coarse_matrix, coarse_matrix + n0 * n0, A.begin());
+  } else if (n0 > 0) {
+    DevBuf e, col;
+    if (!e.alloc(8 * n0) || !col.alloc(8 * n0)) return GRICO_ERR_CUDA;
+    std::vector<double> h(n0);
+    for (int64_t j = 0; j < n0; ++j) {
+      cudaMemsetAsync(e.ptr, 0, 8 * n0, st);
+      double one = 1.0;
+      cudaMemcpyAsync(e.get<double>() + j, &one, 8, cudaMemcpyHostToDevice, st);
+      run_apply<double>(levels[0], true, e.get<double>(), col.get<double>(), 1, st);
+      cudaMemcpyAsync(h.data(), col.ptr, 8 * n0, cudaMemcpyDeviceToHost, st);
+      cudaStreamSynchronize(st);
+      for (int64_t i = 0; i < n0; ++i) A[i * n0 + j] = h[i];
+    }
+  }
+  if (n0 > 0) {
+    // symmetrize check (multigrid.jl:400-420) then factor
+    double scale = 0.0;
+    for (double v : A) scale = std::max(scale, std::fabs(v));
+    for (int64_t i = 0; i < n0; ++i)
+      for (int64_t j = i + 1; j < n0; ++j)
+        if (std::fabs(A[i * n0 + j] - A[j * n0 + i]) > 1.4901161193847656e-08 * scale) {
+          set_error("declared SPD coarse multigrid matrix is not numerically symmetric");
+          return GRICO_ERR_INVALID;
+        }
+    std::vector<double> Lf = A;
+    if (!cholesky(Lf, n0)) { set_error("declared SPD coarse multigrid matrix is not positive definite"); return GRICO_ERR_INVALID; }
+    std::vector<double> inv(n0 * n0);
+    std::vector<double> col(n0);
+    for (int64_t j = 0; j < n0; ++j) {
+      std::fill(col.begin(), col.end(), 0.0);
+      col[j] = 1.0;
+      cholesky_solve(Lf, n0, col);
+      for (int64_t i = 0; i < n0; ++i) inv[i * n0 + j] = col[i];
+    }
+    if (!mg->coarse_inv.upload(inv)) return GRICO_ERR_CUDA;
+  }
+  // Chebyshev: lambda_max(D^-1 A) per smoothed level by power iteration
+  if (opts->smoother == GRICO_SMOOTHER_CHEBYSHEV) {
+    for (int l = 1; l < nlevels; ++l) {
+      const int64_t n = levels[l]->n_red;
+      if (n == 0) continue;
+      std::vector<double> v(n);
+      uint64_t s = 0x9e3779b97f4a7c15ull + uint64_t(l);
+      for (int64_t i = 0; i < n; ++i) {
+        s ^= s << 13; s ^= s >> 7; s ^= s << 17;
+        v[i] = 0.5 + double(s % 1000003) / 1000003.0;
+      }
+      double* x = mg->x[l].get<double>();
+      double* t = mg->t[l].get<double>();
+      cudaMemcpyAsync(x, v.data(), 8 * n, cudaMemcpyHostToDevice, st);
+      double lam = 0.0;
+      for (int it = 0; it < 20; ++it) {
+        run_apply<double>(levels[l], true, x, t, 1, st);
+        scale_kernel<double><<<blocks(n), 256, 0, st>>>(mg->dinv[l].get<double>(), t, t, n);
+        double* sc_dev = levels[l]->scalars.get<double>() + 12;
+        dot_partial<double><<<kRedBlocks, kRedThreads, 0, st>>>(t, t, n, levels[l]->partial.get<double>());
+        reduce_final<<<1, kRedThreads, 0, st>>>(levels[l]->partial.get<double>(), kRedBlocks, sc_dev);
+        dot_partial<double><<<kRedBlocks, kRedThreads, 0, st>>>(x, x, n, levels[l]->partial.get<double>());
+        reduce_final<<<1, kRedThreads, 0, st>>>(levels[l]->partial.get<double>(), kRedBlocks, sc_dev + 1);
+        double sc[2];
+        cudaMemcpyAsync(sc, sc_dev, 16, cudaMemcpyDeviceToHost, st);
+        cudaStreamSynchronize(st);
+        const double tn = std::sqrt(sc[0]), xn = std::sqrt(sc[1]);
+        if (!(tn > 0.0) || !(xn > 0.0)) break;
+        lam = tn / xn;  // power-iteration estimate of the spectral radius of D^-1 A
+        axpby_kernel<double><<<blocks(n), 256, 0, st>>>(1.0 / tn, t, 0.0, x, n);
+      }
+      mg->lmax[l] = lam;
+    }
+  }
+  if (!cuda_ok(cudaStreamSynchronize(st), "mg create")) return GRICO_ERR_CUDA;
+  *out = mg.release();
+  return GRICO_OK;
+}
+
+int grico_mg_destroy(GricoMultigrid* mg) {
+  delete mg;
+  return GRICO_OK;
+}
+
+int grico_mg_vcycle(GricoMultigrid* mg, const double* r, double* z, int flags) {
+  if (!mg || !r || !z) return GRICO_ERR_INVALID;
+  cudaStream_t st = mg->stream;
+  const int64_t n = mg->levels.back()->n_red;
+  const double* rd = r;
+  double* zd = z;
+  if (flags & GRICO_FLAG_HOST_POINTERS) {
+    if (!mg->io_r.ensure(8 * std::max<int64_t>(n, 1)) || !mg->io_z.ensure(8 * std::max<int64_t>(n, 1))) return GRICO_ERR_CUDA;
+    cudaMemcpyAsync(mg->io_r.ptr, r, 8 * n, cudaMemcpyHostToDevice, st);
+    rd = mg->io_r.get<double>();
+    zd = mg->io_z.get<double>();
+  }
+  int rc = mg_vcycle_device(mg, rd, zd, st);
+  if (rc) return rc;
+  if (flags & GRICO_FLAG_HOST_POINTERS) cudaMemcpyAsync(z, zd, 8 * n, cudaMemcpyDeviceToHost, st);
+  return cuda_ok(cudaStreamSynchronize(st), "vcycle") ? GRICO_OK : GRICO_ERR_CUDA;
+}
+
+double grico_mg_lambda_max(GricoMultigrid* mg, int level) {
+  if (!mg || level < 0 || level >= int(mg->lmax.size())) return -1.0;
+  return mg->lmax[level];
+}
+
+}  // extern "C"

@@ -1,0 +1,460 @@
+// Device plan of the matrix-free runtime: the B200 counterpart of the runtime half of
+// Grico.jl's AssemblyPlan (plans.jl:131-145) plus its reduced operator map
+// (assembly.jl:19-27).  C ABI in include/grico_b200.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "cell_kernels.cuh"
+#include "grico_host.h"
+#include "grico_plan_internal.h"
+#include "vector_kernels.cuh"
+
+namespace grico {
+
+DevBuf::~DevBuf() {
+  if (ptr) cudaFree(ptr);
+}
+
+bool cuda_ok(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return true;
+  set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  return false;
+}
+
+// Lagrange collocation derivative on Gauss points via barycentric weights:
+// D[p*q+l] = L_l'(xi_p).
+std::vector<double> collocation_derivative(const std::vector<double>& xi) {
+  const int q = int(xi.size());
+  std::vector<double> lam(q, 1.0), D(q * q, 0.0);
+  for (int j = 0; j < q; ++j)
+    for (int k = 0; k < q; ++k)
+      if (k != j) lam[j] /= (xi[j] - xi[k]);
+  for (int p = 0; p < q; ++p) {
+    double diag = 0.0;
+    for (int l = 0; l < q; ++l) {
+      if (l == p) continue;
+      double v = (lam[l] / lam[p]) / (xi[p] - xi[l]);
+      D[p * q + l] = v;
+      diag -= v;
+    }
+    D[p * q + p] = diag;
+  }
+  return D;
+}
+
+namespace {
+
+int64_t box_count(int dim, const int* deg) {
+  int64_t nb = 1;
+  for (int a = 0; a < dim; ++a) nb *= deg[a] + 1;
+  return nb;
+}
+
+// Compose the cell term map with the reduced map P: every local entry becomes a sparse
+// combination of reduced dofs (the composition x_loc = T P x_red used by reduced applies).
+void compose_reduced(const GricoCellBatchDesc& bd, int64_t nb, const GricoPlanDesc& d,
+                     std::vector<int32_t>& map, std::vector<double>& coef, bool& need_coef,
+                     std::vector<int64_t>& toff, std::vector<int32_t>& tidx, std::vector<double>& tcoef) {
+  const int64_t ne = int64_t(bd.n_cells) * nb;
+  map.assign(ne, -1);
+  coef.assign(ne, 1.0);
+  need_coef = false;
+  toff.assign(1, 0);
+  tidx.clear();
+  tcoef.clear();
+  std::vector<std::pair<int64_t, double>> acc;
+  auto add = [&](int64_t r, double c) {
+    for (auto& t : acc)
+      if (t.first == r) { t.second += c; return; }
+    acc.emplace_back(r, c);
+  };
+  auto add_full = [&](int64_t g, double c) {
+    for (int64_t t = d.red_offsets[g]; t < d.red_offsets[g + 1]; ++t) add(d.red_index[t], c * d.red_coef[t]);
+  };
+  for (int64_t e = 0; e < ne; ++e) {
+    int32_t v = bd.map_index[e];
+    if (v == -1) continue;
+    acc.clear();
+    if (v >= 0) {
+      add_full(v, bd.map_coef ? bd.map_coef[e] : 1.0);
+    } else {
+      int64_t k = -(int64_t(v) + 2);
+      for (int64_t t = bd.tail_offsets[k]; t < bd.tail_offsets[k + 1]; ++t) add_full(bd.tail_index[t], bd.tail_coef[t]);
+    }
+    acc.erase(std::remove_if(acc.begin(), acc.end(), [](auto& t) { return t.second == 0.0; }), acc.end());
+    if (acc.empty()) continue;
+    if (acc.size() == 1) {
+      map[e] = int32_t(acc[0].first);
+      coef[e] = acc[0].second;
+      if (acc[0].second != 1.0) need_coef = true;
+    } else {
+      map[e] = -int32_t(toff.size() - 1) - 2;
+      for (auto& t : acc) {
+        tidx.push_back(int32_t(t.first));
+        tcoef.push_back(t.second);
+      }
+      toff.push_back(int64_t(tidx.size()));
+    }
+  }
+}
+
+void fill_view(BatchView& v, const DevBatch& b, bool reduced) {
+  v.n_cells = b.n_cells;
+  const DevMap& m = reduced ? b.red : b.full;
+  v.map = m.map.get<int32_t>();
+  v.coef = m.coef.get<double>();
+  v.tail_off = m.toff.get<int64_t>();
+  v.tail_idx = m.tidx.get<int32_t>();
+  v.tail_coef = m.tcoef.get<double>();
+  v.h = b.h.get<double>();
+  v.kappa_pts = b.kappa.get<double>();
+  v.B = b.B.get<double>();
+  v.D = b.D.get<double>();
+  v.W = b.W.get<double>();
+  v.G = b.G.get<double>();
+}
+
+template <typename T>
+bool launch_fused(int dim, int N, int Q, const BatchView& v, const T* x, T* y, int64_t nvec, T mass, T kappa, int mode,
+                  const double* src, int nrhs, cudaStream_t st) {
+  if (v.n_cells == 0) return true;
+#define GRICO_L3(NN, QQ)                                                                                     \
+  if (N == NN && Q == QQ) {                                                                                  \
+    constexpr int CPB = (256 / (QQ * QQ)) > 0 ? (256 / (QQ * QQ)) : 1;                                       \
+    dim3 block(QQ * QQ, CPB), grid((v.n_cells + CPB - 1) / CPB, nrhs);                                       \
+    cell_apply_3d<NN, QQ, CPB, T><<<grid, block, 0, st>>>(v, x, y, nvec, mass, kappa, mode, src);            \
+    return true;                                                                                             \
+  }
+#define GRICO_L2(NN, QQ)                                                                                     \
+  if (N == NN && Q == QQ) {                                                                                  \
+    constexpr int CPB = (128 / QQ) > 0 ? (128 / QQ) : 1;                                                     \
+    dim3 block(QQ, CPB), grid((v.n_cells + CPB - 1) / CPB, nrhs);                                            \
+    cell_apply_2d<NN, QQ, CPB, T><<<grid, block, 0, st>>>(v, x, y, nvec, mass, kappa, mode, src);            \
+    return true;                                                                                             \
+  }
+  if (dim == 3) {
+    GRICO_L3(2, 2) GRICO_L3(3, 3) GRICO_L3(4, 4) GRICO_L3(5, 5) GRICO_L3(6, 6) GRICO_L3(7, 7) GRICO_L3(8, 8)
+    GRICO_L3(9, 9) GRICO_L3(2, 3) GRICO_L3(3, 4) GRICO_L3(4, 5) GRICO_L3(5, 6)
+  } else if (dim == 2) {
+    GRICO_L2(2, 2) GRICO_L2(3, 3) GRICO_L2(4, 4) GRICO_L2(5, 5) GRICO_L2(6, 6) GRICO_L2(7, 7) GRICO_L2(8, 8)
+    GRICO_L2(9, 9) GRICO_L2(2, 3) GRICO_L2(3, 4) GRICO_L2(4, 5) GRICO_L2(5, 6)
+  }
+#undef GRICO_L3
+#undef GRICO_L2
+  return false;
+}
+
+template <typename T>
+void launch_batch(const GricoPlan& P, const DevBatch& b, bool reduced, const T* x, T* y, int64_t nvec, int mode,
+                  const double* src, int nrhs, cudaStream_t st) {
+  BatchView v;
+  fill_view(v, b, reduced);
+  const int dim = P.dim;
+  if (mode != 3 && b.isotropic && b.q[0] >= b.n[0] &&
+      launch_fused<T>(dim, b.n[0], b.q[0], v, x, y, nvec, T(P.mass), T(P.kappa), mode, src, nrhs, st))
+    return;
+  int n[3] = {1, 1, 1}, q[3] = {1, 1, 1};
+  for (int a = 0; a < dim; ++a) { n[a] = b.n[a]; q[a] = b.q[a]; }
+  int nb = n[0] * n[1] * n[2], nq = q[0] * q[1] * q[2];
+  size_t smem = sizeof(T) * (nb + (dim + 1) * nq);
+  if (smem > 48 * 1024) cudaFuncSetAttribute(cell_apply_generic<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  dim3 grid(b.n_cells, nrhs);
+  cell_apply_generic<T><<<grid, 128, smem, st>>>(v, dim, n[0], n[1], n[2], q[0], q[1], q[2], x, y, nvec, T(P.mass),
+                                                T(P.kappa), mode, src);
+}
+
+int grid_for(int64_t n) { return int(std::min<int64_t>((n + 255) / 256, 148 * 16)); }
+
+}  // namespace
+
+template <typename T>
+int run_apply(GricoPlan* P, bool reduced, const T* x, T* y, int nrhs, cudaStream_t st) {
+  const int64_t n = reduced ? P->n_red : P->n_full;
+  if (nrhs < 1) return GRICO_ERR_INVALID;
+  cudaMemsetAsync(y, 0, sizeof(T) * n * nrhs, st);
+  for (auto& b : P->batches) launch_batch<T>(*P, b, reduced, x, y, n, 0, nullptr, nrhs, st);
+  if (!reduced && (P->n_fixed + P->n_rel) > 0) {
+    dim3 grid(grid_for(P->n_fixed + P->n_rel), nrhs);
+    constraint_action<T><<<grid, 256, 0, st>>>(P->fixed.get<int64_t>(), P->n_fixed, P->rel_piv.get<int64_t>(),
+                                               P->rel_off.get<int64_t>(), P->rel_idx.get<int64_t>(),
+                                               P->rel_coef.get<double>(), P->n_rel, x, y, n);
+  }
+  return cuda_ok(cudaGetLastError(), "apply launch") ? GRICO_OK : GRICO_ERR_CUDA;
+}
+
+template int run_apply<double>(GricoPlan*, bool, const double*, double*, int, cudaStream_t);
+template int run_apply<float>(GricoPlan*, bool, const float*, float*, int, cudaStream_t);
+
+int reduced_diag_device(GricoPlan* P, double* diag, cudaStream_t st) {
+  cudaMemsetAsync(diag, 0, sizeof(double) * P->n_red, st);
+  for (auto& b : P->batches) launch_batch<double>(*P, b, true, nullptr, diag, P->n_red, 3, nullptr, 1, st);
+  return cuda_ok(cudaGetLastError(), "diagonal launch") ? GRICO_OK : GRICO_ERR_CUDA;
+}
+
+}  // namespace grico
+
+using namespace grico;
+
+extern "C" {
+
+int grico_plan_create(const GricoPlanDesc* d, GricoPlan** out) {
+  if (!d || !out) { set_error("grico_plan_create: null argument"); return GRICO_ERR_INVALID; }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    set_error("grico_plan_create: no CUDA device (the library has no CPU fallback)");
+    return GRICO_ERR_NO_DEVICE;
+  }
+  if (d->form != GRICO_FORM_MASS_DIFFUSION) { set_error("unsupported accumulator form"); return GRICO_ERR_UNSUPPORTED_FORM; }
+  if (d->dim < 1 || d->dim > 3 || d->n_full < 0 || d->n_reduced < 0 || d->n_batches < 0) {
+    set_error("grico_plan_create: invalid sizes");
+    return GRICO_ERR_INVALID;
+  }
+  if (d->n_full >= (int64_t(1) << 31)) { set_error("grico_plan_create: more than 2^31-1 dofs"); return GRICO_ERR_INVALID; }
+  std::unique_ptr<GricoPlan> P(new GricoPlan());
+  P->dim = d->dim;
+  P->mass = d->mass;
+  P->kappa = d->kappa;
+  P->n_full = d->n_full;
+  P->n_red = d->n_reduced;
+  if (!cuda_ok(cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking), "stream")) return GRICO_ERR_CUDA;
+  for (int bi = 0; bi < d->n_batches; ++bi) {
+    const GricoCellBatchDesc& bd = d->batches[bi];
+    DevBatch b;
+    b.n_cells = bd.n_cells;
+    int nmax = 1, qmax = 1;
+    for (int a = 0; a < d->dim; ++a) {
+      b.n[a] = bd.degree[a] + 1;
+      b.q[a] = bd.qpoints[a];
+      if (b.q[a] < 1 || b.n[a] < 1 || b.n[a] > 16 || b.q[a] > 16) { set_error("batch degree/quadrature out of range"); return GRICO_ERR_INVALID; }
+      nmax = std::max(nmax, b.n[a]);
+      qmax = std::max(qmax, b.q[a]);
+    }
+    b.isotropic = true;
+    for (int a = 1; a < d->dim; ++a) b.isotropic &= (b.n[a] == b.n[0] && b.q[a] == b.q[0]);
+    const int64_t nb = box_count(d->dim, b.n);
+    const int64_t ne = int64_t(bd.n_cells) * nb;
+    for (int64_t e = 0; e < ne; ++e) {
+      int32_t v = bd.map_index[e];
+      if (v >= d->n_full || (v <= -2 && -(int64_t(v) + 2) >= bd.n_tail)) {
+        set_error("batch map index out of range");
+        return GRICO_ERR_INVALID;
+      }
+    }
+    // 1-D tables per axis: B, G [dim][nmax*qmax], W [dim][qmax], D of axis 0
+    std::vector<double> B(d->dim * nmax * qmax, 0.0), G(d->dim * nmax * qmax, 0.0), W(d->dim * qmax, 0.0);
+    std::vector<double> Dm;
+    for (int a = 0; a < d->dim; ++a) {
+      std::vector<double> pts(b.q[a]), wts(b.q[a]);
+      gauss_legendre(b.q[a], pts.data(), wts.data());
+      std::vector<double> v(b.n[a] + 1), g(b.n[a] + 1);
+      for (int p = 0; p < b.q[a]; ++p) {
+        fe_basis(pts[p], b.n[a] - 1, v.data(), g.data());
+        for (int i = 0; i < b.n[a]; ++i) {
+          B[a * nmax * qmax + i * b.q[a] + p] = v[i];
+          G[a * nmax * qmax + i * b.q[a] + p] = g[i];
+        }
+        W[a * qmax + p] = wts[p];
+      }
+      if (a == 0) Dm = collocation_derivative(pts);
+    }
+    bool ok = b.B.upload(B) && b.G.upload(G) && b.W.upload(W) && b.D.upload(Dm);
+    ok = ok && b.h.upload(bd.cell_size, size_t(bd.n_cells) * d->dim);
+    if (bd.kappa_points) {
+      int64_t nq = 1;
+      for (int a = 0; a < d->dim; ++a) nq *= b.q[a];
+      ok = ok && b.kappa.upload(bd.kappa_points, size_t(bd.n_cells) * nq);
+    }
+    // full-layout map
+    ok = ok && b.full.map.upload(bd.map_index, size_t(ne));
+    if (bd.map_coef) ok = ok && b.full.coef.upload(bd.map_coef, size_t(ne));
+    if (bd.n_tail > 0) {
+      ok = ok && b.full.toff.upload(bd.tail_offsets, size_t(bd.n_tail + 1));
+      ok = ok && b.full.tidx.upload(bd.tail_index, size_t(bd.tail_offsets[bd.n_tail]));
+      ok = ok && b.full.tcoef.upload(bd.tail_coef, size_t(bd.tail_offsets[bd.n_tail]));
+    }
+    // reduced-layout map
+    std::vector<int32_t> rmap, tidx;
+    std::vector<double> rcoef, tcoef;
+    std::vector<int64_t> toff;
+    bool need_coef = false;
+    compose_reduced(bd, nb, *d, rmap, rcoef, need_coef, toff, tidx, tcoef);
+    ok = ok && b.red.map.upload(rmap);
+    if (need_coef) ok = ok && b.red.coef.upload(rcoef);
+    if (toff.size() > 1) ok = ok && b.red.toff.upload(toff) && b.red.tidx.upload(tidx) && b.red.tcoef.upload(tcoef);
+    b.red_multiterm = toff.size() > 1;
+    if (!ok) return GRICO_ERR_CUDA;
+    P->batches.push_back(std::move(b));
+  }
+  bool ok = true;
+  P->n_fixed = d->n_fixed;
+  if (d->n_fixed) ok = ok && P->fixed.upload(d->fixed_dofs, size_t(d->n_fixed)) && P->fixed_vals.upload(d->fixed_values, size_t(d->n_fixed));
+  P->n_rel = d->n_relations;
+  if (d->n_relations) {
+    ok = ok && P->rel_piv.upload(d->rel_pivot, size_t(d->n_relations)) &&
+         P->rel_off.upload(d->rel_offsets, size_t(d->n_relations + 1)) &&
+         P->rel_idx.upload(d->rel_index, size_t(d->rel_offsets[d->n_relations])) &&
+         P->rel_coef.upload(d->rel_coef, size_t(d->rel_offsets[d->n_relations]));
+  }
+  ok = ok && P->red_off.upload(d->red_offsets, size_t(d->n_full + 1));
+  if (d->red_offsets[d->n_full] > 0)
+    ok = ok && P->red_idx.upload(d->red_index, size_t(d->red_offsets[d->n_full])) &&
+         P->red_coef.upload(d->red_coef, size_t(d->red_offsets[d->n_full]));
+  P->has_shift = false;
+  if (d->red_shift)
+    for (int64_t i = 0; i < d->n_full; ++i)
+      if (d->red_shift[i] != 0.0) { P->has_shift = true; break; }
+  if (P->has_shift) ok = ok && P->shift.upload(d->red_shift, size_t(d->n_full));
+  ok = ok && P->partial.alloc(sizeof(double) * (kRedBlocks + 8)) && P->scalars.alloc(sizeof(double) * 16);
+  if (!ok) return GRICO_ERR_CUDA;
+  if (!cuda_ok(cudaStreamSynchronize(P->stream), "plan upload")) return GRICO_ERR_CUDA;
+  *out = P.release();
+  return GRICO_OK;
+}
+
+int grico_plan_destroy(GricoPlan* P) {
+  if (!P) return GRICO_OK;
+  cudaStreamSynchronize(P->stream);
+  cudaStream_t st = P->stream;
+  delete P;
+  cudaStreamDestroy(st);
+  return GRICO_OK;
+}
+
+int grico_plan_sizes(const GricoPlan* P, int64_t* n_full, int64_t* n_reduced) {
+  if (!P) return GRICO_ERR_INVALID;
+  if (n_full) *n_full = P->n_full;
+  if (n_reduced) *n_reduced = P->n_red;
+  return GRICO_OK;
+}
+
+static int apply_common(GricoPlan* P, bool reduced, const void* x, void* y, int nrhs, int precision, int flags,
+                        void* stream) {
+  if (!P || !x || !y || nrhs < 1) { set_error("apply: invalid argument"); return GRICO_ERR_INVALID; }
+  if (x == y) { set_error("result and coefficient vector must not alias"); return GRICO_ERR_INVALID; }
+  if (precision != GRICO_PREC_FP64 && precision != GRICO_PREC_FP32) { set_error("apply: unknown precision"); return GRICO_ERR_INVALID; }
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : P->stream;
+  const int64_t n = reduced ? P->n_red : P->n_full;
+  const size_t es = precision == GRICO_PREC_FP64 ? sizeof(double) : sizeof(float);
+  const size_t bytes = es * size_t(n) * nrhs;
+  const void* dx = x;
+  void* dy = y;
+  if (flags & GRICO_FLAG_HOST_POINTERS) {
+    if (!P->host_x.ensure(bytes) || !P->host_y.ensure(bytes)) return GRICO_ERR_CUDA;
+    if (!cuda_ok(cudaMemcpyAsync(P->host_x.ptr, x, bytes, cudaMemcpyHostToDevice, st), "copy in")) return GRICO_ERR_CUDA;
+    dx = P->host_x.ptr;
+    dy = P->host_y.ptr;
+  }
+  int rc = precision == GRICO_PREC_FP64
+               ? run_apply<double>(P, reduced, static_cast<const double*>(dx), static_cast<double*>(dy), nrhs, st)
+               : run_apply<float>(P, reduced, static_cast<const float*>(dx), static_cast<float*>(dy), nrhs, st);
+  if (rc != GRICO_OK) return rc;
+  if (flags & GRICO_FLAG_HOST_POINTERS) {
+    if (!cuda_ok(cudaMemcpyAsync(y, dy, bytes, cudaMemcpyDeviceToHost, st), "copy out")) return GRICO_ERR_CUDA;
+    if (!cuda_ok(cudaStreamSynchronize(st), "apply")) return GRICO_ERR_CUDA;
+  }
+  return GRICO_OK;
+}
+
+int grico_apply(GricoPlan* P, const void* x, void* y, int nrhs, int precision, int flags, void* stream) {
+  return apply_common(P, false, x, y, nrhs, precision, flags, stream);
+}
+
+int grico_reduced_apply(GricoPlan* P, const void* x, void* y, int nrhs, int precision, int flags, void* stream) {
+  return apply_common(P, true, x, y, nrhs, precision, flags, stream);
+}
+
+int grico_reduced_rhs(GricoPlan* P, const double* const* source_points, double* b_reduced, int flags) {
+  if (!P || !b_reduced) return GRICO_ERR_INVALID;
+  cudaStream_t st = P->stream;
+  DevBuf full, bred, src;
+  if (!full.alloc(sizeof(double) * std::max<int64_t>(P->n_full, 1))) return GRICO_ERR_CUDA;
+  cudaMemsetAsync(full.ptr, 0, sizeof(double) * P->n_full, st);
+  for (size_t bi = 0; bi < P->batches.size(); ++bi) {
+    const DevBatch& b = P->batches[bi];
+    const double* sp = nullptr;
+    if (source_points && source_points[bi]) {
+      int64_t nq = 1;
+      for (int a = 0; a < P->dim; ++a) nq *= b.q[a];
+      if (flags & GRICO_FLAG_HOST_POINTERS) {
+        if (!src.alloc(sizeof(double) * nq * b.n_cells)) return GRICO_ERR_CUDA;
+        cudaMemcpyAsync(src.ptr, source_points[bi], sizeof(double) * nq * b.n_cells, cudaMemcpyHostToDevice, st);
+        sp = src.get<double>();
+      } else {
+        sp = source_points[bi];
+      }
+    }
+    launch_batch<double>(*P, b, false, nullptr, full.get<double>(), P->n_full, 1, sp, 1, st);
+    if (flags & GRICO_FLAG_HOST_POINTERS) cudaStreamSynchronize(st);
+  }
+  if (P->has_shift) {
+    DevBuf as;
+    if (!as.alloc(sizeof(double) * P->n_full)) return GRICO_ERR_CUDA;
+    cudaMemsetAsync(as.ptr, 0, sizeof(double) * P->n_full, st);
+    for (auto& b : P->batches)
+      launch_batch<double>(*P, b, false, P->shift.get<double>(), as.get<double>(), P->n_full, 0, nullptr, 1, st);
+    axpby_kernel<double><<<grid_for(P->n_full), 256, 0, st>>>(-1.0, as.get<double>(), 1.0, full.get<double>(), P->n_full);
+    cudaStreamSynchronize(st);
+  }
+  double* out = b_reduced;
+  if (flags & GRICO_FLAG_HOST_POINTERS) {
+    if (!bred.alloc(sizeof(double) * std::max<int64_t>(P->n_red, 1))) return GRICO_ERR_CUDA;
+    out = bred.get<double>();
+  }
+  cudaMemsetAsync(out, 0, sizeof(double) * P->n_red, st);
+  project_reduced<<<grid_for(P->n_full), 256, 0, st>>>(P->red_off.get<int64_t>(), P->red_idx.get<int64_t>(),
+                                                        P->red_coef.get<double>(), full.get<double>(), out, P->n_full);
+  if (flags & GRICO_FLAG_HOST_POINTERS)
+    cudaMemcpyAsync(b_reduced, out, sizeof(double) * P->n_red, cudaMemcpyDeviceToHost, st);
+  return cuda_ok(cudaStreamSynchronize(st), "reduced rhs") ? GRICO_OK : GRICO_ERR_CUDA;
+}
+
+int grico_reduced_diagonal(GricoPlan* P, double* diag, int flags) {
+  if (!P || !diag) return GRICO_ERR_INVALID;
+  for (auto& b : P->batches)
+    if (b.red_multiterm) {
+      int rc = exact_reduced_diagonal(P, diag, flags);
+      return rc;
+    }
+  cudaStream_t st = P->stream;
+  DevBuf tmp;
+  double* out = diag;
+  if (flags & GRICO_FLAG_HOST_POINTERS) {
+    if (!tmp.alloc(sizeof(double) * std::max<int64_t>(P->n_red, 1))) return GRICO_ERR_CUDA;
+    out = tmp.get<double>();
+  }
+  int rc = reduced_diag_device(P, out, st);
+  if (rc) return rc;
+  if (flags & GRICO_FLAG_HOST_POINTERS) cudaMemcpyAsync(diag, out, sizeof(double) * P->n_red, cudaMemcpyDeviceToHost, st);
+  return cuda_ok(cudaStreamSynchronize(st), "diagonal") ? GRICO_OK : GRICO_ERR_CUDA;
+}
+
+int grico_expand_reduced(GricoPlan* P, const double* u_red, double* u_full, int flags) {
+  if (!P || !u_red || !u_full) return GRICO_ERR_INVALID;
+  cudaStream_t st = P->stream;
+  DevBuf a, b;
+  const double* in = u_red;
+  double* out = u_full;
+  if (flags & GRICO_FLAG_HOST_POINTERS) {
+    if (!a.alloc(sizeof(double) * std::max<int64_t>(P->n_red, 1)) || !b.alloc(sizeof(double) * std::max<int64_t>(P->n_full, 1)))
+      return GRICO_ERR_CUDA;
+    cudaMemcpyAsync(a.ptr, u_red, sizeof(double) * P->n_red, cudaMemcpyHostToDevice, st);
+    in = a.get<double>();
+    out = b.get<double>();
+  }
+  expand_reduced<<<grid_for(P->n_full), 256, 0, st>>>(P->red_off.get<int64_t>(), P->red_idx.get<int64_t>(),
+                                                       P->red_coef.get<double>(),
+                                                       P->has_shift ? P->shift.get<double>() : nullptr, in, out,
+                                                       P->n_full);
+  if (flags & GRICO_FLAG_HOST_POINTERS) cudaMemcpyAsync(u_full, out, sizeof(double) * P->n_full, cudaMemcpyDeviceToHost, st);
+  return cuda_ok(cudaStreamSynchronize(st), "expand") ? GRICO_OK : GRICO_ERR_CUDA;
+}
+
+}  // extern "C"

@@ -1,0 +1,100 @@
+// Internal layout of a device plan (HBM-resident data of one AssemblyPlan).
+//
+// Per cell batch (cells with one kernel signature):
+//   map      int32 [n_cells * n_box]   local box mode -> dof (>=0), inactive (-1), tail (<= -2)
+//   coef     f64   [n_cells * n_box]   only when some coefficient differs from 1
+//   tail     CSR of multi-term (hanging-node) expansions
+//   h        f64   [n_cells * dim]     cell sizes (affine axis-aligned geometry)
+//   kappa    f64   [n_cells * q^dim]   optional pointwise coefficient
+//   B,G,W,D  1-D tables: basis values, reference derivatives, Gauss weights, collocation
+//            derivative matrix
+// Two maps per batch: full layout (apply!) and reduced layout (composition with P).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "../../include/grico_b200.h"
+
+namespace grico {
+
+bool cuda_ok(cudaError_t e, const char* what);
+
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : ptr(o.ptr), bytes(o.bytes) { o.ptr = nullptr; o.bytes = 0; }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) {
+      if (ptr) cudaFree(ptr);
+      ptr = o.ptr;
+      bytes = o.bytes;
+      o.ptr = nullptr;
+      o.bytes = 0;
+    }
+    return *this;
+  }
+  ~DevBuf();
+  template <typename T>
+  T* get() const { return static_cast<T*>(ptr); }
+  bool alloc(size_t n) {
+    if (ptr) { cudaFree(ptr); ptr = nullptr; }
+    bytes = n;
+    if (n == 0) return true;
+    return cuda_ok(cudaMalloc(&ptr, n), "cudaMalloc");
+  }
+  bool ensure(size_t n) { return n <= bytes && ptr ? true : alloc(n); }
+  template <typename T>
+  bool upload(const T* src, size_t count) {
+    if (!alloc(sizeof(T) * count)) return false;
+    if (count == 0) return true;
+    return cuda_ok(cudaMemcpy(ptr, src, sizeof(T) * count, cudaMemcpyHostToDevice), "upload");
+  }
+  template <typename T>
+  bool upload(const std::vector<T>& v) { return upload(v.data(), v.size()); }
+};
+
+struct DevMap {
+  DevBuf map, coef, toff, tidx, tcoef;
+};
+
+struct DevBatch {
+  int32_t n_cells = 0;
+  int n[3] = {1, 1, 1};
+  int q[3] = {1, 1, 1};
+  bool isotropic = true;
+  bool red_multiterm = false;
+  DevMap full, red;
+  DevBuf h, kappa, B, G, W, D;
+};
+
+}  // namespace grico
+
+struct GricoPlan {
+  int dim = 0;
+  double mass = 0, kappa = 1;
+  int64_t n_full = 0, n_red = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<grico::DevBatch> batches;
+  int64_t n_fixed = 0, n_rel = 0;
+  grico::DevBuf fixed, fixed_vals, rel_piv, rel_off, rel_idx, rel_coef;
+  grico::DevBuf red_off, red_idx, red_coef, shift;
+  bool has_shift = false;
+  grico::DevBuf partial, scalars;
+  grico::DevBuf host_x, host_y;
+  // Krylov workspaces (allocated on first solve)
+  grico::DevBuf w_r, w_z, w_p, w_q, w_x, w_b, w_dinv;
+};
+
+namespace grico {
+template <typename T>
+int run_apply(GricoPlan* P, bool reduced, const T* x, T* y, int nrhs, cudaStream_t st);
+int reduced_diag_device(GricoPlan* P, double* diag, cudaStream_t st);
+int exact_reduced_diagonal(GricoPlan* P, double* diag, int flags);
+int grid_blocks(int64_t n);
+}  // namespace grico

@@ -1,0 +1,16 @@
+"""grico_b200 — B200-native matrix-free runtime for Grico.jl's hot path.
+
+Host-side mirror of Grico.jl's public API for this path (Domain, HpSpace, AffineProblem,
+add_cell_accumulator!, Dirichlet, compile, apply!, solve) on top of the C ABI of
+libgrico_b200.so (include/grico_b200.h).  All compute runs in the library's sm_100a kernels.
+"""
+from ._lib import GricoError, lib
+from .mesh import LOWER, UPPER, CartesianGrid, Domain, grid, refine, uniform_refine
+from .space import (AxisDegrees, ByLeafDegrees, DegreePlusQuadrature, FullTensorBasis, HpSpace, SpaceOptions,
+                    StoredDegrees, TrunkBasis, UniformDegree, active_leaf_count, scalar_dof_count)
+from .problem import (SPD, AffineProblem, AssemblyPlan, BoundaryFace, CGSolver, Diffusion, Dirichlet, FGMRESSolver,
+                      IdentityPreconditioner, JacobiPreconditioner, Load, Mass, MassDiffusion, NonsymmetricOperator,
+                      ScalarField, State, VariableDiffusion, add_cell_accumulator, add_constraint, apply, apply_,
+                      compile, expand_reduced, l2_error, reduced_apply, reduced_diagonal, reduced_rhs,
+                      relative_l2_error, solve)
+from .multigrid import GeometricMultigridPreconditioner

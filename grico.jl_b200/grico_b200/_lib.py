@@ -1,0 +1,192 @@
+"""ctypes binding of libgrico_b200.so (declarations mirror include/grico_b200.h).
+
+The library is the only compute path: if it is missing, or no CUDA device is present when a
+plan is created, calls raise instead of falling back to anything else.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libgrico_b200.so")
+
+GRICO_OK = 0
+GRICO_ERR_INVALID = -1
+GRICO_ERR_UNSUPPORTED_FORM = -2
+GRICO_ERR_NOT_CONVERGED = -3
+GRICO_ERR_NONFINITE = -4
+GRICO_ERR_BREAKDOWN = -5
+GRICO_ERR_CUDA = -6
+GRICO_ERR_NO_DEVICE = -7
+GRICO_ERR_TIMEOUT = -8
+
+GRICO_BASIS_FULL = 0
+GRICO_BASIS_TRUNK = 1
+GRICO_CONTINUITY_CG = 0
+GRICO_CONTINUITY_DG = 1
+GRICO_FORM_MASS_DIFFUSION = 1
+GRICO_PREC_FP64 = 0
+GRICO_PREC_FP32 = 1
+GRICO_FLAG_HOST_POINTERS = 1
+GRICO_PRECOND_IDENTITY = 0
+GRICO_PRECOND_JACOBI = 1
+GRICO_PRECOND_MULTIGRID = 2
+GRICO_SMOOTHER_JACOBI = 0
+GRICO_SMOOTHER_CHEBYSHEV = 1
+
+P = C.c_void_p
+i32p = C.POINTER(C.c_int32)
+i64p = C.POINTER(C.c_int64)
+f64p = C.POINTER(C.c_double)
+
+
+class GricoCellBatchDesc(C.Structure):
+    _fields_ = [
+        ("n_cells", C.c_int32),
+        ("degree", C.c_int32 * 3),
+        ("qpoints", C.c_int32 * 3),
+        ("map_index", i32p),
+        ("map_coef", f64p),
+        ("n_tail", C.c_int64),
+        ("tail_offsets", i64p),
+        ("tail_index", i32p),
+        ("tail_coef", f64p),
+        ("cell_size", f64p),
+        ("kappa_points", f64p),
+    ]
+
+
+class GricoPlanDesc(C.Structure):
+    _fields_ = [
+        ("dim", C.c_int32),
+        ("form", C.c_int32),
+        ("mass", C.c_double),
+        ("kappa", C.c_double),
+        ("n_full", C.c_int64),
+        ("n_batches", C.c_int32),
+        ("batches", C.POINTER(GricoCellBatchDesc)),
+        ("n_fixed", C.c_int64),
+        ("fixed_dofs", i64p),
+        ("fixed_values", f64p),
+        ("n_relations", C.c_int64),
+        ("rel_pivot", i64p),
+        ("rel_offsets", i64p),
+        ("rel_index", i64p),
+        ("rel_coef", f64p),
+        ("rel_rhs", f64p),
+        ("n_reduced", C.c_int64),
+        ("red_offsets", i64p),
+        ("red_index", i64p),
+        ("red_coef", f64p),
+        ("red_shift", f64p),
+    ]
+
+
+class GricoSolveOptions(C.Structure):
+    _fields_ = [
+        ("relative_tolerance", C.c_double),
+        ("absolute_tolerance", C.c_double),
+        ("maxiter", C.c_int32),
+        ("preconditioner", C.c_int32),
+        ("restart", C.c_int32),
+        ("use_initial", C.c_int32),
+    ]
+
+
+class GricoSolveReport(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_int32),
+        ("status", C.c_int32),
+        ("initial_residual", C.c_double),
+        ("final_residual", C.c_double),
+        ("seconds", C.c_double),
+    ]
+
+
+class GricoTransferDesc(C.Structure):
+    _fields_ = [
+        ("n_fine", C.c_int64),
+        ("n_coarse", C.c_int64),
+        ("row_offsets", i64p),
+        ("col_index", i64p),
+        ("values", f64p),
+    ]
+
+
+class GricoMGOptions(C.Structure):
+    _fields_ = [
+        ("smoother", C.c_int32),
+        ("pre_steps", C.c_int32),
+        ("post_steps", C.c_int32),
+        ("jacobi_omega", C.c_double),
+        ("chebyshev_degree", C.c_int32),
+        ("chebyshev_lower", C.c_double),
+        ("precision", C.c_int32),
+    ]
+
+
+# name -> (restype, argtypes); every symbol include/grico_b200.h declares
+SIGNATURES = {
+    "grico_space_build": (C.c_int, [C.c_int, i64p, C.c_int64, i32p, i64p, i32p, C.c_int, C.c_int, C.c_int, C.POINTER(P)]),
+    "grico_space_destroy": (C.c_int, [P]),
+    "grico_space_sizes": (C.c_int, [P, i64p, i64p, i64p, i64p, i64p]),
+    "grico_space_export": (C.c_int, [P, i64p, i64p, i64p, i64p, f64p, i32p, i64p, i32p, i32p, i64p, i64p, i32p]),
+    "grico_gauss_legendre": (C.c_int, [C.c_int, f64p, f64p]),
+    "grico_fe_basis": (C.c_int, [C.c_double, C.c_int, f64p, f64p]),
+    "grico_plan_create": (C.c_int, [C.POINTER(GricoPlanDesc), C.POINTER(P)]),
+    "grico_plan_destroy": (C.c_int, [P]),
+    "grico_plan_sizes": (C.c_int, [P, i64p, i64p]),
+    "grico_apply": (C.c_int, [P, P, P, C.c_int, C.c_int, C.c_int, P]),
+    "grico_reduced_apply": (C.c_int, [P, P, P, C.c_int, C.c_int, C.c_int, P]),
+    "grico_reduced_rhs": (C.c_int, [P, C.POINTER(f64p), f64p, C.c_int]),
+    "grico_reduced_diagonal": (C.c_int, [P, f64p, C.c_int]),
+    "grico_expand_reduced": (C.c_int, [P, f64p, f64p, C.c_int]),
+    "grico_cg_solve": (C.c_int, [P, P, f64p, f64p, C.POINTER(GricoSolveOptions), C.POINTER(GricoSolveReport), C.c_int]),
+    "grico_fgmres_solve": (C.c_int, [P, P, f64p, f64p, C.POINTER(GricoSolveOptions), C.POINTER(GricoSolveReport), C.c_int]),
+    "grico_mg_create": (C.c_int, [C.POINTER(P), C.c_int, C.POINTER(GricoTransferDesc), f64p, C.POINTER(GricoMGOptions), C.POINTER(P)]),
+    "grico_mg_destroy": (C.c_int, [P]),
+    "grico_mg_vcycle": (C.c_int, [P, f64p, f64p, C.c_int]),
+    "grico_mg_lambda_max": (C.c_double, [P, C.c_int]),
+    "grico_last_error": (C.c_char_p, []),
+}
+
+_lib = None
+
+
+def lib():
+    """Load the in-tree shared library once; raise if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"libgrico_b200.so is not built ({LIB_PATH}); run grico.jl_b200/build.py")
+        handle = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(handle, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = handle
+    return _lib
+
+
+class GricoError(ValueError):
+    """Raised for every non-zero status; the reference raises ArgumentError in these cases."""
+
+    def __init__(self, code, message):
+        super().__init__(f"{message} (status {code})")
+        self.code = code
+
+
+def check(code, what=""):
+    if code != GRICO_OK:
+        msg = lib().grico_last_error()
+        msg = msg.decode() if msg else ""
+        raise GricoError(code, f"{what}: {msg}" if what else msg)
+    return code
+
+
+def ptr(array, ctype):
+    """ctypes pointer to a contiguous numpy array (or None)."""
+    if array is None:
+        return None
+    return array.ctypes.data_as(C.POINTER(ctype))

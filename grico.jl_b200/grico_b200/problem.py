@@ -1,0 +1,552 @@
+"""Problems, accumulator forms, compile and the runtime calls (host side of the mirror).
+
+Mirrors `ScalarField`, `AffineProblem`, `add_cell_accumulator!`, `Dirichlet`/`BoundaryFace`,
+`add_constraint!`, `compile`, `apply`/`apply!`, `rhs` and `solve` (problem.jl:47-612,
+plans.jl:170-231, assembly.jl:456-564, solve.jl:219-266).
+
+Julia accumulator callbacks cannot run on the GPU, so cell operators are a closed set of form
+descriptors: `Diffusion`, `MassDiffusion`, `Mass`, `VariableDiffusion` (pointwise coefficient
+tabulated at the quadrature points) and `Load` (right-hand side f(x)).  Any other operator
+object raises GricoError(GRICO_ERR_UNSUPPORTED_FORM), like the reference raises ArgumentError.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _lib as L
+from .mesh import LOWER, UPPER
+
+
+# ---------------------------------------------------------------------------------------
+# forms
+# ---------------------------------------------------------------------------------------
+
+class Diffusion:
+    """TestChannels(0, kappa*grad u) — examples/poisson_matrix_free_gmg/driver.jl:36-38."""
+
+    def __init__(self, kappa=1.0):
+        self.mass, self.kappa, self.coefficient = 0.0, float(kappa), None
+
+
+class MassDiffusion:
+    """TestChannels(mass*u, kappa*grad u) — benchmark/hpmg_scaling.jl:23-25."""
+
+    def __init__(self, mass=1.0, kappa=1.0):
+        self.mass, self.kappa, self.coefficient = float(mass), float(kappa), None
+
+
+class Mass:
+    def __init__(self, mass=1.0):
+        self.mass, self.kappa, self.coefficient = float(mass), 0.0, None
+
+
+class VariableDiffusion:
+    """TestChannels(0, a(x) grad u) with a(x) tabulated at the quadrature points.
+    `coefficient(points)` receives an [n, D] array and returns [n] values."""
+
+    def __init__(self, coefficient, kappa=1.0):
+        self.mass, self.kappa, self.coefficient = 0.0, float(kappa), coefficient
+
+
+class Load:
+    """cell_rhs_accumulate returning f(x) — `source(points)` on an [n, D] array."""
+
+    def __init__(self, source):
+        self.source = source
+
+
+# ---------------------------------------------------------------------------------------
+# fields, constraints, problems
+# ---------------------------------------------------------------------------------------
+
+class ScalarField:
+    def __init__(self, space, name="u"):
+        self.space = space
+        self.name = name
+
+
+class BoundaryFace:
+    def __init__(self, axis, side):
+        if side not in (LOWER, UPPER):
+            raise ValueError("side must be LOWER or UPPER")
+        self.axis, self.side = int(axis), int(side)
+
+
+class Dirichlet:
+    """Strong Dirichlet data on one boundary face; constant values only on the GPU path."""
+
+    def __init__(self, field, boundary, data):
+        self.field, self.boundary = field, boundary
+        if callable(data):
+            raise L.GricoError(L.GRICO_ERR_UNSUPPORTED_FORM, "Dirichlet data must be a constant on the B200 path")
+        self.value = float(data)
+
+
+class SPD:
+    pass
+
+
+class NonsymmetricOperator:
+    pass
+
+
+class AffineProblem:
+    def __init__(self, field, operator_class=None):
+        self.field = field
+        self.operator_class = operator_class or SPD()
+        self.cell_operators = []
+        self.rhs_operators = []
+        self.dirichlet = []
+
+
+def add_cell_accumulator(problem, test_field, *args):
+    """add_cell_accumulator!(problem, test, trial, op) or (problem, test, load) (accumulators.jl:356-370)."""
+    if len(args) == 2:
+        trial, op = args
+        if trial is not test_field or test_field is not problem.field:
+            raise ValueError("the B200 plan supports one scalar field")
+        if not isinstance(op, (Diffusion, MassDiffusion, Mass, VariableDiffusion)):
+            raise L.GricoError(L.GRICO_ERR_UNSUPPORTED_FORM, f"accumulator form {type(op).__name__} is not supported by the GPU plan")
+        problem.cell_operators.append(op)
+    elif len(args) == 1:
+        (op,) = args
+        if not isinstance(op, Load):
+            raise L.GricoError(L.GRICO_ERR_UNSUPPORTED_FORM, f"rhs form {type(op).__name__} is not supported by the GPU plan")
+        problem.rhs_operators.append(op)
+    else:
+        raise TypeError("add_cell_accumulator(problem, test, trial, op) or (problem, test, load)")
+    return problem
+
+
+def add_constraint(problem, constraint):
+    if not isinstance(constraint, Dirichlet):
+        raise L.GricoError(L.GRICO_ERR_UNSUPPORTED_FORM, "only Dirichlet constraints are supported")
+    problem.dirichlet.append(constraint)
+    return problem
+
+
+# ---------------------------------------------------------------------------------------
+# compile
+# ---------------------------------------------------------------------------------------
+
+class _Batch:
+    pass
+
+
+def _gauss(n):
+    pts = np.zeros(n)
+    wts = np.zeros(n)
+    L.check(L.lib().grico_gauss_legendre(n, L.ptr(pts, C.c_double), L.ptr(wts, C.c_double)))
+    return pts, wts
+
+
+def _fe_basis(x, p):
+    v = np.zeros(p + 2)
+    d = np.zeros(p + 2)
+    L.check(L.lib().grico_fe_basis(float(x), p, L.ptr(v, C.c_double), L.ptr(d, C.c_double)))
+    return v[: p + 1], d[: p + 1]
+
+
+def _tables(p, q):
+    """B[i, j] = psi_i(xi_j) on q Gauss points."""
+    pts, wts = _gauss(q)
+    B = np.zeros((p + 1, q))
+    G = np.zeros((p + 1, q))
+    for j in range(q):
+        v, d = _fe_basis(pts[j], p)
+        B[:, j] = v
+        G[:, j] = d
+    return pts, wts, B, G
+
+
+class AssemblyPlan:
+    """Compiled plan: descriptor arrays built here, device data owned by libgrico_b200."""
+
+    def __init__(self, problem):
+        if not problem.cell_operators:
+            raise ValueError("problem has no cell operator")
+        if len(problem.cell_operators) > 1:
+            raise L.GricoError(L.GRICO_ERR_UNSUPPORTED_FORM, "the GPU plan accepts one cell operator form")
+        self.problem = problem
+        self.form = problem.cell_operators[0]
+        space = problem.field.space
+        self.space = space
+        domain = space.domain
+        self.D = D = space.D
+        n_full = space.scalar_dof_count
+        self.n_full = n_full
+        # --- batches by (degrees, quadrature shape), first appearance in Morton order ---
+        sig = np.concatenate([space.degrees, space.qshape], axis=1)
+        _, first, inv = np.unique(sig, axis=0, return_index=True, return_inverse=True)
+        inv = inv.reshape(-1)
+        order_groups = np.argsort(first, kind="stable")
+        self.batches = []
+        for g in order_groups:
+            cells = np.nonzero(inv == g)[0]
+            b = _Batch()
+            b.cells = cells                                      # Morton positions
+            b.leaves = space.leaves[cells]
+            b.degree = tuple(int(v) for v in space.degrees[cells[0]])
+            b.q = tuple(int(v) for v in space.qshape[cells[0]])
+            nb = int(np.prod([d + 1 for d in b.degree]))
+            b.nbox = nb
+            starts = space.box_offsets[cells]
+            ent = (starts[:, None] + np.arange(nb)[None, :]).reshape(-1)
+            lo = space.term_offsets[ent]
+            hi = space.term_offsets[ent + 1]
+            cnt = hi - lo
+            mp = np.full(ent.size, -1, dtype=np.int32)
+            single = cnt == 1
+            mp[single] = space.term_index[lo[single]].astype(np.int32)
+            coef = np.ones(ent.size)
+            coef[single] = space.term_coef[lo[single]]
+            multi = np.nonzero(cnt > 1)[0]
+            if multi.size:
+                mp[multi] = -(np.arange(multi.size, dtype=np.int32) + 2)
+                tcnt = cnt[multi]
+                b.tail_offsets = np.concatenate([[0], np.cumsum(tcnt)]).astype(np.int64)
+                tsrc = np.concatenate([np.arange(l, h) for l, h in zip(lo[multi], hi[multi])])
+                b.tail_index = space.term_index[tsrc].astype(np.int32)
+                b.tail_coef = space.term_coef[tsrc].astype(np.float64)
+            else:
+                b.tail_offsets = b.tail_index = b.tail_coef = None
+            b.map_index = np.ascontiguousarray(mp)
+            b.map_coef = None if np.all(coef == 1.0) else np.ascontiguousarray(coef)
+            b.h = np.ascontiguousarray(domain.cell_size(b.leaves))
+            b.lower = domain.cell_lower(b.leaves)
+            # reference points of the tensor rule, axis 1 fastest
+            b.rules = [_tables(b.degree[a], b.q[a]) for a in range(D)]
+            b.points = self._points(b)                           # [n_cells, nq, D]
+            b.kappa_points = None
+            if self.form.coefficient is not None:
+                vals = np.asarray(self.form.coefficient(b.points.reshape(-1, D)), dtype=np.float64)
+                b.kappa_points = np.ascontiguousarray(vals.reshape(len(cells), -1))
+            self.batches.append(b)
+        # --- Dirichlet: fixed dofs are the dofs with a trace on a selected boundary face ---
+        self._compile_dirichlet(problem)
+        # --- reduced map ---
+        free = np.ones(n_full, dtype=bool)
+        free[self.fixed_dofs] = False
+        self.solve_dofs = np.nonzero(free)[0]
+        self.n_reduced = int(self.solve_dofs.size)
+        reduced_index = np.full(n_full, -1, dtype=np.int64)
+        reduced_index[self.solve_dofs] = np.arange(self.n_reduced)
+        self.reduced_index = reduced_index
+        self.red_offsets = np.concatenate([[0], np.cumsum(free.astype(np.int64))]).astype(np.int64)
+        self.red_index = np.arange(self.n_reduced, dtype=np.int64)
+        self.red_coef = np.ones(self.n_reduced)
+        self.shift = np.zeros(n_full)
+        self.shift[self.fixed_dofs] = self.fixed_values
+        self._create_device_plan()
+
+    def _points(self, b):
+        D = self.D
+        grids = np.meshgrid(*[b.rules[a][0] for a in range(D)], indexing="ij")
+        # axis 1 fastest: flatten in Fortran order
+        ref = np.stack([g.reshape(-1, order="F") for g in grids], axis=1)  # [nq, D]
+        half = 0.5 * b.h
+        center = b.lower + half
+        return center[:, None, :] + ref[None, :, :] * half[:, None, :]
+
+    def _compile_dirichlet(self, problem):
+        space = self.space
+        D = self.D
+        fixed = {}
+        if problem.dirichlet:
+            b_leaf, b_axis, b_side = space.boundary_faces
+            sel = {}
+            for con in problem.dirichlet:
+                key = (con.boundary.axis - 1, con.boundary.side - 1)
+                if key in sel and sel[key] != con.value:
+                    raise ValueError("multiple Dirichlet constraints target the same boundary face")
+                sel[key] = con.value
+            matched = set()
+            for pos, ax, sd in zip(b_leaf, b_axis, b_side):
+                key = (int(ax), int(sd))
+                if key not in sel:
+                    continue
+                matched.add(key)
+                val = sel[key]
+                deg = space.degrees[pos]
+                shape = deg + 1
+                nb = int(np.prod(shape))
+                box = np.arange(nb)
+                digits = []
+                rem = box.copy()
+                for a in range(D):
+                    digits.append(rem % shape[a])
+                    rem //= shape[a]
+                digits = np.stack(digits, axis=1)
+                on_face = digits[:, ax] == sd
+                vertex = np.all(digits <= 1, axis=1)
+                for m in np.nonzero(on_face)[0]:
+                    e = space.box_offsets[pos] + m
+                    for t in range(space.term_offsets[e], space.term_offsets[e + 1]):
+                        d = int(space.term_index[t])
+                        single_vertex = vertex[m] and (space.term_offsets[e + 1] - space.term_offsets[e] == 1)
+                        if d not in fixed:
+                            fixed[d] = 0.0
+                        if single_vertex and val != 0.0:
+                            fixed[d] = val
+            for key in sel:
+                if key not in matched:
+                    raise ValueError("Dirichlet constraint does not match any boundary face")
+        self.fixed_dofs = np.array(sorted(fixed), dtype=np.int64)
+        self.fixed_values = np.array([fixed[d] for d in self.fixed_dofs], dtype=np.float64)
+
+    def _create_device_plan(self):
+        descs = (L.GricoCellBatchDesc * len(self.batches))()
+        for i, b in enumerate(self.batches):
+            d = descs[i]
+            d.n_cells = len(b.cells)
+            for a in range(3):
+                d.degree[a] = b.degree[a] if a < self.D else 0
+                d.qpoints[a] = b.q[a] if a < self.D else 1
+            d.map_index = L.ptr(b.map_index, C.c_int32)
+            d.map_coef = L.ptr(b.map_coef, C.c_double)
+            d.n_tail = 0 if b.tail_offsets is None else len(b.tail_offsets) - 1
+            d.tail_offsets = L.ptr(b.tail_offsets, C.c_int64)
+            d.tail_index = L.ptr(b.tail_index, C.c_int32)
+            d.tail_coef = L.ptr(b.tail_coef, C.c_double)
+            d.cell_size = L.ptr(b.h, C.c_double)
+            d.kappa_points = L.ptr(b.kappa_points, C.c_double)
+        pd = L.GricoPlanDesc()
+        pd.dim = self.D
+        pd.form = L.GRICO_FORM_MASS_DIFFUSION
+        pd.mass = self.form.mass
+        pd.kappa = self.form.kappa
+        pd.n_full = self.n_full
+        pd.n_batches = len(self.batches)
+        pd.batches = descs
+        pd.n_fixed = len(self.fixed_dofs)
+        pd.fixed_dofs = L.ptr(self.fixed_dofs, C.c_int64)
+        pd.fixed_values = L.ptr(self.fixed_values, C.c_double)
+        pd.n_relations = 0
+        pd.n_reduced = self.n_reduced
+        pd.red_offsets = L.ptr(self.red_offsets, C.c_int64)
+        pd.red_index = L.ptr(self.red_index, C.c_int64)
+        pd.red_coef = L.ptr(self.red_coef, C.c_double)
+        pd.red_shift = L.ptr(self.shift, C.c_double)
+        handle = C.c_void_p()
+        L.check(L.lib().grico_plan_create(C.byref(pd), C.byref(handle)), "compile")
+        self.handle = handle
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            try:
+                L.lib().grico_plan_destroy(h)
+            except Exception:
+                pass
+            self.handle = None
+
+    # ---- sizes ----
+    def dof_count(self):
+        return self.n_full
+
+    def reduced_dof_count(self):
+        return self.n_reduced
+
+
+def compile(problem):
+    return AssemblyPlan(problem)
+
+
+# ---------------------------------------------------------------------------------------
+# runtime
+# ---------------------------------------------------------------------------------------
+
+def _vector_call(fn, plan, x, y, n, nrhs=1):
+    """Dispatch host numpy arrays (copied by the library) or torch CUDA tensors (device
+    pointers, current torch stream)."""
+    if isinstance(x, np.ndarray):
+        x = np.ascontiguousarray(x)
+        prec = L.GRICO_PREC_FP64 if x.dtype == np.float64 else L.GRICO_PREC_FP32
+        if x.size != n * nrhs:
+            raise ValueError(f"coefficient vector must have length {n * nrhs}")
+        if y is None:
+            y = np.zeros_like(x)
+        L.check(fn(plan.handle, x.ctypes.data_as(C.c_void_p), y.ctypes.data_as(C.c_void_p), nrhs, prec,
+                   L.GRICO_FLAG_HOST_POINTERS, None), "apply")
+        return y
+    import torch  # device tensors
+
+    if not (isinstance(x, torch.Tensor) and x.is_cuda):
+        raise TypeError("vectors must be numpy arrays or CUDA tensors")
+    if x.numel() != n * nrhs:
+        raise ValueError(f"coefficient vector must have length {n * nrhs}")
+    prec = L.GRICO_PREC_FP64 if x.dtype == torch.float64 else L.GRICO_PREC_FP32
+    if y is None:
+        y = torch.empty_like(x)
+    if y.data_ptr() == x.data_ptr():
+        raise ValueError("result and coefficient vector must not alias")
+    stream = torch.cuda.current_stream().cuda_stream
+    L.check(fn(plan.handle, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), nrhs, prec, 0,
+               C.c_void_p(stream)), "apply")
+    return y
+
+
+def apply(plan, x, nrhs=1):
+    """apply(plan, x) on the full layout (assembly.jl:517-530)."""
+    return _vector_call(L.lib().grico_apply, plan, x, None, plan.n_full, nrhs)
+
+
+def apply_(y, plan, x, nrhs=1):
+    """apply!(y, plan, x)."""
+    return _vector_call(L.lib().grico_apply, plan, x, y, plan.n_full, nrhs)
+
+
+def reduced_apply(plan, x, nrhs=1):
+    """_reduced_apply! (assembly.jl:905-915)."""
+    return _vector_call(L.lib().grico_reduced_apply, plan, x, None, plan.n_reduced, nrhs)
+
+
+def _source_points(plan, problem=None):
+    problem = problem or plan.problem
+    arrays = []
+    for b in plan.batches:
+        if problem.rhs_operators:
+            f = np.zeros(b.points.shape[:2])
+            for op in problem.rhs_operators:
+                f += np.asarray(op.source(b.points.reshape(-1, plan.D)), dtype=np.float64).reshape(f.shape)
+            arrays.append(np.ascontiguousarray(f))
+        else:
+            arrays.append(None)
+    return arrays
+
+
+def reduced_rhs(plan):
+    """Reduced right-hand side P^T (b - A shift) (assembly.jl:917-933)."""
+    arrays = _source_points(plan)
+    ptrs = (L.f64p * len(arrays))(*[L.ptr(a, C.c_double) if a is not None else None for a in arrays])
+    out = np.zeros(plan.n_reduced)
+    L.check(L.lib().grico_reduced_rhs(plan.handle, ptrs, L.ptr(out, C.c_double), L.GRICO_FLAG_HOST_POINTERS), "rhs")
+    return out
+
+
+def reduced_diagonal(plan):
+    out = np.zeros(plan.n_reduced)
+    L.check(L.lib().grico_reduced_diagonal(plan.handle, L.ptr(out, C.c_double), L.GRICO_FLAG_HOST_POINTERS), "diagonal")
+    return out
+
+
+def expand_reduced(plan, ured):
+    ured = np.ascontiguousarray(ured, dtype=np.float64)
+    out = np.zeros(plan.n_full)
+    L.check(L.lib().grico_expand_reduced(plan.handle, L.ptr(ured, C.c_double), L.ptr(out, C.c_double),
+                                         L.GRICO_FLAG_HOST_POINTERS), "expand")
+    return out
+
+
+class IdentityPreconditioner:
+    code = L.GRICO_PRECOND_IDENTITY
+
+
+class JacobiPreconditioner:
+    code = L.GRICO_PRECOND_JACOBI
+
+
+class CGSolver:
+    def __init__(self, preconditioner=None):
+        self.preconditioner = preconditioner or IdentityPreconditioner()
+
+
+class FGMRESSolver:
+    def __init__(self, preconditioner=None, restart=30):
+        self.preconditioner = preconditioner or IdentityPreconditioner()
+        self.restart = int(restart)
+
+
+class State:
+    def __init__(self, plan, coefficients, report=None):
+        self.plan = plan
+        self.coefficients = coefficients
+        self.report = report
+
+
+def solve(plan_or_problem, solver=None, relative_tolerance=None, absolute_tolerance=0.0, maxiter=None,
+          initial_solution=None):
+    """solve(plan; solver=CGSolver(...)) on the reduced system (solve.jl:229-276)."""
+    from .multigrid import GeometricMultigridPreconditioner, build_multigrid
+
+    plan = plan_or_problem if isinstance(plan_or_problem, AssemblyPlan) else compile(plan_or_problem)
+    solver = solver or CGSolver(JacobiPreconditioner())
+    rtol = math.sqrt(np.finfo(np.float64).eps) if relative_tolerance is None else float(relative_tolerance)
+    maxiter = max(1000, 2 * plan.n_reduced) if maxiter is None else int(maxiter)
+    b = reduced_rhs(plan)
+    x = np.zeros(plan.n_reduced) if initial_solution is None else np.array(initial_solution, dtype=np.float64)
+    mg = None
+    pre = solver.preconditioner
+    if isinstance(pre, GeometricMultigridPreconditioner):
+        mg = build_multigrid(plan, pre)
+        code = L.GRICO_PRECOND_MULTIGRID
+    else:
+        code = pre.code
+    opts = L.GricoSolveOptions(rtol, float(absolute_tolerance), int(min(maxiter, 2**31 - 1)), code,
+                               getattr(solver, "restart", 30), 0 if initial_solution is None else 1)
+    rep = L.GricoSolveReport()
+    fn = L.lib().grico_cg_solve if isinstance(solver, CGSolver) else L.lib().grico_fgmres_solve
+    L.check(fn(plan.handle, mg.handle if mg is not None else None, L.ptr(b, C.c_double), L.ptr(x, C.c_double),
+               C.byref(opts), C.byref(rep), L.GRICO_FLAG_HOST_POINTERS), "solve")
+    return State(plan, expand_reduced(plan, x), rep)
+
+
+def l2_error(state, exact):
+    """Quadrature L2 error on the cell rules (verification.jl:201-230, 270-275)."""
+    plan = state.plan
+    err2 = 0.0
+    for b, u in zip(plan.batches, _point_values(plan, state.coefficients)):
+        w = _point_weights(plan, b)
+        ex = np.asarray(exact(b.points.reshape(-1, plan.D)), dtype=np.float64).reshape(u.shape)
+        err2 += float(np.sum(w * (u - ex) ** 2))
+    return math.sqrt(err2)
+
+
+def relative_l2_error(state, exact):
+    plan = state.plan
+    num = l2_error(state, exact)
+    den2 = 0.0
+    for b in plan.batches:
+        w = _point_weights(plan, b)
+        ex = np.asarray(exact(b.points.reshape(-1, plan.D)), dtype=np.float64).reshape(w.shape)
+        den2 += float(np.sum(w * ex ** 2))
+    return num / math.sqrt(den2) if den2 > 0 else num
+
+
+def _point_weights(plan, b):
+    D = plan.D
+    w1 = [b.rules[a][1] for a in range(D)]
+    grids = np.meshgrid(*w1, indexing="ij")
+    ref = np.prod(np.stack([g.reshape(-1, order="F") for g in grids], axis=1), axis=1)
+    det = np.prod(0.5 * b.h, axis=1)
+    return det[:, None] * ref[None, :]
+
+
+def _point_values(plan, full_values):
+    """u at the quadrature points, [n_cells, nq] per batch with points axis 1 fastest."""
+    x = np.asarray(full_values, dtype=np.float64)
+    D = plan.D
+    out = []
+    for b in plan.batches:
+        n = len(b.cells)
+        mp = b.map_index.reshape(n, b.nbox)
+        loc = np.where(mp >= 0, x[np.maximum(mp, 0)], 0.0)
+        if b.map_coef is not None:
+            loc = loc * b.map_coef.reshape(n, b.nbox)
+        if b.tail_offsets is not None:
+            rows, cols = np.nonzero(mp <= -2)
+            for r, c in zip(rows, cols):
+                k = -(int(mp[r, c]) + 2)
+                lo, hi = b.tail_offsets[k], b.tail_offsets[k + 1]
+                loc[r, c] = float(np.dot(b.tail_coef[lo:hi], x[b.tail_index[lo:hi]]))
+        # box index is axis 1 fastest: t axes are [cell, mD, ..., m1]; contract m_a with B_a
+        t = loc.reshape([n] + [b.degree[a] + 1 for a in reversed(range(D))])
+        for a in range(D):
+            ax = D - a  # position of axis a
+            t = np.moveaxis(np.tensordot(t, b.rules[a][2], axes=([ax], [0])), -1, ax)
+        # now axes [cell, qD, ..., q1] -> flatten with q1 fastest (C order on reversed axes)
+        out.append(t.reshape(n, -1))
+    return out

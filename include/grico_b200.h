@@ -1,0 +1,225 @@
+/*
+ * grico_b200.h — C ABI of the B200 matrix-free runtime for Grico.jl's hot path.
+ *
+ * Every entry point is plain C: pointers, sizes and POD structs, no C++ or torch types.
+ * Indices are 0-based (the reference is 1-based; the binding subtracts 1).  Return codes
+ * are GRICO_OK (0) or a negative GRICO_ERR_*; grico_last_error() gives a thread-local
+ * message.  No exception crosses the boundary.
+ *
+ * Reference interfaces each group replaces (paths inside schmaeke/Grico.jl):
+ *   host space compile   src/space.jl:300-326, src/continuity.jl:153-1227,
+ *                        src/topology.jl:232-300, 1502-1545 (Morton order, faces)
+ *   plan create/destroy  compile(problem)            src/plans.jl:170-231
+ *   apply                apply!(result, plan, x, ws) src/assembly.jl:540-564
+ *   reduced apply        _reduced_apply!             src/assembly.jl:905-915
+ *   rhs                  _reduced_rhs!/rhs!          src/assembly.jl:456-478, 917-933
+ *   diagonal             _reduced_diagonal!          src/assembly.jl:662-675
+ *   cg solve             _cg_solve                   src/solve.jl:376-431
+ *   fgmres solve         _fgmres_solve               src/solve.jl:433-589
+ *   multigrid            _vcycle!, transfers         src/multigrid.jl:858-1087
+ */
+#ifndef GRICO_B200_H
+#define GRICO_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (reference raises ArgumentError for every one of these) ---- */
+#define GRICO_OK 0
+#define GRICO_ERR_INVALID -1          /* bad argument, size mismatch, aliasing          */
+#define GRICO_ERR_UNSUPPORTED_FORM -2 /* accumulator form the GPU plan does not know   */
+#define GRICO_ERR_NOT_CONVERGED -3    /* Krylov did not reach tolerance in maxiter      */
+#define GRICO_ERR_NONFINITE -4        /* NaN/Inf in input, diagonal or residual         */
+#define GRICO_ERR_BREAKDOWN -5        /* non-positive CG direction (solve.jl:414-416)   */
+#define GRICO_ERR_CUDA -6             /* CUDA runtime error                             */
+#define GRICO_ERR_NO_DEVICE -7        /* no CUDA device (the library never falls back)  */
+#define GRICO_ERR_TIMEOUT -8          /* bounded device wait gave up                    */
+
+#define GRICO_BASIS_FULL 0  /* FullTensorBasis  basis.jl:60-95  */
+#define GRICO_BASIS_TRUNK 1 /* TrunkBasis       basis.jl:97-126 */
+#define GRICO_CONTINUITY_CG 0
+#define GRICO_CONTINUITY_DG 1
+
+/* Closed set of cell forms.  TestChannels(a0, a_grad) means ∫ a0 v + a_grad·∇v
+ * (accumulators.jl:148-160).  GRICO_FORM_MASS_DIFFUSION: a0 = mass*u, a_grad = kappa*k(x)*∇u
+ * with k(x) = 1 or tabulated per quadrature point.  Anything else is rejected with
+ * GRICO_ERR_UNSUPPORTED_FORM. */
+#define GRICO_FORM_MASS_DIFFUSION 1
+
+#define GRICO_PREC_FP64 0 /* vectors double, arithmetic double                      */
+#define GRICO_PREC_FP32 1 /* vectors float, arithmetic float (mixed-precision path) */
+
+#define GRICO_FLAG_HOST_POINTERS 1 /* vector arguments are host memory: copy in/out */
+
+/* ================================================================================
+ * Host space compile (native replacement of the Julia-side HpSpace construction)
+ * ================================================================================ */
+typedef struct GricoSpace GricoSpace;
+
+/* Build an hp space from active leaves given as (levels, logical coords) per axis,
+ * leaf-major [nleaves*dim].  Leaves are reordered into the reference's Morton order.
+ * Replaces HpSpace(domain, SpaceOptions(...)) — space.jl:300-326, continuity.jl:153-1227. */
+int grico_space_build(int dim, const int64_t* root_counts, int64_t nleaves, const int32_t* leaf_levels,
+                      const int64_t* leaf_coords, const int32_t* leaf_degrees, int basis, int continuity,
+                      int quadrature_extra, GricoSpace** out);
+int grico_space_destroy(GricoSpace* space);
+/* Sizes: scalar dofs, total terms, total box modes (sum over leaves of prod(p+1)),
+ * boundary faces, interfaces (topology.jl:1502-1545). */
+int grico_space_sizes(const GricoSpace* space, int64_t* ndofs, int64_t* nterms, int64_t* nboxes,
+                      int64_t* nboundary, int64_t* ninterfaces);
+/* Copy out: Morton order (position -> input leaf), per-leaf box offsets [nleaves+1], term CSR
+ * over box modes ([nboxes+1], [nterms], [nterms]; inactive/zero modes have empty ranges),
+ * quadrature shape [nleaves*dim], boundary faces (leaf position, axis, side 0=LOWER/1=UPPER)
+ * and interfaces (minus position, plus position, axis).  Any output may be NULL. */
+int grico_space_export(const GricoSpace* space, int64_t* morton_order, int64_t* leaf_box_offset,
+                       int64_t* term_offsets, int64_t* term_index, double* term_coef, int32_t* qshape,
+                       int64_t* bnd_leaf, int32_t* bnd_axis, int32_t* bnd_side, int64_t* if_minus,
+                       int64_t* if_plus, int32_t* if_axis);
+/* 1-D numerics of the product: Gauss-Legendre rule (quadrature.jl:342-410) and the
+ * integrated-Legendre finite-element basis (polynomials.jl:238-247, 403-434). */
+int grico_gauss_legendre(int count, double* points, double* weights);
+int grico_fe_basis(double x, int degree, double* values, double* derivatives);
+
+/* ================================================================================
+ * Device plan (the drop-in for AssemblyPlan's matrix-free runtime)
+ * ================================================================================ */
+
+/* One batch of cells sharing a kernel signature (plans.jl:307-332): same per-axis degree and
+ * tensor quadrature.  Local modes are addressed by their box index (axis 1 fastest,
+ * basis.jl:150-180); trunk-basis cells mark missing box modes inactive. */
+typedef struct GricoCellBatchDesc {
+  int32_t n_cells;
+  int32_t degree[3];          /* per axis; unused axes 0                                  */
+  int32_t qpoints[3];         /* Gauss points per axis (q >= p+1 required)                 */
+  const int32_t* map_index;   /* [n_cells*n_box]: >=0 global dof, -1 inactive, <=-2 tail k=-(v+2) */
+  const double* map_coef;     /* [n_cells*n_box] or NULL (all 1.0)                          */
+  int64_t n_tail;             /* multi-term entries (hanging-node expansions)               */
+  const int64_t* tail_offsets;/* [n_tail+1]                                                 */
+  const int32_t* tail_index;  /* global dofs                                                */
+  const double* tail_coef;
+  const double* cell_size;    /* [n_cells*dim] physical cell sizes h_a                      */
+  const double* kappa_points; /* NULL or [n_cells*prod(q)] pointwise gradient coefficient    */
+} GricoCellBatchDesc;
+
+typedef struct GricoPlanDesc {
+  int32_t dim;                /* 1..3 (sum-factorized kernels for 2 and 3)                  */
+  int32_t form;               /* GRICO_FORM_*                                               */
+  double mass;                /* a0 = mass*u                                                */
+  double kappa;               /* a_grad = kappa*k(x)*grad u                                 */
+  int64_t n_full;             /* full field-layout dofs                                     */
+  int32_t n_batches;
+  const GricoCellBatchDesc* batches;
+  /* constraint rows of the full layout (plans.jl:38-56, assembly.jl:1893-1920) */
+  int64_t n_fixed;
+  const int64_t* fixed_dofs;
+  const double* fixed_values;
+  int64_t n_relations;        /* Dirichlet affine rows: x[p] - sum c x[j] = rhs             */
+  const int64_t* rel_pivot;
+  const int64_t* rel_offsets; /* [n_relations+1]                                            */
+  const int64_t* rel_index;
+  const double* rel_coef;
+  const double* rel_rhs;
+  /* reduced map u_full = shift + P u_red (assembly.jl:19-27): CSR rows per full dof */
+  int64_t n_reduced;
+  const int64_t* red_offsets; /* [n_full+1]                                                 */
+  const int64_t* red_index;
+  const double* red_coef;
+  const double* red_shift;    /* [n_full] or NULL                                           */
+} GricoPlanDesc;
+
+typedef struct GricoPlan GricoPlan;
+
+/* Copies every descriptor array to the device; the caller may free them afterwards.  The plan
+ * owns its workspaces and one CUDA stream.  Calls on one plan are serialised. */
+int grico_plan_create(const GricoPlanDesc* desc, GricoPlan** out);
+int grico_plan_destroy(GricoPlan* plan);
+/* n_full, n_reduced */
+int grico_plan_sizes(const GricoPlan* plan, int64_t* n_full, int64_t* n_reduced);
+
+/* y = A x on the full layout with constraint rows written explicitly (assembly.jl:540-564).
+ * x, y: [nrhs][n_full] device (or host with GRICO_FLAG_HOST_POINTERS) arrays of the precision's
+ * element type; x and y must not alias.  stream: cudaStream_t or NULL for the plan stream. */
+int grico_apply(GricoPlan* plan, const void* x, void* y, int nrhs, int precision, int flags, void* stream);
+/* y_red = P^T A P x_red (assembly.jl:905-915). */
+int grico_reduced_apply(GricoPlan* plan, const void* x, void* y, int nrhs, int precision, int flags,
+                        void* stream);
+/* Reduced right-hand side P^T (b_phys - A shift) from the load tabulated at the quadrature
+ * points of every batch (source[b] = [n_cells*prod(q)] for batch b, NULL => 0) — assembly.jl:917-933. */
+int grico_reduced_rhs(GricoPlan* plan, const double* const* source_points, double* b_reduced, int flags);
+/* Jacobi diagonal of the reduced operator (assembly.jl:662-675 where the reduced map is direct;
+ * exact local-matrix diagonal otherwise, replacing the probe fallback solve.jl:722-738). */
+int grico_reduced_diagonal(GricoPlan* plan, double* diag, int flags);
+/* Reconstruct the full vector u = shift + P u_red (assembly.jl:965-970). */
+int grico_expand_reduced(GricoPlan* plan, const double* u_red, double* u_full, int flags);
+
+/* ---- Krylov solvers on the reduced system ---- */
+#define GRICO_PRECOND_IDENTITY 0
+#define GRICO_PRECOND_JACOBI 1
+#define GRICO_PRECOND_MULTIGRID 2
+
+typedef struct GricoSolveOptions {
+  double relative_tolerance;  /* stop when ||r|| <= max(atol, rtol*||b||) (solve.jl:407-421) */
+  double absolute_tolerance;
+  int32_t maxiter;
+  int32_t preconditioner;     /* GRICO_PRECOND_*                                            */
+  int32_t restart;            /* FGMRES restart (solve.jl:94-99)                            */
+  int32_t use_initial;        /* x holds the initial solution                               */
+} GricoSolveOptions;
+
+typedef struct GricoSolveReport {
+  int32_t iterations;
+  int32_t status;
+  double initial_residual;
+  double final_residual;
+  double seconds;             /* device time of the solve                                  */
+} GricoSolveReport;
+
+typedef struct GricoMultigrid GricoMultigrid;
+
+int grico_cg_solve(GricoPlan* plan, GricoMultigrid* mg, const double* b, double* x,
+                   const GricoSolveOptions* opts, GricoSolveReport* report, int flags);
+int grico_fgmres_solve(GricoPlan* plan, GricoMultigrid* mg, const double* b, double* x,
+                       const GricoSolveOptions* opts, GricoSolveReport* report, int flags);
+
+/* ---- hp geometric multigrid (multigrid.jl:66-96, 309-345, 858-1087) ---- */
+typedef struct GricoTransferDesc {
+  /* prolongation coarse -> fine on reduced vectors as CSR over fine rows; restriction is its
+   * transpose (multigrid.jl:614-636, 1060-1087) */
+  int64_t n_fine, n_coarse;
+  const int64_t* row_offsets; /* [n_fine+1] */
+  const int64_t* col_index;
+  const double* values;
+} GricoTransferDesc;
+
+#define GRICO_SMOOTHER_JACOBI 0     /* damped Jacobi, reference default (multigrid.jl:943-956) */
+#define GRICO_SMOOTHER_CHEBYSHEV 1  /* Chebyshev-Jacobi (no reference counterpart)            */
+
+typedef struct GricoMGOptions {
+  int32_t smoother;
+  int32_t pre_steps, post_steps;
+  double jacobi_omega;          /* 0.8 default (multigrid.jl:70)                            */
+  int32_t chebyshev_degree;
+  double chebyshev_lower;       /* fraction of lambda_max for the lower bound               */
+  int32_t precision;            /* GRICO_PREC_FP64 or GRICO_PREC_FP32 for level applies     */
+} GricoMGOptions;
+
+/* levels[0] is the coarsest; transfers[i] maps level i -> i+1.  coarse_matrix is the dense
+ * reduced operator of level 0 (row-major n0 x n0), factorised by Cholesky on create. */
+int grico_mg_create(GricoPlan* const* levels, int nlevels, const GricoTransferDesc* transfers,
+                    const double* coarse_matrix, const GricoMGOptions* opts, GricoMultigrid** out);
+int grico_mg_destroy(GricoMultigrid* mg);
+/* z = V-cycle(r) on the finest level (multigrid.jl:858-889) */
+int grico_mg_vcycle(GricoMultigrid* mg, const double* r, double* z, int flags);
+/* Chebyshev eigenvalue estimate lambda_max(D^-1 A) of one level (0 if unused, -1 on error). */
+double grico_mg_lambda_max(GricoMultigrid* mg, int level);
+
+const char* grico_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GRICO_B200_H */

@@ -1,0 +1,1076 @@
+"""CPU oracle for the Grico matrix-free hot path — TEST INFRASTRUCTURE ONLY.
+
+This module is a literal, loop-by-loop restatement of the reference algorithms
+that produce the data the GPU path consumes (Grico.jl, Julia).  It exists so the
+tests can check the product (``grico.jl_b200``) against an independent
+derivation.  Only ``tests/``, ``__graft_entry__.smoke()`` and the
+``cpu_baseline`` leg of ``bench.py`` may import it, and only as the checker.
+
+Parity pins (reference known-answer tests restated in ``tests/test_oracle_kat.py``):
+  * polynomial values/derivatives      test/core.jl:152-167
+  * DOF counts, hanging coefficients   test/space.jl:274-320, 639-700
+  * small apply / Dirichlet values     test/matrix_free.jl:305,578,780
+  * GMG level sizes                    test/multigrid.jl:160,171
+
+Each function names the reference file:line it follows.  Floating point
+operation order follows the reference where the reference fixes it (polynomial
+recurrences, Newton, restriction matrices); LAPACK calls use the same drivers
+as Julia's LinearAlgebra (getrf/getrs, syevr, geqp3) through scipy.
+"""
+
+from __future__ import annotations
+
+import math
+from collections import OrderedDict
+
+import numpy as np
+import scipy.linalg as sla
+
+EPS = np.finfo(np.float64).eps
+LOWER, UPPER = 1, 2
+NONE = 0
+
+
+# ---------------------------------------------------------------------------
+# 1-D numerics: src/polynomials.jl, src/quadrature.jl
+# ---------------------------------------------------------------------------
+
+def legendre_values(x: float, n: int) -> list:
+    """P_0..P_n at x (polynomials.jl:294-306; same operation order)."""
+    v = [0.0] * (n + 1)
+    v[0] = 1.0
+    if n >= 1:
+        v[1] = x
+    for k in range(2, n + 1):
+        inv_k = 1.0 / float(k)
+        v[k] = float(2 * k - 1) * inv_k * x * v[k - 1] - float(k - 1) * inv_k * v[k - 2]
+    return v
+
+
+def legendre_values_and_derivatives(x: float, n: int):
+    """P and P' (polynomials.jl:308-326)."""
+    v = [0.0] * (n + 1)
+    d = [0.0] * (n + 1)
+    v[0] = 1.0
+    d[0] = 0.0
+    if n >= 1:
+        v[1] = x
+        d[1] = 1.0
+    for k in range(2, n + 1):
+        inv_k = 1.0 / float(k)
+        first = float(2 * k - 1) * inv_k
+        second = float(k - 1) * inv_k
+        v[k] = first * x * v[k - 1] - second * v[k - 2]
+        d[k] = first * (v[k - 1] + x * d[k - 1]) - second * d[k - 2]
+    return v, d
+
+
+def integrated_legendre_values_and_derivatives(x: float, n: int):
+    """psi_0=(1-x)/2, psi_1=(1+x)/2, psi_k=(P_k-P_{k-2})/sqrt(4k-2); psi_k'=sqrt((2k-1)/2) P_{k-1}
+    (polynomials.jl:403-434)."""
+    v = legendre_values(x, n)
+    d = [0.0] * (n + 1)
+    for k in range(n, 1, -1):
+        d[k] = math.sqrt(float(2 * k - 1) / 2.0) * v[k - 1]
+    d[0] = -0.5
+    if n >= 1:
+        d[1] = 0.5
+    for k in range(n, 1, -1):
+        v[k] = (v[k] - v[k - 2]) / math.sqrt(float(4 * k - 2))
+    v[0] = 0.5 * (1.0 - x)
+    if n >= 1:
+        v[1] = 0.5 * (1.0 + x)
+    return v, d
+
+
+def fe_basis_values_and_derivatives(x: float, p: int):
+    """Degree 0 is the DG constant, else integrated Legendre (polynomials.jl:238-247)."""
+    if p == 0:
+        return [1.0], [0.0]
+    return integrated_legendre_values_and_derivatives(x, p)
+
+
+def gauss_legendre_rule(count: int):
+    """Newton from cosine guesses, mirrored halves, ascending (quadrature.jl:342-410)."""
+    pts = [0.0] * count
+    wts = [0.0] * count
+    tol = 1.0e3 * EPS
+    half = (count + 1) // 2
+    for i in range(1, half + 1):
+        x = math.cos(math.pi * (float(i) - 0.25) / (float(count) + 0.5))
+        converged = False
+        for _ in range(32):
+            v, d = legendre_values_and_derivatives(x, count)
+            delta = v[count] / d[count]
+            x -= delta
+            if abs(delta) <= tol:
+                v, d = legendre_values_and_derivatives(x, count)
+                converged = True
+                break
+        if not converged:
+            raise ValueError("Gauss-Legendre root did not converge")
+        w = 2.0 / ((1.0 - x * x) * d[count] ** 2)
+        pts[i - 1] = -x
+        wts[i - 1] = w
+        m = count - i
+        pts[m] = x
+        wts[m] = w
+    return pts, wts
+
+
+# ---------------------------------------------------------------------------
+# Modes: src/basis.jl
+# ---------------------------------------------------------------------------
+
+def mode_from_linear(index: int, degrees):
+    """Mixed radix, axis 1 fastest (basis.jl:351-365)."""
+    out = []
+    for p in degrees:
+        out.append(index % (p + 1))
+        index //= (p + 1)
+    return tuple(out)
+
+
+def basis_modes(basis: str, degrees):
+    """FullTensor: whole box; Trunk: sum of interior orders <= max degree (basis.jl:97-190)."""
+    total = 1
+    for p in degrees:
+        total *= p + 1
+    modes = [mode_from_linear(i, degrees) for i in range(total)]
+    if basis == "full":
+        return modes
+    limit = max(degrees) if degrees else 0
+    return [m for m in modes if sum(0 if v <= 1 else v for v in m) <= limit]
+
+
+def flatten_mode(mode, shape):
+    """One-based mixed-radix index (space.jl:941-951)."""
+    idx, stride = 1, 1
+    for a in range(len(mode)):
+        idx += mode[a] * stride
+        stride *= shape[a]
+    return idx
+
+
+# ---------------------------------------------------------------------------
+# Topology: src/topology.jl, src/refinement.jl, src/geometry.jl
+# ---------------------------------------------------------------------------
+
+class Grid:
+    """Cartesian refinement tree; cell ids are 1-based like the reference (topology.jl:96-163)."""
+
+    def __init__(self, root_counts):
+        self.D = len(root_counts)
+        self.root_counts = tuple(int(c) for c in root_counts)
+        total = 1
+        for c in self.root_counts:
+            total *= c
+        self.levels = [[0] * (total + 1) for _ in range(self.D)]
+        self.coords = [[0] * (total + 1) for _ in range(self.D)]
+        self.parent = [NONE] * (total + 1)
+        self.first_child = [NONE] * (total + 1)
+        self.split_axis = [0] * (total + 1)
+        self.active = [False] + [True] * total
+        strides = []
+        s = 1
+        for a in range(self.D):
+            strides.append(s)
+            s *= self.root_counts[a]
+        for cell in range(1, total + 1):
+            lin = cell - 1
+            for a in range(self.D):
+                self.coords[a][cell] = (lin // strides[a]) % self.root_counts[a]
+
+    def stored(self):
+        return len(self.parent) - 1
+
+    def refine(self, cell, axis):
+        """Append one midpoint child block (refinement.jl:47-76). axis is 1-based."""
+        assert self.active[cell]
+        a = axis - 1
+        first = self.stored() + 1
+        for off in range(2):
+            for b in range(self.D):
+                if b == a:
+                    self.levels[b].append(self.levels[b][cell] + 1)
+                    self.coords[b].append(2 * self.coords[b][cell] + off)
+                else:
+                    self.levels[b].append(self.levels[b][cell])
+                    self.coords[b].append(self.coords[b][cell])
+            self.parent.append(cell)
+            self.first_child.append(NONE)
+            self.split_axis.append(0)
+            self.active.append(True)
+        self.first_child[cell] = first
+        self.split_axis[cell] = axis
+        self.active[cell] = False
+        return first
+
+    def active_leaves(self):
+        return [c for c in range(1, self.stored() + 1) if self.active[c]]
+
+    def level(self, cell, a):
+        return self.levels[a][cell]
+
+    def coord(self, cell, a):
+        return self.coords[a][cell]
+
+
+def uniform_refine(grid: Grid, depth: int):
+    """Refine every leaf on every axis, axis by axis (benchmark/hpmg_scaling.jl:122-164)."""
+    for _ in range(depth):
+        for leaf in list(grid.active_leaves()):
+            leaves = [leaf]
+            for axis in range(1, grid.D + 1):
+                nxt = []
+                for cur in leaves:
+                    f = grid.refine(cur, axis)
+                    nxt += [f, f + 1]
+                leaves = nxt
+
+
+def morton_ordered_leaves(grid: Grid):
+    """Sort active leaves by Morton code of the lower corner on the finest lattice; bits high to low,
+    axes D..1 within a bit; ties by level tuple then cell id (topology.jl:250-268, 451-463)."""
+    leaves = grid.active_leaves()
+    D = grid.D
+    max_levels = [max(grid.level(l, a) for l in leaves) for a in range(D)]
+    bit_count = 0
+    for a in range(D):
+        value = (grid.root_counts[a] << max_levels[a]) - 1
+        bits = 0
+        while value > 0:
+            bits += 1
+            value >>= 1
+        bit_count = max(bit_count, bits)
+
+    def key(leaf):
+        lower = [grid.coord(leaf, a) << (max_levels[a] - grid.level(leaf, a)) for a in range(D)]
+        code = 0
+        for bit in range(bit_count - 1, -1, -1):
+            for a in range(D - 1, -1, -1):
+                code = (code << 1) | ((lower[a] >> bit) & 1)
+        return (code, tuple(grid.level(leaf, a) for a in range(D)), leaf)
+
+    return sorted(leaves, key=key)
+
+
+class Snapshot:
+    """Morton-ordered leaves, boundary faces and interfaces (topology.jl:232-245, 1502-1545).
+
+    Neighbour search is done on the common finest lattice; the enumeration order matches the
+    reference: leaves in Morton order, axes ascending, UPPER-side partners sorted by their
+    tangential lower corner (axis 1 first)."""
+
+    def __init__(self, grid: Grid):
+        self.grid = grid
+        D = grid.D
+        self.leaves = morton_ordered_leaves(grid)
+        self.leaf_to_index = {leaf: i for i, leaf in enumerate(self.leaves)}
+        self.finest = [max(grid.level(l, a) for l in self.leaves) for a in range(D)]
+        self.lower = {}
+        self.upper = {}
+        for l in self.leaves:
+            self.lower[l] = tuple(grid.coord(l, a) << (self.finest[a] - grid.level(l, a)) for a in range(D))
+            self.upper[l] = tuple((grid.coord(l, a) + 1) << (self.finest[a] - grid.level(l, a)) for a in range(D))
+        self.extent = [grid.root_counts[a] << self.finest[a] for a in range(D)]
+        # index leaves by their lower/upper face coordinate on each axis
+        by_lower = [dict() for _ in range(D)]
+        for l in self.leaves:
+            for a in range(D):
+                by_lower[a].setdefault(self.lower[l][a], []).append(l)
+        self.boundary = []  # (leaf, axis(1-based), side)
+        self.interfaces = []  # (minus, plus, axis(1-based))
+        for l in self.leaves:
+            for a in range(D):
+                for side in (LOWER, UPPER):
+                    coord = self.lower[l][a] if side == LOWER else self.upper[l][a]
+                    if coord == 0 or coord == self.extent[a]:
+                        self.boundary.append((l, a + 1, side))
+        for l in self.leaves:
+            for a in range(D):
+                partners = []
+                for other in by_lower[a].get(self.upper[l][a], []):
+                    ok = True
+                    for b in range(D):
+                        if b == a:
+                            continue
+                        if not (max(self.lower[l][b], self.lower[other][b]) < min(self.upper[l][b], self.upper[other][b])):
+                            ok = False
+                            break
+                    if ok:
+                        partners.append(other)
+                partners.sort(key=lambda o: tuple(0 if b == a else self.lower[o][b] for b in range(D)))
+                for o in partners:
+                    self.interfaces.append((l, o, a + 1))
+
+
+class Domain:
+    """Affine box geometry on a grid (geometry.jl:134-141, 676-711)."""
+
+    def __init__(self, origin, extent, root_counts):
+        self.origin = tuple(float(v) for v in origin)
+        self.extent = tuple(float(v) for v in extent)
+        self.grid = Grid(root_counts)
+        self.D = len(root_counts)
+
+    def cell_size(self, cell, a):
+        root = self.extent[a] / self.grid.root_counts[a]
+        return math.ldexp(root, -self.grid.level(cell, a))
+
+    def cell_lower(self, cell, a):
+        return self.origin[a] + self.cell_size(cell, a) * self.grid.coord(cell, a)
+
+    def center_half(self, cell, a):
+        size = self.cell_size(cell, a)
+        lower = self.origin[a] + size * self.grid.coord(cell, a)
+        half = 0.5 * size
+        return lower + half, half
+
+    def det_biunit(self, cell):
+        prod = 1.0
+        for a in range(self.D):
+            prod *= self.cell_size(cell, a)
+        return math.ldexp(prod, -self.D)
+
+
+# ---------------------------------------------------------------------------
+# Continuity: src/continuity.jl (phases 1-6)
+# ---------------------------------------------------------------------------
+
+def _constraint_tolerance(coefs):
+    scale = 0.0
+    for c in coefs:
+        scale = max(scale, abs(c))
+    return 4.0 * EPS * max(scale, 1.0)
+
+
+class Row:
+    __slots__ = ("vars", "coefs")
+
+    def __init__(self):
+        self.vars = []
+        self.coefs = []
+
+    def add(self, var, c):
+        """continuity.jl:1000-1010"""
+        for i, v in enumerate(self.vars):
+            if v == var:
+                self.coefs[i] += c
+                return
+        self.vars.append(var)
+        self.coefs.append(c)
+
+    def remove_at(self, i):
+        del self.vars[i]
+        del self.coefs[i]
+
+    def remove_var(self, var):
+        for i, v in enumerate(self.vars):
+            if v == var:
+                self.remove_at(i)
+                return
+
+    def cleanup(self):
+        """continuity.jl:681-700"""
+        tol = _constraint_tolerance(self.coefs)
+        i = 0
+        while i < len(self.vars):
+            if abs(self.coefs[i]) <= tol:
+                self.remove_at(i)
+            else:
+                i += 1
+
+    def accumulate(self, src, factor=1.0):
+        for v, c in zip(src.vars, src.coefs):
+            self.add(v, factor * c)
+
+
+def _uf_root(parent, v):
+    root = v
+    while parent[root] != root:
+        root = parent[root]
+    while parent[v] != v:
+        nxt = parent[v]
+        parent[v] = root
+        v = nxt
+    return root
+
+
+def _uf_union(parent, a, b):
+    """Smaller root wins (continuity.jl:1053-1065)."""
+    ra = _uf_root(parent, a)
+    rb = _uf_root(parent, b)
+    if ra == rb:
+        return ra
+    if ra < rb:
+        parent[rb] = ra
+        return ra
+    parent[ra] = rb
+    return rb
+
+
+_RESTRICTION_CACHE = {}
+
+
+def affine_restriction_matrix(source_degree, target_degree, delta, relative):
+    """Collocation on target_degree+1 Gauss points, LU solve (continuity.jl:1158-1198)."""
+    key = (source_degree, target_degree, delta, relative)
+    if key in _RESTRICTION_CACHE:
+        return _RESTRICTION_CACHE[key]
+    scale = math.ldexp(1.0, -delta)
+    shift = 0.0 if delta == 0 else scale * (2.0 * float(relative) + 1.0) - 1.0
+    n = target_degree + 1
+    pts, _ = gauss_legendre_rule(n)
+    basis = np.zeros((n, n))
+    for i in range(n):
+        v, _ = fe_basis_values_and_derivatives(pts[i], target_degree)
+        basis[i, :] = v
+    src = np.zeros((n, source_degree + 1))
+    for i in range(n):
+        xi = scale * pts[i] + shift
+        v, _ = fe_basis_values_and_derivatives(xi, source_degree)
+        src[i, :] = v
+    lu, piv = sla.lu_factor(basis)
+    mat = sla.lu_solve((lu, piv), src)
+    _RESTRICTION_CACHE[key] = mat
+    return mat
+
+
+def _interval_level_coord(lower, upper, finest):
+    length = upper - lower
+    assert length > 0 and (length & (length - 1)) == 0
+    shift = length.bit_length() - 1
+    return finest - shift, lower >> shift
+
+
+def _restriction_coefficient(src_lo, src_hi, tgt_lo, tgt_hi, src_index, src_deg, tgt_deg, tgt_index, finest):
+    """continuity.jl:1085-1147"""
+    sl, sc = _interval_level_coord(src_lo, src_hi, finest)
+    tl, tc = _interval_level_coord(tgt_lo, tgt_hi, finest)
+    delta = tl - sl
+    relative = tc - (sc << delta)
+    mat = affine_restriction_matrix(src_deg, tgt_deg, delta, relative)
+    return float(mat[tgt_index, src_index])
+
+
+class Space:
+    """HpSpace compile (space.jl:300-326, 742-752; continuity.jl phases 1-6).
+
+    degree_fn(leaf) -> degree tuple; basis 'full' or 'trunk'; continuity 'cg' or 'dg' (all axes);
+    quadrature extra points (DegreePlusQuadrature, default 1)."""
+
+    def __init__(self, domain: Domain, degree, basis="trunk", continuity="cg", quadrature_extra=1):
+        self.domain = domain
+        self.grid = domain.grid
+        self.D = domain.D
+        self.basis = basis
+        self.continuity = continuity
+        self.snapshot = Snapshot(self.grid)
+        snap = self.snapshot
+        D = self.D
+        leaves = snap.leaves
+        if callable(degree):
+            self.degrees = [tuple(degree(l)) for l in leaves]
+        else:
+            deg = tuple(degree) if isinstance(degree, (tuple, list)) else (int(degree),) * D
+            self.degrees = [deg for _ in leaves]
+        self.quadrature_extra = quadrature_extra
+        self.qshape = [tuple(max(d + quadrature_extra, 1) for d in degs) for degs in self.degrees]
+        self.patterns = []
+        for degs in self.degrees:
+            modes = basis_modes(basis, degs)
+            self.patterns.append((modes, [m for m in modes if any(v <= 1 for v in m)]))
+        self.next_dof = 1
+        nleaf = len(leaves)
+        self.lookup = [dict() for _ in range(nleaf)]
+        self.face_modes = {}
+        self.boundary_terms = []
+        if continuity == "cg":
+            self._build_boundary_variables()
+            self._compile_boundary_terms()
+        # phase 6
+        self.leaf_modes = []
+        self.leaf_terms = []  # list per leaf: list per mode of [(dof, coef)]
+        for li in range(nleaf):
+            modes_out, terms_out = [], []
+            for mode in self.patterns[li][0]:
+                if continuity == "cg" and any(v <= 1 for v in mode):
+                    var = self.lookup[li][mode]
+                    terms = [(d, c) for (d, c) in self.boundary_terms[var] if c != 0.0]
+                else:
+                    terms = [(self.next_dof, 1.0)]
+                    self.next_dof += 1
+                if terms:
+                    modes_out.append(mode)
+                    terms_out.append(terms)
+            self.leaf_modes.append(modes_out)
+            self.leaf_terms.append(terms_out)
+        self.ndofs = self.next_dof - 1
+
+    # -- phase 3 ---------------------------------------------------------
+    def _fm(self, li, axis, side):
+        return self.face_modes.setdefault((li, axis, side), [])
+
+    def _build_boundary_variables(self):
+        """continuity.jl:223-252"""
+        nxt = 1
+        for li in range(len(self.snapshot.leaves)):
+            for mode in self.patterns[li][1]:
+                var = nxt
+                self.lookup[li][mode] = var
+                for a in range(self.D):
+                    if mode[a] <= 1:
+                        self._fm(li, a + 1, mode[a] + LOWER).append((var, mode))
+                nxt += 1
+        self.nvars = nxt - 1
+        self.boundary_terms = [None] + [[] for _ in range(self.nvars)]
+
+    # -- phases 4/5 ------------------------------------------------------
+    def _matching(self, f, s, axis):
+        snap = self.snapshot
+        lf, ls = snap.leaves[f], snap.leaves[s]
+        for b in range(self.D):
+            if b == axis - 1:
+                continue
+            if snap.lower[lf][b] != snap.lower[ls][b] or snap.upper[lf][b] != snap.upper[ls][b]:
+                return False
+        return True
+
+    def _same_trace_modes(self, f, s, axis):
+        fv = self._fm(f, axis, UPPER)
+        sv = self._fm(s, axis, LOWER)
+        if len(fv) != len(sv):
+            return False
+        for (_, mode) in fv:
+            m2 = tuple(0 if b == axis - 1 else mode[b] for b in range(self.D))
+            if m2 not in self.lookup[s]:
+                return False
+        return True
+
+    def _compile_boundary_terms(self):
+        """continuity.jl:384-422"""
+        snap = self.snapshot
+        parent = list(range(self.nvars + 1))
+        pairs = [(snap.leaf_to_index[m], snap.leaf_to_index[p], ax) for (m, p, ax) in snap.interfaces]
+        constraint_pairs = []
+        for (f, s, axis) in pairs:
+            if self._matching(f, s, axis) and self._same_trace_modes(f, s, axis):
+                for (var, mode) in self._fm(f, axis, UPPER):
+                    m2 = tuple(0 if b == axis - 1 else mode[b] for b in range(self.D))
+                    _uf_union(parent, var, self.lookup[s][m2])
+            else:
+                constraint_pairs.append((f, s, axis))
+        roots = [0] + [_uf_root(parent, v) for v in range(1, self.nvars + 1)]
+        rows = self._face_rows(roots, constraint_pairs)
+        if not rows:
+            free = [0] * (self.nvars + 1)
+            for v in range(1, self.nvars + 1):
+                if roots[v] == v:
+                    free[v] = self.next_dof
+                    self.next_dof += 1
+            for v in range(1, self.nvars + 1):
+                if roots[v] == v:
+                    self.boundary_terms[v] = [(free[v], 1.0)]
+            for v in range(1, self.nvars + 1):
+                if roots[v] != v:
+                    self.boundary_terms[v] = self.boundary_terms[roots[v]]
+            return
+        # components (continuity.jl:809-833)
+        cparent = list(range(self.nvars + 1))
+        for row in rows:
+            if len(row.vars) <= 1:
+                continue
+            for v in row.vars[1:]:
+                _uf_union(cparent, row.vars[0], v)
+        comp_rows = {}
+        for row in rows:
+            if not row.vars:
+                continue
+            comp_rows.setdefault(_uf_root(cparent, row.vars[0]), []).append(row)
+        components = sorted(comp_rows.keys())
+        pivots = [None] * (self.nvars + 1)
+        orders = []
+        for comp in components:
+            local = {}
+            order = []
+            for row in comp_rows[comp]:
+                while True:
+                    changed = False
+                    for i, v in enumerate(row.vars):
+                        expr = local.get(v)
+                        if expr is None:
+                            continue
+                        factor = row.coefs[i]
+                        row.remove_at(i)
+                        row.accumulate(expr, factor)
+                        changed = True
+                        break
+                    row.cleanup()
+                    if not changed:
+                        break
+                if not row.vars:
+                    continue
+                pidx = max(range(len(row.vars)), key=lambda i: row.vars[i])
+                pivot, pcoef = row.vars[pidx], row.coefs[pidx]
+                row.remove_var(pivot)
+                scale = -(1.0 / pcoef)
+                expr = Row()
+                expr.accumulate(row, scale)
+                expr.cleanup()
+                local[pivot] = expr
+                pivots[pivot] = expr
+                order.append(pivot)
+            orders.append(order)
+        free = [0] * (self.nvars + 1)
+        for v in range(1, self.nvars + 1):
+            if roots[v] == v and pivots[v] is None:
+                free[v] = self.next_dof
+                self.next_dof += 1
+        for v in range(1, self.nvars + 1):
+            if roots[v] == v:
+                self.boundary_terms[v] = [] if pivots[v] is not None else [(free[v], 1.0)]
+        for order in orders:
+            for pivot in reversed(order):
+                expr = pivots[pivot]
+                acc = Row()
+                for v, factor in zip(expr.vars, expr.coefs):
+                    if factor == 0.0:
+                        continue
+                    terms = self.boundary_terms[v]
+                    if not terms:
+                        assert free[v] == 0
+                        continue
+                    for (d, c) in terms:
+                        acc.add(d, factor * c)
+                acc.cleanup()
+                self.boundary_terms[pivot] = sorted(zip(acc.vars, acc.coefs), key=lambda t: t[0])
+        for v in range(1, self.nvars + 1):
+            if roots[v] != v:
+                self.boundary_terms[v] = self.boundary_terms[roots[v]]
+
+    def _face_rows(self, roots, constraint_pairs):
+        """continuity.jl:470-530, 566-620"""
+        snap = self.snapshot
+        D = self.D
+        rows = []
+        for (f, s, axis) in constraint_pairs:
+            a0 = axis - 1
+            cdeg = tuple(0 if b == a0 else max(self.degrees[f][b], self.degrees[s][b]) for b in range(D))
+            lf, ls = snap.leaves[f], snap.leaves[s]
+            face = snap.upper[lf][a0]
+            plo = tuple(face if b == a0 else max(snap.lower[lf][b], snap.lower[ls][b]) for b in range(D))
+            phi = tuple(face if b == a0 else min(snap.upper[lf][b], snap.upper[ls][b]) for b in range(D))
+            for cmode in basis_modes("full", cdeg):
+                row = Row()
+                for (li, side, sign) in ((f, UPPER, 1.0), (s, LOWER, -1.0)):
+                    leaf = snap.leaves[li]
+                    for (var, mode) in self._fm(li, axis, side):
+                        coef = 1.0
+                        for b in range(D):
+                            if b == a0:
+                                continue
+                            coef *= _restriction_coefficient(snap.lower[leaf][b], snap.upper[leaf][b], plo[b], phi[b],
+                                                             mode[b], self.degrees[li][b], cdeg[b], cmode[b],
+                                                             snap.finest[b])
+                            if coef == 0.0:
+                                coef = 0.0
+                                break
+                        if coef == 0.0:
+                            continue
+                        row.add(roots[var], sign * coef)
+                row.cleanup()
+                if row.vars:
+                    rows.append(row)
+        return rows
+
+    # -- queries ---------------------------------------------------------
+    def mode_terms(self, leaf, mode):
+        li = self.snapshot.leaf_to_index[leaf]
+        return self.leaf_terms[li][self.leaf_modes[li].index(tuple(mode))]
+
+
+# ---------------------------------------------------------------------------
+# Plan data: integration tables (integration.jl:2161-2191, 2677-2742), Dirichlet
+# (plans.jl:486-972), reduced map (assembly.jl:112-314), colouring (plans.jl:307-396)
+# ---------------------------------------------------------------------------
+
+class Plan:
+    """A compiled scalar affine problem with cell forms.
+
+    form: ('mass_diffusion', mu, kappa) meaning TestChannels(mu*u, kappa*grad u);
+    kappa_fn: optional callable x -> kappa(x) multiplying the gradient channel pointwise.
+    dirichlet: list of (axis, side, value) with constant values."""
+
+    def __init__(self, space: Space, mu=0.0, kappa=1.0, kappa_fn=None, source=None, dirichlet=()):
+        self.space = space
+        dom = space.domain
+        D = space.D
+        snap = space.snapshot
+        self.mu, self.kappa, self.kappa_fn, self.source = mu, kappa, kappa_fn, source
+        self.ndofs = space.ndofs
+        self.cells = []
+        for li, leaf in enumerate(snap.leaves):
+            q = space.qshape[li]
+            rules = [gauss_legendre_rule(n) for n in q]
+            degs = space.degrees[li]
+            modes = space.leaf_modes[li]
+            det = dom.det_biunit(leaf)
+            ch = [dom.center_half(leaf, a) for a in range(D)]
+            inv_j = [1.0 / ch[a][1] for a in range(D)]
+            axis_v, axis_g = [], []
+            for a in range(D):
+                V = np.zeros((degs[a] + 1, q[a]))
+                G = np.zeros((degs[a] + 1, q[a]))
+                for j in range(q[a]):
+                    v, d = fe_basis_values_and_derivatives(rules[a][0][j], degs[a])
+                    V[:, j] = v
+                    G[:, j] = [inv_j[a] * dd for dd in d]
+                axis_v.append(V)
+                axis_g.append(G)
+            npts = int(np.prod(q))
+            pts = np.zeros((npts, D))
+            w = np.zeros(npts)
+            for p in range(npts):
+                idx = mode_from_linear(p, tuple(n - 1 for n in q))
+                wt = 1.0
+                for a in range(D):
+                    wt *= rules[a][1][idx[a]]
+                w[p] = wt * det
+                for a in range(D):
+                    pts[p, a] = ch[a][0] + rules[a][0][idx[a]] * ch[a][1]
+            nm = len(modes)
+            vals = np.ones((nm, npts))
+            grads = np.ones((D, nm, npts))
+            for p in range(npts):
+                idx = mode_from_linear(p, tuple(n - 1 for n in q))
+                for i, m in enumerate(modes):
+                    val = 1.0
+                    for a in range(D):
+                        val *= axis_v[a][m[a], idx[a]]
+                    vals[i, p] = val
+                    for a in range(D):
+                        g = axis_g[a][m[a], idx[a]]
+                        for b in range(D):
+                            if b != a:
+                                g *= axis_v[b][m[b], idx[b]]
+                        grads[a, i, p] = g
+            terms = space.leaf_terms[li]
+            self.cells.append(dict(leaf=leaf, modes=modes, terms=terms, w=w, pts=pts, vals=vals, grads=grads,
+                                   axis_v=axis_v, axis_g=axis_g, q=q, degs=degs))
+        self.colors = self._colour()
+        self.fixed, self.fixed_values, self.rows = self._dirichlet(dirichlet)
+        self.fixed_mask = np.zeros(self.ndofs + 1, dtype=bool)
+        self.fixed_mask[self.fixed] = True
+        self.blocked = np.zeros(self.ndofs + 1, dtype=bool)
+        for (pivot, _, _, _) in self.rows:
+            self.blocked[pivot] = True
+        self._reduced_map()
+
+    # -- colouring (plans.jl:368-424) ------------------------------------------------
+    def _colour(self):
+        """One batch when all cells share a signature; greedy first-fit colours in batch order."""
+        batches = OrderedDict()
+        for ci, c in enumerate(self.cells):
+            sig = (len(c["w"]), len(c["modes"]), tuple(len(t) for t in c["terms"]))
+            batches.setdefault(sig, []).append(ci)
+        order = []
+        for items in batches.values():
+            colour_sets, colour_items = [], []
+            for ci in items:
+                dofs = {d for t in self.cells[ci]["terms"] for (d, _) in t}
+                for k, s in enumerate(colour_sets):
+                    if not (s & dofs):
+                        s |= dofs
+                        colour_items[k].append(ci)
+                        break
+                else:
+                    colour_sets.append(set(dofs))
+                    colour_items.append([ci])
+            order.append(colour_items)
+        return order
+
+    # -- Dirichlet (plans.jl:486-972) -----------------------------------------------
+    def _dirichlet(self, dirichlet):
+        if not dirichlet:
+            return [], [], []
+        space = self.space
+        dom = space.domain
+        D = space.D
+        snap = space.snapshot
+        faces = []
+        for (leaf, axis, side) in snap.boundary:
+            for (ax, sd, val) in dirichlet:
+                if ax == axis and sd == side:
+                    faces.append((leaf, axis, side, val))
+        involved = sorted({d for (leaf, _, _, _) in faces
+                           for t in space.leaf_terms[snap.leaf_to_index[leaf]] for (d, _) in t})
+        pos = {d: i for i, d in enumerate(involved)}
+        n = len(involved)
+        G = np.zeros((n, n))
+        rhs = np.zeros(n)
+        for (leaf, axis, side, val) in faces:
+            li = snap.leaf_to_index[leaf]
+            a0 = axis - 1
+            degs = space.degrees[li]
+            q = space.qshape[li]
+            rules = [gauss_legendre_rule(nq) for nq in q]
+            face_q = [1 if b == a0 else q[b] for b in range(D)]
+            face_det = 1.0
+            for b in range(D):
+                if b != a0:
+                    face_det *= dom.cell_size(leaf, b)
+            face_det = math.ldexp(face_det, -(D - 1))
+            modes = space.leaf_modes[li]
+            terms = space.leaf_terms[li]
+            npts = int(np.prod(face_q))
+            for p in range(npts):
+                idx = mode_from_linear(p, tuple(nq - 1 for nq in face_q))
+                wt = 1.0
+                xi = []
+                for b in range(D):
+                    if b == a0:
+                        xi.append(-1.0 if side == LOWER else 1.0)
+                    else:
+                        xi.append(rules[b][0][idx[b]])
+                        wt *= rules[b][1][idx[b]]
+                wt *= face_det
+                phi = []
+                for m in modes:
+                    v = 1.0
+                    for b in range(D):
+                        vb, _ = fe_basis_values_and_derivatives(xi[b], degs[b])
+                        v *= vb[m[b]]
+                    phi.append(v)
+                for i in range(len(modes)):
+                    for (gi, ci) in terms[i]:
+                        r = pos[gi]
+                        if phi[i] != 0.0 and val != 0.0:
+                            rhs[r] += ci * phi[i] * wt * val
+                        for j in range(len(modes)):
+                            for (gj, cj) in terms[j]:
+                                G[r, pos[gj]] += ci * phi[i] * phi[j] * wt * cj
+        evals, evecs = sla.eigh(G, driver="evr")
+        order = np.argsort(-evals, kind="stable")
+        evals, evecs = evals[order], evecs[:, order]
+        scale = np.max(np.abs(evals)) if n else 0.0
+        tol = 0.0 if scale == 0 else 1000 * EPS * scale * max(n, 1)
+        count = int(np.sum(evals > tol))
+        if count == 0:
+            return [], [], []
+        C = evecs[:, :count].T.copy()
+        targets = (evecs.T @ rhs)[:count] / evals[:count]
+        _, _, perm = sla.qr(C, pivoting=True, mode="economic")
+        pivcols = list(perm[:count])
+        freecols = [c for c in range(n) if c not in set(pivcols)]
+        P = C[:, pivcols]
+        shift = np.linalg.solve(P, targets)
+        fixed, fixed_vals, rows = [], [], []
+        if freecols:
+            coupling = -np.linalg.solve(P, C[:, freecols])
+        for r in range(count):
+            idx, co = [], []
+            for k, fc in enumerate(freecols):
+                if abs(coupling[r, k]) > tol:
+                    idx.append(involved[fc])
+                    co.append(float(coupling[r, k]))
+            pivot = involved[pivcols[r]]
+            if not idx:
+                fixed.append(pivot)
+                fixed_vals.append(float(shift[r]))
+            else:
+                rows.append((pivot, idx, co, float(shift[r])))
+        perm2 = np.argsort(fixed, kind="stable")
+        fixed = [fixed[i] for i in perm2]
+        fixed_vals = [fixed_vals[i] for i in perm2]
+        rows.sort(key=lambda r: r[0])
+        return fixed, fixed_vals, rows
+
+    # -- reduced map (assembly.jl:112-314) ------------------------------------------
+    def _reduced_map(self):
+        n = self.ndofs
+        constrained = self.fixed_mask | self.blocked
+        self.solve_dofs = [d for d in range(1, n + 1) if not constrained[d]]
+        self.reduced_index = np.zeros(n + 1, dtype=np.int64)
+        for i, d in enumerate(self.solve_dofs):
+            self.reduced_index[d] = i + 1
+        fixed_val = dict(zip(self.fixed, self.fixed_values))
+        rows = {r[0]: r for r in self.rows}
+        cache = {}
+
+        def expand(d):
+            if d in cache:
+                return cache[d]
+            if self.reduced_index[d] != 0:
+                out = (0.0, {int(self.reduced_index[d]): 1.0})
+            elif d in fixed_val:
+                out = (fixed_val[d], {})
+            elif d in rows:
+                _, idx, co, rhs = rows[d]
+                shift, red = rhs, {}
+                for j, c in zip(idx, co):
+                    s2, r2 = expand(j)
+                    shift += c * s2
+                    for k, v in r2.items():
+                        red[k] = red.get(k, 0.0) + c * v
+                out = (shift, red)
+            else:
+                out = (0.0, {})
+            cache[d] = out
+            return out
+
+        self.shift = np.zeros(n + 1)
+        self.P_rows = []
+        for d in range(1, n + 1):
+            s, red = expand(d)
+            self.shift[d] = s
+            self.P_rows.append(sorted(red.items()))
+
+    # -- runtime (assembly.jl:540-564, 905-915; accumulators.jl:1022-1054) ----------
+    def local_apply(self, c, xloc):
+        w = c["w"]
+        u = c["vals"].T @ xloc
+        g = np.einsum("ainp,n->aip", c["grads"][:, :, None, :], xloc)[:, :, 0] if False else \
+            np.stack([c["grads"][a].T @ xloc for a in range(self.space.D)])
+        kap = self.kappa * (np.array([self.kappa_fn(tuple(p)) for p in c["pts"]]) if self.kappa_fn else 1.0)
+        t0 = w * self.mu * u
+        tg = w * kap * g
+        y = c["vals"] @ t0 + sum(c["grads"][a] @ tg[a] for a in range(self.space.D))
+        return y
+
+    def apply(self, x):
+        """y = A x on the full layout (1-based arrays of length ndofs+1 are used internally)."""
+        x1 = np.concatenate([[0.0], np.asarray(x, dtype=np.float64)])
+        y1 = np.zeros(self.ndofs + 1)
+        for colours in self.colors:
+            for items in colours:
+                for ci in items:
+                    c = self.cells[ci]
+                    xloc = np.array([sum(cc * x1[d] for (d, cc) in t) for t in c["terms"]])
+                    yloc = self.local_apply(c, xloc)
+                    for i, t in enumerate(c["terms"]):
+                        if yloc[i] == 0.0:
+                            continue
+                        for (d, cc) in t:
+                            if self.fixed_mask[d] or self.blocked[d]:
+                                continue
+                            y1[d] += cc * yloc[i]
+        for d in self.fixed:
+            y1[d] = x1[d]
+        for (pivot, idx, co, _) in self.rows:
+            v = x1[pivot]
+            for j, c in zip(idx, co):
+                v -= c * x1[j]
+            y1[pivot] = v
+        return y1[1:]
+
+    def apply_physical(self, x):
+        x1 = np.concatenate([[0.0], np.asarray(x, dtype=np.float64)])
+        y1 = np.zeros(self.ndofs + 1)
+        for c in self.cells:
+            xloc = np.array([sum(cc * x1[d] for (d, cc) in t) for t in c["terms"]])
+            yloc = self.local_apply(c, xloc)
+            for i, t in enumerate(c["terms"]):
+                for (d, cc) in t:
+                    y1[d] += cc * yloc[i]
+        return y1[1:]
+
+    def expand(self, xr, include_shift=False):
+        xf = np.zeros(self.ndofs)
+        for d in range(1, self.ndofs + 1):
+            v = self.shift[d] if include_shift else 0.0
+            for (k, c) in self.P_rows[d - 1]:
+                v += c * xr[k - 1]
+            xf[d - 1] = v
+        return xf
+
+    def project(self, yf):
+        yr = np.zeros(len(self.solve_dofs))
+        for d in range(1, self.ndofs + 1):
+            for (k, c) in self.P_rows[d - 1]:
+                yr[k - 1] += c * yf[d - 1]
+        return yr
+
+    def reduced_apply(self, xr):
+        return self.project(self.apply_physical(self.expand(xr)))
+
+    def physical_diagonal(self):
+        """cell_diagonal! basis probe + coefficient-squared scatter (accumulators.jl:1056-1083,
+        assembly.jl:1811-1825)."""
+        out = np.zeros(self.ndofs + 1)
+        D = self.space.D
+        for c in self.cells:
+            kap = self.kappa * (np.array([self.kappa_fn(tuple(p)) for p in c["pts"]]) if self.kappa_fn else 1.0)
+            diag = c["vals"] ** 2 @ (c["w"] * self.mu) + sum((c["grads"][a] ** 2) @ (c["w"] * kap) for a in range(D))
+            for i, t in enumerate(c["terms"]):
+                for (d, cc) in t:
+                    out[d] += cc * cc * diag[i]
+        return out[1:]
+
+    def reduced_diagonal(self):
+        """Direct copy when the map is an injection, else None (assembly.jl:662-726)."""
+        for c in self.cells:
+            for t in c["terms"]:
+                if len(t) != 1:
+                    return None
+        pd = self.physical_diagonal()
+        return np.array([pd[d - 1] for d in self.solve_dofs])
+
+    def rhs_physical(self):
+        out = np.zeros(self.ndofs + 1)
+        for c in self.cells:
+            f = np.array([self.source(tuple(p)) for p in c["pts"]])
+            loc = c["vals"] @ (c["w"] * f)
+            for i, t in enumerate(c["terms"]):
+                if loc[i] == 0.0:
+                    continue
+                for (d, cc) in t:
+                    out[d] += cc * loc[i]
+        return out[1:]
+
+    def reduced_rhs(self):
+        b = self.rhs_physical()
+        if np.any(self.shift[1:] != 0.0):
+            b = b - self.apply_physical(self.shift[1:])
+        return self.project(b)
+
+
+def cg_solve(apply_fn, b, precond=None, rtol=1e-10, atol=0.0, maxiter=10000):
+    """PCG with the unpreconditioned stop rule (solve.jl:376-431)."""
+    n = len(b)
+    x = np.zeros(n)
+    r = b.copy()
+    z = precond(r) if precond else r.copy()
+    p = z.copy()
+    rz = float(np.dot(r, z))
+    tol = max(atol, rtol * math.sqrt(float(np.dot(b, b))))
+    if float(np.dot(r, r)) <= tol * tol:
+        return x, 0
+    for it in range(1, maxiter + 1):
+        ap = apply_fn(p)
+        den = float(np.dot(p, ap))
+        if not den > 0:
+            raise ValueError("CG encountered a non-positive operator direction")
+        alpha = rz / den
+        x += alpha * p
+        r -= alpha * ap
+        if float(np.dot(r, r)) <= tol * tol:
+            return x, it
+        z = precond(r) if precond else r.copy()
+        rz_new = float(np.dot(r, z))
+        beta = rz_new / rz
+        p = z + beta * p
+        rz = rz_new
+    raise ValueError("CG did not converge")
+
+
+def l2_error(plan: Plan, full_values, exact):
+    """Cell quadrature L2 error (verification.jl:201-230)."""
+    x1 = np.concatenate([[0.0], np.asarray(full_values)])
+    err2 = 0.0
+    for c in plan.cells:
+        xloc = np.array([sum(cc * x1[d] for (d, cc) in t) for t in c["terms"]])
+        u = c["vals"].T @ xloc
+        ex = np.array([exact(tuple(p)) for p in c["pts"]])
+        err2 += float(np.sum(c["w"] * (u - ex) ** 2))
+    return math.sqrt(err2)
