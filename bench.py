@@ -1,0 +1,286 @@
+#!/usr/bin/env python
+"""Benchmark: FP64 matrix-free apply DOFs/s on the 3-D Poisson workload (64^3 cells, p = 4,
+Gauss 5^3, homogeneous Dirichlet: 16,974,593 dofs), one step = one full-layout apply!.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU runs (torchrun) are independent replicas per rank (weak scaling, no data-path
+collective); the job value is the sum over ranks with the max time over ranks.
+The reference arm times the CPU restatement of Grico's tensor-product apply (the oracle's C
+kernel, all host threads) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "grico.jl_b200"))
+
+WORKLOAD = {"workload": "poisson3d_64cube_p4_dirichlet", "cells": "64x64x64", "degree": 4,
+            "quadrature": "gauss 5x5x5", "dofs": 16974593, "form": "TestChannels(0, grad u)",
+            "layout": "full (apply!)"}
+METRIC = "DOFs/s matrix-free apply; time-to-1e-8 L² error (learned+mixed vs plain GPU)"
+UNIT = "DOFs/s"
+# flops per cell of the collocation schedule (2 q n (n^2 + q n + q^2) + 2 D q^(D+1)) * 2 + pointwise
+N1 = Q1 = 5
+FLOPS_PER_CELL = 2 * (2 * Q1 * N1 * (N1 * N1 + Q1 * N1 + Q1 * Q1) + 2 * 3 * Q1 ** 4) + 9 * Q1 ** 3
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+def sample_vector(n):
+    """_diagnostic_sample_vector (diagnostics.jl:107-121): sin(0.013 i) + 0.25 cos(0.037 i)."""
+    i = np.arange(1, n + 1, dtype=np.float64)
+    return np.sin(0.013 * i) + 0.25 * np.cos(0.037 * i)
+
+
+class ClockSampler:
+    """nvidia-smi clocks during the timed region (SM MHz, max, throttle reasons)."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([v.strip() for v in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if len(s) > 3 + k and s[3 + k] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def build_problem(gb):
+    domain = gb.Domain((0.0, 0.0, 0.0), (1.0, 1.0, 1.0), (4, 4, 4))
+    gb.uniform_refine(domain, 4)
+    space = gb.HpSpace(domain, gb.SpaceOptions(basis=gb.FullTensorBasis(), degree=gb.UniformDegree(4)))
+    u = gb.ScalarField(space)
+    prob = gb.AffineProblem(u)
+    gb.add_cell_accumulator(prob, u, u, gb.Diffusion())
+    for a in (1, 2, 3):
+        for side in (gb.LOWER, gb.UPPER):
+            gb.add_constraint(prob, gb.Dirichlet(u, gb.BoundaryFace(a, side), 0.0))
+    return prob
+
+
+def cpu_reference_run(steps, warmup, budget_s=20.0):
+    """Time the oracle's C restatement of the reference tensor apply on the full workload with
+    every host thread.  Returns (DOFs/s, seconds per apply, threads, sample description)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import grico_oracle as go
+    import oracle_lib as ol
+    import uniform_maps as um
+
+    counts, p = (64, 64, 64), 4
+    coords, m, ndofs = um.uniform_space(counts, p)
+    order, off = um.parity_colours(coords)
+    pts, W = go.gauss_legendre_rule(p + 1)
+    B = np.zeros((p + 1, p + 1))
+    G = np.zeros((p + 1, p + 1))
+    for j, x in enumerate(pts):
+        v, d = go.integrated_legendre_values_and_derivatives(x, p)
+        B[:, j] = v
+        G[:, j] = d
+    h = np.full((len(coords), 3), 1.0 / 64)
+    x = sample_vector(ndofs)
+    y = np.zeros(ndofs)
+    threads = ol.max_threads()
+    args = (3, p + 1, p + 1, m.astype(np.int32), h, B, G, np.array(W), 0.0, 1.0, None, order, off)
+    t0 = time.perf_counter()
+    ol.tensor_apply(*args, x, y, threads=threads)  # warm-up, also sizes the sample
+    one = time.perf_counter() - t0
+    reps = max(1, min(steps, int(budget_s / max(one, 1e-6))))
+    times = []
+    for _ in range(reps):
+        y[:] = 0.0
+        t0 = time.perf_counter()
+        ol.tensor_apply(*args, x, y, threads=threads)
+        times.append(time.perf_counter() - t0)
+    sec = float(np.median(times))
+    sample = f"{reps} full applies of the 64^3 p=4 workload ({ndofs} dofs), median"
+    return ndofs / sec, sec, threads, sample
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    value, sec, threads, sample = cpu_reference_run(args.steps, args.warmup)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (diagnostic sample vector)",
+            "config": dict(WORKLOAD, parallelism="host threads"), "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    import grico_b200 as gb
+    from grico_b200 import _lib as L
+
+    prob = build_problem(gb)
+    plan = gb.compile(prob)
+    n = plan.n_full
+    x = torch.tensor(sample_vector(n), device="cuda")
+    y = torch.empty_like(x)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        L.check(L.lib().grico_apply(plan.handle, x.data_ptr(), y.data_ptr(), 1, L.GRICO_PREC_FP64, 0,
+                                    stream.cuda_stream), "apply")
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            step()
+        end.record(stream)
+        torch.cuda.synchronize()
+    ms = start.elapsed_time(end) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    dofs_per_s = n / (ms * 1e-3) * world
+
+    # ---- end to end through the C ABI with pinned host buffers (copies inside the timed region) ----
+    hx = torch.tensor(sample_vector(n)).pin_memory()
+    hy = torch.empty(n, dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        L.check(L.lib().grico_apply(plan.handle, hx.data_ptr(), hy.data_ptr(), 1, L.GRICO_PREC_FP64,
+                                    L.GRICO_FLAG_HOST_POINTERS, None), "apply")
+
+    for _ in range(2):
+        e2e_step()
+    e2e_steps = max(3, min(args.steps, 20))
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = n / e2e_s * world
+    # check the e2e result equals the device result
+    assert torch.allclose(hy.cuda(), y, rtol=0, atol=1e-12 * float(y.abs().max()))
+
+    if rank == 0:
+        peak, peak_kind = load_peaks()
+        alg_bytes = 2 * 8 * n
+        achieved = alg_bytes / (ms * 1e-3) / 1e9
+        ncells = 64 ** 3
+        fp64_tflops = FLOPS_PER_CELL * ncells / (ms * 1e-3) / 1e12
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "cell_apply_3d_p4_poisson64.txt")
+        if os.path.exists(tpath):
+            for line in open(tpath):
+                if line.startswith("traffic_bytes_per_full_apply:"):
+                    traffic = float(line.split(":", 1)[1])
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            value, sec, threads, sample = cpu_reference_run(3, 1, budget_s=15.0)
+            cpu = {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
+        out = {
+            "metric": METRIC, "value": dofs_per_s, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (diagnostic sample vector)",
+            "config": dict(WORKLOAD, parallelism=f"replicas x{world}" if world > 1 else "single GPU",
+                           l2="inputs larger than L2 (x, y 136 MB each, maps 131 MB)"),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
+            "gpu_launches": 2 * args.steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "note": "achieved = 2*8*n_full bytes / apply time; FP64 pipe is the binding roof",
+                         "fp64_tflops": fp64_tflops, "flops_per_cell": FLOPS_PER_CELL},
+            "clocks": clocks.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

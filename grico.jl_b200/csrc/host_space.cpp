@@ -284,6 +284,7 @@ struct Space {
   std::vector<int64_t> term_index;    // 0-based global dof
   std::vector<double> term_coef;
   int64_t ndofs = 0;
+  double min_pivot = 1e300;  // smallest |pivot coefficient| met in the elimination
 };
 
 namespace {
@@ -571,6 +572,7 @@ void compile_continuity(Space& s) {
         if (!row.vars.empty()) rows.push_back(std::move(row));
       }
     }
+
     is_pivot.assign(nvars, 0);
     std::vector<std::vector<int64_t>> orders;
     std::unordered_map<int64_t, Row> pivots;
@@ -629,6 +631,7 @@ void compile_continuity(Space& s) {
           local[pivot] = &stored;
           is_pivot[pivot] = 1;
           order.push_back(pivot);
+          s.min_pivot = std::min(s.min_pivot, std::fabs(pcoef));
         }
         orders.push_back(std::move(order));
       }

@@ -165,7 +165,7 @@ def _tables(p, q):
 class AssemblyPlan:
     """Compiled plan: descriptor arrays built here, device data owned by libgrico_b200."""
 
-    def __init__(self, problem):
+    def __init__(self, problem, device=True):
         if not problem.cell_operators:
             raise ValueError("problem has no cell operator")
         if len(problem.cell_operators) > 1:
@@ -240,7 +240,9 @@ class AssemblyPlan:
         self.red_coef = np.ones(self.n_reduced)
         self.shift = np.zeros(n_full)
         self.shift[self.fixed_dofs] = self.fixed_values
-        self._create_device_plan()
+        self.handle = None
+        if device:
+            self._create_device_plan()
 
     def _points(self, b):
         D = self.D
@@ -351,8 +353,10 @@ class AssemblyPlan:
         return self.n_reduced
 
 
-def compile(problem):
-    return AssemblyPlan(problem)
+def compile(problem, device=True):
+    """compile(problem) -> AssemblyPlan (plans.jl:170-231).  device=False builds only the host
+    descriptor (no CUDA call), which the CPU tests compare with the oracle."""
+    return AssemblyPlan(problem, device=device)
 
 
 # ---------------------------------------------------------------------------------------

@@ -484,6 +484,7 @@ class Space:
         self.next_dof = 1
         nleaf = len(leaves)
         self.lookup = [dict() for _ in range(nleaf)]
+        self.min_pivot = math.inf
         self.face_modes = {}
         self.boundary_terms = []
         if continuity == "cg":
@@ -591,6 +592,7 @@ class Space:
         components = sorted(comp_rows.keys())
         pivots = [None] * (self.nvars + 1)
         orders = []
+        self.min_pivot = math.inf
         for comp in components:
             local = {}
             order = []
@@ -613,6 +615,7 @@ class Space:
                     continue
                 pidx = max(range(len(row.vars)), key=lambda i: row.vars[i])
                 pivot, pcoef = row.vars[pidx], row.coefs[pidx]
+                self.min_pivot = min(self.min_pivot, abs(pcoef))
                 row.remove_var(pivot)
                 scale = -(1.0 / pcoef)
                 expr = Row()
@@ -739,22 +742,20 @@ class Plan:
                 w[p] = wt * det
                 for a in range(D):
                     pts[p, a] = ch[a][0] + rules[a][0][idx[a]] * ch[a][1]
-            nm = len(modes)
-            vals = np.ones((nm, npts))
-            grads = np.ones((D, nm, npts))
-            for p in range(npts):
-                idx = mode_from_linear(p, tuple(n - 1 for n in q))
-                for i, m in enumerate(modes):
-                    val = 1.0
-                    for a in range(D):
-                        val *= axis_v[a][m[a], idx[a]]
-                    vals[i, p] = val
-                    for a in range(D):
-                        g = axis_g[a][m[a], idx[a]]
-                        for b in range(D):
-                            if b != a:
-                                g *= axis_v[b][m[b], idx[b]]
-                        grads[a, i, p] = g
+            # full shape tables values[mode, point], gradients[axis, mode, point] as tensor
+            # products of the 1-D tables (integration.jl:2717-2740)
+            mi = np.array(modes, dtype=np.int64).reshape(len(modes), D)
+            pi = np.array([mode_from_linear(p, tuple(n - 1 for n in q)) for p in range(npts)],
+                          dtype=np.int64).reshape(npts, D)
+            fv = [axis_v[a][mi[:, a]][:, pi[:, a]] for a in range(D)]
+            fg = [axis_g[a][mi[:, a]][:, pi[:, a]] for a in range(D)]
+            vals = np.ones((len(modes), npts))
+            for a in range(D):
+                vals = vals * fv[a]
+            grads = np.ones((D, len(modes), npts))
+            for a in range(D):
+                for b in range(D):
+                    grads[a] = grads[a] * (fg[b] if b == a else fv[b])
             terms = space.leaf_terms[li]
             self.cells.append(dict(leaf=leaf, modes=modes, terms=terms, w=w, pts=pts, vals=vals, grads=grads,
                                    axis_v=axis_v, axis_g=axis_g, q=q, degs=degs))
@@ -824,6 +825,8 @@ class Plan:
             modes = space.leaf_modes[li]
             terms = space.leaf_terms[li]
             npts = int(np.prod(face_q))
+            phi = np.zeros((npts, len(modes)))
+            wts = np.zeros(npts)
             for p in range(npts):
                 idx = mode_from_linear(p, tuple(nq - 1 for nq in face_q))
                 wt = 1.0
@@ -834,22 +837,26 @@ class Plan:
                     else:
                         xi.append(rules[b][0][idx[b]])
                         wt *= rules[b][1][idx[b]]
-                wt *= face_det
-                phi = []
-                for m in modes:
+                wts[p] = wt * face_det
+                tables = [fe_basis_values_and_derivatives(xi[b], degs[b])[0] for b in range(D)]
+                for i, m in enumerate(modes):
                     v = 1.0
                     for b in range(D):
-                        vb, _ = fe_basis_values_and_derivatives(xi[b], degs[b])
-                        v *= vb[m[b]]
-                    phi.append(v)
-                for i in range(len(modes)):
-                    for (gi, ci) in terms[i]:
-                        r = pos[gi]
-                        if phi[i] != 0.0 and val != 0.0:
-                            rhs[r] += ci * phi[i] * wt * val
-                        for j in range(len(modes)):
-                            for (gj, cj) in terms[j]:
-                                G[r, pos[gj]] += ci * phi[i] * phi[j] * wt * cj
+                        v *= tables[b][m[b]]
+                    phi[p, i] = v
+            # face mass matrix and load, scattered through the term maps (plans.jl:563-612, 668-702)
+            local_g = phi.T @ (wts[:, None] * phi)
+            local_r = phi.T @ wts * val
+            cols = sorted({pos[d] for t in terms for (d, _) in t})
+            cpos = {c: k for k, c in enumerate(cols)}
+            T = np.zeros((len(modes), len(cols)))
+            for i, t in enumerate(terms):
+                for (d, c) in t:
+                    T[i, cpos[pos[d]]] += c
+            ix = np.array(cols)
+            G[np.ix_(ix, ix)] += T.T @ local_g @ T
+            if val != 0.0:
+                rhs[ix] += T.T @ local_r
         evals, evecs = sla.eigh(G, driver="evr")
         order = np.argsort(-evals, kind="stable")
         evals, evecs = evals[order], evecs[:, order]

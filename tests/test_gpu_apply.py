@@ -1,0 +1,150 @@
+"""GPU parity: the sm_100a cell kernels through the C ABI against the oracle.
+
+FP64 tolerance: max|y - y_oracle| / max|y_oracle| <= 1e-12 (the reference's own test
+tolerance for coefficient data is 1e-12; the GPU sums contributions in another order, so
+bit equality is not expected for floating point results)."""
+import math
+
+import numpy as np
+import pytest
+
+import grico_b200 as gb
+from cases import CASES, build, rel_err, sample_vector
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_full_apply_matches_oracle(cuda, name):
+    oplan, prob = build(name, mu=0.7, kappa=1.3)
+    plan = gb.compile(prob)
+    x = sample_vector(plan.n_full)
+    y = gb.apply(plan, x)
+    assert rel_err(y, oplan.apply(x)) <= TOL
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_reduced_apply_matches_oracle(cuda, name):
+    oplan, prob = build(name)
+    plan = gb.compile(prob)
+    xr = sample_vector(plan.n_reduced, seed=7)
+    assert plan.n_reduced == len(oplan.solve_dofs)
+    assert rel_err(gb.reduced_apply(plan, xr), oplan.reduced_apply(xr)) <= TOL
+
+
+@pytest.mark.parametrize("name", ["2d_p4", "3d_p4", "3d_p1", "3d_p3_trunk", "1d_p3", "2d_p3_over"])
+def test_reduced_diagonal_matches_oracle(cuda, name):
+    oplan, prob = build(name, mu=0.25, kappa=2.0)
+    plan = gb.compile(prob)
+    assert rel_err(gb.reduced_diagonal(plan), oplan.reduced_diagonal()) <= TOL
+
+
+def test_variable_coefficient_apply(cuda):
+    kfn = lambda x: np.exp(np.sin(3.0 * x[:, 0]) * np.cos(2.0 * x[:, 1]) + 0.3 * x[:, 2])
+    oplan, prob = build("3d_p4", kappa_fn=kfn)
+    plan = gb.compile(prob)
+    x = sample_vector(plan.n_full, seed=3)
+    assert rel_err(gb.apply(plan, x), oplan.apply(x)) <= TOL
+
+
+@pytest.mark.parametrize("name", ["2d_p4", "3d_p4", "2d_p2_hanging", "3d_p2_hanging", "1d_p3"])
+def test_reduced_rhs_matches_oracle(cuda, name):
+    D = len(CASES[name][0])
+    src = lambda x: np.prod(np.sin(np.pi * x), axis=1) * D * np.pi ** 2 + 0.5 * x[:, 0]
+    oplan, prob = build(name, source=src)
+    plan = gb.compile(prob)
+    assert rel_err(gb.reduced_rhs(plan), oplan.reduced_rhs()) <= TOL
+
+
+def test_mass_kat_1d(cuda):  # test/matrix_free.jl:538-579: apply(mass, ones(2)) ≈ [0.5, 0.5]; rhs ≈ [0.5, 0.5]
+    d = gb.Domain((0.0,), (1.0,), (1,))
+    s = gb.HpSpace(d, gb.SpaceOptions(degree=gb.UniformDegree(1), continuity="dg"))
+    u = gb.ScalarField(s)
+    prob = gb.AffineProblem(u)
+    gb.add_cell_accumulator(prob, u, u, gb.Mass(1.0))
+    gb.add_cell_accumulator(prob, u, gb.Load(lambda x: np.ones(len(x))))
+    plan = gb.compile(prob)
+    assert np.allclose(gb.apply(plan, np.ones(2)), [0.5, 0.5], atol=1e-12)
+    assert np.allclose(gb.reduced_rhs(plan), [0.5, 0.5], atol=1e-12)
+
+
+@pytest.mark.parametrize("name", ["2d_p4", "3d_p4", "3d_p2_hanging"])
+def test_cg_jacobi_matches_oracle(cuda, name):
+    import grico_oracle as go
+
+    D = len(CASES[name][0])
+    src = lambda x: np.prod(np.sin(np.pi * x), axis=1) * D * np.pi ** 2
+    oplan, prob = build(name, source=src)
+    plan = gb.compile(prob)
+    state = gb.solve(plan, solver=gb.CGSolver(gb.JacobiPreconditioner()), relative_tolerance=1e-12)
+    diag = oplan.reduced_diagonal()
+    pre = (lambda r: r / diag) if diag is not None else None
+    xr, _ = go.cg_solve(oplan.reduced_apply, oplan.reduced_rhs(), precond=pre, rtol=1e-12)
+    ref = oplan.expand(xr, include_shift=True)
+    assert rel_err(state.coefficients, ref) <= 1e-9
+
+
+def test_poisson_example_accuracy(cuda):  # test/examples.jl:6-12: 2x2, p=2, L2 <= 2e-2
+    d = gb.Domain((0.0, 0.0), (1.0, 1.0), (2, 2))
+    s = gb.HpSpace(d, gb.SpaceOptions(basis=gb.FullTensorBasis(), degree=gb.UniformDegree(2)))
+    u = gb.ScalarField(s)
+    prob = gb.AffineProblem(u)
+    exact = lambda x: np.sin(np.pi * x[:, 0]) * np.sin(np.pi * x[:, 1])
+    gb.add_cell_accumulator(prob, u, u, gb.Diffusion())
+    gb.add_cell_accumulator(prob, u, gb.Load(lambda x: 2 * np.pi ** 2 * exact(x)))
+    for a in (1, 2):
+        for side in (gb.LOWER, gb.UPPER):
+            gb.add_constraint(prob, gb.Dirichlet(u, gb.BoundaryFace(a, side), 0.0))
+    state = gb.solve(prob, solver=gb.CGSolver(gb.JacobiPreconditioner()), relative_tolerance=1e-10)
+    assert gb.l2_error(state, exact) <= 2e-2
+
+
+def test_fgmres_matches_cg(cuda):
+    src = lambda x: np.prod(np.sin(np.pi * x), axis=1)
+    _, prob = build("3d_p4", source=src)
+    plan = gb.compile(prob)
+    a = gb.solve(plan, solver=gb.CGSolver(gb.JacobiPreconditioner()), relative_tolerance=1e-12)
+    b = gb.solve(plan, solver=gb.FGMRESSolver(gb.JacobiPreconditioner(), restart=30), relative_tolerance=1e-12)
+    assert rel_err(b.coefficients, a.coefficients) <= 1e-9
+
+
+def test_multi_rhs_equals_single(cuda):
+    _, prob = build("3d_p4", mu=0.5)
+    plan = gb.compile(prob)
+    xs = np.stack([sample_vector(plan.n_full, seed=s) for s in (1, 2, 3)])
+    ys = gb.apply(plan, xs.reshape(-1).copy(), nrhs=3).reshape(3, -1)
+    for k in range(3):
+        assert rel_err(ys[k], gb.apply(plan, xs[k].copy())) <= 1e-14
+
+
+def test_fp32_apply_close_to_fp64(cuda):
+    _, prob = build("3d_p4", mu=0.5)
+    plan = gb.compile(prob)
+    x = sample_vector(plan.n_full, seed=11)
+    y64 = gb.apply(plan, x)
+    y32 = gb.apply(plan, x.astype(np.float32))
+    assert y32.dtype == np.float32
+    assert rel_err(y32, y64) <= 1e-5
+
+
+def test_device_tensors_and_aliasing(cuda):
+    import torch
+
+    _, prob = build("3d_p4")
+    plan = gb.compile(prob)
+    x = torch.tensor(sample_vector(plan.n_full, seed=5), device="cuda")
+    y = gb.apply(plan, x)
+    assert rel_err(y.cpu().numpy(), gb.apply(plan, x.cpu().numpy())) <= 1e-14
+    with pytest.raises(ValueError):
+        gb.apply_(x, plan, x)
+    with pytest.raises(ValueError):
+        gb.apply(plan, np.zeros(plan.n_full + 1))
+
+
+def test_cg_not_converged_status(cuda):
+    _, prob = build("3d_p4", source=lambda x: np.ones(len(x)))
+    plan = gb.compile(prob)
+    with pytest.raises(gb.GricoError) as err:
+        gb.solve(plan, solver=gb.CGSolver(gb.JacobiPreconditioner()), relative_tolerance=1e-14, maxiter=2)
+    assert err.value.code == -3
