@@ -37,6 +37,7 @@ struct BatchView {
   const double* D;           // [q*q]   D[p*q+l] = L_l'(xi_p)
   const double* W;           // [q]     reference Gauss weights
   const double* G;           // [n*q]   reference derivative table psi_i'(xi_p)
+  const uint8_t* skip;       // nullable: cells excluded from the diagonal kernel
 };
 
 template <typename T>
@@ -379,6 +380,7 @@ __global__ void cell_apply_generic(BatchView b, int dim, int n0, int n1, int n2,
   T* xl = sm;            // nb
   T* flux = xl + nb;     // (dim+1)*nq
   const int64_t cell = blockIdx.x;
+  if (mode == 3 && b.skip && b.skip[cell]) return;
   const int rhs = blockIdx.y;
   x += rhs * n_vec;
   y += rhs * n_vec;

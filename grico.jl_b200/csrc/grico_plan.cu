@@ -51,9 +51,10 @@ std::vector<double> collocation_derivative(const std::vector<double>& xi) {
 
 namespace {
 
-int64_t box_count(int dim, const int* deg) {
+// number of box modes prod(n_a) for per-axis mode counts n_a = degree_a + 1
+int64_t box_count(int dim, const int* n) {
   int64_t nb = 1;
-  for (int a = 0; a < dim; ++a) nb *= deg[a] + 1;
+  for (int a = 0; a < dim; ++a) nb *= n[a];
   return nb;
 }
 
@@ -119,6 +120,7 @@ void fill_view(BatchView& v, const DevBatch& b, bool reduced) {
   v.D = b.D.get<double>();
   v.W = b.W.get<double>();
   v.G = b.G.get<double>();
+  v.skip = reduced ? b.skip.get<uint8_t>() : nullptr;
 }
 
 template <typename T>
@@ -174,6 +176,105 @@ int grid_for(int64_t n) { return int(std::min<int64_t>((n + 255) / 256, 148 * 16
 
 }  // namespace
 
+// Exact reduced-diagonal contribution sum_{i,j} M_ir A_ij M_jr of one cell whose reduced map is
+// not a direct injection.  The local matrix A of TestChannels(mass*u, kappa*k(x)*grad u) is
+// assembled from the 1-D tables (cell_matrix! semantics, accumulators.jl:968-1001).
+void accumulate_hanging_diagonal(const GricoPlanDesc& d, const GricoCellBatchDesc& bd, const DevBatch& b, int64_t c,
+                                 int64_t nb, const std::vector<int32_t>& rmap, const std::vector<double>& rcoef,
+                                 const std::vector<int64_t>& toff, const std::vector<int32_t>& tidx,
+                                 const std::vector<double>& tcoef, const std::vector<double>& B,
+                                 const std::vector<double>& G, const std::vector<double>& W, int nmax, int qmax,
+                                 std::map<int64_t, double>& out) {
+  const int dim = d.dim;
+  int n[3] = {1, 1, 1}, q[3] = {1, 1, 1};
+  double h[3] = {1, 1, 1}, detJ = 1.0;
+  for (int a = 0; a < dim; ++a) {
+    n[a] = b.n[a];
+    q[a] = b.q[a];
+    h[a] = bd.cell_size[c * dim + a];
+    detJ *= 0.5 * h[a];
+  }
+  auto Bv = [&](int a, int i, int p) { return B[a * nmax * qmax + i * q[a] + p]; };
+  auto Gv = [&](int a, int i, int p) { return G[a * nmax * qmax + i * q[a] + p] * (2.0 / h[a]); };
+  // reduced terms of every local mode
+  std::vector<std::vector<std::pair<int64_t, double>>> terms(nb);
+  for (int64_t i = 0; i < nb; ++i) {
+    int32_t v = rmap[c * nb + i];
+    if (v >= 0) terms[i].emplace_back(v, rcoef[c * nb + i]);
+    else if (v <= -2) {
+      int64_t k = -(int64_t(v) + 2);
+      for (int64_t t = toff[k]; t < toff[k + 1]; ++t) terms[i].emplace_back(tidx[t], tcoef[t]);
+    }
+  }
+  auto digit = [&](int64_t i, int a) {
+    for (int e = 0; e < a; ++e) i /= n[e];
+    return int(i % n[a]);
+  };
+  std::vector<double> A(nb * nb, 0.0);
+  if (!bd.kappa_points) {
+    // 1-D mass and stiffness factors: A = detJ [mass prod_a M_a + kappa sum_a s_a^2 K_a prod_{b!=a} M_b]
+    std::vector<double> M1(3 * 16 * 16, 0.0), K1(3 * 16 * 16, 0.0);
+    for (int a = 0; a < dim; ++a)
+      for (int i = 0; i < n[a]; ++i)
+        for (int j = 0; j < n[a]; ++j) {
+          double m = 0.0, k = 0.0;
+          for (int p = 0; p < q[a]; ++p) {
+            m += W[a * qmax + p] * Bv(a, i, p) * Bv(a, j, p);
+            k += W[a * qmax + p] * Gv(a, i, p) * Gv(a, j, p);
+          }
+          M1[a * 256 + i * 16 + j] = m;
+          K1[a * 256 + i * 16 + j] = k;
+        }
+    for (int64_t i = 0; i < nb; ++i)
+      for (int64_t j = 0; j < nb; ++j) {
+        double mp = 1.0, st = 0.0;
+        for (int a = 0; a < dim; ++a) mp *= M1[a * 256 + digit(i, a) * 16 + digit(j, a)];
+        for (int a = 0; a < dim; ++a) {
+          double t = K1[a * 256 + digit(i, a) * 16 + digit(j, a)];
+          for (int e = 0; e < dim; ++e)
+            if (e != a) t *= M1[e * 256 + digit(i, e) * 16 + digit(j, e)];
+          st += t;
+        }
+        A[i * nb + j] = detJ * (d.mass * mp + d.kappa * st);
+      }
+  } else {
+    const int64_t nq = int64_t(q[0]) * q[1] * q[2];
+    for (int64_t p = 0; p < nq; ++p) {
+      int pi[3] = {int(p % q[0]), int((p / q[0]) % q[1]), int(p / (int64_t(q[0]) * q[1]))};
+      double w = detJ;
+      for (int a = 0; a < dim; ++a) w *= W[a * qmax + pi[a]];
+      double kap = d.kappa * bd.kappa_points[c * nq + p];
+      std::vector<double> phi(nb), gr(3 * nb);
+      for (int64_t i = 0; i < nb; ++i) {
+        double bv[3] = {1, 1, 1};
+        for (int a = 0; a < dim; ++a) bv[a] = Bv(a, digit(i, a), pi[a]);
+        phi[i] = bv[0] * bv[1] * bv[2];
+        for (int a = 0; a < dim; ++a) {
+          double g = Gv(a, digit(i, a), pi[a]);
+          for (int e = 0; e < dim; ++e)
+            if (e != a) g *= bv[e];
+          gr[a * nb + i] = g;
+        }
+      }
+      for (int64_t i = 0; i < nb; ++i)
+        for (int64_t j = 0; j < nb; ++j) {
+          double g = 0.0;
+          for (int a = 0; a < dim; ++a) g += gr[a * nb + i] * gr[a * nb + j];
+          A[i * nb + j] += w * (d.mass * phi[i] * phi[j] + kap * g);
+        }
+    }
+  }
+  std::map<int64_t, std::vector<std::pair<int64_t, double>>> by_dof;
+  for (int64_t i = 0; i < nb; ++i)
+    for (auto& t : terms[i]) by_dof[t.first].emplace_back(i, t.second);
+  for (auto& kv : by_dof) {
+    double s = 0.0;
+    for (auto& x : kv.second)
+      for (auto& y : kv.second) s += x.second * A[x.first * nb + y.first] * y.second;
+    out[kv.first] += s;
+  }
+}
+
 template <typename T>
 int run_apply(GricoPlan* P, bool reduced, const T* x, T* y, int nrhs, cudaStream_t st) {
   const int64_t n = reduced ? P->n_red : P->n_full;
@@ -195,6 +296,9 @@ template int run_apply<float>(GricoPlan*, bool, const float*, float*, int, cudaS
 int reduced_diag_device(GricoPlan* P, double* diag, cudaStream_t st) {
   cudaMemsetAsync(diag, 0, sizeof(double) * P->n_red, st);
   for (auto& b : P->batches) launch_batch<double>(*P, b, true, nullptr, diag, P->n_red, 3, nullptr, 1, st);
+  if (P->n_hang > 0)
+    add_sparse<<<grid_for(P->n_hang), 256, 0, st>>>(P->hang_idx.get<int64_t>(), P->hang_val.get<double>(), P->n_hang,
+                                                    diag);
   return cuda_ok(cudaGetLastError(), "diagonal launch") ? GRICO_OK : GRICO_ERR_CUDA;
 }
 
@@ -204,8 +308,66 @@ using namespace grico;
 
 extern "C" {
 
+// Host-side validation of a plan descriptor; runs before any CUDA call so malformed descriptors
+// are rejected with a precise message (the reference validates plans in check_* helpers).
+static int validate_plan_desc(const GricoPlanDesc* d) {
+  if (d->form != GRICO_FORM_MASS_DIFFUSION) { set_error("unsupported accumulator form"); return GRICO_ERR_UNSUPPORTED_FORM; }
+  if (d->dim < 1 || d->dim > 3 || d->n_full < 0 || d->n_reduced < 0 || d->n_batches < 0 || (d->n_batches && !d->batches)) {
+    set_error("grico_plan_create: invalid sizes");
+    return GRICO_ERR_INVALID;
+  }
+  if (d->n_full >= (int64_t(1) << 31)) { set_error("grico_plan_create: more than 2^31-1 dofs"); return GRICO_ERR_INVALID; }
+  if (!d->red_offsets) { set_error("grico_plan_create: reduced map missing"); return GRICO_ERR_INVALID; }
+  for (int bi = 0; bi < d->n_batches; ++bi) {
+    const GricoCellBatchDesc& bd = d->batches[bi];
+    if (bd.n_cells < 0 || (bd.n_cells > 0 && (!bd.map_index || !bd.cell_size))) {
+      set_error("batch " + std::to_string(bi) + ": missing map or cell sizes");
+      return GRICO_ERR_INVALID;
+    }
+    int n[3] = {1, 1, 1};
+    for (int a = 0; a < d->dim; ++a) {
+      n[a] = bd.degree[a] + 1;
+      if (n[a] < 1 || n[a] > 16 || bd.qpoints[a] < 1 || bd.qpoints[a] > 16) {
+        set_error("batch " + std::to_string(bi) + ": degree/quadrature out of range");
+        return GRICO_ERR_INVALID;
+      }
+    }
+    if (bd.n_tail < 0 || (bd.n_tail > 0 && (!bd.tail_offsets || !bd.tail_index || !bd.tail_coef))) {
+      set_error("batch " + std::to_string(bi) + ": invalid multi-term tail");
+      return GRICO_ERR_INVALID;
+    }
+    const int64_t ne = int64_t(bd.n_cells) * box_count(d->dim, n);
+    for (int64_t e = 0; e < ne; ++e) {
+      const int32_t v = bd.map_index[e];
+      if (v >= d->n_full || (v <= -2 && -(int64_t(v) + 2) >= bd.n_tail)) {
+        set_error("batch " + std::to_string(bi) + ": map entry " + std::to_string(e) + " = " + std::to_string(v) +
+                  " out of range (n_full " + std::to_string(d->n_full) + ", tails " + std::to_string(bd.n_tail) + ")");
+        return GRICO_ERR_INVALID;
+      }
+    }
+    for (int64_t k = 0; k < bd.n_tail; ++k)
+      for (int64_t t = bd.tail_offsets[k]; t < bd.tail_offsets[k + 1]; ++t)
+        if (bd.tail_index[t] < 0 || bd.tail_index[t] >= d->n_full) {
+          set_error("batch " + std::to_string(bi) + ": tail index out of range");
+          return GRICO_ERR_INVALID;
+        }
+  }
+  for (int64_t i = 0; i < d->n_fixed; ++i)
+    if (d->fixed_dofs[i] < 0 || d->fixed_dofs[i] >= d->n_full) { set_error("fixed dof out of range"); return GRICO_ERR_INVALID; }
+  for (int64_t r = 0; r < d->n_relations; ++r) {
+    if (d->rel_pivot[r] < 0 || d->rel_pivot[r] >= d->n_full) { set_error("relation pivot out of range"); return GRICO_ERR_INVALID; }
+    for (int64_t t = d->rel_offsets[r]; t < d->rel_offsets[r + 1]; ++t)
+      if (d->rel_index[t] < 0 || d->rel_index[t] >= d->n_full) { set_error("relation index out of range"); return GRICO_ERR_INVALID; }
+  }
+  for (int64_t i = 0; i < d->n_full; ++i)
+    for (int64_t t = d->red_offsets[i]; t < d->red_offsets[i + 1]; ++t)
+      if (d->red_index[t] < 0 || d->red_index[t] >= d->n_reduced) { set_error("reduced map index out of range"); return GRICO_ERR_INVALID; }
+  return GRICO_OK;
+}
+
 int grico_plan_create(const GricoPlanDesc* d, GricoPlan** out) {
   if (!d || !out) { set_error("grico_plan_create: null argument"); return GRICO_ERR_INVALID; }
+  if (int rc = validate_plan_desc(d)) return rc;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     cudaGetLastError();
@@ -290,8 +452,43 @@ int grico_plan_create(const GricoPlanDesc* d, GricoPlan** out) {
     if (need_coef) ok = ok && b.red.coef.upload(rcoef);
     if (toff.size() > 1) ok = ok && b.red.toff.upload(toff) && b.red.tidx.upload(tidx) && b.red.tcoef.upload(tcoef);
     b.red_multiterm = toff.size() > 1;
+    // Cells whose reduced map couples several local modes to one reduced dof (hanging-node
+    // expansions) need off-diagonal local entries for the exact Jacobi diagonal; the reference
+    // probes with one reduced apply per dof instead (solve.jl:722-738).  Their contribution is
+    // computed here once from the tensor-product local matrix; the device diagonal kernel skips
+    // them.
+    {
+      std::vector<uint8_t> skip(bd.n_cells, 0);
+      int64_t hanging = 0;
+      std::vector<std::pair<int64_t, double>> ent;
+      for (int64_t c = 0; c < bd.n_cells; ++c) {
+        ent.clear();
+        for (int64_t i = 0; i < nb; ++i) {
+          int32_t v = rmap[c * nb + i];
+          if (v >= 0) ent.emplace_back(v, 0.0);
+          else if (v <= -2) { skip[c] = 1; break; }
+        }
+        if (!skip[c]) {
+          std::sort(ent.begin(), ent.end());
+          for (size_t k = 1; k < ent.size(); ++k)
+            if (ent[k].first == ent[k - 1].first) { skip[c] = 1; break; }
+        }
+        if (!skip[c]) continue;
+        ++hanging;
+        accumulate_hanging_diagonal(*d, bd, b, c, nb, rmap, rcoef, toff, tidx, tcoef, B, G, W, nmax, qmax,
+                                    P->hang_diag);
+      }
+      if (hanging) ok = ok && b.skip.upload(skip);
+    }
     if (!ok) return GRICO_ERR_CUDA;
     P->batches.push_back(std::move(b));
+  }
+  if (!P->hang_diag.empty()) {
+    std::vector<int64_t> hi;
+    std::vector<double> hv;
+    for (auto& kv : P->hang_diag) { hi.push_back(kv.first); hv.push_back(kv.second); }
+    if (!P->hang_idx.upload(hi) || !P->hang_val.upload(hv)) return GRICO_ERR_CUDA;
+    P->n_hang = int64_t(hi.size());
   }
   bool ok = true;
   P->n_fixed = d->n_fixed;
@@ -418,11 +615,6 @@ int grico_reduced_rhs(GricoPlan* P, const double* const* source_points, double* 
 
 int grico_reduced_diagonal(GricoPlan* P, double* diag, int flags) {
   if (!P || !diag) return GRICO_ERR_INVALID;
-  for (auto& b : P->batches)
-    if (b.red_multiterm) {
-      int rc = exact_reduced_diagonal(P, diag, flags);
-      return rc;
-    }
   cudaStream_t st = P->stream;
   DevBuf tmp;
   double* out = diag;

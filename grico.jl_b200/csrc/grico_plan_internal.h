@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <map>
 #include <vector>
 
 #include "../../include/grico_b200.h"
@@ -71,6 +72,7 @@ struct DevBatch {
   bool red_multiterm = false;
   DevMap full, red;
   DevBuf h, kappa, B, G, W, D;
+  DevBuf skip;  // uint8 per cell: hanging cells whose diagonal is added from the host
 };
 
 }  // namespace grico
@@ -85,6 +87,9 @@ struct GricoPlan {
   grico::DevBuf fixed, fixed_vals, rel_piv, rel_off, rel_idx, rel_coef;
   grico::DevBuf red_off, red_idx, red_coef, shift;
   bool has_shift = false;
+  std::map<int64_t, double> hang_diag;  // exact diagonal contributions of hanging cells
+  grico::DevBuf hang_idx, hang_val;
+  int64_t n_hang = 0;
   grico::DevBuf partial, scalars;
   grico::DevBuf host_x, host_y;
   // Krylov workspaces (allocated on first solve)
@@ -95,6 +100,5 @@ namespace grico {
 template <typename T>
 int run_apply(GricoPlan* P, bool reduced, const T* x, T* y, int nrhs, cudaStream_t st);
 int reduced_diag_device(GricoPlan* P, double* diag, cudaStream_t st);
-int exact_reduced_diagonal(GricoPlan* P, double* diag, int flags);
 int grid_blocks(int64_t n);
 }  // namespace grico

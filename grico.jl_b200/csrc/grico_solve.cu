@@ -16,14 +16,6 @@ namespace grico {
 
 int grid_blocks(int64_t n) { return int(std::min<int64_t>((n + 255) / 256, kRedBlocks)); }
 
-int exact_reduced_diagonal(GricoPlan* P, double* diag, int flags) {
-  (void)P;
-  (void)diag;
-  (void)flags;
-  set_error("reduced diagonal with multi-term maps is computed by grico_reduced_diagonal_probe");
-  return GRICO_ERR_INVALID;
-}
-
 constexpr int GRICO_NOT_DONE = 1;
 
 namespace {

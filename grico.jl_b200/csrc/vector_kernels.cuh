@@ -156,6 +156,13 @@ static __global__ void invert_diagonal(const double* __restrict__ d, double* __r
   }
 }
 
+// y[idx[k]] += val[k]
+static __global__ void add_sparse(const int64_t* __restrict__ idx, const double* __restrict__ val, int64_t n,
+                                  double* __restrict__ y) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    atomicAdd(y + idx[i], val[i]);
+}
+
 }  // namespace grico
 
 namespace grico {

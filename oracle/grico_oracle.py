@@ -1023,6 +1023,23 @@ class Plan:
         pd = self.physical_diagonal()
         return np.array([pd[d - 1] for d in self.solve_dofs])
 
+    def probe_reduced_diagonal(self):
+        """One reduced apply per unit vector (solve.jl:722-738) — the reference's fallback when
+        the reduced map is not a direct injection."""
+        n = len(self.solve_dofs)
+        out = np.zeros(n)
+        e = np.zeros(n)
+        for i in range(n):
+            e[i] = 1.0
+            out[i] = self.reduced_apply(e)[i]
+            e[i] = 0.0
+        return out
+
+    def jacobi_diagonal(self):
+        """_jacobi_inverse_diagonal's diagonal (solve.jl:713-720): local kernels, else probing."""
+        d = self.reduced_diagonal()
+        return d if d is not None else self.probe_reduced_diagonal()
+
     def rhs_physical(self):
         out = np.zeros(self.ndofs + 1)
         for c in self.cells:

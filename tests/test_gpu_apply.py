@@ -33,11 +33,21 @@ def test_reduced_apply_matches_oracle(cuda, name):
     assert rel_err(gb.reduced_apply(plan, xr), oplan.reduced_apply(xr)) <= TOL
 
 
-@pytest.mark.parametrize("name", ["2d_p4", "3d_p4", "3d_p1", "3d_p3_trunk", "1d_p3", "2d_p3_over"])
+@pytest.mark.parametrize("name", ["2d_p4", "3d_p4", "3d_p1", "3d_p3_trunk", "1d_p3", "2d_p3_over",
+                                  "2d_p2_hanging", "3d_p2_hanging"])
 def test_reduced_diagonal_matches_oracle(cuda, name):
+    """Direct maps: local diagonal kernels (assembly.jl:662-675); hanging maps: the exact
+    diagonal against the reference's probing fallback (solve.jl:722-738)."""
     oplan, prob = build(name, mu=0.25, kappa=2.0)
     plan = gb.compile(prob)
-    assert rel_err(gb.reduced_diagonal(plan), oplan.reduced_diagonal()) <= TOL
+    assert rel_err(gb.reduced_diagonal(plan), oplan.jacobi_diagonal()) <= TOL
+
+
+def test_hanging_diagonal_with_variable_coefficient(cuda):
+    kfn = lambda x: 1.0 + x[:, 0] ** 2 + 0.5 * x[:, 1]
+    oplan, prob = build("3d_p2_hanging", mu=0.3, kappa_fn=kfn)
+    plan = gb.compile(prob)
+    assert rel_err(gb.reduced_diagonal(plan), oplan.probe_reduced_diagonal()) <= TOL
 
 
 def test_variable_coefficient_apply(cuda):
@@ -78,8 +88,8 @@ def test_cg_jacobi_matches_oracle(cuda, name):
     oplan, prob = build(name, source=src)
     plan = gb.compile(prob)
     state = gb.solve(plan, solver=gb.CGSolver(gb.JacobiPreconditioner()), relative_tolerance=1e-12)
-    diag = oplan.reduced_diagonal()
-    pre = (lambda r: r / diag) if diag is not None else None
+    diag = oplan.jacobi_diagonal()
+    pre = lambda r: r / diag
     xr, _ = go.cg_solve(oplan.reduced_apply, oplan.reduced_rhs(), precond=pre, rtol=1e-12)
     ref = oplan.expand(xr, include_shift=True)
     assert rel_err(state.coefficients, ref) <= 1e-9
