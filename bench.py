@@ -167,6 +167,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--soak", type=float, default=1.5, help="seconds of untimed load while clocks are sampled")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", 0))
@@ -192,7 +193,8 @@ def main():
     n = plan.n_full
     x = torch.tensor(sample_vector(n), device="cuda")
     y = torch.empty_like(x)
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()  # explicit stream: the kernels and the timing events share it
+    torch.cuda.synchronize()
 
     def step():
         L.check(L.lib().grico_apply(plan.handle, x.data_ptr(), y.data_ptr(), 1, L.GRICO_PREC_FP64, 0,
@@ -207,11 +209,19 @@ def main():
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clocks:
+        # untimed soak of identical steps so the clock samples cover a loaded GPU
+        t_soak = time.perf_counter()
+        while time.perf_counter() - t_soak < args.soak:
+            for _ in range(50):
+                step()
+            torch.cuda.synchronize()
         start.record(stream)
         for _ in range(args.steps):
             step()
         end.record(stream)
         torch.cuda.synchronize()
+        # keep the sampler running for at least a few samples on short regions
+        time.sleep(0.3)
     ms = start.elapsed_time(end) / args.steps
     if world > 1:
         t = torch.tensor([ms], device="cuda")
@@ -243,6 +253,7 @@ def main():
         e2e_s = float(t.item())
     e2e_value = n / e2e_s * world
     # check the e2e result equals the device result
+    torch.cuda.synchronize()
     assert torch.allclose(hy.cuda(), y, rtol=0, atol=1e-12 * float(y.abs().max()))
 
     if rank == 0:

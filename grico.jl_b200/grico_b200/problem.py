@@ -44,11 +44,11 @@ class Mass:
 
 
 class VariableDiffusion:
-    """TestChannels(0, a(x) grad u) with a(x) tabulated at the quadrature points.
+    """TestChannels(mass*u, kappa*a(x) grad u) with a(x) tabulated at the quadrature points.
     `coefficient(points)` receives an [n, D] array and returns [n] values."""
 
-    def __init__(self, coefficient, kappa=1.0):
-        self.mass, self.kappa, self.coefficient = 0.0, float(kappa), coefficient
+    def __init__(self, coefficient, kappa=1.0, mass=0.0):
+        self.mass, self.kappa, self.coefficient = float(mass), float(kappa), coefficient
 
 
 class Load:
@@ -387,10 +387,20 @@ def _vector_call(fn, plan, x, y, n, nrhs=1):
         y = torch.empty_like(x)
     if y.data_ptr() == x.data_ptr():
         raise ValueError("result and coefficient vector must not alias")
-    stream = torch.cuda.current_stream().cuda_stream
     L.check(fn(plan.handle, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), nrhs, prec, 0,
-               C.c_void_p(stream)), "apply")
+               C.c_void_p(torch_stream_handle())), "apply")
     return y
+
+
+CUDA_STREAM_LEGACY = 1  # cudaStreamLegacy: the library reads a NULL stream as "the plan's stream"
+
+
+def torch_stream_handle():
+    """Handle of torch's current stream as the library expects it (legacy default stream -> 0x1)."""
+    import torch
+
+    h = torch.cuda.current_stream().cuda_stream
+    return h if h else CUDA_STREAM_LEGACY
 
 
 def apply(plan, x, nrhs=1):

@@ -61,7 +61,7 @@ def build(name, mu=0.0, kappa=1.0, kappa_fn=None, source=None):
     u = gb.ScalarField(psp)
     prob = gb.AffineProblem(u)
     if kappa_fn is not None:
-        form = gb.VariableDiffusion(kappa_fn, kappa=kappa)
+        form = gb.VariableDiffusion(kappa_fn, kappa=kappa, mass=mu)
     elif mu == 0.0:
         form = gb.Diffusion(kappa)
     else:
