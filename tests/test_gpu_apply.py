@@ -116,7 +116,7 @@ def test_fgmres_matches_cg(cuda):
     plan = gb.compile(prob)
     a = gb.solve(plan, solver=gb.CGSolver(gb.JacobiPreconditioner()), relative_tolerance=1e-12)
     b = gb.solve(plan, solver=gb.FGMRESSolver(gb.JacobiPreconditioner(), restart=30), relative_tolerance=1e-12)
-    assert rel_err(b.coefficients, a.coefficients) <= 1e-9
+    assert rel_err(b.coefficients, a.coefficients) <= 1e-8  # both stop at ||r|| <= 1e-12 ||b||
 
 
 def test_multi_rhs_equals_single(cuda):
