@@ -63,33 +63,46 @@ __device__ __forceinline__ void scatter_entry(const BatchView& b, int64_t e, T v
   for (int64_t t = b.tail_off[k]; t < b.tail_off[k + 1]; ++t) atomicAdd(y + b.tail_idx[t], T(b.tail_coef[t]) * val);
 }
 
-// mode: 0 = operator apply, 1 = load (rhs) from src points, 2 = operator apply without scatter
-// masks (same as 0).
+// 1-D tables of one (n, q) signature, passed by value so that fully unrolled contractions read
+// them as constant-bank operands instead of shared-memory loads.
+template <int N, int Q, typename T>
+struct Tables1D {
+  T B[N * Q];  // B[i*Q+p] = psi_i(xi_p)
+  T D[Q * Q];  // D[p*Q+l] = L_l'(xi_p)
+  T W[Q];      // Gauss weights
+};
+
+// mode: 0 = operator apply, 1 = load (rhs) from tabulated source values at the points.
+//
+// One cell is handled by Q*Q threads; every contraction step gives each thread one whole line
+// of the cell's Q^3 point box along the contracted axis (z-lines: thread (x, y); y-lines:
+// thread (x, z); x-lines: thread (y, z)), so a step costs one line of shared-memory loads and
+// stores per thread for N*Q (or Q*Q) FMAs.  Three buffers per cell hold u / r, the x-flux and
+// the y-flux.  Sequence: z, y, x interpolation; x derivative; y derivative; z derivative and
+// the pointwise flux on z-lines; transposed z, y, x derivatives; transposed x, y, z
+// interpolation; scatter.
 template <int N, int Q, int CPB, typename T>
-__global__ void __launch_bounds__(Q* Q* CPB) cell_apply_3d(BatchView b, const T* __restrict__ x, T* __restrict__ y,
+__global__ void __launch_bounds__(Q* Q* CPB) cell_apply_3d(BatchView b, const Tables1D<N, Q, T> tab,
+                                                           const T* __restrict__ x, T* __restrict__ y,
                                                            int64_t n_vec, T mass, T kappa, int mode,
                                                            const double* __restrict__ src) {
   constexpr int Q3 = Q * Q * Q;
   constexpr int NB = N * N * N;
-  __shared__ T sB[N * Q], sD[Q * Q], sW[Q];
-  __shared__ T S0[CPB][Q3], S1[CPB][Q3];
-  const int tid = threadIdx.x + threadIdx.y * blockDim.x;
-  for (int i = tid; i < N * Q; i += blockDim.x * blockDim.y) sB[i] = T(b.B[i]);
-  for (int i = tid; i < Q * Q; i += blockDim.x * blockDim.y) sD[i] = T(b.D[i]);
-  for (int i = tid; i < Q; i += blockDim.x * blockDim.y) sW[i] = T(b.W[i]);
-  const int tx = threadIdx.x % Q, ty = threadIdx.x / Q, c = threadIdx.y;
+  constexpr int PITCH = Q3 | 1;  // odd per-cell pitch spreads cells over the banks
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* smem = reinterpret_cast<T*>(smem_raw);
+  const int c = threadIdx.y;
+  T* S0 = smem + (3 * c + 0) * PITCH;
+  T* S1 = smem + (3 * c + 1) * PITCH;
+  T* S2 = smem + (3 * c + 2) * PITCH;
+  const int ta = threadIdx.x % Q, tb = threadIdx.x / Q;
   const int64_t cell = int64_t(blockIdx.x) * CPB + c;
   const bool act = cell < b.n_cells;
-  const int rhs = blockIdx.y;
-  x += rhs * n_vec;
-  y += rhs * n_vec;
-  T* s0 = S0[c];
-  T* s1 = S1[c];
-  __syncthreads();
+  x += blockIdx.y * n_vec;
+  y += blockIdx.y * n_vec;
+  auto at = [](int ix, int iy, int iz) { return ix + Q * (iy + Q * iz); };
 
-  T u[Q];
-  T dx[Q], dy[Q], dz[Q];
-  T h0 = 1, h1 = 1, h2 = 1;
+  T h0 = T(1), h1 = T(1), h2 = T(1);
   if (act) {
     h0 = T(b.h[cell * 3 + 0]);
     h1 = T(b.h[cell * 3 + 1]);
@@ -97,152 +110,177 @@ __global__ void __launch_bounds__(Q* Q* CPB) cell_apply_3d(BatchView b, const T*
   }
   const T sx = T(2) / h0, sy = T(2) / h1, sz = T(2) / h2;
   const T detJ = h0 * h1 * h2 * T(0.125);
+  T line[Q], out[Q];
 
   if (mode != 1) {
-    // ---- gather + interpolate along z (registers) ----
-    T reg[N];
-    if (act && tx < N && ty < N) {
+    // 1. gather + z interpolation on z-lines (x = ta < N, y = tb < N)
+    if (ta < N && tb < N) {
+      T in[N];
 #pragma unroll
-      for (int k = 0; k < N; ++k) reg[k] = gather_entry<T>(b, cell * NB + tx + N * (ty + N * k), x);
-#pragma unroll
-      for (int q = 0; q < Q; ++q) {
-        T s = T(0);
-#pragma unroll
-        for (int k = 0; k < N; ++k) s += sB[k * Q + q] * reg[k];
-        s0[tx + Q * (ty + Q * q)] = s;
-      }
-    }
-    __syncthreads();
-    // ---- y ----
-    T col[Q];
-    if (tx < N) {
+      for (int k = 0; k < N; ++k) in[k] = act ? gather_entry<T>(b, cell * NB + ta + N * (tb + N * k), x) : T(0);
 #pragma unroll
       for (int q = 0; q < Q; ++q) {
         T s = T(0);
 #pragma unroll
-        for (int j = 0; j < N; ++j) s += sB[j * Q + ty] * s0[tx + Q * (j + Q * q)];
-        col[q] = s;
+        for (int k = 0; k < N; ++k) s += tab.B[k * Q + q] * in[k];
+        S0[at(ta, tb, q)] = s;
       }
     }
     __syncthreads();
-    if (tx < N) {
+    // 2. y interpolation on y-lines (x = ta < N, z = tb)
+    if (ta < N) {
 #pragma unroll
-      for (int q = 0; q < Q; ++q) s0[tx + Q * (ty + Q * q)] = col[q];
+      for (int j = 0; j < N; ++j) line[j] = S0[at(ta, j, tb)];
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        T s = T(0);
+#pragma unroll
+        for (int j = 0; j < N; ++j) s += tab.B[j * Q + q] * line[j];
+        out[q] = s;
+      }
+#pragma unroll
+      for (int q = 0; q < Q; ++q) S0[at(ta, q, tb)] = out[q];
     }
     __syncthreads();
-    // ---- x ----
+    // 3. x interpolation and x derivative on x-lines (y = ta, z = tb)
+    {
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      T s = T(0);
+      for (int i = 0; i < N; ++i) line[i] = S0[at(i, ta, tb)];
 #pragma unroll
-      for (int i = 0; i < N; ++i) s += sB[i * Q + tx] * s0[i + Q * (ty + Q * q)];
-      u[q] = s;
-    }
-    // ---- collocation derivatives ----
+      for (int q = 0; q < Q; ++q) {
+        T s = T(0);
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      T s = T(0);
+        for (int i = 0; i < N; ++i) s += tab.B[i * Q + q] * line[i];
+        out[q] = s;
+      }
 #pragma unroll
-      for (int l = 0; l < Q; ++l) s += sD[q * Q + l] * u[l];
-      dz[q] = s;
+      for (int q = 0; q < Q; ++q) {
+        T s = T(0);
+#pragma unroll
+        for (int l = 0; l < Q; ++l) s += tab.D[q * Q + l] * out[l];
+        S0[at(q, ta, tb)] = out[q];
+        S2[at(q, ta, tb)] = s;
+      }
     }
     __syncthreads();
+    // 4. y derivative on y-lines (x = ta, z = tb)
+    {
 #pragma unroll
-    for (int q = 0; q < Q; ++q) s0[tx + Q * (ty + Q * q)] = u[q];
+      for (int l = 0; l < Q; ++l) line[l] = S0[at(ta, l, tb)];
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        T s = T(0);
+#pragma unroll
+        for (int l = 0; l < Q; ++l) s += tab.D[q * Q + l] * line[l];
+        S1[at(ta, q, tb)] = s;
+      }
+    }
     __syncthreads();
+  }
+  // 5. z derivative, pointwise flux and transposed z derivative on z-lines (x = ta, y = tb)
+  {
+    const T wxy = tab.W[ta] * tab.W[tb] * detJ;
+    if (mode == 1) {
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      T a = T(0), bb = T(0);
+      for (int q = 0; q < Q; ++q) {
+        const T f = act && src ? T(src[cell * Q3 + at(ta, tb, q)]) : T(0);
+        S0[at(ta, tb, q)] = wxy * tab.W[q] * f;
+      }
+    } else {
+      T u[Q], dz[Q];
+#pragma unroll
+      for (int l = 0; l < Q; ++l) u[l] = S0[at(ta, tb, l)];
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        T s = T(0);
+#pragma unroll
+        for (int l = 0; l < Q; ++l) s += tab.D[q * Q + l] * u[l];
+        dz[q] = s;
+      }
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        const int p = at(ta, tb, q);
+        const T w = wxy * tab.W[q];
+        T k = kappa;
+        if (b.kappa_pts && act) k *= T(b.kappa_pts[cell * Q3 + p]);
+        const T wk = w * k;
+        S2[p] = S2[p] * (wk * sx * sx);
+        S1[p] = S1[p] * (wk * sy * sy);
+        dz[q] *= wk * sz * sz;
+        u[q] *= w * mass;
+      }
 #pragma unroll
       for (int l = 0; l < Q; ++l) {
-        a += sD[tx * Q + l] * s0[l + Q * (ty + Q * q)];
-        bb += sD[ty * Q + l] * s0[tx + Q * (l + Q * q)];
-      }
-      dx[q] = a;
-      dy[q] = bb;
-    }
-  }
-  // ---- pointwise flux ----
-  T r[Q];
-  {
-    const T wxy = sW[tx] * sW[ty] * detJ;
+        T s = u[l];
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      const T w = wxy * sW[q];
-      if (mode == 1) {
-        T f = act && src ? T(src[cell * Q3 + tx + Q * (ty + Q * q)]) : T(0);
-        r[q] = w * f;
-        dx[q] = dy[q] = dz[q] = T(0);
-      } else {
-        T k = kappa;
-        if (b.kappa_pts && act) k *= T(b.kappa_pts[cell * Q3 + tx + Q * (ty + Q * q)]);
-        const T wk = w * k;
-        r[q] = w * mass * u[q];
-        dx[q] *= wk * sx * sx;
-        dy[q] *= wk * sy * sy;
-        dz[q] *= wk * sz * sz;
+        for (int q = 0; q < Q; ++q) s += tab.D[q * Q + l] * dz[q];
+        S0[at(ta, tb, l)] = s;
       }
     }
   }
+  __syncthreads();
   if (mode != 1) {
-    __syncthreads();
+    // 6. transposed y derivative on y-lines (x = ta, z = tb)
+    {
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      s0[tx + Q * (ty + Q * q)] = dx[q];
-      s1[tx + Q * (ty + Q * q)] = dy[q];
-    }
-    __syncthreads();
+      for (int q = 0; q < Q; ++q) line[q] = S1[at(ta, q, tb)];
 #pragma unroll
-    for (int l = 0; l < Q; ++l) {
-      T s = r[l];
+      for (int l = 0; l < Q; ++l) {
+        T s = S0[at(ta, l, tb)];
 #pragma unroll
-      for (int q = 0; q < Q; ++q) s += sD[q * Q + l] * dz[q];
-#pragma unroll
-      for (int q = 0; q < Q; ++q) {
-        s += sD[q * Q + tx] * s0[q + Q * (ty + Q * l)];
-        s += sD[q * Q + ty] * s1[tx + Q * (q + Q * l)];
+        for (int q = 0; q < Q; ++q) s += tab.D[q * Q + l] * line[q];
+        S0[at(ta, l, tb)] = s;
       }
-      u[l] = s;
     }
-  } else {
-#pragma unroll
-    for (int l = 0; l < Q; ++l) u[l] = r[l];
+    __syncthreads();
   }
-  // ---- transposed interpolation ----
-  __syncthreads();
+  // 7. transposed x derivative and transposed x interpolation on x-lines (y = ta, z = tb)
+  {
 #pragma unroll
-  for (int q = 0; q < Q; ++q) s0[tx + Q * (ty + Q * q)] = u[q];
-  __syncthreads();
-  T t[Q];
-  if (tx < N) {
+    for (int l = 0; l < Q; ++l) out[l] = S0[at(l, ta, tb)];
+    if (mode != 1) {
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
+      for (int q = 0; q < Q; ++q) line[q] = S2[at(q, ta, tb)];
+#pragma unroll
+      for (int l = 0; l < Q; ++l) {
+        T s = out[l];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) s += tab.D[q * Q + l] * line[q];
+        out[l] = s;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
       T s = T(0);
 #pragma unroll
-      for (int p = 0; p < Q; ++p) s += sB[tx * Q + p] * s0[p + Q * (ty + Q * q)];
-      t[q] = s;
+      for (int q = 0; q < Q; ++q) s += tab.B[i * Q + q] * out[q];
+      S0[at(i, ta, tb)] = s;
     }
   }
   __syncthreads();
-  if (tx < N) {
+  // 8. transposed y interpolation on y-lines (x = ta < N, z = tb)
+  if (ta < N) {
 #pragma unroll
-    for (int q = 0; q < Q; ++q) s0[tx + Q * (ty + Q * q)] = t[q];
-  }
-  __syncthreads();
-  if (act && tx < N && ty < N) {
+    for (int q = 0; q < Q; ++q) line[q] = S0[at(ta, q, tb)];
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
+    for (int j = 0; j < N; ++j) {
       T s = T(0);
 #pragma unroll
-      for (int p = 0; p < Q; ++p) s += sB[ty * Q + p] * s0[tx + Q * (p + Q * q)];
-      t[q] = s;
+      for (int q = 0; q < Q; ++q) s += tab.B[j * Q + q] * line[q];
+      S0[at(ta, j, tb)] = s;
     }
+  }
+  __syncthreads();
+  // 9. transposed z interpolation on z-lines (x = ta < N, y = tb < N) and scatter
+  if (act && ta < N && tb < N) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) line[q] = S0[at(ta, tb, q)];
 #pragma unroll
     for (int k = 0; k < N; ++k) {
       T s = T(0);
 #pragma unroll
-      for (int q = 0; q < Q; ++q) s += sB[k * Q + q] * t[q];
-      scatter_entry<T>(b, cell * NB + tx + N * (ty + N * k), s, y);
+      for (int q = 0; q < Q; ++q) s += tab.B[k * Q + q] * line[q];
+      scatter_entry<T>(b, cell * NB + ta + N * (tb + N * k), s, y);
     }
   }
 }

@@ -123,15 +123,28 @@ void fill_view(BatchView& v, const DevBatch& b, bool reduced) {
   v.skip = reduced ? b.skip.get<uint8_t>() : nullptr;
 }
 
+template <int N, int Q, typename T>
+Tables1D<N, Q, T> make_tables(const DevBatch& b) {
+  Tables1D<N, Q, T> t;
+  for (int i = 0; i < N * Q; ++i) t.B[i] = T(b.hB[i]);
+  for (int i = 0; i < Q * Q; ++i) t.D[i] = T(b.hD[i]);
+  for (int i = 0; i < Q; ++i) t.W[i] = T(b.hW[i]);
+  return t;
+}
+
 template <typename T>
-bool launch_fused(int dim, int N, int Q, const BatchView& v, const T* x, T* y, int64_t nvec, T mass, T kappa, int mode,
-                  const double* src, int nrhs, cudaStream_t st) {
+bool launch_fused(int dim, const DevBatch& bt, const BatchView& v, const T* x, T* y, int64_t nvec, T mass, T kappa,
+                  int mode, const double* src, int nrhs, cudaStream_t st) {
   if (v.n_cells == 0) return true;
+  const int N = bt.n[0], Q = bt.q[0];
 #define GRICO_L3(NN, QQ)                                                                                     \
   if (N == NN && Q == QQ) {                                                                                  \
     constexpr int CPB = (256 / (QQ * QQ)) > 0 ? (256 / (QQ * QQ)) : 1;                                       \
+    const size_t smem = size_t(3) * CPB * ((QQ * QQ * QQ) | 1) * sizeof(T);                                  \
+    auto kern = cell_apply_3d<NN, QQ, CPB, T>;                                                              \
+    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)); \
     dim3 block(QQ * QQ, CPB), grid((v.n_cells + CPB - 1) / CPB, nrhs);                                       \
-    cell_apply_3d<NN, QQ, CPB, T><<<grid, block, 0, st>>>(v, x, y, nvec, mass, kappa, mode, src);            \
+    kern<<<grid, block, smem, st>>>(v, make_tables<NN, QQ, T>(bt), x, y, nvec, mass, kappa, mode, src);     \
     return true;                                                                                             \
   }
 #define GRICO_L2(NN, QQ)                                                                                     \
@@ -160,7 +173,7 @@ void launch_batch(const GricoPlan& P, const DevBatch& b, bool reduced, const T* 
   fill_view(v, b, reduced);
   const int dim = P.dim;
   if (mode != 3 && b.isotropic && b.q[0] >= b.n[0] &&
-      launch_fused<T>(dim, b.n[0], b.q[0], v, x, y, nvec, T(P.mass), T(P.kappa), mode, src, nrhs, st))
+      launch_fused<T>(dim, b, v, x, y, nvec, T(P.mass), T(P.kappa), mode, src, nrhs, st))
     return;
   int n[3] = {1, 1, 1}, q[3] = {1, 1, 1};
   for (int a = 0; a < dim; ++a) { n[a] = b.n[a]; q[a] = b.q[a]; }
@@ -427,6 +440,9 @@ int grico_plan_create(const GricoPlanDesc* d, GricoPlan** out) {
       }
       if (a == 0) Dm = collocation_derivative(pts);
     }
+    b.hB.assign(B.begin(), B.begin() + b.n[0] * b.q[0]);
+    b.hD = Dm;
+    b.hW.assign(W.begin(), W.begin() + b.q[0]);
     bool ok = b.B.upload(B) && b.G.upload(G) && b.W.upload(W) && b.D.upload(Dm);
     ok = ok && b.h.upload(bd.cell_size, size_t(bd.n_cells) * d->dim);
     if (bd.kappa_points) {

@@ -73,6 +73,7 @@ struct DevBatch {
   DevMap full, red;
   DevBuf h, kappa, B, G, W, D;
   DevBuf skip;  // uint8 per cell: hanging cells whose diagonal is added from the host
+  std::vector<double> hB, hD, hW;  // axis-0 tables on the host (kernel parameters)
 };
 
 }  // namespace grico
