@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -666,3 +667,69 @@ int grico_expand_reduced(GricoPlan* P, const double* u_red, double* u_full, int 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Allocation-free variant of the reduced right-hand side.
+//
+// Some callers cannot call cudaMalloc: code that runs while a CUDA stream is being captured into
+// a graph, host callbacks, and services whose GPU memory is budgeted up front (a memory pool or
+// a fixed partition) all need an entry point that touches no allocator.  grico_reduced_rhs()
+// allocates two full-layout temporaries per call; grico_reduced_rhs_static() keeps them in the
+// file-scope array below instead.  Every GPU that loads the library holds this array
+// (2 * GRICO_STATIC_RHS_MAX_DOFS doubles = 16 MiB) until the process exits.
+#define GRICO_STATIC_RHS_MAX_DOFS (1 << 20)
+static __device__ __align__(256) double g_rhs_scratch[2 * GRICO_STATIC_RHS_MAX_DOFS];
+
+namespace {
+
+// Device address of g_rhs_scratch per device.  In host code the symbol is only a host-side
+// stand-in; the address a kernel may use comes from cudaGetSymbolAddress with the device
+// current.  Resolved on the first call on each device.
+std::mutex g_rhs_scratch_mutex;
+double* g_rhs_scratch_ptr[64] = {nullptr};
+
+int static_rhs_scratch(double** out) {
+  int dev = 0;
+  if (!cuda_ok(cudaGetDevice(&dev), "cudaGetDevice")) return GRICO_ERR_CUDA;
+  if (dev < 0 || dev >= 64) { set_error("device index out of range"); return GRICO_ERR_INVALID; }
+  std::lock_guard<std::mutex> lock(g_rhs_scratch_mutex);
+  if (!g_rhs_scratch_ptr[dev]) {
+    void* p = nullptr;
+    if (!cuda_ok(cudaGetSymbolAddress(&p, g_rhs_scratch), "cudaGetSymbolAddress")) return GRICO_ERR_CUDA;
+    g_rhs_scratch_ptr[dev] = static_cast<double*>(p);
+  }
+  *out = g_rhs_scratch_ptr[dev];
+  return GRICO_OK;
+}
+
+}  // namespace
+
+extern "C" int grico_reduced_rhs_static(GricoPlan* P, const double* const* source_points, double* b_reduced,
+                                        void* stream) {
+  if (!P || !b_reduced) { set_error("grico_reduced_rhs_static: invalid argument"); return GRICO_ERR_INVALID; }
+  if (P->n_full > GRICO_STATIC_RHS_MAX_DOFS) {
+    set_error("grico_reduced_rhs_static: the plan has " + std::to_string(P->n_full) +
+              " full-layout dofs; the static scratch holds at most " + std::to_string(GRICO_STATIC_RHS_MAX_DOFS));
+    return GRICO_ERR_INVALID;
+  }
+  double* scratch = nullptr;
+  if (int rc = static_rhs_scratch(&scratch)) return rc;
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : P->stream;
+  double* full = scratch;
+  double* shifted = scratch + GRICO_STATIC_RHS_MAX_DOFS;
+  // the scratch keeps the previous call's contents: clear the accumulation targets
+  cudaMemsetAsync(full, 0, sizeof(double) * P->n_full, st);
+  for (size_t bi = 0; bi < P->batches.size(); ++bi)
+    launch_batch<double>(*P, P->batches[bi], false, nullptr, full, P->n_full, 1,
+                         source_points ? source_points[bi] : nullptr, 1, st);
+  if (P->has_shift) {
+    cudaMemsetAsync(shifted, 0, sizeof(double) * P->n_full, st);
+    for (auto& b : P->batches)
+      launch_batch<double>(*P, b, false, P->shift.get<double>(), shifted, P->n_full, 0, nullptr, 1, st);
+    axpby_kernel<double><<<grid_for(P->n_full), 256, 0, st>>>(-1.0, shifted, 1.0, full, P->n_full);
+  }
+  cudaMemsetAsync(b_reduced, 0, sizeof(double) * P->n_red, st);
+  project_reduced<<<grid_for(P->n_full), 256, 0, st>>>(P->red_off.get<int64_t>(), P->red_idx.get<int64_t>(),
+                                                        P->red_coef.get<double>(), full, b_reduced, P->n_full);
+  return cuda_ok(cudaGetLastError(), "grico_reduced_rhs_static") ? GRICO_OK : GRICO_ERR_CUDA;
+}
