@@ -123,12 +123,20 @@ void lu_solve_inplace(int n, std::vector<double>& a, std::vector<double>& b, int
   for (int k = 0; k < n; ++k)
     if (piv[k] != k)
       for (int j = 0; j < nrhs; ++j) std::swap(b[k * nrhs + j], b[piv[k] * nrhs + j]);
+  // column-oriented substitutions in the order of the reference BLAS dtrsm used by getrs:
+  // forward with unit L (k ascending), backward with U (k descending, divide before use)
   for (int j = 0; j < nrhs; ++j) {
-    for (int i = 0; i < n; ++i)
-      for (int k = 0; k < i; ++k) b[i * nrhs + j] -= a[i * n + k] * b[k * nrhs + j];
-    for (int i = n - 1; i >= 0; --i) {
-      for (int k = i + 1; k < n; ++k) b[i * nrhs + j] -= a[i * n + k] * b[k * nrhs + j];
-      b[i * nrhs + j] /= a[i * n + i];
+    for (int k = 0; k < n; ++k) {
+      const double bk = b[k * nrhs + j];
+      if (bk != 0.0)
+        for (int i = k + 1; i < n; ++i) b[i * nrhs + j] -= bk * a[i * n + k];
+    }
+    for (int k = n - 1; k >= 0; --k) {
+      if (b[k * nrhs + j] != 0.0) {
+        b[k * nrhs + j] /= a[k * n + k];
+        const double bk = b[k * nrhs + j];
+        for (int i = 0; i < k; ++i) b[i * nrhs + j] -= bk * a[i * n + k];
+      }
     }
   }
 }
@@ -138,6 +146,13 @@ void lu_solve_inplace(int n, std::vector<double>& a, std::vector<double>& b, int
 // Restriction of a source 1-D basis on an interval to a target basis on a dyadic subinterval
 // (continuity.jl:1158-1198).  Returns a (target_degree+1) x (source_degree+1) row-major matrix.
 std::vector<double> affine_restriction_matrix(int src_deg, int tgt_deg, int delta, long long rel) {
+  if (delta == 0) {
+    // Same interval: the hierarchical family is nested (psi_0..psi_p are shared by every degree
+    // >= p), so the collocation solve reproduces the identity embedding; state it exactly.
+    std::vector<double> e((tgt_deg + 1) * (src_deg + 1), 0.0);
+    for (int i = 0; i <= src_deg && i <= tgt_deg; ++i) e[i * (src_deg + 1) + i] = 1.0;
+    return e;
+  }
   double scale = std::ldexp(1.0, -delta);
   double shift = delta == 0 ? 0.0 : scale * (2.0 * double(rel) + 1.0) - 1.0;
   int n = tgt_deg + 1;
@@ -826,3 +841,206 @@ int grico_fe_basis(double x, int degree, double* values, double* derivatives) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Multigrid transfer between two compiled spaces on the same grid (multigrid.jl:614-848).
+//
+// Every coarse leaf is either a leaf of the fine space (p-coarsening) or the parent of two fine
+// leaves (one h-coarsening split).  Local entries are tensor products of 1-D restriction
+// matrices (coarse degree -> fine degree on the child interval); the reduced transfer follows
+// _append_field_reduced_transfer_entries!: coarse modes are expanded through the coarse term
+// map and reduced map, accumulated per fine (leaf, mode), then mapped to the fine reduced dof of
+// single-term fine modes with the inverse term coefficient.  Duplicate (coarse, fine) pairs
+// must agree (multigrid.jl:837-848); the first value is kept.
+struct Transfer {
+  int64_t n_fine = 0, n_coarse = 0;
+  std::vector<int64_t> row_off, col;
+  std::vector<double> val;
+};
+
+namespace grico {
+namespace {
+
+struct LeafKey {
+  std::array<int64_t, 6> k;
+  bool operator==(const LeafKey& o) const { return k == o.k; }
+};
+struct LeafKeyHash {
+  size_t operator()(const LeafKey& x) const {
+    uint64_t h = 1469598103934665603ull;
+    for (int64_t v : x.k) h ^= uint64_t(v) + 0x9e3779b97f4a7c15ull + (h << 6) + (h >> 2);
+    return size_t(h);
+  }
+};
+
+LeafKey leaf_key(const Space& s, int64_t leaf) {
+  LeafKey key;
+  key.k.fill(0);
+  for (int a = 0; a < s.dim; ++a) {
+    key.k[a] = s.levels[leaf * s.dim + a];
+    key.k[3 + a] = s.coords[leaf * s.dim + a];
+  }
+  return key;
+}
+
+}  // namespace
+}  // namespace grico
+
+extern "C" int grico_transfer_build(const GricoSpace* coarse_space, const GricoSpace* fine_space,
+                                    const int64_t* coarse_red_offsets, const int64_t* coarse_red_index,
+                                    const double* coarse_red_coef, int64_t n_coarse_reduced,
+                                    const int64_t* fine_reduced_index, int64_t n_fine_reduced,
+                                    GricoTransfer** out) {
+  using namespace grico;
+  try {
+    auto* C = reinterpret_cast<const Space*>(coarse_space);
+    auto* F = reinterpret_cast<const Space*>(fine_space);
+    if (!C || !F || !out || C->dim != F->dim) { set_error("grico_transfer_build: invalid arguments"); return GRICO_ERR_INVALID; }
+    const int D = C->dim;
+    std::unordered_map<LeafKey, int64_t, LeafKeyHash> fine_pos;
+    fine_pos.reserve(size_t(F->nleaves) * 2);
+    for (int64_t l = 0; l < F->nleaves; ++l) fine_pos[leaf_key(*F, l)] = l;
+    std::unordered_map<uint64_t, std::vector<double>> mats;
+    auto matrix = [&](int sdeg, int tdeg, int delta, int64_t rel) -> const std::vector<double>& {
+      uint64_t key = (uint64_t(sdeg) << 56) | (uint64_t(tdeg) << 48) | (uint64_t(delta) << 40) | uint64_t(rel);
+      auto it = mats.find(key);
+      if (it == mats.end()) it = mats.emplace(key, affine_restriction_matrix(sdeg, tdeg, delta, rel)).first;
+      return it->second;
+    };
+    // Every fine leaf lies under exactly one coarse leaf, so the target expansion of a fine
+    // (leaf, mode) is complete once its coarse leaf has been processed.
+    struct Triple { int64_t fine, coarse; double v; };
+    std::vector<Triple> triples;
+    std::vector<std::pair<int64_t, double>> source;
+    std::vector<std::vector<std::pair<int64_t, double>>> local;
+    auto add_to = [](std::vector<std::pair<int64_t, double>>& v, int64_t k, double x) {
+      if (x == 0.0) return;
+      for (auto& t : v)
+        if (t.first == k) { t.second += x; return; }
+      v.emplace_back(k, x);
+    };
+    for (int64_t cl = 0; cl < C->nleaves; ++cl) {
+      std::vector<int64_t> fines;
+      auto same = fine_pos.find(leaf_key(*C, cl));
+      if (same != fine_pos.end()) {
+        fines.push_back(same->second);
+      } else {
+        for (int a = 0; a < D && fines.size() != 2; ++a) {
+          fines.clear();
+          for (int off = 0; off < 2; ++off) {
+            LeafKey k = leaf_key(*C, cl);
+            k.k[a] += 1;
+            k.k[3 + a] = 2 * k.k[3 + a] + off;
+            auto it = fine_pos.find(k);
+            if (it != fine_pos.end()) fines.push_back(it->second);
+          }
+        }
+        if (fines.size() != 2) {
+          set_error("fine multigrid space does not contain the coarse leaf or its two children");
+          return GRICO_ERR_INVALID;
+        }
+      }
+      const Pattern& cp = C->patterns[C->pattern_of[cl]];
+      for (int64_t fl : fines) {
+        const Pattern& fp = F->patterns[F->pattern_of[fl]];
+        const std::vector<double>* M[3] = {nullptr, nullptr, nullptr};
+        for (int a = 0; a < D; ++a) {
+          int delta = F->levels[fl * D + a] - C->levels[cl * D + a];
+          int64_t rel = F->coords[fl * D + a] - (C->coords[cl * D + a] << delta);
+          if (fp.deg[a] < cp.deg[a]) { set_error("fine multigrid level must represent every coarse mode exactly"); return GRICO_ERR_INVALID; }
+          M[a] = &matrix(cp.deg[a], fp.deg[a], delta, rel);
+        }
+        local.assign(fp.box, {});
+        for (int cbox : cp.modes) {
+          int64_t ce = C->leaf_box_offset[cl] + cbox;
+          if (C->term_offsets[ce] == C->term_offsets[ce + 1]) continue;
+          source.clear();
+          for (int64_t t = C->term_offsets[ce]; t < C->term_offsets[ce + 1]; ++t) {
+            int64_t g = C->term_index[t];
+            for (int64_t p = coarse_red_offsets[g]; p < coarse_red_offsets[g + 1]; ++p)
+              add_to(source, coarse_red_index[p], C->term_coef[t] * coarse_red_coef[p]);
+          }
+          if (source.empty()) continue;
+          int cm[3] = {0, 0, 0};
+          for (int a = 0; a < D; ++a) cm[a] = mode_digit(cbox, cp.shape, a);
+          for (int fbox : fp.modes) {
+            double coef = 1.0;
+            for (int a = 0; a < D && coef != 0.0; ++a) {
+              const double m = (*M[a])[mode_digit(fbox, fp.shape, a) * (cp.deg[a] + 1) + cm[a]];
+              // 1-D restriction entries of O(eps) are rounding residues of exact zeros
+              coef *= std::fabs(m) <= 4.0 * 2.220446049250313e-16 ? 0.0 : m;
+            }
+            if (coef == 0.0) continue;
+            if (!std::isfinite(coef)) { set_error("multigrid transfer coefficient must be finite"); return GRICO_ERR_INVALID; }
+            for (auto& sp : source) add_to(local[fbox], sp.first, coef * sp.second);
+          }
+        }
+        for (int fbox = 0; fbox < fp.box; ++fbox) {
+          if (local[fbox].empty()) continue;
+          int64_t fe = F->leaf_box_offset[fl] + fbox;
+          if (F->term_offsets[fe + 1] - F->term_offsets[fe] != 1) continue;
+          int64_t t = F->term_offsets[fe];
+          int64_t r = fine_reduced_index[F->term_index[t]];
+          if (r < 0) continue;
+          double inv = 1.0 / F->term_coef[t];
+          for (auto& sp : local[fbox]) {
+            double c = inv * sp.second;
+            if (c != 0.0) triples.push_back({r, sp.first, c});
+          }
+        }
+      }
+    }
+    std::stable_sort(triples.begin(), triples.end(), [](const Triple& a, const Triple& b) {
+      return a.fine != b.fine ? a.fine < b.fine : a.coarse < b.coarse;
+    });
+    std::vector<int64_t> row_count(n_fine_reduced, 0);
+    std::vector<int64_t> cols;
+    std::vector<double> vals;
+    cols.reserve(triples.size());
+    vals.reserve(triples.size());
+    for (size_t i = 0; i < triples.size();) {
+      size_t j = i + 1;
+      while (j < triples.size() && triples[j].fine == triples[i].fine && triples[j].coarse == triples[i].coarse) {
+        double a = triples[i].v, c = triples[j].v;
+        double scale = std::max({1.0, std::fabs(a), std::fabs(c)});
+        if (std::fabs(a - c) > 10000 * 2.220446049250313e-16 * scale) {
+          set_error("inconsistent duplicate multigrid transfer entry");
+          return GRICO_ERR_INVALID;
+        }
+        ++j;
+      }
+      cols.push_back(triples[i].coarse);
+      vals.push_back(triples[i].v);
+      row_count[triples[i].fine]++;
+      i = j;
+    }
+    auto* T = new Transfer();
+    T->n_fine = n_fine_reduced;
+    T->n_coarse = n_coarse_reduced;
+    T->row_off.assign(n_fine_reduced + 1, 0);
+    for (int64_t r = 0; r < n_fine_reduced; ++r) T->row_off[r + 1] = T->row_off[r] + row_count[r];
+    T->col.swap(cols);
+    T->val.swap(vals);
+    *out = reinterpret_cast<GricoTransfer*>(T);
+    return GRICO_OK;
+  } catch (const std::exception& e) {
+    set_error(std::string("grico_transfer_build: ") + e.what());
+    return GRICO_ERR_INVALID;
+  }
+}
+
+extern "C" int grico_transfer_export(const GricoTransfer* transfer, int64_t* nnz, int64_t* row_offsets,
+                                     int64_t* col_index, double* values) {
+  auto* T = reinterpret_cast<const Transfer*>(transfer);
+  if (!T) return GRICO_ERR_INVALID;
+  if (nnz) *nnz = T->row_off.back();
+  if (row_offsets) std::copy(T->row_off.begin(), T->row_off.end(), row_offsets);
+  if (col_index) std::copy(T->col.begin(), T->col.end(), col_index);
+  if (values) std::copy(T->val.begin(), T->val.end(), values);
+  return GRICO_OK;
+}
+
+extern "C" int grico_transfer_destroy(GricoTransfer* transfer) {
+  delete reinterpret_cast<Transfer*>(transfer);
+  return GRICO_OK;
+}

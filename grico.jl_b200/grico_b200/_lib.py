@@ -132,6 +132,9 @@ SIGNATURES = {
     "grico_space_destroy": (C.c_int, [P]),
     "grico_space_sizes": (C.c_int, [P, i64p, i64p, i64p, i64p, i64p]),
     "grico_space_export": (C.c_int, [P, i64p, i64p, i64p, i64p, f64p, i32p, i64p, i32p, i32p, i64p, i64p, i32p]),
+    "grico_transfer_build": (C.c_int, [P, P, i64p, i64p, f64p, C.c_int64, i64p, C.c_int64, C.POINTER(P)]),
+    "grico_transfer_export": (C.c_int, [P, i64p, i64p, i64p, f64p]),
+    "grico_transfer_destroy": (C.c_int, [P]),
     "grico_gauss_legendre": (C.c_int, [C.c_int, f64p, f64p]),
     "grico_fe_basis": (C.c_int, [C.c_double, C.c_int, f64p, f64p]),
     "grico_plan_create": (C.c_int, [C.POINTER(GricoPlanDesc), C.POINTER(P)]),

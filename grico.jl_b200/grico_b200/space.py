@@ -109,31 +109,29 @@ class HpSpace:
                                       L.ptr(crd, C.c_int64), L.ptr(deg, C.c_int32), options.basis.code,
                                       L.GRICO_CONTINUITY_CG if cg else L.GRICO_CONTINUITY_DG,
                                       options.quadrature.extra_points, C.byref(handle)), "HpSpace")
-        try:
-            sizes = [C.c_int64() for _ in range(5)]
-            L.check(lib.grico_space_sizes(handle, *[C.byref(s) for s in sizes]))
-            ndofs, nterms, nboxes, nbnd, nif = (s.value for s in sizes)
-            n = len(leaves)
-            order = np.zeros(n, dtype=np.int64)
-            box_off = np.zeros(n + 1, dtype=np.int64)
-            t_off = np.zeros(nboxes + 1, dtype=np.int64)
-            t_idx = np.zeros(nterms, dtype=np.int64)
-            t_coef = np.zeros(nterms, dtype=np.float64)
-            qshape = np.zeros(n * self.D, dtype=np.int32)
-            b_leaf = np.zeros(nbnd, dtype=np.int64)
-            b_axis = np.zeros(nbnd, dtype=np.int32)
-            b_side = np.zeros(nbnd, dtype=np.int32)
-            i_m = np.zeros(nif, dtype=np.int64)
-            i_p = np.zeros(nif, dtype=np.int64)
-            i_a = np.zeros(nif, dtype=np.int32)
-            L.check(lib.grico_space_export(handle, L.ptr(order, C.c_int64), L.ptr(box_off, C.c_int64),
-                                           L.ptr(t_off, C.c_int64), L.ptr(t_idx, C.c_int64),
-                                           L.ptr(t_coef, C.c_double), L.ptr(qshape, C.c_int32),
-                                           L.ptr(b_leaf, C.c_int64), L.ptr(b_axis, C.c_int32),
-                                           L.ptr(b_side, C.c_int32), L.ptr(i_m, C.c_int64),
-                                           L.ptr(i_p, C.c_int64), L.ptr(i_a, C.c_int32)))
-        finally:
-            lib.grico_space_destroy(handle)
+        self.handle = handle  # kept for multigrid transfers; destroyed with the space
+        sizes = [C.c_int64() for _ in range(5)]
+        L.check(lib.grico_space_sizes(handle, *[C.byref(s) for s in sizes]))
+        ndofs, nterms, nboxes, nbnd, nif = (s.value for s in sizes)
+        n = len(leaves)
+        order = np.zeros(n, dtype=np.int64)
+        box_off = np.zeros(n + 1, dtype=np.int64)
+        t_off = np.zeros(nboxes + 1, dtype=np.int64)
+        t_idx = np.zeros(nterms, dtype=np.int64)
+        t_coef = np.zeros(nterms, dtype=np.float64)
+        qshape = np.zeros(n * self.D, dtype=np.int32)
+        b_leaf = np.zeros(nbnd, dtype=np.int64)
+        b_axis = np.zeros(nbnd, dtype=np.int32)
+        b_side = np.zeros(nbnd, dtype=np.int32)
+        i_m = np.zeros(nif, dtype=np.int64)
+        i_p = np.zeros(nif, dtype=np.int64)
+        i_a = np.zeros(nif, dtype=np.int32)
+        L.check(lib.grico_space_export(handle, L.ptr(order, C.c_int64), L.ptr(box_off, C.c_int64),
+                                       L.ptr(t_off, C.c_int64), L.ptr(t_idx, C.c_int64),
+                                       L.ptr(t_coef, C.c_double), L.ptr(qshape, C.c_int32),
+                                       L.ptr(b_leaf, C.c_int64), L.ptr(b_axis, C.c_int32),
+                                       L.ptr(b_side, C.c_int32), L.ptr(i_m, C.c_int64),
+                                       L.ptr(i_p, C.c_int64), L.ptr(i_a, C.c_int32)))
         self.leaves = leaves[order]                      # Morton order, cell ids
         self.degrees = degrees[order]                    # [n, D]
         self.qshape = qshape.reshape(n, self.D)
@@ -145,6 +143,15 @@ class HpSpace:
         self.boundary_faces = (b_leaf, b_axis, b_side)  # positions in Morton order, 0-based axis, 0/1 side
         self.interfaces = (i_m, i_p, i_a)
         self.leaf_to_index = {int(l): i for i, l in enumerate(self.leaves)}
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            try:
+                L.lib().grico_space_destroy(h)
+            except Exception:
+                pass
+            self.handle = None
 
     # ---- queries mirroring the reference API ----
     def active_leaf_count(self):

@@ -78,6 +78,19 @@ int grico_space_export(const GricoSpace* space, int64_t* morton_order, int64_t* 
                        int64_t* term_offsets, int64_t* term_index, double* term_coef, int32_t* qshape,
                        int64_t* bnd_leaf, int32_t* bnd_axis, int32_t* bnd_side, int64_t* if_minus,
                        int64_t* if_plus, int32_t* if_axis);
+/* Reduced-space multigrid prolongation from a coarse space to the next finer space on the same
+ * grid (p-coarsened leaf or one h-split), replacing _compile_multigrid_transfer
+ * (multigrid.jl:614-848).  The coarse reduced map is CSR (full dof -> reduced dofs); the fine
+ * reduced map is an index per full dof (-1 when constrained).  Result: CSR over fine reduced
+ * rows, columns sorted (coarse reduced dofs). */
+typedef struct GricoTransfer GricoTransfer;
+int grico_transfer_build(const GricoSpace* coarse_space, const GricoSpace* fine_space,
+                         const int64_t* coarse_red_offsets, const int64_t* coarse_red_index,
+                         const double* coarse_red_coef, int64_t n_coarse_reduced,
+                         const int64_t* fine_reduced_index, int64_t n_fine_reduced, GricoTransfer** out);
+int grico_transfer_export(const GricoTransfer* transfer, int64_t* nnz, int64_t* row_offsets,
+                          int64_t* col_index, double* values);
+int grico_transfer_destroy(GricoTransfer* transfer);
 /* 1-D numerics of the product: Gauss-Legendre rule (quadrature.jl:342-410) and the
  * integrated-Legendre finite-element basis (polynomials.jl:238-247, 403-434). */
 int grico_gauss_legendre(int count, double* points, double* weights);

@@ -229,10 +229,10 @@ def uniform_refine(grid: Grid, depth: int):
                 leaves = nxt
 
 
-def morton_ordered_leaves(grid: Grid):
+def morton_ordered_leaves(grid: Grid, leaves=None):
     """Sort active leaves by Morton code of the lower corner on the finest lattice; bits high to low,
     axes D..1 within a bit; ties by level tuple then cell id (topology.jl:250-268, 451-463)."""
-    leaves = grid.active_leaves()
+    leaves = grid.active_leaves() if leaves is None else [int(l) for l in leaves]
     D = grid.D
     max_levels = [max(grid.level(l, a) for l in leaves) for a in range(D)]
     bit_count = 0
@@ -262,10 +262,10 @@ class Snapshot:
     reference: leaves in Morton order, axes ascending, UPPER-side partners sorted by their
     tangential lower corner (axis 1 first)."""
 
-    def __init__(self, grid: Grid):
+    def __init__(self, grid: Grid, leaves=None):
         self.grid = grid
         D = grid.D
-        self.leaves = morton_ordered_leaves(grid)
+        self.leaves = morton_ordered_leaves(grid, leaves)
         self.leaf_to_index = {leaf: i for i, leaf in enumerate(self.leaves)}
         self.finest = [max(grid.level(l, a) for l in self.leaves) for a in range(D)]
         self.lower = {}
@@ -460,13 +460,13 @@ class Space:
     degree_fn(leaf) -> degree tuple; basis 'full' or 'trunk'; continuity 'cg' or 'dg' (all axes);
     quadrature extra points (DegreePlusQuadrature, default 1)."""
 
-    def __init__(self, domain: Domain, degree, basis="trunk", continuity="cg", quadrature_extra=1):
+    def __init__(self, domain: Domain, degree, basis="trunk", continuity="cg", quadrature_extra=1, leaves=None):
         self.domain = domain
         self.grid = domain.grid
         self.D = domain.D
         self.basis = basis
         self.continuity = continuity
-        self.snapshot = Snapshot(self.grid)
+        self.snapshot = Snapshot(self.grid, leaves)
         snap = self.snapshot
         D = self.D
         leaves = snap.leaves
@@ -1098,3 +1098,170 @@ def l2_error(plan: Plan, full_values, exact):
         ex = np.array([exact(tuple(p)) for p in c["pts"]])
         err2 += float(np.sum(c["w"] * (u - ex) ** 2))
     return math.sqrt(err2)
+
+
+# ---------------------------------------------------------------------------
+# hp geometric multigrid: src/multigrid.jl
+# ---------------------------------------------------------------------------
+
+def coarsened_degree(degree, lower, sequence="bisect"):
+    """multigrid.jl:470-499"""
+    if degree <= lower:
+        return degree
+    if sequence == "bisect":
+        return max(degree // 2, lower)
+    if sequence == "decrease_by_one":
+        return max(degree - 1, lower)
+    return lower
+
+
+def hp_multigrid_levels(space: Space, min_degree=1, max_levels=16, sequence="bisect"):
+    """Coarse-to-fine list of (leaves, {leaf: degrees}) (multigrid.jl:443-469, 514-586)."""
+    cg = space.continuity == "cg"
+    grid = space.grid
+    leaves = list(space.snapshot.leaves)
+    degs = {leaf: tuple(space.degrees[i]) for i, leaf in enumerate(leaves)}
+    levels = [(leaves, dict(degs))]
+    while len(levels) < max_levels:
+        nd = {}
+        for leaf, d in degs.items():
+            nd[leaf] = tuple(coarsened_degree(v, min(v, max(min_degree, 1 if cg else 0)), sequence) for v in d)
+        if nd == degs:
+            break
+        degs = nd
+        levels.append((leaves, dict(degs)))
+    while len(levels) < max_levels:
+        active = set(leaves)
+        cands = []
+        for cell in range(1, grid.stored() + 1):
+            f = grid.first_child[cell]
+            if f and f in active and (f + 1) in active:
+                cands.append(cell)
+        if not cands:
+            break
+        child_to_parent = {}
+        for c in cands:
+            f = grid.first_child[c]
+            child_to_parent[f] = c
+            child_to_parent[f + 1] = c
+            degs[c] = tuple(min(a, b) for a, b in zip(degs[f], degs[f + 1]))
+            del degs[f]
+            del degs[f + 1]
+        new, emitted = [], set()
+        for leaf in leaves:
+            p = child_to_parent.get(leaf)
+            if p is None:
+                new.append(leaf)
+            elif p not in emitted:
+                emitted.add(p)
+                new.append(p)
+        leaves = morton_ordered_leaves(grid, new)
+        levels.append((leaves, dict(degs)))
+    levels.reverse()
+    return levels
+
+
+def multigrid_transfer(coarse: Plan, fine: Plan):
+    """Reduced prolongation entries {(coarse_red, fine_red): value}, 1-based reduced indices
+    (multigrid.jl:614-848)."""
+    cs, fs = coarse.space, fine.space
+    grid = cs.grid
+    D = cs.D
+    fine_index = fs.snapshot.leaf_to_index
+    entries = {}
+    cred = {d: coarse.P_rows[d - 1] for d in range(1, coarse.ndofs + 1)}
+    for ci, cleaf in enumerate(cs.snapshot.leaves):
+        if cleaf in fine_index:
+            fines = [cleaf]
+        else:
+            f = grid.first_child[cleaf]
+            fines = [f, f + 1]
+        for fleaf in fines:
+            fi = fine_index[fleaf]
+            mats = []
+            for a in range(D):
+                delta = grid.level(fleaf, a) - grid.level(cleaf, a)
+                rel = grid.coord(fleaf, a) - (grid.coord(cleaf, a) << delta)
+                mats.append(affine_restriction_matrix(cs.degrees[ci][a], fs.degrees[fi][a], delta, rel))
+            target = {}
+            for cm, cterms in zip(cs.leaf_modes[ci], cs.leaf_terms[ci]):
+                source = {}
+                for (d, c) in cterms:
+                    for (r, pc) in cred[d]:
+                        source[r] = source.get(r, 0.0) + c * pc
+                for fm in fs.leaf_modes[fi]:
+                    coef = 1.0
+                    for a in range(D):
+                        coef *= mats[a][fm[a], cm[a]]
+                    if coef == 0.0:
+                        continue
+                    tv = target.setdefault(fm, {})
+                    for r, v in source.items():
+                        if coef * v != 0.0:
+                            tv[r] = tv.get(r, 0.0) + coef * v
+            for fm, tv in target.items():
+                terms = fs.leaf_terms[fi][fs.leaf_modes[fi].index(fm)]
+                if len(terms) != 1:
+                    continue
+                d, c = terms[0]
+                rf = int(fine.reduced_index[d])
+                if rf == 0:
+                    continue
+                for r, v in tv.items():
+                    val = (1.0 / c) * v
+                    if val == 0.0:
+                        continue
+                    key = (r, rf)
+                    if key in entries:
+                        old = entries[key]
+                        assert abs(old - val) <= 10000 * EPS * max(1.0, abs(old), abs(val))
+                    else:
+                        entries[key] = val
+    return entries
+
+
+class Multigrid:
+    """V-cycle with damped Jacobi smoothing and a dense Cholesky coarse solve
+    (multigrid.jl:858-956, common.jl:272-330)."""
+
+    def __init__(self, plans, pre=2, post=2, omega=0.8):
+        self.plans = plans
+        self.pre, self.post, self.omega = pre, post, omega
+        self.transfers = [multigrid_transfer(plans[i], plans[i + 1]) for i in range(len(plans) - 1)]
+        self.P = []
+        for i, ent in enumerate(self.transfers):
+            M = np.zeros((len(plans[i + 1].solve_dofs), len(plans[i].solve_dofs)))
+            for (rc, rf), v in ent.items():
+                M[rf - 1, rc - 1] = v
+            self.P.append(M)
+        self.dinv = [1.0 / p.jacobi_diagonal() for p in plans]
+        c = plans[0]
+        n0 = len(c.solve_dofs)
+        A0 = np.zeros((n0, n0))
+        for j in range(n0):
+            e = np.zeros(n0)
+            e[j] = 1.0
+            A0[:, j] = c.reduced_apply(e)
+        self.L0 = np.linalg.cholesky(A0)
+
+    def smooth(self, level, x, b, steps):
+        p = self.plans[level]
+        for _ in range(steps):
+            r = b - p.reduced_apply(x)
+            x = x + self.omega * self.dinv[level] * r
+        return x
+
+    def vcycle(self, level, b):
+        if level == 0:
+            y = np.linalg.solve(self.L0, b)
+            return np.linalg.solve(self.L0.T, y)
+        x = np.zeros_like(b)
+        x = self.smooth(level, x, b, self.pre)
+        r = b - self.plans[level].reduced_apply(x)
+        bc = self.P[level - 1].T @ r
+        xc = self.vcycle(level - 1, bc)
+        x = x + self.P[level - 1] @ xc
+        return self.smooth(level, x, b, self.post)
+
+    def apply(self, r):
+        return self.vcycle(len(self.plans) - 1, r)

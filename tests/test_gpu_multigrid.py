@@ -1,0 +1,88 @@
+"""Device hp-GMG against the oracle's restatement of the V-cycle (multigrid.jl:858-1087)."""
+import numpy as np
+import pytest
+
+import grico_oracle as go
+import grico_b200 as gb
+from grico_b200.multigrid import GeometricMultigridPreconditioner, build_multigrid
+from test_multigrid_host import CASES, _oracle_levels
+from cases import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _pair(name, source=None):
+    origin, extent, roots, refine, p, faces = CASES[name]
+    od, pdm = go.Domain(origin, extent, roots), gb.Domain(origin, extent, roots)
+    refine(od.grid)
+    refine(pdm.grid)
+    oplans = _oracle_levels(od, p, faces)
+    s = gb.HpSpace(pdm, gb.SpaceOptions(basis=gb.FullTensorBasis(), degree=gb.UniformDegree(p)))
+    u = gb.ScalarField(s)
+    prob = gb.AffineProblem(u)
+    gb.add_cell_accumulator(prob, u, u, gb.MassDiffusion(1.0, 1.0))
+    if source is not None:
+        gb.add_cell_accumulator(prob, u, gb.Load(source))
+    for a, side in faces:
+        gb.add_constraint(prob, gb.Dirichlet(u, gb.BoundaryFace(a, side), 0.0))
+    return oplans, gb.compile(prob)
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_vcycle_matches_oracle(cuda, name):
+    oplans, plan = _pair(name)
+    mg = build_multigrid(plan, GeometricMultigridPreconditioner())
+    omg = go.Multigrid(oplans)
+    r = np.random.default_rng(4).standard_normal(plan.n_reduced)
+    assert mg.level_sizes() == [len(o.solve_dofs) for o in oplans]
+    assert rel_err(mg.vcycle(r), omg.apply(r)) <= 1e-11
+
+
+@pytest.mark.parametrize("name", ["2d_p4", "3d_p2"])
+def test_cg_gmg_matches_oracle(cuda, name):
+    D = len(CASES[name][0])
+    src = lambda x: np.prod(np.sin(np.pi * x), axis=1) * (1.0 + D * np.pi ** 2)
+    oplans, plan = _pair(name, source=src)
+    state = gb.solve(plan, solver=gb.CGSolver(GeometricMultigridPreconditioner()), relative_tolerance=1e-12)
+    omg = go.Multigrid(oplans)
+    fine = oplans[-1]
+    fine.source = lambda x: float(src(np.array([x]))[0])
+    xr, iters = go.cg_solve(fine.reduced_apply, fine.reduced_rhs(), precond=omg.apply, rtol=1e-12)
+    assert state.report.iterations == iters
+    assert rel_err(state.coefficients, fine.expand(xr, include_shift=True)) <= 1e-9
+
+
+def test_poisson_gmg_example_accuracy(cuda):  # examples/poisson_matrix_free_gmg, test/examples.jl:6-12
+    d = gb.Domain((0.0, 0.0), (1.0, 1.0), (2, 2))
+    s = gb.HpSpace(d, gb.SpaceOptions(basis=gb.FullTensorBasis(), degree=gb.UniformDegree(2)))
+    u = gb.ScalarField(s)
+    prob = gb.AffineProblem(u)
+    exact = lambda x: np.sin(np.pi * x[:, 0]) * np.sin(np.pi * x[:, 1])
+    gb.add_cell_accumulator(prob, u, u, gb.Diffusion())
+    gb.add_cell_accumulator(prob, u, gb.Load(lambda x: 2 * np.pi ** 2 * exact(x)))
+    for a in (1, 2):
+        for side in (gb.LOWER, gb.UPPER):
+            gb.add_constraint(prob, gb.Dirichlet(u, gb.BoundaryFace(a, side), 0.0))
+    state = gb.solve(prob, solver=gb.CGSolver(GeometricMultigridPreconditioner()), relative_tolerance=1e-10)
+    assert gb.l2_error(state, exact) <= 2e-2
+
+
+def test_chebyshev_smoother_converges_faster_than_jacobi(cuda):
+    d = gb.Domain((0.0, 0.0, 0.0), (1.0, 1.0, 1.0), (2, 2, 2))
+    gb.uniform_refine(d, 2)
+    s = gb.HpSpace(d, gb.SpaceOptions(basis=gb.FullTensorBasis(), degree=gb.UniformDegree(4)))
+    u = gb.ScalarField(s)
+    prob = gb.AffineProblem(u)
+    gb.add_cell_accumulator(prob, u, u, gb.Diffusion())
+    gb.add_cell_accumulator(prob, u, gb.Load(lambda x: np.prod(np.sin(np.pi * x), axis=1)))
+    for a in (1, 2, 3):
+        for side in (gb.LOWER, gb.UPPER):
+            gb.add_constraint(prob, gb.Dirichlet(u, gb.BoundaryFace(a, side), 0.0))
+    plan = gb.compile(prob)
+    jac = gb.solve(plan, solver=gb.CGSolver(GeometricMultigridPreconditioner()), relative_tolerance=1e-10)
+    che = gb.solve(plan, solver=gb.CGSolver(GeometricMultigridPreconditioner(smoother="chebyshev",
+                                                                             pre_smoothing_steps=1,
+                                                                             post_smoothing_steps=1)),
+                   relative_tolerance=1e-10)
+    assert rel_err(che.coefficients, jac.coefficients) <= 1e-7
+    assert che.report.iterations < jac.report.iterations
