@@ -519,3 +519,236 @@ __global__ void cell_apply_generic(BatchView b, int dim, int n0, int n1, int n2,
 }
 
 }  // namespace grico
+
+namespace grico {
+
+// Point-quadrature items: one cell's modes evaluated at an arbitrary list of reference points.
+// Covers non-tensor cells (finite-cell cut cells, accumulators.jl:1022-1054), boundary faces
+// and embedded surfaces (_accumulate_one_sided_apply_basis!, accumulators.jl:1133-1161).
+// kind 1 (cell):    TestChannels(mass*u, kappa*k(x)*grad u)
+// kind 2 (nitsche): TestChannels(-du/dn + eta*u, -u*n)   (symmetric Nitsche, driver.jl:52-62)
+struct PointView {
+  int32_t n_items;
+  int kind;
+  int n[3];
+  const int32_t* map;
+  const double* coef;
+  const int64_t* tail_off;
+  const int32_t* tail_idx;
+  const double* tail_coef;
+  const double* h;         // [n_items*dim]
+  const int64_t* pt_off;   // [n_items+1]
+  const double* ref;       // [n_points*dim]
+  const double* w;         // [n_points]
+  const double* nrm;       // [n_points*dim] or null
+  const double* eta;       // [n_items] or null
+  const double* kpts;      // [n_points] or null
+  const uint8_t* skip;     // nullable: items excluded from the diagonal kernel (host computes them)
+};
+
+constexpr int kPointChunk = 32;
+constexpr int kPointThreads = 128;
+constexpr int kPointWarps = kPointThreads / 32;
+constexpr int kMaxModes = 6;  // modes per thread: box <= 768
+
+// psi_0..psi_p and derivatives at x (polynomials.jl:403-434) on the device
+template <typename T>
+__device__ void fe_basis_dev(T x, int p, T* v, T* d) {
+  if (p == 0) {
+    v[0] = T(1);
+    d[0] = T(0);
+    return;
+  }
+  T pm2 = T(1), pm1 = x;  // P_{k-2}, P_{k-1}
+  v[0] = T(0.5) * (T(1) - x);
+  v[1] = T(0.5) * (T(1) + x);
+  d[0] = T(-0.5);
+  d[1] = T(0.5);
+  for (int k = 2; k <= p; ++k) {
+    const T inv_k = T(1) / T(k);
+    const T pk = T(2 * k - 1) * inv_k * x * pm1 - T(k - 1) * inv_k * pm2;
+    v[k] = (pk - pm2) / sqrt(T(4 * k - 2));
+    d[k] = sqrt(T(2 * k - 1) / T(2)) * pm1;
+    pm2 = pm1;
+    pm1 = pk;
+  }
+}
+
+// value and gradient of box mode (m0, m1, m2) at chunk point pp from the staged 1-D tables
+template <typename T, int D>
+__device__ __forceinline__ void mode_value_grad(const T* tv, const T* td, int nmax, int pp, const int* mi, T& phi,
+                                                T* grad) {
+  T v[D], g[D];
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    v[a] = tv[(pp * D + a) * nmax + mi[a]];
+    g[a] = td[(pp * D + a) * nmax + mi[a]];
+  }
+  phi = v[0];
+#pragma unroll
+  for (int a = 1; a < D; ++a) phi *= v[a];
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    T gg = g[a];
+#pragma unroll
+    for (int e = 0; e < D; ++e)
+      if (e != a) gg *= v[e];
+    grad[a] = gg;
+  }
+}
+
+// mode: 0 apply, 1 rhs (src per point), 3 local diagonal.  One block per item (blockIdx.x)
+// and right-hand side (blockIdx.y); points are staged in chunks of kPointChunk: 1-D tables per
+// (point, axis), then one warp per point reduces u and grad u over the modes, then one thread
+// per mode projects the point fluxes.
+template <typename T, int D>
+__global__ void __launch_bounds__(kPointThreads) point_apply(PointView b, const T* __restrict__ x, T* __restrict__ y,
+                                                             int64_t n_vec, T mass, T kappa, int mode,
+                                                             const double* __restrict__ src) {
+  extern __shared__ unsigned char smem_raw[];
+  int nn[3] = {b.n[0], D > 1 ? b.n[1] : 1, D > 2 ? b.n[2] : 1};
+  const int nb = nn[0] * nn[1] * nn[2];
+  const int nmax = max(nn[0], max(nn[1], nn[2]));
+  T* xl = reinterpret_cast<T*>(smem_raw);                       // nb
+  T* tv = xl + nb;                                               // [chunk][D][nmax] values
+  T* td = tv + kPointChunk * D * nmax;                           // [chunk][D][nmax] derivatives
+  T* fl = td + kPointChunk * D * nmax;                           // [chunk][D+1] flux
+  const int64_t item = blockIdx.x;
+  if (mode == 3 && b.skip && b.skip[item]) return;
+  x += blockIdx.y * n_vec;
+  y += blockIdx.y * n_vec;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  T scale[D];
+#pragma unroll
+  for (int a = 0; a < D; ++a) scale[a] = T(2) / T(b.h[item * D + a]);
+  const T eta = b.eta ? T(b.eta[item]) : T(0);
+  BatchView bv;
+  bv.n_cells = b.n_items;
+  bv.map = b.map;
+  bv.coef = b.coef;
+  bv.tail_off = b.tail_off;
+  bv.tail_idx = b.tail_idx;
+  bv.tail_coef = b.tail_coef;
+  if (mode == 0)
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) xl[i] = gather_entry<T>(bv, item * nb + i, x);
+  T acc[kMaxModes];
+#pragma unroll
+  for (int k = 0; k < kMaxModes; ++k) acc[k] = T(0);
+  const int64_t p_begin = b.pt_off[item], p_end = b.pt_off[item + 1];
+  for (int64_t p0 = p_begin; p0 < p_end; p0 += kPointChunk) {
+    const int cnt = int(p_end - p0 < int64_t(kPointChunk) ? p_end - p0 : int64_t(kPointChunk));
+    __syncthreads();
+    for (int t = threadIdx.x; t < cnt * D; t += blockDim.x) {
+      const int pp = t / D, a = t - pp * D;
+      T* v = tv + (pp * D + a) * nmax;
+      T* d = td + (pp * D + a) * nmax;
+      fe_basis_dev<T>(T(b.ref[(p0 + pp) * D + a]), nn[a] - 1, v, d);
+      for (int i = 0; i < nn[a]; ++i) d[i] *= scale[a];
+    }
+    __syncthreads();
+    if (mode == 1) {
+      for (int pp = threadIdx.x; pp < cnt; pp += blockDim.x) {
+        const int64_t pg = p0 + pp;
+        const T w = T(b.w[pg]);
+        const T g = src ? T(src[pg]) : T(0);
+        if (b.kind == 2) {
+          fl[pp * (D + 1)] = w * eta * g;
+#pragma unroll
+          for (int a = 0; a < D; ++a) fl[pp * (D + 1) + 1 + a] = -w * g * T(b.nrm[pg * D + a]);
+        } else {
+          fl[pp * (D + 1)] = w * g;
+#pragma unroll
+          for (int a = 0; a < D; ++a) fl[pp * (D + 1) + 1 + a] = T(0);
+        }
+      }
+      __syncthreads();
+    } else if (mode == 0) {
+      for (int pp = warp; pp < cnt; pp += kPointWarps) {
+        T u = T(0), g[D];
+#pragma unroll
+        for (int a = 0; a < D; ++a) g[a] = T(0);
+        for (int i = lane; i < nb; i += 32) {
+          const int mi[3] = {i % nn[0], (i / nn[0]) % nn[1], i / (nn[0] * nn[1])};
+          T phi, grad[D];
+          mode_value_grad<T, D>(tv, td, nmax, pp, mi, phi, grad);
+          const T xi = xl[i];
+          u += xi * phi;
+#pragma unroll
+          for (int a = 0; a < D; ++a) g[a] += xi * grad[a];
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+          u += __shfl_xor_sync(0xffffffffu, u, off);
+#pragma unroll
+          for (int a = 0; a < D; ++a) g[a] += __shfl_xor_sync(0xffffffffu, g[a], off);
+        }
+        if (lane == 0) {
+          const int64_t pg = p0 + pp;
+          const T w = T(b.w[pg]);
+          if (b.kind == 2) {
+            T dn = T(0);
+#pragma unroll
+            for (int a = 0; a < D; ++a) dn += g[a] * T(b.nrm[pg * D + a]);
+            fl[pp * (D + 1)] = w * (-dn + eta * u);
+#pragma unroll
+            for (int a = 0; a < D; ++a) fl[pp * (D + 1) + 1 + a] = -w * u * T(b.nrm[pg * D + a]);
+          } else {
+            const T k = b.kpts ? kappa * T(b.kpts[pg]) : kappa;
+            fl[pp * (D + 1)] = w * mass * u;
+#pragma unroll
+            for (int a = 0; a < D; ++a) fl[pp * (D + 1) + 1 + a] = w * k * g[a];
+          }
+        }
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int k = 0; k < kMaxModes; ++k) {
+      const int i = threadIdx.x + k * blockDim.x;
+      if (i >= nb) break;
+      const int mi[3] = {i % nn[0], (i / nn[0]) % nn[1], i / (nn[0] * nn[1])};
+      T s = T(0);
+      for (int pp = 0; pp < cnt; ++pp) {
+        T phi, grad[D];
+        mode_value_grad<T, D>(tv, td, nmax, pp, mi, phi, grad);
+        if (mode == 3) {
+          const int64_t pg = p0 + pp;
+          const T w = T(b.w[pg]);
+          if (b.kind == 2) {
+            T dn = T(0);
+#pragma unroll
+            for (int a = 0; a < D; ++a) dn += grad[a] * T(b.nrm[pg * D + a]);
+            s += w * (eta * phi * phi - T(2) * phi * dn);
+          } else {
+            const T kk = b.kpts ? kappa * T(b.kpts[pg]) : kappa;
+            T gg = T(0);
+#pragma unroll
+            for (int a = 0; a < D; ++a) gg += grad[a] * grad[a];
+            s += w * (mass * phi * phi + kk * gg);
+          }
+        } else {
+          s += fl[pp * (D + 1)] * phi;
+#pragma unroll
+          for (int a = 0; a < D; ++a) s += fl[pp * (D + 1) + 1 + a] * grad[a];
+        }
+      }
+      acc[k] += s;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kMaxModes; ++k) {
+    const int i = threadIdx.x + k * blockDim.x;
+    if (i >= nb) break;
+    if (mode == 3) {
+      const int v = b.map[item * nb + i];
+      if (v >= 0) {
+        const T c = b.coef ? T(b.coef[item * nb + i]) : T(1);
+        atomicAdd(y + v, c * c * acc[k]);
+      }
+    } else {
+      scatter_entry<T>(bv, item * nb + i, acc[k], y);
+    }
+  }
+}
+
+}  // namespace grico

@@ -52,6 +52,9 @@ std::vector<double> collocation_derivative(const std::vector<double>& xi) {
 
 namespace {
 
+inline int32_t item_count(const GricoCellBatchDesc& b) { return b.n_cells; }
+inline int32_t item_count(const GricoPointBatchDesc& b) { return b.n_items; }
+
 // number of box modes prod(n_a) for per-axis mode counts n_a = degree_a + 1
 int64_t box_count(int dim, const int* n) {
   int64_t nb = 1;
@@ -61,10 +64,11 @@ int64_t box_count(int dim, const int* n) {
 
 // Compose the cell term map with the reduced map P: every local entry becomes a sparse
 // combination of reduced dofs (the composition x_loc = T P x_red used by reduced applies).
-void compose_reduced(const GricoCellBatchDesc& bd, int64_t nb, const GricoPlanDesc& d,
+template <typename Desc>
+void compose_reduced(const Desc& bd, int64_t nb, const GricoPlanDesc& d,
                      std::vector<int32_t>& map, std::vector<double>& coef, bool& need_coef,
                      std::vector<int64_t>& toff, std::vector<int32_t>& tidx, std::vector<double>& tcoef) {
-  const int64_t ne = int64_t(bd.n_cells) * nb;
+  const int64_t ne = int64_t(item_count(bd)) * nb;
   map.assign(ne, -1);
   coef.assign(ne, 1.0);
   need_coef = false;
@@ -188,7 +192,108 @@ void launch_batch(const GricoPlan& P, const DevBatch& b, bool reduced, const T* 
 
 int grid_for(int64_t n) { return int(std::min<int64_t>((n + 255) / 256, 148 * 16)); }
 
+template <typename T>
+void launch_points(const GricoPlan& P, const DevPointBatch& pb, bool reduced, const T* x, T* y, int64_t nvec, int mode,
+                   const double* src, int nrhs, cudaStream_t st) {
+  if (pb.n_items == 0) return;
+  PointView v;
+  v.n_items = pb.n_items;
+  v.kind = pb.kind;
+  for (int a = 0; a < 3; ++a) v.n[a] = pb.n[a];
+  const DevMap& m = reduced ? pb.red : pb.full;
+  v.map = m.map.get<int32_t>();
+  v.coef = m.coef.get<double>();
+  v.tail_off = m.toff.get<int64_t>();
+  v.tail_idx = m.tidx.get<int32_t>();
+  v.tail_coef = m.tcoef.get<double>();
+  v.h = pb.h.get<double>();
+  v.pt_off = pb.pt_off.get<int64_t>();
+  v.ref = pb.ref.get<double>();
+  v.w = pb.w.get<double>();
+  v.nrm = pb.nrm.get<double>();
+  v.eta = pb.eta.get<double>();
+  v.kpts = pb.kpts.get<double>();
+  v.skip = reduced ? pb.skip.get<uint8_t>() : nullptr;
+  const int D = P.dim;
+  const int nb = pb.n[0] * (D > 1 ? pb.n[1] : 1) * (D > 2 ? pb.n[2] : 1);
+  const int nmax = std::max(pb.n[0], std::max(D > 1 ? pb.n[1] : 1, D > 2 ? pb.n[2] : 1));
+  const size_t smem = sizeof(T) * (size_t(nb) + 2 * size_t(kPointChunk) * D * nmax + size_t(kPointChunk) * (D + 1));
+  dim3 grid(pb.n_items, nrhs);
+  auto go = [&](auto kernel) {
+    if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    kernel<<<grid, kPointThreads, smem, st>>>(v, x, y, nvec, T(P.mass), T(P.kappa), mode, src);
+  };
+  if (D == 1) go(point_apply<T, 1>);
+  else if (D == 2) go(point_apply<T, 2>);
+  else go(point_apply<T, 3>);
+}
+
 }  // namespace
+
+// Exact local-matrix diagonal contribution of one point item whose reduced map is not a direct
+// injection (cell_diagonal!/face and surface diagonals, accumulators.jl:1056-1083, 1163-1187).
+void accumulate_point_item_diagonal(const GricoPlanDesc& d, const GricoPointBatchDesc& pb, const int* n, int64_t it,
+                                    int64_t nb, const std::vector<int32_t>& rmap, const std::vector<double>& rcoef,
+                                    const std::vector<int64_t>& toff, const std::vector<int32_t>& tidx,
+                                    const std::vector<double>& tcoef, std::map<int64_t, double>& out) {
+  const int D = d.dim;
+  std::vector<double> A(nb * nb, 0.0), phi(nb), gr(3 * nb);
+  double v[3][17], dv[3][17];
+  for (int64_t p = pb.point_offsets[it]; p < pb.point_offsets[it + 1]; ++p) {
+    for (int a = 0; a < D; ++a) {
+      fe_basis(pb.ref_points[p * D + a], n[a] - 1, v[a], dv[a]);
+      const double s = 2.0 / pb.cell_size[it * D + a];
+      for (int i = 0; i < n[a]; ++i) dv[a][i] *= s;
+    }
+    for (int64_t i = 0; i < nb; ++i) {
+      int mi[3] = {int(i % n[0]), int((i / n[0]) % n[1]), int(i / (n[0] * n[1]))};
+      double val = 1.0;
+      for (int a = 0; a < D; ++a) val *= v[a][mi[a]];
+      phi[i] = val;
+      for (int a = 0; a < D; ++a) {
+        double g = dv[a][mi[a]];
+        for (int e = 0; e < D; ++e)
+          if (e != a) g *= v[e][mi[e]];
+        gr[a * nb + i] = g;
+      }
+    }
+    const double w = pb.weights[p];
+    for (int64_t i = 0; i < nb; ++i)
+      for (int64_t j = 0; j < nb; ++j) {
+        double aij;
+        if (pb.kind == GRICO_ITEM_NITSCHE) {
+          // test i, trial j: phi_i(-dn phi_j + eta phi_j) + grad phi_i . (-phi_j n)
+          double dnj = 0.0, dni = 0.0;
+          for (int a = 0; a < D; ++a) {
+            dnj += gr[a * nb + j] * pb.normals[p * D + a];
+            dni += gr[a * nb + i] * pb.normals[p * D + a];
+          }
+          aij = phi[i] * (-dnj + pb.eta[it] * phi[j]) - dni * phi[j];
+        } else {
+          double g = 0.0;
+          for (int a = 0; a < D; ++a) g += gr[a * nb + i] * gr[a * nb + j];
+          const double k = d.kappa * (pb.kappa_points ? pb.kappa_points[p] : 1.0);
+          aij = d.mass * phi[i] * phi[j] + k * g;
+        }
+        A[i * nb + j] += w * aij;
+      }
+  }
+  std::map<int64_t, std::vector<std::pair<int64_t, double>>> by_dof;
+  for (int64_t i = 0; i < nb; ++i) {
+    const int32_t e = rmap[it * nb + i];
+    if (e >= 0) by_dof[e].emplace_back(i, rcoef[it * nb + i]);
+    else if (e <= -2) {
+      const int64_t k = -(int64_t(e) + 2);
+      for (int64_t t = toff[k]; t < toff[k + 1]; ++t) by_dof[tidx[t]].emplace_back(i, tcoef[t]);
+    }
+  }
+  for (auto& kv : by_dof) {
+    double s = 0.0;
+    for (auto& a : kv.second)
+      for (auto& b : kv.second) s += a.second * A[a.first * nb + b.first] * b.second;
+    out[kv.first] += s;
+  }
+}
 
 // Exact reduced-diagonal contribution sum_{i,j} M_ir A_ij M_jr of one cell whose reduced map is
 // not a direct injection.  The local matrix A of TestChannels(mass*u, kappa*k(x)*grad u) is
@@ -295,6 +400,7 @@ int run_apply(GricoPlan* P, bool reduced, const T* x, T* y, int nrhs, cudaStream
   if (nrhs < 1) return GRICO_ERR_INVALID;
   cudaMemsetAsync(y, 0, sizeof(T) * n * nrhs, st);
   for (auto& b : P->batches) launch_batch<T>(*P, b, reduced, x, y, n, 0, nullptr, nrhs, st);
+  for (auto& pb : P->pbatches) launch_points<T>(*P, pb, reduced, x, y, n, 0, nullptr, nrhs, st);
   if (!reduced && (P->n_fixed + P->n_rel) > 0) {
     dim3 grid(grid_for(P->n_fixed + P->n_rel), nrhs);
     constraint_action<T><<<grid, 256, 0, st>>>(P->fixed.get<int64_t>(), P->n_fixed, P->rel_piv.get<int64_t>(),
@@ -310,6 +416,7 @@ template int run_apply<float>(GricoPlan*, bool, const float*, float*, int, cudaS
 int reduced_diag_device(GricoPlan* P, double* diag, cudaStream_t st) {
   cudaMemsetAsync(diag, 0, sizeof(double) * P->n_red, st);
   for (auto& b : P->batches) launch_batch<double>(*P, b, true, nullptr, diag, P->n_red, 3, nullptr, 1, st);
+  for (auto& pb : P->pbatches) launch_points<double>(*P, pb, true, nullptr, diag, P->n_red, 3, nullptr, 1, st);
   if (P->n_hang > 0)
     add_sparse<<<grid_for(P->n_hang), 256, 0, st>>>(P->hang_idx.get<int64_t>(), P->hang_val.get<double>(), P->n_hang,
                                                     diag);
@@ -365,6 +472,38 @@ static int validate_plan_desc(const GricoPlanDesc* d) {
           set_error("batch " + std::to_string(bi) + ": tail index out of range");
           return GRICO_ERR_INVALID;
         }
+  }
+  if (d->n_point_batches < 0 || (d->n_point_batches && !d->point_batches)) {
+    set_error("grico_plan_create: invalid point batches");
+    return GRICO_ERR_INVALID;
+  }
+  for (int bi = 0; bi < d->n_point_batches; ++bi) {
+    const GricoPointBatchDesc& pb = d->point_batches[bi];
+    const std::string tag = "point batch " + std::to_string(bi);
+    if (pb.kind != GRICO_ITEM_CELL && pb.kind != GRICO_ITEM_NITSCHE) { set_error(tag + ": unknown item kind"); return GRICO_ERR_UNSUPPORTED_FORM; }
+    if (pb.n_items < 0 || (pb.n_items > 0 && (!pb.map_index || !pb.cell_size || !pb.point_offsets || !pb.ref_points || !pb.weights))) {
+      set_error(tag + ": missing arrays");
+      return GRICO_ERR_INVALID;
+    }
+    if (pb.kind == GRICO_ITEM_NITSCHE && pb.n_items > 0 && (!pb.normals || !pb.eta)) { set_error(tag + ": Nitsche items need normals and eta"); return GRICO_ERR_INVALID; }
+    int n[3] = {1, 1, 1};
+    for (int a = 0; a < d->dim; ++a) {
+      n[a] = pb.degree[a] + 1;
+      if (n[a] < 1 || n[a] > 16) { set_error(tag + ": degree out of range"); return GRICO_ERR_INVALID; }
+    }
+    const int64_t nb = box_count(d->dim, n);
+    if (nb > int64_t(kMaxModes) * kPointThreads) { set_error(tag + ": too many local modes for point items"); return GRICO_ERR_INVALID; }
+    if (pb.point_offsets && pb.n_items > 0 && pb.point_offsets[0] != 0) { set_error(tag + ": point offsets must start at 0"); return GRICO_ERR_INVALID; }
+    for (int64_t it = 0; it < pb.n_items; ++it)
+      if (pb.point_offsets[it + 1] < pb.point_offsets[it]) { set_error(tag + ": point offsets must not decrease"); return GRICO_ERR_INVALID; }
+    if (pb.n_tail < 0 || (pb.n_tail > 0 && (!pb.tail_offsets || !pb.tail_index || !pb.tail_coef))) { set_error(tag + ": invalid tail"); return GRICO_ERR_INVALID; }
+    for (int64_t e = 0; e < int64_t(pb.n_items) * nb; ++e) {
+      const int32_t v = pb.map_index[e];
+      if (v >= d->n_full || (v <= -2 && -(int64_t(v) + 2) >= pb.n_tail)) { set_error(tag + ": map entry out of range"); return GRICO_ERR_INVALID; }
+    }
+    for (int64_t k = 0; k < pb.n_tail; ++k)
+      for (int64_t t = pb.tail_offsets[k]; t < pb.tail_offsets[k + 1]; ++t)
+        if (pb.tail_index[t] < 0 || pb.tail_index[t] >= d->n_full) { set_error(tag + ": tail index out of range"); return GRICO_ERR_INVALID; }
   }
   for (int64_t i = 0; i < d->n_fixed; ++i)
     if (d->fixed_dofs[i] < 0 || d->fixed_dofs[i] >= d->n_full) { set_error("fixed dof out of range"); return GRICO_ERR_INVALID; }
@@ -500,6 +639,56 @@ int grico_plan_create(const GricoPlanDesc* d, GricoPlan** out) {
     if (!ok) return GRICO_ERR_CUDA;
     P->batches.push_back(std::move(b));
   }
+  for (int bi = 0; bi < d->n_point_batches; ++bi) {
+    const GricoPointBatchDesc& pd = d->point_batches[bi];
+    DevPointBatch pb;
+    pb.n_items = pd.n_items;
+    pb.kind = pd.kind;
+    for (int a = 0; a < d->dim; ++a) pb.n[a] = pd.degree[a] + 1;
+    const int64_t nb = box_count(d->dim, pb.n);
+    const int64_t ne = int64_t(pd.n_items) * nb;
+    pb.n_points = pd.n_items > 0 ? pd.point_offsets[pd.n_items] : 0;
+    bool ok = pb.full.map.upload(pd.map_index, size_t(ne)) && pb.h.upload(pd.cell_size, size_t(pd.n_items) * d->dim) &&
+              pb.pt_off.upload(pd.point_offsets, size_t(pd.n_items + 1)) &&
+              pb.ref.upload(pd.ref_points, size_t(pb.n_points) * d->dim) && pb.w.upload(pd.weights, size_t(pb.n_points));
+    if (pd.map_coef) ok = ok && pb.full.coef.upload(pd.map_coef, size_t(ne));
+    if (pd.n_tail > 0)
+      ok = ok && pb.full.toff.upload(pd.tail_offsets, size_t(pd.n_tail + 1)) &&
+           pb.full.tidx.upload(pd.tail_index, size_t(pd.tail_offsets[pd.n_tail])) &&
+           pb.full.tcoef.upload(pd.tail_coef, size_t(pd.tail_offsets[pd.n_tail]));
+    if (pd.kind == GRICO_ITEM_NITSCHE)
+      ok = ok && pb.nrm.upload(pd.normals, size_t(pb.n_points) * d->dim) && pb.eta.upload(pd.eta, size_t(pd.n_items));
+    if (pd.kappa_points) ok = ok && pb.kpts.upload(pd.kappa_points, size_t(pb.n_points));
+    std::vector<int32_t> rmap, tidx;
+    std::vector<double> rcoef, tcoef;
+    std::vector<int64_t> toff;
+    bool need_coef = false;
+    compose_reduced(pd, nb, *d, rmap, rcoef, need_coef, toff, tidx, tcoef);
+    ok = ok && pb.red.map.upload(rmap);
+    if (need_coef) ok = ok && pb.red.coef.upload(rcoef);
+    if (toff.size() > 1) ok = ok && pb.red.toff.upload(toff) && pb.red.tidx.upload(tidx) && pb.red.tcoef.upload(tcoef);
+    std::vector<uint8_t> skip(pd.n_items, 0);
+    int64_t hanging = 0;
+    std::vector<int64_t> seen;
+    for (int64_t it = 0; it < pd.n_items; ++it) {
+      seen.clear();
+      for (int64_t i = 0; i < nb; ++i) {
+        const int32_t v = rmap[it * nb + i];
+        if (v >= 0) seen.push_back(v);
+        else if (v <= -2) { skip[it] = 1; break; }
+      }
+      if (!skip[it]) {
+        std::sort(seen.begin(), seen.end());
+        if (std::adjacent_find(seen.begin(), seen.end()) != seen.end()) skip[it] = 1;
+      }
+      if (!skip[it]) continue;
+      ++hanging;
+      accumulate_point_item_diagonal(*d, pd, pb.n, it, nb, rmap, rcoef, toff, tidx, tcoef, P->hang_diag);
+    }
+    if (hanging) ok = ok && pb.skip.upload(skip);
+    if (!ok) return GRICO_ERR_CUDA;
+    P->pbatches.push_back(std::move(pb));
+  }
   if (!P->hang_diag.empty()) {
     std::vector<int64_t> hi;
     std::vector<double> hv;
@@ -608,12 +797,30 @@ int grico_reduced_rhs(GricoPlan* P, const double* const* source_points, double* 
     launch_batch<double>(*P, b, false, nullptr, full.get<double>(), P->n_full, 1, sp, 1, st);
     if (flags & GRICO_FLAG_HOST_POINTERS) cudaStreamSynchronize(st);
   }
+  for (size_t bi = 0; bi < P->pbatches.size(); ++bi) {
+    const DevPointBatch& pb = P->pbatches[bi];
+    const size_t slot = P->batches.size() + bi;
+    const double* sp = nullptr;
+    if (source_points && source_points[slot] && pb.n_points > 0) {
+      if (flags & GRICO_FLAG_HOST_POINTERS) {
+        if (!src.alloc(sizeof(double) * pb.n_points)) return GRICO_ERR_CUDA;
+        cudaMemcpyAsync(src.ptr, source_points[slot], sizeof(double) * pb.n_points, cudaMemcpyHostToDevice, st);
+        sp = src.get<double>();
+      } else {
+        sp = source_points[slot];
+      }
+    }
+    launch_points<double>(*P, pb, false, nullptr, full.get<double>(), P->n_full, 1, sp, 1, st);
+    if (flags & GRICO_FLAG_HOST_POINTERS) cudaStreamSynchronize(st);
+  }
   if (P->has_shift) {
     DevBuf as;
     if (!as.alloc(sizeof(double) * P->n_full)) return GRICO_ERR_CUDA;
     cudaMemsetAsync(as.ptr, 0, sizeof(double) * P->n_full, st);
     for (auto& b : P->batches)
       launch_batch<double>(*P, b, false, P->shift.get<double>(), as.get<double>(), P->n_full, 0, nullptr, 1, st);
+    for (auto& pb : P->pbatches)
+      launch_points<double>(*P, pb, false, P->shift.get<double>(), as.get<double>(), P->n_full, 0, nullptr, 1, st);
     axpby_kernel<double><<<grid_for(P->n_full), 256, 0, st>>>(-1.0, as.get<double>(), 1.0, full.get<double>(), P->n_full);
     cudaStreamSynchronize(st);
   }
@@ -722,10 +929,15 @@ extern "C" int grico_reduced_rhs_static(GricoPlan* P, const double* const* sourc
   for (size_t bi = 0; bi < P->batches.size(); ++bi)
     launch_batch<double>(*P, P->batches[bi], false, nullptr, full, P->n_full, 1,
                          source_points ? source_points[bi] : nullptr, 1, st);
+  for (size_t bi = 0; bi < P->pbatches.size(); ++bi)
+    launch_points<double>(*P, P->pbatches[bi], false, nullptr, full, P->n_full, 1,
+                          source_points ? source_points[P->batches.size() + bi] : nullptr, 1, st);
   if (P->has_shift) {
     cudaMemsetAsync(shifted, 0, sizeof(double) * P->n_full, st);
     for (auto& b : P->batches)
       launch_batch<double>(*P, b, false, P->shift.get<double>(), shifted, P->n_full, 0, nullptr, 1, st);
+    for (auto& pb : P->pbatches)
+      launch_points<double>(*P, pb, false, P->shift.get<double>(), shifted, P->n_full, 0, nullptr, 1, st);
     axpby_kernel<double><<<grid_for(P->n_full), 256, 0, st>>>(-1.0, shifted, 1.0, full, P->n_full);
   }
   cudaMemsetAsync(b_reduced, 0, sizeof(double) * P->n_red, st);

@@ -76,6 +76,15 @@ struct DevBatch {
   std::vector<double> hB, hD, hW;  // axis-0 tables on the host (kernel parameters)
 };
 
+struct DevPointBatch {
+  int32_t n_items = 0;
+  int kind = 1;
+  int n[3] = {1, 1, 1};
+  int64_t n_points = 0;
+  DevMap full, red;
+  DevBuf h, pt_off, ref, w, nrm, eta, kpts, skip;
+};
+
 }  // namespace grico
 
 struct GricoPlan {
@@ -84,6 +93,7 @@ struct GricoPlan {
   int64_t n_full = 0, n_red = 0;
   cudaStream_t stream = nullptr;
   std::vector<grico::DevBatch> batches;
+  std::vector<grico::DevPointBatch> pbatches;
   int64_t n_fixed = 0, n_rel = 0;
   grico::DevBuf fixed, fixed_vals, rel_piv, rel_off, rel_idx, rel_coef;
   grico::DevBuf red_off, red_idx, red_coef, shift;

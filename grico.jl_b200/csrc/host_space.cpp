@@ -23,6 +23,7 @@
 #include <stdexcept>
 #include <string>
 #include <unordered_map>
+#include <set>
 #include <unordered_set>
 #include <vector>
 
@@ -300,6 +301,7 @@ struct Space {
   std::vector<double> term_coef;
   int64_t ndofs = 0;
   double min_pivot = 1e300;  // smallest |pivot coefficient| met in the elimination
+  int64_t noise_rows = 0;    // redundant continuity rows dropped at rounding-noise level
 };
 
 namespace {
@@ -419,36 +421,35 @@ void enumerate_faces(Space& s) {
       for (int b = 0; b < D; ++b) p[b] = s.lower[l * D + b];
       p[a] = U;
       int64_t first = containing(p);
-      if (first < 0) continue;
-      if (s.lower[first * D + a] != U) continue;  // not a face-adjacent leaf
-      bool covers = true;
-      for (int b = 0; b < D; ++b)
+      bool covers = first >= 0 && s.lower[first * D + a] == U;
+      for (int b = 0; covers && b < D; ++b)
         if (b != a) covers &= s.lower[first * D + b] <= s.lower[l * D + b] && s.upper[first * D + b] >= s.upper[l * D + b];
       if (covers) {
         partners.push_back(first);
       } else {
-        // finer partners tile the face: flood over lower corners inside the face box
+        // Finer partners, possibly with gaps (leaves removed from a physical domain): flood
+        // the face from its lower corner, jumping across every leaf found and stepping one
+        // finest-lattice unit across holes, so every leaf touching the face is reached.
         std::vector<std::array<int64_t, kMaxDim>> stack;
         std::unordered_set<int64_t> seen;
+        std::set<std::array<int64_t, kMaxDim>> probed;
         std::array<int64_t, kMaxDim> c0 = {0, 0, 0};
         for (int b = 0; b < D; ++b) c0[b] = p[b];
         stack.push_back(c0);
         while (!stack.empty()) {
           auto c = stack.back();
           stack.pop_back();
+          if (!probed.insert(c).second) continue;
           int64_t q = containing(c.data());
-          if (q < 0 || seen.count(q)) continue;
-          seen.insert(q);
-          partners.push_back(q);
+          if (q >= 0 && !seen.count(q)) {
+            seen.insert(q);
+            partners.push_back(q);
+          }
           for (int b = 0; b < D; ++b) {
             if (b == a) continue;
             auto n = c;
-            n[b] = s.upper[q * D + b];
-            if (n[b] < s.upper[l * D + b]) {
-              for (int e = 0; e < D; ++e)
-                if (e != a && e != b) n[e] = std::max(c[e], s.lower[q * D + e]);
-              stack.push_back(n);
-            }
+            n[b] = q >= 0 ? s.upper[q * D + b] : c[b] + 1;
+            if (n[b] < s.upper[l * D + b]) stack.push_back(n);
           }
         }
       }
@@ -616,6 +617,9 @@ void compile_continuity(Space& s) {
         std::vector<int64_t> order;
         for (size_t ri : kv.second) {
           Row& row = rows[ri];
+          // largest magnitude that entered the row: the scale of its rounding noise
+          double seen = 0.0;
+          for (double c : row.coefs) seen = std::max(seen, std::fabs(c));
           while (true) {
             bool changed = false;
             for (size_t i = 0; i < row.vars.size(); ++i) {
@@ -623,6 +627,7 @@ void compile_continuity(Space& s) {
               if (it == local.end()) continue;
               double factor = row.coefs[i];
               row.remove_at(i);
+              for (double c : it->second->coefs) seen = std::max(seen, std::fabs(factor * c));
               row.accumulate(*it->second, factor);
               changed = true;
               break;
@@ -631,6 +636,13 @@ void compile_continuity(Space& s) {
             if (!changed) break;
           }
           if (row.vars.empty()) continue;
+          // A redundant row (its constraint already implied by earlier pivots) cancels to
+          // rounding noise; the reference's cleanup (4 eps against max(scale, 1)) can keep such
+          // a residue and would then eliminate a free variable.  Rows whose every remaining
+          // coefficient is at noise level relative to what was summed into them are dropped.
+          double left = 0.0;
+          for (double c : row.coefs) left = std::max(left, std::fabs(c));
+          if (left <= 256.0 * 2.220446049250313e-16 * seen) { ++s.noise_rows; continue; }
           size_t pidx = 0;
           for (size_t i = 1; i < row.vars.size(); ++i)
             if (row.vars[i] > row.vars[pidx]) pidx = i;

@@ -9,8 +9,11 @@ from .mesh import LOWER, UPPER, CartesianGrid, Domain, grid, refine, uniform_ref
 from .space import (AxisDegrees, ByLeafDegrees, DegreePlusQuadrature, FullTensorBasis, HpSpace, SpaceOptions,
                     StoredDegrees, TrunkBasis, UniformDegree, active_leaf_count, scalar_dof_count)
 from .problem import (SPD, AffineProblem, AssemblyPlan, BoundaryFace, CGSolver, Diffusion, Dirichlet, FGMRESSolver,
-                      IdentityPreconditioner, JacobiPreconditioner, Load, Mass, MassDiffusion, NonsymmetricOperator,
-                      ScalarField, State, VariableDiffusion, add_cell_accumulator, add_constraint, apply, apply_,
-                      compile, expand_reduced, l2_error, reduced_apply, reduced_diagonal, reduced_rhs,
-                      relative_l2_error, solve)
+                      IdentityPreconditioner, JacobiPreconditioner, Load, Mass, MassDiffusion, Nitsche,
+                      NonsymmetricOperator, ScalarField, State, VariableDiffusion, add_boundary_accumulator,
+                      add_cell_accumulator, add_cell_quadrature, add_constraint, add_surface_accumulator,
+                      add_surface_quadrature, apply, apply_, compile, expand_reduced, l2_error, reduced_apply,
+                      reduced_diagonal, reduced_rhs, relative_l2_error, solve)
+from .regions import (FiniteCellExtension, ImplicitRegion, PhysicalDomain, PhysicalMeasure, SurfaceQuadrature,
+                      finite_cell_quadrature, sphere_surface_quadrature)
 from .multigrid import GeometricMultigridPreconditioner

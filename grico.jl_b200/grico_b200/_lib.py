@@ -26,6 +26,8 @@ GRICO_BASIS_TRUNK = 1
 GRICO_CONTINUITY_CG = 0
 GRICO_CONTINUITY_DG = 1
 GRICO_FORM_MASS_DIFFUSION = 1
+GRICO_ITEM_CELL = 1
+GRICO_ITEM_NITSCHE = 2
 GRICO_PREC_FP64 = 0
 GRICO_PREC_FP32 = 1
 GRICO_FLAG_HOST_POINTERS = 1
@@ -57,6 +59,27 @@ class GricoCellBatchDesc(C.Structure):
     ]
 
 
+class GricoPointBatchDesc(C.Structure):
+    _fields_ = [
+        ("n_items", C.c_int32),
+        ("kind", C.c_int32),
+        ("degree", C.c_int32 * 3),
+        ("map_index", i32p),
+        ("map_coef", f64p),
+        ("n_tail", C.c_int64),
+        ("tail_offsets", i64p),
+        ("tail_index", i32p),
+        ("tail_coef", f64p),
+        ("cell_size", f64p),
+        ("point_offsets", i64p),
+        ("ref_points", f64p),
+        ("weights", f64p),
+        ("normals", f64p),
+        ("eta", f64p),
+        ("kappa_points", f64p),
+    ]
+
+
 class GricoPlanDesc(C.Structure):
     _fields_ = [
         ("dim", C.c_int32),
@@ -80,6 +103,8 @@ class GricoPlanDesc(C.Structure):
         ("red_index", i64p),
         ("red_coef", f64p),
         ("red_shift", f64p),
+        ("n_point_batches", C.c_int32),
+        ("point_batches", C.POINTER(GricoPointBatchDesc)),
     ]
 
 

@@ -58,6 +58,19 @@ class Load:
         self.source = source
 
 
+class Nitsche:
+    """Symmetric Nitsche Dirichlet data u = g on boundary faces or embedded surfaces
+    (examples/annular_nitsche_fcm/driver.jl:45-76): bilinear TestChannels(-du/dn + eta*u, -u*n),
+    right-hand side TestChannels(eta*g, -g*n), eta = penalty / min(cell_size).  `data(points)`
+    returns g on an [n, D] array (None: g = 0)."""
+
+    def __init__(self, penalty, data=None):
+        self.penalty = float(penalty)
+        if not self.penalty >= 0.0:
+            raise ValueError("penalty must be non-negative")
+        self.data = data
+
+
 # ---------------------------------------------------------------------------------------
 # fields, constraints, problems
 # ---------------------------------------------------------------------------------------
@@ -100,6 +113,12 @@ class AffineProblem:
         self.cell_operators = []
         self.rhs_operators = []
         self.dirichlet = []
+        self.surface_operators = []        # bilinear Nitsche forms on embedded surfaces
+        self.surface_rhs_operators = []
+        self.boundary_operators = []       # (BoundaryFace, Nitsche)
+        self.boundary_rhs_operators = []
+        self.surfaces = []                 # SurfaceQuadrature attachments
+        self.cell_quadratures = {}         # leaf -> (reference points, reference weights)
 
 
 def add_cell_accumulator(problem, test_field, *args):
@@ -118,6 +137,77 @@ def add_cell_accumulator(problem, test_field, *args):
         problem.rhs_operators.append(op)
     else:
         raise TypeError("add_cell_accumulator(problem, test, trial, op) or (problem, test, load)")
+    return problem
+
+
+def add_surface_accumulator(problem, test_field, *args):
+    """add_surface_accumulator!(problem, test, trial, op) or (problem, test, op)
+    (accumulators.jl:435-466); the B200 plan recognises the symmetric Nitsche form."""
+    if test_field is not problem.field:
+        raise ValueError("the B200 plan supports one scalar field")
+    if len(args) == 2:
+        trial, op = args
+        if trial is not test_field:
+            raise ValueError("the B200 plan supports one scalar field")
+        if not isinstance(op, Nitsche):
+            raise L.GricoError(L.GRICO_ERR_UNSUPPORTED_FORM, f"surface form {type(op).__name__} is not supported by the GPU plan")
+        problem.surface_operators.append(op)
+    elif len(args) == 1:
+        (op,) = args
+        if not isinstance(op, Nitsche):
+            raise L.GricoError(L.GRICO_ERR_UNSUPPORTED_FORM, f"surface rhs form {type(op).__name__} is not supported by the GPU plan")
+        problem.surface_rhs_operators.append(op)
+    else:
+        raise TypeError("add_surface_accumulator(problem, test, trial, op) or (problem, test, op)")
+    return problem
+
+
+def add_boundary_accumulator(problem, boundary, test_field, *args):
+    """add_boundary_accumulator!(problem, boundary, test, trial, op) or (problem, boundary, test, op)
+    (accumulators.jl:396-411) with the symmetric Nitsche form."""
+    if not isinstance(boundary, BoundaryFace):
+        raise TypeError("boundary must be a BoundaryFace")
+    if test_field is not problem.field:
+        raise ValueError("the B200 plan supports one scalar field")
+    if len(args) == 2:
+        trial, op = args
+        if trial is not test_field:
+            raise ValueError("the B200 plan supports one scalar field")
+        if not isinstance(op, Nitsche):
+            raise L.GricoError(L.GRICO_ERR_UNSUPPORTED_FORM, f"boundary form {type(op).__name__} is not supported by the GPU plan")
+        problem.boundary_operators.append((boundary, op))
+    elif len(args) == 1:
+        (op,) = args
+        if not isinstance(op, Nitsche):
+            raise L.GricoError(L.GRICO_ERR_UNSUPPORTED_FORM, f"boundary rhs form {type(op).__name__} is not supported by the GPU plan")
+        problem.boundary_rhs_operators.append((boundary, op))
+    else:
+        raise TypeError("add_boundary_accumulator(problem, boundary, test, trial, op) or (problem, boundary, test, op)")
+    return problem
+
+
+def add_surface_quadrature(problem, surface):
+    """add_surface_quadrature!(problem, surface) (embedded.jl:181-184); also accepts a list."""
+    from .regions import SurfaceQuadrature
+
+    items = surface if isinstance(surface, (list, tuple)) else [surface]
+    for it in items:
+        if not isinstance(it, SurfaceQuadrature):
+            raise TypeError("expected SurfaceQuadrature items")
+        problem.surfaces.append(it)
+    return problem
+
+
+def add_cell_quadrature(problem, leaf, points, weights):
+    """add_cell_quadrature!(problem, leaf, quadrature) (embedded.jl:203-207): override one leaf's
+    cell rule with explicit biunit reference points and reference weights."""
+    pts = np.atleast_2d(np.asarray(points, dtype=np.float64))
+    w = np.asarray(weights, dtype=np.float64).reshape(-1)
+    if pts.shape != (w.size, problem.field.space.D):
+        raise ValueError("cell quadrature points and weights must match the dimension")
+    if np.any(np.abs(pts) > 1.0 + 1e-12):
+        raise ValueError("cell quadrature points must lie in the biunit cell")
+    problem.cell_quadratures[int(leaf)] = (pts, w)
     return problem
 
 
@@ -162,6 +252,62 @@ def _tables(p, q):
     return pts, wts, B, G
 
 
+def _item_maps(space, cells, b):
+    """Box-mode maps of the leaves at Morton positions `cells` (single terms inline, multi-term
+    expansions into a tail CSR), stored on `b` as map_index/map_coef/tail_*/nbox."""
+    degree = tuple(int(v) for v in space.degrees[cells[0]]) if len(cells) else ()
+    nb = int(np.prod([d + 1 for d in degree])) if len(cells) else 0
+    b.nbox = nb
+    starts = space.box_offsets[cells]
+    ent = (starts[:, None] + np.arange(nb)[None, :]).reshape(-1)
+    lo = space.term_offsets[ent]
+    hi = space.term_offsets[ent + 1]
+    cnt = hi - lo
+    mp = np.full(ent.size, -1, dtype=np.int32)
+    single = cnt == 1
+    mp[single] = space.term_index[lo[single]].astype(np.int32)
+    coef = np.ones(ent.size)
+    coef[single] = space.term_coef[lo[single]]
+    multi = np.nonzero(cnt > 1)[0]
+    if multi.size:
+        mp[multi] = -(np.arange(multi.size, dtype=np.int32) + 2)
+        tcnt = cnt[multi]
+        b.tail_offsets = np.concatenate([[0], np.cumsum(tcnt)]).astype(np.int64)
+        tsrc = np.concatenate([np.arange(l, h) for l, h in zip(lo[multi], hi[multi])])
+        b.tail_index = space.term_index[tsrc].astype(np.int32)
+        b.tail_coef = space.term_coef[tsrc].astype(np.float64)
+    else:
+        b.tail_offsets = b.tail_index = b.tail_coef = None
+    b.map_index = np.ascontiguousarray(mp)
+    b.map_coef = None if np.all(coef == 1.0) else np.ascontiguousarray(coef)
+
+
+def fe_basis_table(x, p):
+    """psi_0..psi_p and derivatives at every entry of x: ([n, p+1], [n, p+1])
+    (polynomials.jl:403-434, vectorised)."""
+    x = np.asarray(x, dtype=np.float64)
+    v = np.zeros((x.size, p + 1))
+    d = np.zeros((x.size, p + 1))
+    if p == 0:
+        v[:, 0] = 1.0
+        return v, d
+    v[:, 0] = 0.5 * (1.0 - x)
+    v[:, 1] = 0.5 * (1.0 + x)
+    d[:, 0] = -0.5
+    d[:, 1] = 0.5
+    pm2, pm1 = np.ones_like(x), x.copy()
+    for k in range(2, p + 1):
+        pk = ((2 * k - 1) * x * pm1 - (k - 1) * pm2) / k
+        v[:, k] = (pk - pm2) / math.sqrt(4 * k - 2)
+        d[:, k] = math.sqrt((2 * k - 1) / 2.0) * pm1
+        pm2, pm1 = pm1, pk
+    return v, d
+
+
+class _PointBatch:
+    pass
+
+
 class AssemblyPlan:
     """Compiled plan: descriptor arrays built here, device data owned by libgrico_b200."""
 
@@ -178,53 +324,63 @@ class AssemblyPlan:
         self.D = D = space.D
         n_full = space.scalar_dof_count
         self.n_full = n_full
-        # --- batches by (degrees, quadrature shape), first appearance in Morton order ---
+        from .regions import FiniteCellExtension, PhysicalDomain
+
+        physical = isinstance(domain, PhysicalDomain)
+        if physical and (problem.dirichlet or problem.boundary_operators or problem.boundary_rhs_operators):
+            raise L.GricoError(L.GRICO_ERR_UNSUPPORTED_FORM,
+                               "boundary-face constraints and forms on a PhysicalDomain are not supported by the GPU plan")
+        # --- which leaves integrate on point rules: cut cells and explicit cell quadratures ---
+        point_rule = {}
+        for leaf, rule in problem.cell_quadratures.items():
+            if leaf not in space.leaf_to_index:
+                raise ValueError(f"cell quadrature leaf {leaf} is not an active leaf")
+            point_rule[space.leaf_to_index[leaf]] = rule
+        self.n_cut = 0
+        if physical and not (isinstance(domain.cell_measure, FiniteCellExtension) and domain.cell_measure.alpha == 1.0):
+            cls = domain.classify(space.leaves)
+            cut = np.nonzero(cls == 2)[0]
+            cut = np.array([c for c in cut if int(c) not in point_rule], dtype=np.int64)
+            self.n_cut = int(cut.size)
+            if cut.size:
+                qs = space.qshape[cut]
+                for qsig in np.unique(qs, axis=0):
+                    sel = cut[np.all(qs == qsig, axis=1)]
+                    rules = domain.cut_cell_quadrature(space.leaves[sel], tuple(int(v) for v in qsig), _gauss)
+                    for c, r in zip(sel, rules):
+                        if r is not None:        # no candidate at all: the tensor rule stays
+                            point_rule[int(c)] = r
+        tensor_mask = np.ones(len(space.leaves), dtype=bool)
+        tensor_mask[list(point_rule)] = False
+        # --- tensor batches by (degrees, quadrature shape), first appearance in Morton order ---
         sig = np.concatenate([space.degrees, space.qshape], axis=1)
-        _, first, inv = np.unique(sig, axis=0, return_index=True, return_inverse=True)
-        inv = inv.reshape(-1)
-        order_groups = np.argsort(first, kind="stable")
         self.batches = []
-        for g in order_groups:
-            cells = np.nonzero(inv == g)[0]
-            b = _Batch()
-            b.cells = cells                                      # Morton positions
-            b.leaves = space.leaves[cells]
-            b.degree = tuple(int(v) for v in space.degrees[cells[0]])
-            b.q = tuple(int(v) for v in space.qshape[cells[0]])
-            nb = int(np.prod([d + 1 for d in b.degree]))
-            b.nbox = nb
-            starts = space.box_offsets[cells]
-            ent = (starts[:, None] + np.arange(nb)[None, :]).reshape(-1)
-            lo = space.term_offsets[ent]
-            hi = space.term_offsets[ent + 1]
-            cnt = hi - lo
-            mp = np.full(ent.size, -1, dtype=np.int32)
-            single = cnt == 1
-            mp[single] = space.term_index[lo[single]].astype(np.int32)
-            coef = np.ones(ent.size)
-            coef[single] = space.term_coef[lo[single]]
-            multi = np.nonzero(cnt > 1)[0]
-            if multi.size:
-                mp[multi] = -(np.arange(multi.size, dtype=np.int32) + 2)
-                tcnt = cnt[multi]
-                b.tail_offsets = np.concatenate([[0], np.cumsum(tcnt)]).astype(np.int64)
-                tsrc = np.concatenate([np.arange(l, h) for l, h in zip(lo[multi], hi[multi])])
-                b.tail_index = space.term_index[tsrc].astype(np.int32)
-                b.tail_coef = space.term_coef[tsrc].astype(np.float64)
-            else:
-                b.tail_offsets = b.tail_index = b.tail_coef = None
-            b.map_index = np.ascontiguousarray(mp)
-            b.map_coef = None if np.all(coef == 1.0) else np.ascontiguousarray(coef)
-            b.h = np.ascontiguousarray(domain.cell_size(b.leaves))
-            b.lower = domain.cell_lower(b.leaves)
-            # reference points of the tensor rule, axis 1 fastest
-            b.rules = [_tables(b.degree[a], b.q[a]) for a in range(D)]
-            b.points = self._points(b)                           # [n_cells, nq, D]
-            b.kappa_points = None
-            if self.form.coefficient is not None:
-                vals = np.asarray(self.form.coefficient(b.points.reshape(-1, D)), dtype=np.float64)
-                b.kappa_points = np.ascontiguousarray(vals.reshape(len(cells), -1))
-            self.batches.append(b)
+        tensor_cells = np.nonzero(tensor_mask)[0]
+        if tensor_cells.size:
+            _, first, inv = np.unique(sig[tensor_cells], axis=0, return_index=True, return_inverse=True)
+            inv = inv.reshape(-1)
+            for g in np.argsort(first, kind="stable"):
+                cells = tensor_cells[inv == g]
+                b = _Batch()
+                b.cells = cells                                      # Morton positions
+                b.leaves = space.leaves[cells]
+                b.degree = tuple(int(v) for v in space.degrees[cells[0]])
+                b.q = tuple(int(v) for v in space.qshape[cells[0]])
+                _item_maps(space, cells, b)
+                b.h = np.ascontiguousarray(domain.cell_size(b.leaves))
+                b.lower = domain.cell_lower(b.leaves)
+                # reference points of the tensor rule, axis 1 fastest
+                b.rules = [_tables(b.degree[a], b.q[a]) for a in range(D)]
+                b.points = self._points(b)                           # [n_cells, nq, D]
+                b.kappa_points = None
+                if self.form.coefficient is not None:
+                    vals = np.asarray(self.form.coefficient(b.points.reshape(-1, D)), dtype=np.float64)
+                    b.kappa_points = np.ascontiguousarray(vals.reshape(len(cells), -1))
+                self.batches.append(b)
+        # --- point-quadrature items: cut cells, faces, embedded surfaces ---
+        self.point_batches = []
+        self._build_cell_items(point_rule)
+        self._build_nitsche_items(problem)
         # --- Dirichlet: fixed dofs are the dofs with a trace on a selected boundary face ---
         self._compile_dirichlet(problem)
         # --- reduced map ---
@@ -243,6 +399,119 @@ class AssemblyPlan:
         self.handle = None
         if device:
             self._create_device_plan()
+
+    def _new_point_batch(self, kind, positions, degree):
+        space, domain, D = self.space, self.space.domain, self.D
+        pb = _PointBatch()
+        pb.kind = kind
+        pb.cells = np.asarray(positions, dtype=np.int64)
+        pb.leaves = space.leaves[pb.cells]
+        pb.degree = degree
+        _item_maps(space, pb.cells, pb)
+        pb.h = np.ascontiguousarray(domain.cell_size(pb.leaves))
+        pb.lower = domain.cell_lower(pb.leaves)
+        return pb
+
+    def _finish_point_batch(self, pb, refs, weights, normals=None, eta=None):
+        D = self.D
+        counts = np.array([len(w) for w in weights], dtype=np.int64)
+        pb.point_offsets = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+        pb.ref_points = np.ascontiguousarray(np.concatenate(refs).reshape(-1, D)) if len(refs) else np.zeros((0, D))
+        pb.weights = np.ascontiguousarray(np.concatenate(weights)) if len(weights) else np.zeros(0)
+        pb.normals = None if normals is None else np.ascontiguousarray(np.concatenate(normals).reshape(-1, D))
+        pb.eta = None if eta is None else np.ascontiguousarray(eta, dtype=np.float64)
+        item = np.repeat(np.arange(len(pb.cells)), counts)
+        half = 0.5 * pb.h[item]
+        pb.points = (pb.lower[item] + half) + pb.ref_points * half           # physical points [P, D]
+        pb.kappa_points = None
+        if pb.kind == L.GRICO_ITEM_CELL and self.form.coefficient is not None:
+            pb.kappa_points = np.ascontiguousarray(
+                np.asarray(self.form.coefficient(pb.points), dtype=np.float64).reshape(-1))
+        self.point_batches.append(pb)
+
+    def _build_cell_items(self, point_rule):
+        """Cut cells and explicit cell rules: kind-1 items grouped by degree (Morton order)."""
+        space, D = self.space, self.D
+        if not point_rule:
+            return
+        pos = np.array(sorted(point_rule), dtype=np.int64)
+        degs = space.degrees[pos]
+        for dsig in np.unique(degs, axis=0):
+            sel = pos[np.all(degs == dsig, axis=1)]
+            pb = self._new_point_batch(L.GRICO_ITEM_CELL, sel, tuple(int(v) for v in dsig))
+            det = np.prod(0.5 * pb.h, axis=1)
+            refs = [point_rule[int(c)][0] for c in sel]
+            wts = [point_rule[int(c)][1] * det[i] for i, c in enumerate(sel)]
+            self._finish_point_batch(pb, refs, wts)
+
+    def _build_nitsche_items(self, problem):
+        """Boundary-face items (integration.jl:2230-2256) and embedded-surface items
+        (integration.jl:2338-2357) of the Nitsche forms, grouped by degree."""
+        from .regions import physical_surface_data
+
+        space, D = self.space, self.D
+        domain = space.domain
+        bil = problem.surface_operators
+        rhs = problem.surface_rhs_operators
+        if len(bil) > 1 or len(rhs) > 1:
+            raise L.GricoError(L.GRICO_ERR_UNSUPPORTED_FORM, "the GPU plan accepts one surface form and one surface load")
+        if rhs and not bil:
+            raise L.GricoError(L.GRICO_ERR_UNSUPPORTED_FORM, "a Nitsche surface load needs the matching Nitsche surface form")
+        if bil and rhs and bil[0].penalty != rhs[0].penalty:
+            raise L.GricoError(L.GRICO_ERR_UNSUPPORTED_FORM, "Nitsche surface form and load must share the penalty")
+        items = []   # (position, ref pts, phys weights, phys normals, penalty, data, src tag)
+        if bil and problem.surfaces:
+            op = bil[0]
+            g = rhs[0].data if rhs else None
+            for sq in sorted(problem.surfaces, key=lambda s: s.leaf):
+                if sq.leaf not in space.leaf_to_index:
+                    raise ValueError(f"surface quadrature leaf {sq.leaf} is not an active leaf")
+                w, n = physical_surface_data(domain, sq.leaf, sq)
+                items.append((space.leaf_to_index[sq.leaf], sq.points, w, n, op.penalty, g))
+        # boundary faces: one bilinear and at most one load per face
+        bops = {}
+        for bf, op in problem.boundary_operators:
+            key = (bf.axis - 1, bf.side - 1)
+            if key in bops:
+                raise L.GricoError(L.GRICO_ERR_UNSUPPORTED_FORM, "one boundary form per face on the GPU plan")
+            bops[key] = [op, None]
+        for bf, op in problem.boundary_rhs_operators:
+            key = (bf.axis - 1, bf.side - 1)
+            if key not in bops or bops[key][1] is not None or bops[key][0].penalty != op.penalty:
+                raise L.GricoError(L.GRICO_ERR_UNSUPPORTED_FORM,
+                                   "a Nitsche boundary load needs the matching Nitsche boundary form")
+            bops[key][1] = op.data
+        if bops:
+            b_leaf, b_axis, b_side = space.boundary_faces
+            for pos, ax, sd in zip(b_leaf, b_axis, b_side):
+                key = (int(ax), int(sd))
+                if key not in bops:
+                    continue
+                op, g = bops[key]
+                q = space.qshape[pos]
+                rules = [_gauss(int(q[a])) if a != ax else (np.array([-1.0 if sd == 0 else 1.0]), np.array([1.0]))
+                         for a in range(D)]
+                grids = np.meshgrid(*[r[0] for r in rules], indexing="ij")
+                wg = np.meshgrid(*[r[1] for r in rules], indexing="ij")
+                ref = np.stack([gg.reshape(-1, order="F") for gg in grids], axis=1)
+                wref = np.ones(ref.shape[0])
+                for a in range(D):
+                    wref = wref * wg[a].reshape(-1, order="F")
+                h = domain.cell_size(space.leaves[[pos]])[0]
+                scale = 1.0 if D == 1 else math.ldexp(float(np.prod([h[a] for a in range(D) if a != ax])), -(D - 1))
+                nrm = np.zeros((ref.shape[0], D))
+                nrm[:, ax] = -1.0 if sd == 0 else 1.0
+                items.append((int(pos), ref, wref * scale, nrm, op.penalty, g))
+        if not items:
+            return
+        degs = np.array([space.degrees[it[0]] for it in items]).reshape(len(items), D)
+        for dsig in np.unique(degs, axis=0):
+            sel = [i for i in range(len(items)) if np.all(degs[i] == dsig)]
+            pb = self._new_point_batch(L.GRICO_ITEM_NITSCHE, [items[i][0] for i in sel], tuple(int(v) for v in dsig))
+            eta = np.array([items[i][4] / float(np.min(pb.h[k])) for k, i in enumerate(sel)])
+            pb.data = [items[i][5] for i in sel]
+            self._finish_point_batch(pb, [items[i][1] for i in sel], [items[i][2] for i in sel],
+                                     [items[i][3] for i in sel], eta)
 
     def _points(self, b):
         D = self.D
@@ -315,7 +584,29 @@ class AssemblyPlan:
             d.tail_coef = L.ptr(b.tail_coef, C.c_double)
             d.cell_size = L.ptr(b.h, C.c_double)
             d.kappa_points = L.ptr(b.kappa_points, C.c_double)
+        pdescs = (L.GricoPointBatchDesc * max(1, len(self.point_batches)))()
+        for i, b in enumerate(self.point_batches):
+            d = pdescs[i]
+            d.n_items = len(b.cells)
+            d.kind = b.kind
+            for a in range(3):
+                d.degree[a] = b.degree[a] if a < self.D else 0
+            d.map_index = L.ptr(b.map_index, C.c_int32)
+            d.map_coef = L.ptr(b.map_coef, C.c_double)
+            d.n_tail = 0 if b.tail_offsets is None else len(b.tail_offsets) - 1
+            d.tail_offsets = L.ptr(b.tail_offsets, C.c_int64)
+            d.tail_index = L.ptr(b.tail_index, C.c_int32)
+            d.tail_coef = L.ptr(b.tail_coef, C.c_double)
+            d.cell_size = L.ptr(b.h, C.c_double)
+            d.point_offsets = L.ptr(b.point_offsets, C.c_int64)
+            d.ref_points = L.ptr(b.ref_points, C.c_double)
+            d.weights = L.ptr(b.weights, C.c_double)
+            d.normals = L.ptr(b.normals, C.c_double)
+            d.eta = L.ptr(b.eta, C.c_double)
+            d.kappa_points = L.ptr(b.kappa_points, C.c_double)
         pd = L.GricoPlanDesc()
+        pd.n_point_batches = len(self.point_batches)
+        pd.point_batches = pdescs
         pd.dim = self.D
         pd.form = L.GRICO_FORM_MASS_DIFFUSION
         pd.mass = self.form.mass
@@ -419,6 +710,8 @@ def reduced_apply(plan, x, nrhs=1):
 
 
 def _source_points(plan, problem=None):
+    """Per-point source values: f at the cell points of every tensor batch, then per point
+    batch f at cell-item points or the Nitsche data g at face/surface points."""
     problem = problem or plan.problem
     arrays = []
     for b in plan.batches:
@@ -429,6 +722,26 @@ def _source_points(plan, problem=None):
             arrays.append(np.ascontiguousarray(f))
         else:
             arrays.append(None)
+    for b in plan.point_batches:
+        if b.kind == L.GRICO_ITEM_CELL:
+            if problem.rhs_operators:
+                f = np.zeros(b.points.shape[0])
+                for op in problem.rhs_operators:
+                    f += np.asarray(op.source(b.points), dtype=np.float64).reshape(-1)
+                arrays.append(np.ascontiguousarray(f))
+            else:
+                arrays.append(None)
+        else:
+            g = np.zeros(b.points.shape[0])
+            any_data = False
+            for k, fn in enumerate(b.data):
+                if fn is None:
+                    continue
+                lo, hi = b.point_offsets[k], b.point_offsets[k + 1]
+                if hi > lo:
+                    g[lo:hi] = np.asarray(fn(b.points[lo:hi]), dtype=np.float64).reshape(-1)
+                any_data = True
+            arrays.append(np.ascontiguousarray(g) if any_data else None)
     return arrays
 
 
@@ -508,14 +821,26 @@ def solve(plan_or_problem, solver=None, relative_tolerance=None, absolute_tolera
     return State(plan, expand_reduced(plan, x), rep)
 
 
+def _quadrature_sets(plan):
+    """(weights, physical points) of every cell rule: tensor batches and cell point items."""
+    out = []
+    for b in plan.batches:
+        out.append((_point_weights(plan, b).reshape(-1), b.points.reshape(-1, plan.D)))
+    for b in plan.point_batches:
+        if b.kind == L.GRICO_ITEM_CELL:
+            out.append((b.weights, b.points))
+    return out
+
+
 def l2_error(state, exact):
-    """Quadrature L2 error on the cell rules (verification.jl:201-230, 270-275)."""
+    """Quadrature L2 error on the cell rules, cut-cell rules included (verification.jl:201-230,
+    270-275)."""
     plan = state.plan
     err2 = 0.0
-    for b, u in zip(plan.batches, _point_values(plan, state.coefficients)):
-        w = _point_weights(plan, b)
-        ex = np.asarray(exact(b.points.reshape(-1, plan.D)), dtype=np.float64).reshape(u.shape)
-        err2 += float(np.sum(w * (u - ex) ** 2))
+    values = _point_values(plan, state.coefficients) + _point_item_values(plan, state.coefficients)
+    for (w, pts), u in zip(_quadrature_sets(plan), values):
+        ex = np.asarray(exact(pts), dtype=np.float64).reshape(-1)
+        err2 += float(np.sum(w * (u.reshape(-1) - ex) ** 2))
     return math.sqrt(err2)
 
 
@@ -523,11 +848,45 @@ def relative_l2_error(state, exact):
     plan = state.plan
     num = l2_error(state, exact)
     den2 = 0.0
-    for b in plan.batches:
-        w = _point_weights(plan, b)
-        ex = np.asarray(exact(b.points.reshape(-1, plan.D)), dtype=np.float64).reshape(w.shape)
+    for w, pts in _quadrature_sets(plan):
+        ex = np.asarray(exact(pts), dtype=np.float64).reshape(-1)
         den2 += float(np.sum(w * ex ** 2))
     return num / math.sqrt(den2) if den2 > 0 else num
+
+
+def _local_coefficients(b, x):
+    n = len(b.cells)
+    mp = b.map_index.reshape(n, b.nbox)
+    loc = np.where(mp >= 0, x[np.maximum(mp, 0)], 0.0)
+    if b.map_coef is not None:
+        loc = loc * b.map_coef.reshape(n, b.nbox)
+    if b.tail_offsets is not None:
+        rows, cols = np.nonzero(mp <= -2)
+        for r, c in zip(rows, cols):
+            k = -(int(mp[r, c]) + 2)
+            lo, hi = b.tail_offsets[k], b.tail_offsets[k + 1]
+            loc[r, c] = float(np.dot(b.tail_coef[lo:hi], x[b.tail_index[lo:hi]]))
+    return loc
+
+
+def _point_item_values(plan, full_values):
+    """u at the points of every cell point item batch."""
+    x = np.asarray(full_values, dtype=np.float64)
+    D = plan.D
+    out = []
+    for b in plan.point_batches:
+        if b.kind != L.GRICO_ITEM_CELL:
+            continue
+        loc = _local_coefficients(b, x)
+        counts = np.diff(b.point_offsets)
+        item = np.repeat(np.arange(len(b.cells)), counts)
+        phi = np.ones((b.ref_points.shape[0], 1))
+        for a in range(D):
+            va, _ = fe_basis_table(b.ref_points[:, a], b.degree[a])
+            # box index axis 1 fastest: new = old + stride * m_a
+            phi = (va[:, :, None] * phi[:, None, :]).reshape(phi.shape[0], -1)
+        out.append(np.einsum("pm,pm->p", phi, loc[item]))
+    return out
 
 
 def _point_weights(plan, b):
@@ -546,16 +905,7 @@ def _point_values(plan, full_values):
     out = []
     for b in plan.batches:
         n = len(b.cells)
-        mp = b.map_index.reshape(n, b.nbox)
-        loc = np.where(mp >= 0, x[np.maximum(mp, 0)], 0.0)
-        if b.map_coef is not None:
-            loc = loc * b.map_coef.reshape(n, b.nbox)
-        if b.tail_offsets is not None:
-            rows, cols = np.nonzero(mp <= -2)
-            for r, c in zip(rows, cols):
-                k = -(int(mp[r, c]) + 2)
-                lo, hi = b.tail_offsets[k], b.tail_offsets[k + 1]
-                loc[r, c] = float(np.dot(b.tail_coef[lo:hi], x[b.tail_index[lo:hi]]))
+        loc = _local_coefficients(b, x)
         # box index is axis 1 fastest: t axes are [cell, mD, ..., m1]; contract m_a with B_a
         t = loc.reshape([n] + [b.degree[a] + 1 for a in reversed(range(D))])
         for a in range(D):

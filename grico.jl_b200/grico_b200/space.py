@@ -93,7 +93,12 @@ class HpSpace:
         self.options = options
         self.D = domain.D
         grid = domain.grid
-        leaves = grid.active_leaves() if active is None else np.asarray(active, dtype=np.int64)
+        if active is not None:
+            leaves = np.asarray(active, dtype=np.int64)
+        elif hasattr(domain, "active_leaves"):
+            leaves = domain.active_leaves()     # PhysicalDomain: drops :outside leaves
+        else:
+            leaves = grid.active_leaves()
         self.input_leaves = leaves
         degrees = options.degree.degrees(domain, leaves)
         cg = options.continuity == "cg"

@@ -117,6 +117,34 @@ typedef struct GricoCellBatchDesc {
   const double* kappa_points; /* NULL or [n_cells*prod(q)] pointwise gradient coefficient    */
 } GricoCellBatchDesc;
 
+/* Point-quadrature items (one cell's modes at an arbitrary list of reference points):
+ * non-tensor cells such as finite-cell cut cells (accumulators.jl:1022-1054), boundary faces
+ * and embedded surfaces (accumulators.jl:1133-1161, 1202-1214).  All items of a batch share the
+ * cell degree.  GRICO_ITEM_CELL uses the plan's mass/kappa form; GRICO_ITEM_NITSCHE is the
+ * symmetric Nitsche form TestChannels(-du/dn + eta*u, -u*n)
+ * (examples/annular_nitsche_fcm/driver.jl:52-62) with eta per item. */
+#define GRICO_ITEM_CELL 1
+#define GRICO_ITEM_NITSCHE 2
+
+typedef struct GricoPointBatchDesc {
+  int32_t n_items;
+  int32_t kind;               /* GRICO_ITEM_*                                               */
+  int32_t degree[3];
+  const int32_t* map_index;   /* [n_items*n_box], same encoding as GricoCellBatchDesc       */
+  const double* map_coef;
+  int64_t n_tail;
+  const int64_t* tail_offsets;
+  const int32_t* tail_index;
+  const double* tail_coef;
+  const double* cell_size;    /* [n_items*dim]                                              */
+  const int64_t* point_offsets; /* [n_items+1]                                              */
+  const double* ref_points;   /* [n_points*dim] reference coordinates in [-1,1]^dim         */
+  const double* weights;      /* [n_points] physical weights                                */
+  const double* normals;      /* [n_points*dim] unit normals (GRICO_ITEM_NITSCHE)           */
+  const double* eta;          /* [n_items] penalty (GRICO_ITEM_NITSCHE)                     */
+  const double* kappa_points; /* [n_points] or NULL (GRICO_ITEM_CELL)                       */
+} GricoPointBatchDesc;
+
 typedef struct GricoPlanDesc {
   int32_t dim;                /* 1..3 (sum-factorized kernels for 2 and 3)                  */
   int32_t form;               /* GRICO_FORM_*                                               */
@@ -141,6 +169,8 @@ typedef struct GricoPlanDesc {
   const int64_t* red_index;
   const double* red_coef;
   const double* red_shift;    /* [n_full] or NULL                                           */
+  int32_t n_point_batches;    /* point-quadrature items (cut cells, faces, surfaces)        */
+  const GricoPointBatchDesc* point_batches;
 } GricoPlanDesc;
 
 typedef struct GricoPlan GricoPlan;
@@ -160,7 +190,9 @@ int grico_apply(GricoPlan* plan, const void* x, void* y, int nrhs, int precision
 int grico_reduced_apply(GricoPlan* plan, const void* x, void* y, int nrhs, int precision, int flags,
                         void* stream);
 /* Reduced right-hand side P^T (b_phys - A shift) from the load tabulated at the quadrature
- * points of every batch (source[b] = [n_cells*prod(q)] for batch b, NULL => 0) — assembly.jl:917-933. */
+ * points of every batch: source[b] = [n_cells*prod(q)] for cell batch b, then one array of
+ * [n_points] per point batch (cells: f; Nitsche items: boundary data g giving
+ * TestChannels(eta*g, -g*n)); NULL => 0 — assembly.jl:917-933. */
 int grico_reduced_rhs(GricoPlan* plan, const double* const* source_points, double* b_reduced, int flags);
 /* Allocation-free variant of grico_reduced_rhs for callers that cannot allocate GPU memory
  * (code running while a stream is captured into a CUDA graph, host callbacks, services with a

@@ -485,6 +485,7 @@ class Space:
         nleaf = len(leaves)
         self.lookup = [dict() for _ in range(nleaf)]
         self.min_pivot = math.inf
+        self.noise_pivots = 0
         self.face_modes = {}
         self.boundary_terms = []
         if continuity == "cg":
@@ -616,6 +617,8 @@ class Space:
                 pidx = max(range(len(row.vars)), key=lambda i: row.vars[i])
                 pivot, pcoef = row.vars[pidx], row.coefs[pidx]
                 self.min_pivot = min(self.min_pivot, abs(pcoef))
+                if abs(pcoef) < 1e-10:
+                    self.noise_pivots += 1      # diagnostic only: a rounding-residue pivot
                 row.remove_var(pivot)
                 scale = -(1.0 / pcoef)
                 expr = Row()
@@ -705,7 +708,13 @@ class Plan:
     kappa_fn: optional callable x -> kappa(x) multiplying the gradient channel pointwise.
     dirichlet: list of (axis, side, value) with constant values."""
 
-    def __init__(self, space: Space, mu=0.0, kappa=1.0, kappa_fn=None, source=None, dirichlet=()):
+    def __init__(self, space: Space, mu=0.0, kappa=1.0, kappa_fn=None, source=None, dirichlet=(),
+                 cell_rules=None, surface_items=()):
+        """cell_rules: {leaf: (reference points [n, D], reference weights [n])} replacing the
+        tensor rule of those leaves (finite-cell cut cells, add_cell_quadrature!);
+        surface_items: [(leaf, reference points, physical weights, physical unit normals,
+        penalty, g)] symmetric Nitsche items (boundary faces or embedded surfaces)."""
+        cell_rules = cell_rules or {}
         self.space = space
         dom = space.domain
         D = space.D
@@ -714,6 +723,12 @@ class Plan:
         self.ndofs = space.ndofs
         self.cells = []
         for li, leaf in enumerate(snap.leaves):
+            if leaf in cell_rules:
+                ref, wref = cell_rules[leaf]
+                c = self._point_item(li, leaf, ref)
+                c["w"] = np.asarray(wref, dtype=np.float64) * dom.det_biunit(leaf)
+                self.cells.append(c)
+                continue
             q = space.qshape[li]
             rules = [gauss_legendre_rule(n) for n in q]
             degs = space.degrees[li]
@@ -759,6 +774,15 @@ class Plan:
             terms = space.leaf_terms[li]
             self.cells.append(dict(leaf=leaf, modes=modes, terms=terms, w=w, pts=pts, vals=vals, grads=grads,
                                    axis_v=axis_v, axis_g=axis_g, q=q, degs=degs))
+        self.surfaces = []
+        for (leaf, ref, wphys, nphys, penalty, g) in surface_items:
+            li = snap.leaf_to_index[leaf]
+            c = self._point_item(li, leaf, ref)
+            c["w"] = np.asarray(wphys, dtype=np.float64)
+            c["normals"] = np.asarray(nphys, dtype=np.float64).reshape(-1, D)
+            c["eta"] = penalty / min(dom.cell_size(leaf, a) for a in range(D))
+            c["g"] = g
+            self.surfaces.append(c)
         self.colors = self._colour()
         self.fixed, self.fixed_values, self.rows = self._dirichlet(dirichlet)
         self.fixed_mask = np.zeros(self.ndofs + 1, dtype=bool)
@@ -767,6 +791,54 @@ class Plan:
         for (pivot, _, _, _) in self.rows:
             self.blocked[pivot] = True
         self._reduced_map()
+
+    def _point_item(self, li, leaf, ref):
+        """Full value/gradient tables of one leaf's modes at arbitrary reference points
+        (_compile_field_values, integration.jl:2527-2560, non-tensor branch)."""
+        space, dom, D = self.space, self.space.domain, self.space.D
+        degs = space.degrees[li]
+        modes = space.leaf_modes[li]
+        ref = np.asarray(ref, dtype=np.float64).reshape(-1, D)
+        npts = ref.shape[0]
+        ch = [dom.center_half(leaf, a) for a in range(D)]
+        vals = np.ones((len(modes), npts))
+        grads = np.ones((D, len(modes), npts))
+        pts = np.zeros((npts, D))
+        for p in range(npts):
+            tv, tg = [], []
+            for a in range(D):
+                v, d = fe_basis_values_and_derivatives(ref[p, a], degs[a])
+                tv.append(v)
+                tg.append([dd / ch[a][1] for dd in d])
+                pts[p, a] = ch[a][0] + ref[p, a] * ch[a][1]
+            for i, m in enumerate(modes):
+                val = 1.0
+                for a in range(D):
+                    val *= tv[a][m[a]]
+                vals[i, p] = val
+                for a in range(D):
+                    g = 1.0
+                    for b in range(D):
+                        g *= tg[b][m[b]] if b == a else tv[b][m[b]]
+                    grads[a, i, p] = g
+        return dict(leaf=leaf, modes=modes, terms=space.leaf_terms[li], pts=pts, vals=vals, grads=grads,
+                    q=None, degs=degs)
+
+    def surface_local_apply(self, c, xloc):
+        """TestChannels(-du/dn + eta*u, -u*n) at every point (driver.jl:52-62), projected with
+        the full tables (_accumulate_one_sided_apply_basis!, accumulators.jl:1133-1161)."""
+        D = self.space.D
+        u = c["vals"].T @ xloc
+        g = np.stack([c["grads"][a].T @ xloc for a in range(D)])
+        dn = sum(g[a] * c["normals"][:, a] for a in range(D))
+        t0 = c["w"] * (-dn + c["eta"] * u)
+        return c["vals"] @ t0 + sum(c["grads"][a] @ (-c["w"] * u * c["normals"][:, a]) for a in range(D))
+
+    def _items(self):
+        for c in self.cells:
+            yield c, self.local_apply
+        for c in self.surfaces:
+            yield c, self.surface_local_apply
 
     # -- colouring (plans.jl:368-424) ------------------------------------------------
     def _colour(self):
@@ -937,8 +1009,7 @@ class Plan:
     def local_apply(self, c, xloc):
         w = c["w"]
         u = c["vals"].T @ xloc
-        g = np.einsum("ainp,n->aip", c["grads"][:, :, None, :], xloc)[:, :, 0] if False else \
-            np.stack([c["grads"][a].T @ xloc for a in range(self.space.D)])
+        g = np.stack([c["grads"][a].T @ xloc for a in range(self.space.D)])
         kap = self.kappa * (np.array([self.kappa_fn(tuple(p)) for p in c["pts"]]) if self.kappa_fn else 1.0)
         t0 = w * self.mu * u
         tg = w * kap * g
@@ -962,6 +1033,14 @@ class Plan:
                             if self.fixed_mask[d] or self.blocked[d]:
                                 continue
                             y1[d] += cc * yloc[i]
+        for c in self.surfaces:
+            xloc = np.array([sum(cc * x1[d] for (d, cc) in t) for t in c["terms"]])
+            yloc = self.surface_local_apply(c, xloc)
+            for i, t in enumerate(c["terms"]):
+                for (d, cc) in t:
+                    if self.fixed_mask[d] or self.blocked[d]:
+                        continue
+                    y1[d] += cc * yloc[i]
         for d in self.fixed:
             y1[d] = x1[d]
         for (pivot, idx, co, _) in self.rows:
@@ -974,9 +1053,9 @@ class Plan:
     def apply_physical(self, x):
         x1 = np.concatenate([[0.0], np.asarray(x, dtype=np.float64)])
         y1 = np.zeros(self.ndofs + 1)
-        for c in self.cells:
+        for c, fn in self._items():
             xloc = np.array([sum(cc * x1[d] for (d, cc) in t) for t in c["terms"]])
-            yloc = self.local_apply(c, xloc)
+            yloc = fn(c, xloc)
             for i, t in enumerate(c["terms"]):
                 for (d, cc) in t:
                     y1[d] += cc * yloc[i]
@@ -1012,11 +1091,17 @@ class Plan:
             for i, t in enumerate(c["terms"]):
                 for (d, cc) in t:
                     out[d] += cc * cc * diag[i]
+        for c in self.surfaces:
+            dn = sum(c["grads"][a] * c["normals"][:, a][None, :] for a in range(D))
+            diag = (c["eta"] * c["vals"] ** 2 - 2.0 * c["vals"] * dn) @ c["w"]
+            for i, t in enumerate(c["terms"]):
+                for (d, cc) in t:
+                    out[d] += cc * cc * diag[i]
         return out[1:]
 
     def reduced_diagonal(self):
         """Direct copy when the map is an injection, else None (assembly.jl:662-726)."""
-        for c in self.cells:
+        for c in self.cells + self.surfaces:
             for t in c["terms"]:
                 if len(t) != 1:
                     return None
@@ -1042,12 +1127,25 @@ class Plan:
 
     def rhs_physical(self):
         out = np.zeros(self.ndofs + 1)
+        D = self.space.D
         for c in self.cells:
+            if self.source is None:
+                break
             f = np.array([self.source(tuple(p)) for p in c["pts"]])
             loc = c["vals"] @ (c["w"] * f)
             for i, t in enumerate(c["terms"]):
                 if loc[i] == 0.0:
                     continue
+                for (d, cc) in t:
+                    out[d] += cc * loc[i]
+        for c in self.surfaces:
+            if c["g"] is None:
+                continue
+            g = np.array([c["g"](tuple(p)) for p in c["pts"]])
+            # TestChannels(eta*g, -g*n) (driver.jl:65-76)
+            loc = c["vals"] @ (c["w"] * c["eta"] * g) + sum(c["grads"][a] @ (-c["w"] * g * c["normals"][:, a])
+                                                            for a in range(D))
+            for i, t in enumerate(c["terms"]):
                 for (d, cc) in t:
                     out[d] += cc * loc[i]
         return out[1:]
@@ -1265,3 +1363,165 @@ class Multigrid:
 
     def apply(self, r):
         return self.vcycle(len(self.plans) - 1, r)
+
+
+# ---------------------------------------------------------------------------
+# Finite cells and embedded surfaces: src/regions.jl, src/embedded.jl
+# ---------------------------------------------------------------------------
+
+def classifier_value(classifier, x):
+    """regions.jl:819-830; `classifier` takes an [n, D] array (one row here)."""
+    v = classifier(np.asarray(x, dtype=np.float64).reshape(1, -1))
+    v = np.asarray(v).reshape(-1)[0]
+    if isinstance(v, (bool, np.bool_)):
+        return -1.0 if v else 1.0
+    v = float(v)
+    if not math.isfinite(v):
+        raise ValueError("finite-cell classifier values must be finite")
+    return v
+
+
+def map_from_biunit_cube(dom: Domain, leaf, xi):
+    """center + xi * half per axis (geometry.jl:571-578)."""
+    out = []
+    for a in range(dom.D):
+        c, h = dom.center_half(leaf, a)
+        out.append(c + xi[a] * h)
+    return out
+
+
+def _subcell_corner(lower, upper, mask):
+    """regions.jl:424-427"""
+    return [upper[a] if (mask >> a) & 1 else lower[a] for a in range(len(lower))]
+
+
+def classify_subcell(dom: Domain, leaf, classifier, lower, upper):
+    """regions.jl:736-757: corners then centre; 'outside' / 'inside' / 'cut'."""
+    D = dom.D
+    neg = pos = False
+    for mask in range(1 << D):
+        v = classifier_value(classifier, map_from_biunit_cube(dom, leaf, _subcell_corner(lower, upper, mask)))
+        neg |= v < 0.0
+        pos |= v > 0.0
+    center = [0.5 * (lower[a] + upper[a]) for a in range(D)]
+    v = classifier_value(classifier, map_from_biunit_cube(dom, leaf, center))
+    neg |= v < 0.0
+    pos |= v > 0.0
+    if not neg:
+        return "outside"
+    if not pos:
+        return "inside"
+    return "cut"
+
+
+def classify_leaf(dom: Domain, leaf, classifier):
+    D = dom.D
+    return classify_subcell(dom, leaf, classifier, [-1.0] * D, [1.0] * D)
+
+
+def physical_active_leaves(dom: Domain, classifier):
+    """regions.jl:267-279"""
+    leaves = [l for l in dom.grid.active_leaves() if classify_leaf(dom, l, classifier) != "outside"]
+    if not leaves:
+        raise ValueError("physical domains must contain at least one active physical leaf")
+    return leaves
+
+
+def _tensor_points(qshape):
+    """TensorQuadrature points and weights, axis 1 fastest (quadrature.jl:219-226)."""
+    D = len(qshape)
+    rules = [gauss_legendre_rule(q) for q in qshape]
+    pts, wts = [], []
+    for p in range(int(np.prod(qshape))):
+        idx = mode_from_linear(p, tuple(q - 1 for q in qshape))
+        pts.append([rules[a][0][idx[a]] for a in range(D)])
+        w = 1.0
+        for a in range(D):
+            w *= rules[a][1][idx[a]]
+        wts.append(w)
+    return pts, wts
+
+
+def _append_subcell_quadrature(points, weights, dom, leaf, classifier, base, lower, upper, filter_points):
+    """regions.jl:759-792 plus the sliver fallback of regions.jl:794-817."""
+    D = dom.D
+    center = [0.5 * (lower[a] + upper[a]) for a in range(D)]
+    half = [0.5 * (upper[a] - lower[a]) for a in range(D)]
+    scale = 1.0
+    for a in range(D):
+        scale *= half[a]
+    appended = False
+    for eta, w in zip(*base):
+        xi = [center[a] + half[a] * eta[a] for a in range(D)]
+        if filter_points and not classifier_value(classifier, map_from_biunit_cube(dom, leaf, xi)) < 0.0:
+            continue
+        points.append(xi)
+        weights.append(w * scale)
+        appended = True
+    if filter_points and not appended:
+        total = (1 << D) + 1
+        vol = 1.0
+        for a in range(D):
+            vol *= upper[a] - lower[a]
+        sw = vol / total
+        if classifier_value(classifier, map_from_biunit_cube(dom, leaf, center)) < 0.0:
+            points.append(center)
+            weights.append(sw)
+        for mask in range(1 << D):
+            xi = _subcell_corner(lower, upper, mask)
+            if classifier_value(classifier, map_from_biunit_cube(dom, leaf, xi)) < 0.0:
+                points.append(xi)
+                weights.append(sw)
+
+
+def _collect_candidates(points, weights, dom, leaf, classifier, base, lower, upper, depth, max_depth):
+    """regions.jl:477-510 (depth-first, child masks in increasing order)."""
+    cls = classify_subcell(dom, leaf, classifier, lower, upper)
+    if cls == "inside":
+        _append_subcell_quadrature(points, weights, dom, leaf, classifier, base, lower, upper, False)
+        return
+    if cls == "outside":
+        return
+    if depth >= max_depth:
+        _append_subcell_quadrature(points, weights, dom, leaf, classifier, base, lower, upper, True)
+        return
+    D = dom.D
+    mid = [0.5 * (lower[a] + upper[a]) for a in range(D)]
+    for mask in range(1 << D):
+        cl = [mid[a] if (mask >> a) & 1 else lower[a] for a in range(D)]
+        cu = [upper[a] if (mask >> a) & 1 else mid[a] for a in range(D)]
+        _collect_candidates(points, weights, dom, leaf, classifier, base, cl, cu, depth + 1, max_depth)
+
+
+def finite_cell_candidates(dom: Domain, leaf, qshape, classifier, max_depth):
+    """Unfitted candidate rule of one leaf: None outside, the tensor rule inside, the octree
+    candidates when cut (regions.jl:297-322 before the moment fit)."""
+    D = dom.D
+    cls = classify_leaf(dom, leaf, classifier)
+    if cls == "outside":
+        return None
+    base = _tensor_points(qshape)
+    if cls == "inside":
+        return np.array(base[0]), np.array(base[1])
+    points, weights = [], []
+    _collect_candidates(points, weights, dom, leaf, classifier, base, [-1.0] * D, [1.0] * D, 0, max_depth)
+    if not points:
+        return None
+    return np.array(points), np.array(weights)
+
+
+def physical_surface_data(dom: Domain, leaf, ref_weights, ref_normals):
+    """integration.jl:2501-2516: w * det(J) / |J n|, J^-1 n / |J^-1 n| for diagonal J."""
+    D = dom.D
+    J = [0.5 * dom.cell_size(leaf, a) for a in range(D)]
+    det = 1.0
+    for a in range(D):
+        det *= J[a]
+    ws, ns = [], []
+    for w, n in zip(ref_weights, ref_normals):
+        mapped = math.sqrt(sum((J[a] * n[a]) ** 2 for a in range(D)))
+        ws.append(w * det / mapped)
+        t = [n[a] / J[a] for a in range(D)]
+        mag = math.sqrt(sum(v * v for v in t))
+        ns.append([v / mag for v in t])
+    return np.array(ws), np.array(ns)

@@ -68,15 +68,17 @@ def test_dof_maps_match_oracle(name, basis, p):
     osp = go.Space(od, p, basis=basis)
     psp = gb.HpSpace(pd, gb.SpaceOptions(basis=gb.TrunkBasis() if basis == "trunk" else gb.FullTensorBasis(),
                                          degree=gb.UniformDegree(p)))
-    assert osp.ndofs == psp.scalar_dof_count
     assert list(osp.snapshot.leaves) == [int(v) for v in psp.leaves]
     if osp.min_pivot < 1e-10:
         # A redundant continuity row cancelled to rounding level but stayed above the reference's
-        # cleanup tolerance (continuity.jl:1213-1223), so its pivot is rounding noise: the
-        # reference's own result depends on the last bits of its LU.  Check that the product
-        # space is continuous instead of comparing coefficients.
+        # cleanup tolerance (continuity.jl:1213-1223), so its pivot is rounding noise that
+        # eliminates a free variable: the reference's own result depends on the last bits of
+        # its LU.  The product drops such rows, so it keeps one more dof per noise pivot; check
+        # that count and that the product space is continuous.
+        assert psp.scalar_dof_count == osp.ndofs + osp.noise_pivots
         _check_continuity(pd, psp, p)
         return
+    assert osp.ndofs == psp.scalar_dof_count
     for li, leaf in enumerate(osp.snapshot.leaves):
         assert len(osp.leaf_modes[li]) == psp.local_mode_count(leaf)
         for mode, terms in zip(osp.leaf_modes[li], osp.leaf_terms[li]):
