@@ -102,7 +102,8 @@ def annulus(refine=None, degree=None, depth=None, penalty=None, hanging=False, w
     return oplan, prob, plan, exact
 
 
-def shell(refine=None, degree=None, depth=None, device=True, source=True, oracle=True, tolerance=1e-8):
+def shell(refine=None, degree=None, depth=None, device=True, source=True, oracle=True, tolerance=1e-8,
+          cell_measure=None):
     """3-D shell 0.4 < |x - c| < 0.9 in [0, 2]^3 with Nitsche spheres, u = sin 2x cos 3y e^{z/2}."""
     o = dict(SHELL)
     o.update({k: v for k, v in dict(refine=refine, degree=degree, depth=depth).items() if v is not None})
@@ -115,7 +116,7 @@ def shell(refine=None, degree=None, depth=None, device=True, source=True, oracle
     bg = gb.Domain((0.0, 0.0, 0.0), (2.0, 2.0, 2.0), (1, 1, 1))
     go.uniform_refine(od.grid, o["refine"])
     gb.uniform_refine(bg, o["refine"])
-    pd = gb.PhysicalDomain(bg, gb.ImplicitRegion(lev, subdivision_depth=o["depth"]))
+    pd = gb.PhysicalDomain(bg, gb.ImplicitRegion(lev, subdivision_depth=o["depth"]), cell_measure=cell_measure)
     sp = gb.HpSpace(pd, gb.SpaceOptions(basis=gb.FullTensorBasis(), degree=gb.UniformDegree(p)))
     u = gb.ScalarField(sp)
     prob = gb.AffineProblem(u)
@@ -130,6 +131,7 @@ def shell(refine=None, degree=None, depth=None, device=True, source=True, oracle
     gb.add_surface_quadrature(prob, surfaces)
     oplan = None
     if oracle:
+        assert cell_measure is None
         osp = go.Space(od, p, basis="full", leaves=go.physical_active_leaves(od, lev))
         oplan = go.Plan(osp, mu=0.0, kappa=1.0, source=_scalar(f), cell_rules=_oracle_rules(od, osp, lev, o["depth"]),
                         surface_items=_oracle_surfaces(od, surfaces, penalty, shell_exact))
@@ -180,7 +182,9 @@ def box_nitsche(dim=2, degree=3, refine=2, penalty=20.0, mu=0.0, device=True):
         scale = math.ldexp(scale, -(dim - 1))
         nrm = np.zeros((len(wts), dim))
         nrm[:, axis - 1] = -1.0 if side == go.LOWER else 1.0
-        items.append((leaf, pts, np.array(wts) * scale, nrm, penalty, _scalar(exact)))
+        # face rules carry tangential weights only (integration.jl:2846-2862); the 1-point
+        # Gauss rule used for the normal axis above has weight 2
+        items.append((leaf, pts, 0.5 * np.array(wts) * scale, nrm, penalty, _scalar(exact)))
     oplan = go.Plan(osp, mu=mu, kappa=1.0, source=_scalar(f), surface_items=items)
     plan = gb.compile(prob, device=device)
     return oplan, prob, plan, exact
