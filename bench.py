@@ -160,10 +160,12 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def solve_legs(gb, L, plan, prob):
-    """CG + hp-GMG on the same workload with f = 3 pi^2 prod sin(pi x_i) (exact u = prod sin):
-    device seconds of the Krylov solve (CUDA events inside grico_cg_solve), iterations and the
-    relative L2 error against the exact solution (verification.jl:297-304)."""
+def solve_legs(gb, L, plan, prob, target=1e-8):
+    """Time to relative L2 error <= `target` on the same workload with f = 3 pi^2 prod sin(pi x_i)
+    (exact u = prod sin): each method solves with ||r|| <= rtol ||b|| for rtol = 1e-6, 1e-7, ...
+    and reports the first solve whose relative L2 error (verification.jl:297-304) meets the
+    target.  Times are device seconds of the Krylov solve (CUDA events inside grico_cg_solve);
+    the hierarchy set-up is reported separately."""
     import ctypes as C
 
     from grico_b200.multigrid import GeometricMultigridPreconditioner, build_multigrid
@@ -172,25 +174,40 @@ def solve_legs(gb, L, plan, prob):
     prob.rhs_operators = [gb.Load(lambda X: 3.0 * np.pi ** 2 * exact(X))]
     b = gb.reduced_rhs(plan)
     legs = {
-        "fp64_cg_gmg_jacobi_v22 (reference method)": GeometricMultigridPreconditioner(),
-        "fp64_cg_gmg_chebyshev3_v11": GeometricMultigridPreconditioner(smoother="chebyshev", pre_smoothing_steps=1,
-                                                                        post_smoothing_steps=1),
+        "fp64_cg_gmg_jacobi_v22 (reference method)": (GeometricMultigridPreconditioner(), 2000),
+        "fp64_cg_gmg_chebyshev3_v22 (plain FP64 GPU)": (
+            GeometricMultigridPreconditioner(smoother="chebyshev", pre_smoothing_steps=2, post_smoothing_steps=2), 500),
+        "mixed_cg_fp64_gmg_chebyshev3_v22_fp32": (
+            GeometricMultigridPreconditioner(smoother="chebyshev", pre_smoothing_steps=2, post_smoothing_steps=2,
+                                             precision="fp32"), 500),
+        "mixed_cg_fp64_gmg_chebyshev3_v11_fp32": (
+            GeometricMultigridPreconditioner(smoother="chebyshev", pre_smoothing_steps=1, post_smoothing_steps=1,
+                                             precision="fp32"), 500),
     }
     out = {}
-    for name, opts in legs.items():
+    for name, (opts, maxiter) in legs.items():
         t0 = time.perf_counter()
         mg = build_multigrid(plan, opts)
         setup = time.perf_counter() - t0
-        x = np.zeros(plan.n_reduced)
-        so = L.GricoSolveOptions(1e-9, 0.0, 2000, L.GRICO_PRECOND_MULTIGRID, 30, 0)
-        rep = L.GricoSolveReport()
-        rc = L.lib().grico_cg_solve(plan.handle, mg.handle, L.ptr(b, C.c_double), L.ptr(x, C.c_double),
-                                    C.byref(so), C.byref(rep), L.GRICO_FLAG_HOST_POINTERS)
-        state = gb.State(plan, gb.expand_reduced(plan, x), rep)
-        err = gb.relative_l2_error(state, exact)
-        out[name] = {"status": int(rc), "iterations": int(rep.iterations), "solve_seconds": float(rep.seconds),
-                     "host_setup_seconds": setup, "levels": len(mg.plans), "relative_l2_error": err,
-                     "stop": "||r|| <= 1e-9 ||b||"}
+        tries = []
+        hit = None
+        for rtol in (1e-4, 1e-5, 1e-6, 1e-7, 1e-8, 1e-9, 1e-10):
+            x = np.zeros(plan.n_reduced)
+            so = L.GricoSolveOptions(rtol, 0.0, maxiter, L.GRICO_PRECOND_MULTIGRID, 30, 0)
+            rep = L.GricoSolveReport()
+            rc = L.lib().grico_cg_solve(plan.handle, mg.handle, L.ptr(b, C.c_double), L.ptr(x, C.c_double),
+                                        C.byref(so), C.byref(rep), L.GRICO_FLAG_HOST_POINTERS)
+            err = gb.relative_l2_error(gb.State(plan, gb.expand_reduced(plan, x), rep), exact)
+            tries.append({"rtol": rtol, "status": int(rc), "iterations": int(rep.iterations),
+                          "solve_seconds": float(rep.seconds), "relative_l2_error": err})
+            if rc == 0 and err <= target:
+                hit = tries[-1]
+                break
+            if rc != 0:
+                break
+        out[name] = {"time_to_target_seconds": hit["solve_seconds"] if hit else None,
+                     "iterations": hit["iterations"] if hit else None, "target_relative_l2": target,
+                     "host_setup_seconds": setup, "levels": len(mg.plans), "tries": tries}
         del mg
     return out
 

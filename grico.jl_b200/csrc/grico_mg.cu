@@ -9,6 +9,11 @@
 // The coarsest level is solved in FP64 with the dense Cholesky factor of its reduced matrix
 // (common.jl:272-330); the factor is inverted once on the host and applied as a dense
 // matrix-vector product.
+//
+// Working precision: with GRICO_PREC_FP32 every level below the caller (smoother applies,
+// residuals, transfers, Chebyshev/Jacobi updates) runs in FP32 on FP32 copies of D^-1 and of
+// the transfer values; the caller's residual and correction stay FP64 (the outer Krylov
+// iteration owns them) and the coarsest solve stays FP64.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -25,10 +30,13 @@ struct GricoMultigrid {
     int64_t nf = 0, nc = 0;
     grico::DevBuf p_off, p_idx, p_val;  // fine rows
     grico::DevBuf r_off, r_idx, r_val;  // coarse rows (transpose)
+    grico::DevBuf p_val32, r_val32;     // FP32 copies (FP32 working precision)
   };
   std::vector<GricoPlan*> levels;
   std::vector<Transfer> xfer;
-  std::vector<grico::DevBuf> dinv, b, x, r, t, d;
+  std::vector<grico::DevBuf> dinv, b, x, r, t, d;           // FP64 level vectors
+  std::vector<grico::DevBuf> dinv32, b32, x32, r32, t32, d32;  // FP32 level vectors
+  grico::DevBuf coarse_b, coarse_x;                         // FP64 coarse solve in FP32 mode
   std::vector<double> lmax;
   grico::DevBuf coarse_inv;
   int64_t n0 = 0;
@@ -41,39 +49,47 @@ namespace grico {
 
 namespace {
 
+template <typename T>
 __global__ void csr_gather(const int64_t* __restrict__ off, const int64_t* __restrict__ idx,
-                           const double* __restrict__ val, const double* __restrict__ x, double* __restrict__ y,
+                           const T* __restrict__ val, const T* __restrict__ x, T* __restrict__ y,
                            int64_t nrows, int accumulate) {
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nrows; i += int64_t(gridDim.x) * blockDim.x) {
-    double s = 0.0;
+    T s = T(0);
     for (int64_t t = off[i]; t < off[i + 1]; ++t) s += val[t] * x[idx[t]];
     y[i] = accumulate ? y[i] + s : s;
   }
 }
 
 // x += w * dinv * (b - ax)
-__global__ void jacobi_smooth(double* __restrict__ x, const double* __restrict__ b, const double* __restrict__ ax,
-                              const double* __restrict__ dinv, double w, int64_t n) {
+template <typename T>
+__global__ void jacobi_smooth(T* __restrict__ x, const T* __restrict__ b, const T* __restrict__ ax,
+                              const T* __restrict__ dinv, T w, int64_t n) {
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
     x[i] += w * dinv[i] * (b[i] - ax[i]);
 }
 
 // d = c1*d + c2*dinv*(b - ax); x += d
-__global__ void chebyshev_step(double* __restrict__ x, double* __restrict__ d, const double* __restrict__ b,
-                               const double* __restrict__ ax, const double* __restrict__ dinv, double c1, double c2,
-                               int64_t n) {
+template <typename T>
+__global__ void chebyshev_step(T* __restrict__ x, T* __restrict__ d, const T* __restrict__ b,
+                               const T* __restrict__ ax, const T* __restrict__ dinv, T c1, T c2, int64_t n) {
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-    double di = c1 * d[i] + c2 * dinv[i] * (b[i] - ax[i]);
+    T di = c1 * d[i] + c2 * dinv[i] * (b[i] - ax[i]);
     d[i] = di;
     x[i] += di;
   }
 }
 
 // r = b - ax
-__global__ void residual_kernel(double* __restrict__ r, const double* __restrict__ b, const double* __restrict__ ax,
-                                int64_t n) {
+template <typename T>
+__global__ void residual_kernel(T* __restrict__ r, const T* __restrict__ b, const T* __restrict__ ax, int64_t n) {
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
     r[i] = b[i] - ax[i];
+}
+
+template <typename S, typename D>
+__global__ void cast_kernel(const S* __restrict__ x, D* __restrict__ y, int64_t n) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    y[i] = D(x[i]);
 }
 
 // y = M x for a dense row-major n x n matrix (one warp per row)
@@ -120,19 +136,47 @@ void cholesky_solve(const std::vector<double>& l, int64_t n, std::vector<double>
   }
 }
 
-void level_apply(GricoMultigrid* mg, int l, const double* x, double* y, cudaStream_t st) {
-  run_apply<double>(mg->levels[l], true, x, y, 1, st);
+template <typename T>
+struct LevelBufs;
+template <>
+struct LevelBufs<double> {
+  static double* b(GricoMultigrid* m, int l) { return m->b[l].get<double>(); }
+  static double* x(GricoMultigrid* m, int l) { return m->x[l].get<double>(); }
+  static double* r(GricoMultigrid* m, int l) { return m->r[l].get<double>(); }
+  static double* t(GricoMultigrid* m, int l) { return m->t[l].get<double>(); }
+  static double* d(GricoMultigrid* m, int l) { return m->d[l].get<double>(); }
+  static const double* dinv(GricoMultigrid* m, int l) { return m->dinv[l].get<double>(); }
+  static const double* pval(GricoMultigrid::Transfer& X) { return X.p_val.get<double>(); }
+  static const double* rval(GricoMultigrid::Transfer& X) { return X.r_val.get<double>(); }
+};
+template <>
+struct LevelBufs<float> {
+  static float* b(GricoMultigrid* m, int l) { return m->b32[l].get<float>(); }
+  static float* x(GricoMultigrid* m, int l) { return m->x32[l].get<float>(); }
+  static float* r(GricoMultigrid* m, int l) { return m->r32[l].get<float>(); }
+  static float* t(GricoMultigrid* m, int l) { return m->t32[l].get<float>(); }
+  static float* d(GricoMultigrid* m, int l) { return m->d32[l].get<float>(); }
+  static const float* dinv(GricoMultigrid* m, int l) { return m->dinv32[l].get<float>(); }
+  static const float* pval(GricoMultigrid::Transfer& X) { return X.p_val32.get<float>(); }
+  static const float* rval(GricoMultigrid::Transfer& X) { return X.r_val32.get<float>(); }
+};
+
+template <typename T>
+void level_apply(GricoMultigrid* mg, int l, const T* x, T* y, cudaStream_t st) {
+  run_apply<T>(mg->levels[l], true, x, y, 1, st);
 }
 
-void smooth(GricoMultigrid* mg, int l, double* x, const double* b, int steps, cudaStream_t st) {
+template <typename T>
+void smooth(GricoMultigrid* mg, int l, T* x, const T* b, int steps, cudaStream_t st) {
+  using B = LevelBufs<T>;
   const int64_t n = mg->levels[l]->n_red;
-  double* t = mg->t[l].get<double>();
-  const double* dinv = mg->dinv[l].get<double>();
+  T* t = B::t(mg, l);
+  const T* dinv = B::dinv(mg, l);
   if (steps <= 0) return;
   if (mg->opts.smoother == GRICO_SMOOTHER_JACOBI) {
     for (int s = 0; s < steps; ++s) {
-      level_apply(mg, l, x, t, st);
-      jacobi_smooth<<<blocks(n), 256, 0, st>>>(x, b, t, dinv, mg->opts.jacobi_omega, n);
+      level_apply<T>(mg, l, x, t, st);
+      jacobi_smooth<T><<<blocks(n), 256, 0, st>>>(x, b, t, dinv, T(mg->opts.jacobi_omega), n);
     }
     return;
   }
@@ -140,43 +184,57 @@ void smooth(GricoMultigrid* mg, int l, double* x, const double* b, int steps, cu
   const double lmin = lmax * mg->opts.chebyshev_lower;
   const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin);
   const double sigma = theta / delta;
-  double* d = mg->d[l].get<double>();
+  T* d = B::d(mg, l);
   for (int s = 0; s < steps; ++s) {
     double rho_old = 1.0 / sigma;
     for (int k = 0; k < mg->opts.chebyshev_degree; ++k) {
-      level_apply(mg, l, x, t, st);
+      level_apply<T>(mg, l, x, t, st);
       if (k == 0) {
-        chebyshev_step<<<blocks(n), 256, 0, st>>>(x, d, b, t, dinv, 0.0, 1.0 / theta, n);
+        chebyshev_step<T><<<blocks(n), 256, 0, st>>>(x, d, b, t, dinv, T(0), T(1.0 / theta), n);
       } else {
         const double rho = 1.0 / (2.0 * sigma - rho_old);
-        chebyshev_step<<<blocks(n), 256, 0, st>>>(x, d, b, t, dinv, rho * rho_old, 2.0 * rho / delta, n);
+        chebyshev_step<T><<<blocks(n), 256, 0, st>>>(x, d, b, t, dinv, T(rho * rho_old), T(2.0 * rho / delta), n);
         rho_old = rho;
       }
     }
   }
 }
 
-void vcycle(GricoMultigrid* mg, int l, double* x, const double* b, cudaStream_t st) {
+void coarse_solve(GricoMultigrid* mg, double* x, const double* b, cudaStream_t st) {
+  const int64_t n = mg->levels[0]->n_red;
+  if (n > 0) dense_matvec<<<int((n * 32 + 255) / 256), 256, 0, st>>>(mg->coarse_inv.get<double>(), b, x, n);
+}
+
+void coarse_solve(GricoMultigrid* mg, float* x, const float* b, cudaStream_t st) {
+  // the coarsest solve stays FP64
+  const int64_t n = mg->levels[0]->n_red;
+  if (n == 0) return;
+  cast_kernel<float, double><<<blocks(n), 256, 0, st>>>(b, mg->coarse_b.get<double>(), n);
+  coarse_solve(mg, mg->coarse_x.get<double>(), mg->coarse_b.get<double>(), st);
+  cast_kernel<double, float><<<blocks(n), 256, 0, st>>>(mg->coarse_x.get<double>(), x, n);
+}
+
+template <typename T>
+void vcycle(GricoMultigrid* mg, int l, T* x, const T* b, cudaStream_t st) {
+  using B = LevelBufs<T>;
   const int64_t n = mg->levels[l]->n_red;
-  cudaMemsetAsync(x, 0, sizeof(double) * n, st);
   if (l == 0) {
-    if (n > 0) dense_matvec<<<int((n * 32 + 255) / 256), 256, 0, st>>>(mg->coarse_inv.get<double>(), b, x, n);
+    coarse_solve(mg, x, b, st);
     return;
   }
-  smooth(mg, l, x, b, mg->opts.pre_steps, st);
-  double* t = mg->t[l].get<double>();
-  double* r = mg->r[l].get<double>();
-  level_apply(mg, l, x, t, st);
-  residual_kernel<<<blocks(n), 256, 0, st>>>(r, b, t, n);
+  cudaMemsetAsync(x, 0, sizeof(T) * n, st);
+  smooth<T>(mg, l, x, b, mg->opts.pre_steps, st);
+  T* t = B::t(mg, l);
+  T* r = B::r(mg, l);
+  level_apply<T>(mg, l, x, t, st);
+  residual_kernel<T><<<blocks(n), 256, 0, st>>>(r, b, t, n);
   auto& X = mg->xfer[l - 1];
-  double* bc = mg->b[l - 1].get<double>();
-  double* xc = mg->x[l - 1].get<double>();
-  csr_gather<<<blocks(X.nc), 256, 0, st>>>(X.r_off.get<int64_t>(), X.r_idx.get<int64_t>(), X.r_val.get<double>(), r,
-                                           bc, X.nc, 0);
-  vcycle(mg, l - 1, xc, bc, st);
-  csr_gather<<<blocks(X.nf), 256, 0, st>>>(X.p_off.get<int64_t>(), X.p_idx.get<int64_t>(), X.p_val.get<double>(), xc,
-                                           x, X.nf, 1);
-  smooth(mg, l, x, b, mg->opts.post_steps, st);
+  T* bc = B::b(mg, l - 1);
+  T* xc = B::x(mg, l - 1);
+  csr_gather<T><<<blocks(X.nc), 256, 0, st>>>(X.r_off.get<int64_t>(), X.r_idx.get<int64_t>(), B::rval(X), r, bc, X.nc, 0);
+  vcycle<T>(mg, l - 1, xc, bc, st);
+  csr_gather<T><<<blocks(X.nf), 256, 0, st>>>(X.p_off.get<int64_t>(), X.p_idx.get<int64_t>(), B::pval(X), xc, x, X.nf, 1);
+  smooth<T>(mg, l, x, b, mg->opts.post_steps, st);
 }
 
 }  // namespace
@@ -184,7 +242,16 @@ void vcycle(GricoMultigrid* mg, int l, double* x, const double* b, cudaStream_t 
 int mg_vcycle_device(GricoMultigrid* mg, const double* r, double* z, cudaStream_t st) {
   if (!mg) return GRICO_ERR_INVALID;
   const int L = int(mg->levels.size());
-  vcycle(mg, L - 1, z, r, st);
+  if (mg->opts.precision == GRICO_PREC_FP32) {
+    const int64_t n = mg->levels[L - 1]->n_red;
+    float* b32 = mg->b32[L - 1].get<float>();
+    float* x32 = mg->x32[L - 1].get<float>();
+    cast_kernel<double, float><<<blocks(n), 256, 0, st>>>(r, b32, n);
+    vcycle<float>(mg, L - 1, x32, b32, st);
+    cast_kernel<float, double><<<blocks(n), 256, 0, st>>>(x32, z, n);
+  } else {
+    vcycle<double>(mg, L - 1, z, r, st);
+  }
   return cuda_ok(cudaGetLastError(), "vcycle") ? GRICO_OK : GRICO_ERR_CUDA;
 }
 
@@ -210,8 +277,13 @@ int grico_mg_create(GricoPlan* const* levels, int nlevels, const GricoTransferDe
     set_error("grico_mg_create: Chebyshev degree must be >= 1 and the lower bound fraction in (0,1)");
     return GRICO_ERR_INVALID;
   }
+  if (opts->precision != GRICO_PREC_FP64 && opts->precision != GRICO_PREC_FP32) {
+    set_error("grico_mg_create: precision must be GRICO_PREC_FP64 or GRICO_PREC_FP32");
+    return GRICO_ERR_INVALID;
+  }
   std::unique_ptr<GricoMultigrid> mg(new GricoMultigrid());
   mg->opts = *opts;
+  const bool fp32 = opts->precision == GRICO_PREC_FP32;
   mg->stream = levels[nlevels - 1]->stream;
   cudaStream_t st = mg->stream;
   for (int l = 0; l < nlevels; ++l) {
@@ -225,6 +297,14 @@ int grico_mg_create(GricoPlan* const* levels, int nlevels, const GricoTransferDe
   mg->t.resize(nlevels);
   mg->d.resize(nlevels);
   mg->lmax.assign(nlevels, 0.0);
+  if (fp32) {
+    mg->dinv32.resize(nlevels);
+    mg->b32.resize(nlevels);
+    mg->x32.resize(nlevels);
+    mg->r32.resize(nlevels);
+    mg->t32.resize(nlevels);
+    mg->d32.resize(nlevels);
+  }
   for (int l = 0; l < nlevels; ++l) {
     const int64_t n = std::max<int64_t>(levels[l]->n_red, 1);
     if (!mg->b[l].alloc(8 * n) || !mg->x[l].alloc(8 * n) || !mg->r[l].alloc(8 * n) || !mg->t[l].alloc(8 * n) ||
@@ -236,6 +316,18 @@ int grico_mg_create(GricoPlan* const* levels, int nlevels, const GricoTransferDe
       if (!mg->dinv[l].alloc(8 * n)) return GRICO_ERR_CUDA;
       cudaMemcpyAsync(mg->dinv[l].ptr, levels[l]->w_dinv.ptr, 8 * levels[l]->n_red, cudaMemcpyDeviceToDevice, st);
     }
+    if (fp32) {
+      if (!mg->b32[l].alloc(4 * n) || !mg->x32[l].alloc(4 * n) || !mg->r32[l].alloc(4 * n) ||
+          !mg->t32[l].alloc(4 * n) || !mg->d32[l].alloc(4 * n) || !mg->dinv32[l].alloc(4 * n))
+        return GRICO_ERR_CUDA;
+      if (l > 0)
+        cast_kernel<double, float><<<blocks(n), 256, 0, st>>>(mg->dinv[l].get<double>(), mg->dinv32[l].get<float>(),
+                                                              levels[l]->n_red);
+    }
+  }
+  if (fp32) {
+    const int64_t n0 = std::max<int64_t>(levels[0]->n_red, 1);
+    if (!mg->coarse_b.alloc(8 * n0) || !mg->coarse_x.alloc(8 * n0)) return GRICO_ERR_CUDA;
   }
   for (int l = 0; l + 1 < nlevels; ++l) {
     const GricoTransferDesc& T = transfers[l];
@@ -264,6 +356,10 @@ int grico_mg_create(GricoPlan* const* levels, int nlevels, const GricoTransferDe
     bool ok = X.p_off.upload(T.row_offsets, size_t(T.n_fine + 1)) && X.p_idx.upload(T.col_index, size_t(nnz)) &&
               X.p_val.upload(T.values, size_t(nnz)) && X.r_off.upload(roff) && X.r_idx.upload(ridx) &&
               X.r_val.upload(rval);
+    if (ok && fp32) {
+      std::vector<float> pv(T.values, T.values + nnz), rv(rval.begin(), rval.end());
+      ok = X.p_val32.upload(pv) && X.r_val32.upload(rv);
+    }
     if (!ok) return GRICO_ERR_CUDA;
     mg->xfer.push_back(std::move(X));
   }

@@ -88,3 +88,29 @@ def test_chebyshev_smoother_converges_faster_than_jacobi(cuda):
                    relative_tolerance=1e-10)
     assert rel_err(che.coefficients, jac.coefficients) <= 1e-7
     assert che.report.iterations < jac.report.iterations
+
+
+@pytest.mark.parametrize("smoother", ["jacobi", "chebyshev"])
+def test_fp32_vcycle_close_to_fp64(cuda, smoother):
+    """FP32 working precision below an FP64 caller: the V-cycle agrees with the FP64 one to FP32
+    rounding (the coarsest solve is FP64 in both)."""
+    _, plan = _pair("3d_p2")
+    kw = dict(smoother=smoother)
+    mg64 = build_multigrid(plan, GeometricMultigridPreconditioner(**kw))
+    mg32 = build_multigrid(plan, GeometricMultigridPreconditioner(precision="fp32", **kw))
+    r = np.random.default_rng(9).standard_normal(plan.n_reduced)
+    assert rel_err(mg32.vcycle(r), mg64.vcycle(r)) <= 1e-5
+
+
+def test_mixed_precision_cg_gmg_reaches_fp64_accuracy(cuda):
+    """FP64 outer PCG (residuals, dot products, updates) with the FP32 V-cycle reaches the same
+    FP64 solution as the all-FP64 solve: the preconditioner's precision limits only the rate."""
+    D = 3
+    src = lambda x: np.prod(np.sin(np.pi * x), axis=1) * (1.0 + D * np.pi ** 2)
+    _, plan = _pair("3d_p2", source=src)
+    s64 = gb.solve(plan, solver=gb.CGSolver(GeometricMultigridPreconditioner(smoother="chebyshev")),
+                   relative_tolerance=1e-12)
+    s32 = gb.solve(plan, solver=gb.CGSolver(GeometricMultigridPreconditioner(smoother="chebyshev", precision="fp32")),
+                   relative_tolerance=1e-12)
+    assert rel_err(s32.coefficients, s64.coefficients) <= 1e-10
+    assert s32.report.iterations <= s64.report.iterations + 3
