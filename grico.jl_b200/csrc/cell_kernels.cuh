@@ -752,3 +752,286 @@ __global__ void __launch_bounds__(kPointThreads) point_apply(PointView b, const 
 }
 
 }  // namespace grico
+
+namespace grico {
+
+// Finite-cell cut cells as lists of octree subcells.  The candidate rule of a cut cell
+// (regions.jl:477-510, 759-792) is the union of the cell's tensor rule mapped onto inside
+// subcells and onto terminal cut subcells with the points of positive classifier value
+// dropped, so each subcell is a tensor-product cell of its own: the 1-D basis tables at the
+// subcell's Gauss points depend only on its level and position, and sum factorisation applies.
+// One block per cut cell; each warp takes whole subcells and accumulates into its own copy of
+// the local result, the copies are summed and scattered once per cell.
+struct SubcellView {
+  int32_t n_items;
+  const int32_t* map;
+  const double* coef;
+  const int64_t* tail_off;
+  const int32_t* tail_idx;
+  const double* tail_coef;
+  const double* h;          // [n_items*dim]
+  const int64_t* sub_off;   // [n_items+1]
+  const int32_t* level;     // [n_sub]
+  const int32_t* pos;       // [n_sub*dim]
+  const uint64_t* mask;     // [n_sub]: bit p keeps tensor point p (axis 1 fastest)
+  const double* ws;         // [n_sub]: weight factor (2^(-dim*level) times the measure factor)
+  const double* kpts;       // [n_sub*Q^dim] or null
+  const uint8_t* skip;      // diagonal kernel skips these items (host computes them)
+};
+
+template <int Q, typename T>
+struct SubTables {
+  T eta[Q];     // Gauss points
+  T W[Q];       // Gauss weights
+  T Dm[Q * Q];  // Dm[p*Q+l] = L_l'(eta_p), collocation derivative
+};
+
+constexpr int kSubThreads = 128;
+constexpr int kSubWarps = kSubThreads / 32;
+
+template <int D, int N, int Q>
+struct SubSizes {
+  static constexpr int NB = D == 3 ? N * N * N : N * N;
+  static constexpr int QP = D == 3 ? Q * Q * Q : Q * Q;
+  static constexpr int A1 = D == 3 ? N * N * Q : 1;  // after the z stage
+  static constexpr int A2 = D == 3 ? N * Q * Q : N * Q;
+  // per-warp scratch: value and derivative tables, A1, A2, U, G[D], R, local result (last)
+  static constexpr int WARP = 2 * D * N * Q + A1 + A2 + QP * (D + 2) + NB;
+};
+
+// mode: 0 apply, 1 rhs (src[n_sub*QP] at the subcell points), 3 local diagonal
+template <typename T, int D, int N, int Q>
+__global__ void __launch_bounds__(kSubThreads) subcell_apply(SubcellView b, const SubTables<Q, T> tab,
+                                                            const T* __restrict__ x, T* __restrict__ y, int64_t n_vec,
+                                                            T mass, T kappa, int mode, const double* __restrict__ src) {
+  using S = SubSizes<D, N, Q>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* xl = reinterpret_cast<T*>(smem_raw);  // NB, shared by the warps
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  T* tb = xl + S::NB + warp * S::WARP;  // [D][N*Q] values at the subcell points
+  T* td = tb + D * N * Q;               // [D][N*Q] physical derivatives (diagonal only)
+  T* a1 = td + D * N * Q;
+  T* a2 = a1 + S::A1;
+  T* U = a2 + S::A2;
+  T* G = U + S::QP;                     // [D][QP]
+  T* R = G + D * S::QP;
+  T* yl = R + S::QP;                    // NB
+  const int64_t item = blockIdx.x;
+  if (mode == 3 && b.skip && b.skip[item]) return;
+  x += blockIdx.y * n_vec;
+  y += blockIdx.y * n_vec;
+  BatchView bv;
+  bv.n_cells = b.n_items;
+  bv.map = b.map;
+  bv.coef = b.coef;
+  bv.tail_off = b.tail_off;
+  bv.tail_idx = b.tail_idx;
+  bv.tail_coef = b.tail_coef;
+  if (mode == 0)
+    for (int i = threadIdx.x; i < S::NB; i += blockDim.x) xl[i] = gather_entry<T>(bv, item * S::NB + i, x);
+  for (int i = lane; i < S::NB; i += 32) yl[i] = T(0);
+  T hs[D];
+  T det = T(1);
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    hs[a] = T(b.h[item * D + a]);
+    det *= T(0.5) * hs[a];
+  }
+  __syncthreads();
+  const int64_t s_begin = b.sub_off[item], s_end = b.sub_off[item + 1];
+  for (int64_t s = s_begin + warp; s < s_end; s += kSubWarps) {
+    const int lev = b.level[s];
+    const T half = ldexp(T(1), -lev);
+    T sc[D];  // d/dx = (1 / half) * (2 / h) d/d eta
+#pragma unroll
+    for (int a = 0; a < D; ++a) sc[a] = T(2) / (hs[a] * half);
+    const uint64_t msk = b.mask[s];
+    const T wsub = T(b.ws[s]) * det;
+    // 1-D tables at the subcell's Gauss points
+    for (int t = lane; t < D * Q; t += 32) {
+      const int a = t / Q, j = t - a * Q;
+      const T c = T(-1) + T(2 * b.pos[s * D + a] + 1) * half;
+      T v[N], dv[N];
+      fe_basis_dev<T>(c + half * tab.eta[j], N - 1, v, dv);
+#pragma unroll
+      for (int m = 0; m < N; ++m) {
+        tb[a * N * Q + m * Q + j] = v[m];
+        td[a * N * Q + m * Q + j] = dv[m] * T(2) / hs[a];
+      }
+    }
+    __syncwarp();
+    const T* Bx = tb;
+    const T* By = tb + N * Q;
+    const T* Bz = tb + 2 * N * Q;
+    if (mode == 3) {
+      // local diagonal: sum_p w_p (mass phi_i^2 + k |grad phi_i|^2) for the lane's modes
+      for (int i = lane; i < S::NB; i += 32) {
+        const int mi[3] = {i % N, (i / N) % N, D == 3 ? i / (N * N) : 0};
+        T acc = T(0);
+        for (int p = 0; p < S::QP; ++p) {
+          if (!((msk >> p) & 1ull)) continue;
+          const int pq[3] = {p % Q, (p / Q) % Q, D == 3 ? p / (Q * Q) : 0};
+          T v[D], g[D];
+#pragma unroll
+          for (int a = 0; a < D; ++a) {
+            v[a] = tb[a * N * Q + mi[a] * Q + pq[a]];
+            g[a] = td[a * N * Q + mi[a] * Q + pq[a]];
+          }
+          T w = wsub;
+#pragma unroll
+          for (int a = 0; a < D; ++a) w *= tab.W[pq[a]];
+          T phi = T(1), gg = T(0);
+#pragma unroll
+          for (int a = 0; a < D; ++a) phi *= v[a];
+#pragma unroll
+          for (int a = 0; a < D; ++a) {
+            T ga = g[a];
+#pragma unroll
+            for (int e = 0; e < D; ++e)
+              if (e != a) ga *= v[e];
+            gg += ga * ga;
+          }
+          const T k = b.kpts ? kappa * T(b.kpts[s * S::QP + p]) : kappa;
+          acc += w * (mass * phi * phi + k * gg);
+        }
+        yl[i] += acc;
+      }
+      __syncwarp();
+      continue;
+    }
+    if (mode == 0) {
+      // interpolation: (z), y, x stages
+      const T* in = xl;
+      if constexpr (D == 3) {
+        for (int o = lane; o < S::A1; o += 32) {
+          const int i = o % N, j = (o / N) % N, kq = o / (N * N);
+          T acc = T(0);
+#pragma unroll
+          for (int k = 0; k < N; ++k) acc += Bz[k * Q + kq] * xl[i + N * (j + N * k)];
+          a1[o] = acc;
+        }
+        __syncwarp();
+        in = a1;
+      }
+      for (int o = lane; o < S::A2; o += 32) {
+        const int i = o % N, jq = (o / N) % Q, kq = D == 3 ? o / (N * Q) : 0;
+        T acc = T(0);
+#pragma unroll
+        for (int j = 0; j < N; ++j) acc += By[j * Q + jq] * in[i + N * (j + N * kq)];
+        a2[o] = acc;
+      }
+      __syncwarp();
+      for (int o = lane; o < S::QP; o += 32) {
+        const int iq = o % Q, rest = o / Q;
+        T acc = T(0);
+#pragma unroll
+        for (int i = 0; i < N; ++i) acc += Bx[i * Q + iq] * a2[i + N * rest];
+        U[o] = acc;
+      }
+      __syncwarp();
+      // collocation derivatives and the pointwise flux
+      for (int o = lane; o < S::QP; o += 32) {
+        const int pq[3] = {o % Q, (o / Q) % Q, D == 3 ? o / (Q * Q) : 0};
+        T w = ((msk >> o) & 1ull) ? wsub : T(0);
+#pragma unroll
+        for (int a = 0; a < D; ++a) w *= tab.W[pq[a]];
+        const T k = b.kpts ? kappa * T(b.kpts[s * S::QP + o]) : kappa;
+        T g[D];
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+          const int stride = a == 0 ? 1 : (a == 1 ? Q : Q * Q);
+          const int base = o - pq[a] * stride;
+          T acc = T(0);
+#pragma unroll
+          for (int l = 0; l < Q; ++l) acc += tab.Dm[pq[a] * Q + l] * U[base + l * stride];
+          g[a] = acc * sc[a];
+        }
+        R[o] = w * mass * U[o];
+#pragma unroll
+        for (int a = 0; a < D; ++a) G[a * S::QP + o] = w * k * g[a];
+      }
+    } else {
+      for (int o = lane; o < S::QP; o += 32) {
+        const int pq[3] = {o % Q, (o / Q) % Q, D == 3 ? o / (Q * Q) : 0};
+        T w = ((msk >> o) & 1ull) ? wsub : T(0);
+#pragma unroll
+        for (int a = 0; a < D; ++a) w *= tab.W[pq[a]];
+        R[o] = src ? w * T(src[s * S::QP + o]) : T(0);
+      }
+    }
+    __syncwarp();
+    // transposed collocation derivatives into U (values only for the load)
+    if (mode == 0) {
+      for (int o = lane; o < S::QP; o += 32) {
+        const int pq[3] = {o % Q, (o / Q) % Q, D == 3 ? o / (Q * Q) : 0};
+        T acc = R[o];
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+          const int stride = a == 0 ? 1 : (a == 1 ? Q : Q * Q);
+          const int base = o - pq[a] * stride;
+          T s2 = T(0);
+#pragma unroll
+          for (int l = 0; l < Q; ++l) s2 += tab.Dm[l * Q + pq[a]] * G[a * S::QP + base + l * stride];
+          acc += s2 * sc[a];
+        }
+        U[o] = acc;
+      }
+    } else {
+      for (int o = lane; o < S::QP; o += 32) U[o] = R[o];
+    }
+    __syncwarp();
+    // transposed interpolation: x, y, (z) stages into the warp's local result
+    for (int o = lane; o < S::A2; o += 32) {
+      const int i = o % N, rest = o / N;
+      T acc = T(0);
+#pragma unroll
+      for (int iq = 0; iq < Q; ++iq) acc += Bx[i * Q + iq] * U[iq + Q * rest];
+      a2[o] = acc;
+    }
+    __syncwarp();
+    if constexpr (D == 3) {
+      for (int o = lane; o < S::A1; o += 32) {
+        const int i = o % N, j = (o / N) % N, kq = o / (N * N);
+        T acc = T(0);
+#pragma unroll
+        for (int jq = 0; jq < Q; ++jq) acc += By[j * Q + jq] * a2[i + N * (jq + Q * kq)];
+        a1[o] = acc;
+      }
+      __syncwarp();
+      for (int o = lane; o < S::NB; o += 32) {
+        const int i = o % N, j = (o / N) % N, k = o / (N * N);
+        T acc = T(0);
+#pragma unroll
+        for (int kq = 0; kq < Q; ++kq) acc += Bz[k * Q + kq] * a1[i + N * (j + N * kq)];
+        yl[o] += acc;
+      }
+    } else {
+      for (int o = lane; o < S::NB; o += 32) {
+        const int i = o % N, j = o / N;
+        T acc = T(0);
+#pragma unroll
+        for (int jq = 0; jq < Q; ++jq) acc += By[j * Q + jq] * a2[i + N * jq];
+        yl[o] += acc;
+      }
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  // sum the warps' local results (the last NB entries of each warp's scratch) and scatter once
+  for (int i = threadIdx.x; i < S::NB; i += blockDim.x) {
+    T acc = T(0);
+#pragma unroll
+    for (int w = 0; w < kSubWarps; ++w) acc += xl[S::NB + w * S::WARP + S::WARP - S::NB + i];
+    if (mode == 3) {
+      const int v = b.map[item * S::NB + i];
+      if (v >= 0) {
+        const T c = b.coef ? T(b.coef[item * S::NB + i]) : T(1);
+        atomicAdd(y + v, c * c * acc);
+      }
+    } else {
+      scatter_entry<T>(bv, item * S::NB + i, acc, y);
+    }
+  }
+}
+
+}  // namespace grico

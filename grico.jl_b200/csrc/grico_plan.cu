@@ -192,10 +192,71 @@ void launch_batch(const GricoPlan& P, const DevBatch& b, bool reduced, const T* 
 
 int grid_for(int64_t n) { return int(std::min<int64_t>((n + 255) / 256, 148 * 16)); }
 
+template <typename T, int D, int N, int Q>
+void launch_subcells_nq(const GricoPlan& P, const DevPointBatch& pb, const SubcellView& v, const T* x, T* y,
+                        int64_t nvec, int mode, const double* src, int nrhs, cudaStream_t st) {
+  SubTables<Q, T> tab;
+  for (int j = 0; j < Q; ++j) {
+    tab.eta[j] = T(pb.hEta[j]);
+    tab.W[j] = T(pb.hW[j]);
+  }
+  for (int j = 0; j < Q * Q; ++j) tab.Dm[j] = T(pb.hDm[j]);
+  using S = SubSizes<D, N, Q>;
+  const size_t smem = sizeof(T) * size_t(S::NB + kSubWarps * S::WARP);
+  auto kernel = subcell_apply<T, D, N, Q>;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  dim3 grid(pb.n_items, nrhs);
+  kernel<<<grid, kSubThreads, smem, st>>>(v, tab, x, y, nvec, T(P.mass), T(P.kappa), mode, src);
+}
+
+// (modes per axis, points per axis) pairs compiled for the subcell kernel
+#define GRICO_SUB3(X) X(2, 2) X(2, 3) X(3, 3) X(2, 4) X(3, 4) X(4, 4)
+#define GRICO_SUB2(X)                                                                                     \
+  X(2, 2) X(2, 3) X(3, 3) X(3, 4) X(4, 4) X(4, 5) X(5, 5) X(5, 6) X(6, 6) X(6, 7) X(7, 7) X(7, 8) X(8, 8)
+
+bool subcell_shape_supported(int dim, int n, int q) {
+#define GRICO_SUB_CHECK(NN, QQ) if (n == NN && q == QQ) return true;
+  if (dim == 3) { GRICO_SUB3(GRICO_SUB_CHECK) }
+  if (dim == 2) { GRICO_SUB2(GRICO_SUB_CHECK) }
+#undef GRICO_SUB_CHECK
+  return false;
+}
+
+template <typename T>
+void launch_subcells(const GricoPlan& P, const DevPointBatch& pb, bool reduced, const T* x, T* y, int64_t nvec,
+                     int mode, const double* src, int nrhs, cudaStream_t st) {
+  SubcellView v;
+  v.n_items = pb.n_items;
+  const DevMap& m = reduced ? pb.red : pb.full;
+  v.map = m.map.get<int32_t>();
+  v.coef = m.coef.get<double>();
+  v.tail_off = m.toff.get<int64_t>();
+  v.tail_idx = m.tidx.get<int32_t>();
+  v.tail_coef = m.tcoef.get<double>();
+  v.h = pb.h.get<double>();
+  v.sub_off = pb.sub_off.get<int64_t>();
+  v.level = pb.sub_level.get<int32_t>();
+  v.pos = pb.sub_pos.get<int32_t>();
+  v.mask = pb.sub_mask.get<uint64_t>();
+  v.ws = pb.sub_w.get<double>();
+  v.kpts = pb.kpts.get<double>();
+  v.skip = reduced ? pb.skip.get<uint8_t>() : nullptr;
+  const int n = pb.n[0], q = pb.q[0];
+#define GRICO_SUB_LAUNCH3(NN, QQ) \
+  if (n == NN && q == QQ) return launch_subcells_nq<T, 3, NN, QQ>(P, pb, v, x, y, nvec, mode, src, nrhs, st);
+#define GRICO_SUB_LAUNCH2(NN, QQ) \
+  if (n == NN && q == QQ) return launch_subcells_nq<T, 2, NN, QQ>(P, pb, v, x, y, nvec, mode, src, nrhs, st);
+  if (P.dim == 3) { GRICO_SUB3(GRICO_SUB_LAUNCH3) }
+  if (P.dim == 2) { GRICO_SUB2(GRICO_SUB_LAUNCH2) }
+#undef GRICO_SUB_LAUNCH3
+#undef GRICO_SUB_LAUNCH2
+}
+
 template <typename T>
 void launch_points(const GricoPlan& P, const DevPointBatch& pb, bool reduced, const T* x, T* y, int64_t nvec, int mode,
                    const double* src, int nrhs, cudaStream_t st) {
   if (pb.n_items == 0) return;
+  if (pb.kind == GRICO_ITEM_SUBCELLS) return launch_subcells<T>(P, pb, reduced, x, y, nvec, mode, src, nrhs, st);
   PointView v;
   v.n_items = pb.n_items;
   v.kind = pb.kind;
@@ -233,16 +294,16 @@ void launch_points(const GricoPlan& P, const DevPointBatch& pb, bool reduced, co
 // Exact local-matrix diagonal contribution of one point item whose reduced map is not a direct
 // injection (cell_diagonal!/face and surface diagonals, accumulators.jl:1056-1083, 1163-1187).
 void accumulate_point_item_diagonal(const GricoPlanDesc& d, const GricoPointBatchDesc& pb, const int* n, int64_t it,
-                                    int64_t nb, const std::vector<int32_t>& rmap, const std::vector<double>& rcoef,
+                                    int64_t pit, int64_t nb, const std::vector<int32_t>& rmap, const std::vector<double>& rcoef,
                                     const std::vector<int64_t>& toff, const std::vector<int32_t>& tidx,
                                     const std::vector<double>& tcoef, std::map<int64_t, double>& out) {
   const int D = d.dim;
   std::vector<double> A(nb * nb, 0.0), phi(nb), gr(3 * nb);
   double v[3][17], dv[3][17];
-  for (int64_t p = pb.point_offsets[it]; p < pb.point_offsets[it + 1]; ++p) {
+  for (int64_t p = pb.point_offsets[pit]; p < pb.point_offsets[pit + 1]; ++p) {
     for (int a = 0; a < D; ++a) {
       fe_basis(pb.ref_points[p * D + a], n[a] - 1, v[a], dv[a]);
-      const double s = 2.0 / pb.cell_size[it * D + a];
+      const double s = 2.0 / pb.cell_size[pit * D + a];
       for (int i = 0; i < n[a]; ++i) dv[a][i] *= s;
     }
     for (int64_t i = 0; i < nb; ++i) {
@@ -268,7 +329,7 @@ void accumulate_point_item_diagonal(const GricoPlanDesc& d, const GricoPointBatc
             dnj += gr[a * nb + j] * pb.normals[p * D + a];
             dni += gr[a * nb + i] * pb.normals[p * D + a];
           }
-          aij = phi[i] * (-dnj + pb.eta[it] * phi[j]) - dni * phi[j];
+          aij = phi[i] * (-dnj + pb.eta[pit] * phi[j]) - dni * phi[j];
         } else {
           double g = 0.0;
           for (int a = 0; a < D; ++a) g += gr[a * nb + i] * gr[a * nb + j];
@@ -293,6 +354,49 @@ void accumulate_point_item_diagonal(const GricoPlanDesc& d, const GricoPointBatc
       for (auto& b : kv.second) s += a.second * A[a.first * nb + b.first] * b.second;
     out[kv.first] += s;
   }
+}
+
+// The same for a subcell item: its kept subcell points are listed as one point item.
+void accumulate_subcell_item_diagonal(const GricoPlanDesc& d, const GricoPointBatchDesc& pb, const int* n, int64_t it,
+                                      int64_t nb, const std::vector<int32_t>& rmap, const std::vector<double>& rcoef,
+                                      const std::vector<int64_t>& toff, const std::vector<int32_t>& tidx,
+                                      const std::vector<double>& tcoef, std::map<int64_t, double>& out) {
+  const int D = d.dim;
+  const int q = pb.qpoints[0];
+  std::vector<double> eta(q), W(q);
+  gauss_legendre(q, eta.data(), W.data());
+  int qp = 1;
+  for (int a = 0; a < D; ++a) qp *= q;
+  double det = 1.0;
+  for (int a = 0; a < D; ++a) det *= 0.5 * pb.cell_size[it * D + a];
+  std::vector<double> ref, w, kp;
+  for (int64_t s = pb.subcell_offsets[it]; s < pb.subcell_offsets[it + 1]; ++s) {
+    const double half = std::ldexp(1.0, -pb.subcell_level[s]);
+    for (int p = 0; p < qp; ++p) {
+      if (!((pb.subcell_mask[s] >> p) & 1ull)) continue;
+      int rem = p;
+      double wt = pb.subcell_weight[s] * det;
+      for (int a = 0; a < D; ++a) {
+        const int j = rem % q;
+        rem /= q;
+        const double c = -1.0 + double(2 * pb.subcell_pos[s * D + a] + 1) * half;
+        ref.push_back(c + half * eta[j]);
+        wt *= W[j];
+      }
+      w.push_back(wt);
+      if (pb.kappa_points) kp.push_back(pb.kappa_points[s * qp + p]);
+    }
+  }
+  GricoPointBatchDesc one = {};
+  one.n_items = 1;
+  one.kind = GRICO_ITEM_CELL;
+  int64_t offs[2] = {0, int64_t(w.size())};
+  one.point_offsets = offs;
+  one.ref_points = ref.data();
+  one.weights = w.data();
+  one.cell_size = pb.cell_size + it * D;
+  one.kappa_points = pb.kappa_points ? kp.data() : nullptr;
+  accumulate_point_item_diagonal(d, one, n, it, 0, nb, rmap, rcoef, toff, tidx, tcoef, out);
 }
 
 // Exact reduced-diagonal contribution sum_{i,j} M_ir A_ij M_jr of one cell whose reduced map is
@@ -480,10 +584,38 @@ static int validate_plan_desc(const GricoPlanDesc* d) {
   for (int bi = 0; bi < d->n_point_batches; ++bi) {
     const GricoPointBatchDesc& pb = d->point_batches[bi];
     const std::string tag = "point batch " + std::to_string(bi);
-    if (pb.kind != GRICO_ITEM_CELL && pb.kind != GRICO_ITEM_NITSCHE) { set_error(tag + ": unknown item kind"); return GRICO_ERR_UNSUPPORTED_FORM; }
-    if (pb.n_items < 0 || (pb.n_items > 0 && (!pb.map_index || !pb.cell_size || !pb.point_offsets || !pb.ref_points || !pb.weights))) {
+    if (pb.kind != GRICO_ITEM_CELL && pb.kind != GRICO_ITEM_NITSCHE && pb.kind != GRICO_ITEM_SUBCELLS) {
+      set_error(tag + ": unknown item kind");
+      return GRICO_ERR_UNSUPPORTED_FORM;
+    }
+    const bool sub = pb.kind == GRICO_ITEM_SUBCELLS;
+    if (pb.n_items < 0 || (pb.n_items > 0 && (!pb.map_index || !pb.cell_size ||
+                                              (!sub && (!pb.point_offsets || !pb.ref_points || !pb.weights)) ||
+                                              (sub && (!pb.subcell_offsets || !pb.subcell_level || !pb.subcell_pos ||
+                                                       !pb.subcell_mask || !pb.subcell_weight))))) {
       set_error(tag + ": missing arrays");
       return GRICO_ERR_INVALID;
+    }
+    if (sub) {
+      const int nn = pb.degree[0] + 1, q = pb.qpoints[0];
+      int qp = 1;
+      for (int a = 0; a < d->dim; ++a) {
+        if (pb.degree[a] != pb.degree[0] || pb.qpoints[a] != q) { set_error(tag + ": subcell items need isotropic degree and quadrature"); return GRICO_ERR_UNSUPPORTED_FORM; }
+        qp *= q;
+      }
+      if (qp > 64 || !subcell_shape_supported(d->dim, nn, q)) { set_error(tag + ": subcell kernel not compiled for this degree/quadrature"); return GRICO_ERR_UNSUPPORTED_FORM; }
+      if (pb.n_items > 0 && pb.subcell_offsets[0] != 0) { set_error(tag + ": subcell offsets must start at 0"); return GRICO_ERR_INVALID; }
+      for (int64_t it = 0; it < pb.n_items; ++it)
+        if (pb.subcell_offsets[it + 1] < pb.subcell_offsets[it]) { set_error(tag + ": subcell offsets must not decrease"); return GRICO_ERR_INVALID; }
+      const int64_t ns = pb.n_items > 0 ? pb.subcell_offsets[pb.n_items] : 0;
+      for (int64_t s2 = 0; s2 < ns; ++s2) {
+        const int lev = pb.subcell_level[s2];
+        if (lev < 0 || lev > 30) { set_error(tag + ": subcell level out of range"); return GRICO_ERR_INVALID; }
+        for (int a = 0; a < d->dim; ++a) {
+          const int32_t ps = pb.subcell_pos[s2 * d->dim + a];
+          if (ps < 0 || int64_t(ps) >= (int64_t(1) << lev)) { set_error(tag + ": subcell position out of range"); return GRICO_ERR_INVALID; }
+        }
+      }
     }
     if (pb.kind == GRICO_ITEM_NITSCHE && pb.n_items > 0 && (!pb.normals || !pb.eta)) { set_error(tag + ": Nitsche items need normals and eta"); return GRICO_ERR_INVALID; }
     int n[3] = {1, 1, 1};
@@ -493,8 +625,8 @@ static int validate_plan_desc(const GricoPlanDesc* d) {
     }
     const int64_t nb = box_count(d->dim, n);
     if (nb > int64_t(kMaxModes) * kPointThreads) { set_error(tag + ": too many local modes for point items"); return GRICO_ERR_INVALID; }
-    if (pb.point_offsets && pb.n_items > 0 && pb.point_offsets[0] != 0) { set_error(tag + ": point offsets must start at 0"); return GRICO_ERR_INVALID; }
-    for (int64_t it = 0; it < pb.n_items; ++it)
+    if (!sub && pb.point_offsets && pb.n_items > 0 && pb.point_offsets[0] != 0) { set_error(tag + ": point offsets must start at 0"); return GRICO_ERR_INVALID; }
+    for (int64_t it = 0; !sub && it < pb.n_items; ++it)
       if (pb.point_offsets[it + 1] < pb.point_offsets[it]) { set_error(tag + ": point offsets must not decrease"); return GRICO_ERR_INVALID; }
     if (pb.n_tail < 0 || (pb.n_tail > 0 && (!pb.tail_offsets || !pb.tail_index || !pb.tail_coef))) { set_error(tag + ": invalid tail"); return GRICO_ERR_INVALID; }
     for (int64_t e = 0; e < int64_t(pb.n_items) * nb; ++e) {
@@ -647,10 +779,28 @@ int grico_plan_create(const GricoPlanDesc* d, GricoPlan** out) {
     for (int a = 0; a < d->dim; ++a) pb.n[a] = pd.degree[a] + 1;
     const int64_t nb = box_count(d->dim, pb.n);
     const int64_t ne = int64_t(pd.n_items) * nb;
-    pb.n_points = pd.n_items > 0 ? pd.point_offsets[pd.n_items] : 0;
-    bool ok = pb.full.map.upload(pd.map_index, size_t(ne)) && pb.h.upload(pd.cell_size, size_t(pd.n_items) * d->dim) &&
-              pb.pt_off.upload(pd.point_offsets, size_t(pd.n_items + 1)) &&
-              pb.ref.upload(pd.ref_points, size_t(pb.n_points) * d->dim) && pb.w.upload(pd.weights, size_t(pb.n_points));
+    bool ok = pb.full.map.upload(pd.map_index, size_t(ne)) && pb.h.upload(pd.cell_size, size_t(pd.n_items) * d->dim);
+    if (pd.kind == GRICO_ITEM_SUBCELLS) {
+      int qp = 1;
+      for (int a = 0; a < d->dim; ++a) {
+        pb.q[a] = pd.qpoints[a];
+        qp *= pd.qpoints[a];
+      }
+      pb.n_sub = pd.n_items > 0 ? pd.subcell_offsets[pd.n_items] : 0;
+      pb.n_points = pb.n_sub * qp;
+      ok = ok && pb.sub_off.upload(pd.subcell_offsets, size_t(pd.n_items + 1)) &&
+           pb.sub_level.upload(pd.subcell_level, size_t(pb.n_sub)) &&
+           pb.sub_pos.upload(pd.subcell_pos, size_t(pb.n_sub) * d->dim) &&
+           pb.sub_mask.upload(pd.subcell_mask, size_t(pb.n_sub)) && pb.sub_w.upload(pd.subcell_weight, size_t(pb.n_sub));
+      pb.hEta.resize(pb.q[0]);
+      pb.hW.resize(pb.q[0]);
+      gauss_legendre(pb.q[0], pb.hEta.data(), pb.hW.data());
+      pb.hDm = collocation_derivative(pb.hEta);
+    } else {
+      pb.n_points = pd.n_items > 0 ? pd.point_offsets[pd.n_items] : 0;
+      ok = ok && pb.pt_off.upload(pd.point_offsets, size_t(pd.n_items + 1)) &&
+           pb.ref.upload(pd.ref_points, size_t(pb.n_points) * d->dim) && pb.w.upload(pd.weights, size_t(pb.n_points));
+    }
     if (pd.map_coef) ok = ok && pb.full.coef.upload(pd.map_coef, size_t(ne));
     if (pd.n_tail > 0)
       ok = ok && pb.full.toff.upload(pd.tail_offsets, size_t(pd.n_tail + 1)) &&
@@ -683,7 +833,10 @@ int grico_plan_create(const GricoPlanDesc* d, GricoPlan** out) {
       }
       if (!skip[it]) continue;
       ++hanging;
-      accumulate_point_item_diagonal(*d, pd, pb.n, it, nb, rmap, rcoef, toff, tidx, tcoef, P->hang_diag);
+      if (pd.kind == GRICO_ITEM_SUBCELLS)
+        accumulate_subcell_item_diagonal(*d, pd, pb.n, it, nb, rmap, rcoef, toff, tidx, tcoef, P->hang_diag);
+      else
+        accumulate_point_item_diagonal(*d, pd, pb.n, it, it, nb, rmap, rcoef, toff, tidx, tcoef, P->hang_diag);
     }
     if (hanging) ok = ok && pb.skip.upload(skip);
     if (!ok) return GRICO_ERR_CUDA;

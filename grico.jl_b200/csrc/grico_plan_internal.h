@@ -80,9 +80,14 @@ struct DevPointBatch {
   int32_t n_items = 0;
   int kind = 1;
   int n[3] = {1, 1, 1};
-  int64_t n_points = 0;
+  int64_t n_points = 0;  // points (kind 3: subcells x prod(q), the size of source/kappa arrays)
   DevMap full, red;
   DevBuf h, pt_off, ref, w, nrm, eta, kpts, skip;
+  // GRICO_ITEM_SUBCELLS
+  int q[3] = {1, 1, 1};
+  int64_t n_sub = 0;
+  DevBuf sub_off, sub_level, sub_pos, sub_mask, sub_w;
+  std::vector<double> hEta, hW, hDm;  // Gauss points, weights, collocation derivative (q[0])
 };
 
 }  // namespace grico

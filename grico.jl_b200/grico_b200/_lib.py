@@ -28,6 +28,10 @@ GRICO_CONTINUITY_DG = 1
 GRICO_FORM_MASS_DIFFUSION = 1
 GRICO_ITEM_CELL = 1
 GRICO_ITEM_NITSCHE = 2
+GRICO_ITEM_SUBCELLS = 3
+# (modes per axis, points per axis) pairs the subcell kernel is compiled for, per dimension
+SUBCELL_SHAPES = {3: {(2, 2), (2, 3), (3, 3), (2, 4), (3, 4), (4, 4)},
+                  2: {(n, q) for n in range(2, 9) for q in (n, n + 1) if q <= 8}}
 GRICO_PREC_FP64 = 0
 GRICO_PREC_FP32 = 1
 GRICO_FLAG_HOST_POINTERS = 1
@@ -77,6 +81,12 @@ class GricoPointBatchDesc(C.Structure):
         ("normals", f64p),
         ("eta", f64p),
         ("kappa_points", f64p),
+        ("qpoints", C.c_int32 * 3),
+        ("subcell_offsets", i64p),
+        ("subcell_level", i32p),
+        ("subcell_pos", i32p),
+        ("subcell_mask", C.POINTER(C.c_uint64)),
+        ("subcell_weight", f64p),
     ]
 
 

@@ -308,6 +308,44 @@ class _PointBatch:
     pass
 
 
+def _subcell_supported(D, degree, qshape):
+    if D not in L.SUBCELL_SHAPES or len(set(degree)) != 1 or len(set(qshape)) != 1:
+        return False
+    return (degree[0] + 1, qshape[0]) in L.SUBCELL_SHAPES[D] and int(np.prod(qshape)) <= 64
+
+
+def _subcell_point_chunks(b, chunk=65536):
+    """(physical points [m*qp, D], weights [m*qp] incl. det and the keep mask, item index [m*qp],
+    reference points [m*qp, D]) of the subcell points of a GRICO_ITEM_SUBCELLS batch, `chunk`
+    subcells at a time, in the order of the kernel's source arrays (subcell-major, tensor point
+    minor, axis 1 fastest)."""
+    D = b.h.shape[1]
+    q = b.q[0]
+    pts, wts = _gauss(q)
+    grids = np.meshgrid(*([pts] * D), indexing="ij")
+    eta = np.stack([g.reshape(-1, order="F") for g in grids], axis=1)       # [qp, D]
+    wg = np.meshgrid(*([wts] * D), indexing="ij")
+    W = np.ones(eta.shape[0])
+    for a in range(D):
+        W = W * wg[a].reshape(-1, order="F")
+    qp = eta.shape[0]
+    bitpos = np.arange(qp, dtype=np.uint64)
+    nsub = len(b.subcell_level)
+    item_of = np.repeat(np.arange(len(b.cells)), np.diff(b.subcell_offsets))
+    det = np.prod(0.5 * b.h, axis=1)
+    for s0 in range(0, nsub, chunk):
+        s1 = min(nsub, s0 + chunk)
+        half = np.ldexp(1.0, -b.subcell_level[s0:s1].astype(np.int64))[:, None]
+        c = -1.0 + (2.0 * b.subcell_pos[s0:s1] + 1.0) * half                  # [m, D]
+        xi = c[:, None, :] + half[:, :, None] * eta[None, :, :]                # [m, qp, D]
+        it = item_of[s0:s1]
+        hh = 0.5 * b.h[it]
+        X = (b.lower[it] + hh)[:, None, :] + xi * hh[:, None, :]
+        keep = ((b.subcell_mask[s0:s1, None] >> bitpos[None, :]) & np.uint64(1)).astype(bool)
+        w = W[None, :] * (b.subcell_weight[s0:s1] * det[it])[:, None] * keep
+        yield X.reshape(-1, D), w.reshape(-1), np.repeat(it, qp), xi.reshape(-1, D)
+
+
 class AssemblyPlan:
     """Compiled plan: descriptor arrays built here, device data owned by libgrico_b200."""
 
@@ -337,21 +375,28 @@ class AssemblyPlan:
                 raise ValueError(f"cell quadrature leaf {leaf} is not an active leaf")
             point_rule[space.leaf_to_index[leaf]] = rule
         self.n_cut = 0
+        sub_groups = []      # (Morton positions, degree, qshape) integrated as octree subcells
         if physical and not (isinstance(domain.cell_measure, FiniteCellExtension) and domain.cell_measure.alpha == 1.0):
             cls = domain.classify(space.leaves)
             cut = np.nonzero(cls == 2)[0]
             cut = np.array([c for c in cut if int(c) not in point_rule], dtype=np.int64)
             self.n_cut = int(cut.size)
             if cut.size:
-                qs = space.qshape[cut]
-                for qsig in np.unique(qs, axis=0):
-                    sel = cut[np.all(qs == qsig, axis=1)]
-                    rules = domain.cut_cell_quadrature(space.leaves[sel], tuple(int(v) for v in qsig), _gauss)
+                sig_cut = np.concatenate([space.degrees[cut], space.qshape[cut]], axis=1)
+                for sg in np.unique(sig_cut, axis=0):
+                    sel = cut[np.all(sig_cut == sg, axis=1)]
+                    deg, qsig = tuple(int(v) for v in sg[:D]), tuple(int(v) for v in sg[D:])
+                    if domain.quadrature == "candidates" and _subcell_supported(D, deg, qsig):
+                        sub_groups.append((sel, deg, qsig))
+                        continue
+                    rules = domain.cut_cell_quadrature(space.leaves[sel], qsig, _gauss)
                     for c, r in zip(sel, rules):
                         if r is not None:        # no candidate at all: the tensor rule stays
                             point_rule[int(c)] = r
         tensor_mask = np.ones(len(space.leaves), dtype=bool)
         tensor_mask[list(point_rule)] = False
+        for sel, _, _ in sub_groups:
+            tensor_mask[sel] = False
         # --- tensor batches by (degrees, quadrature shape), first appearance in Morton order ---
         sig = np.concatenate([space.degrees, space.qshape], axis=1)
         self.batches = []
@@ -379,7 +424,8 @@ class AssemblyPlan:
                 self.batches.append(b)
         # --- point-quadrature items: cut cells, faces, embedded surfaces ---
         self.point_batches = []
-        self._build_cell_items(point_rule)
+        extra = self._build_subcell_items(sub_groups)
+        self._build_cell_items(point_rule, extra)
         self._build_nitsche_items(problem)
         # --- Dirichlet: fixed dofs are the dofs with a trace on a selected boundary face ---
         self._compile_dirichlet(problem)
@@ -429,20 +475,71 @@ class AssemblyPlan:
                 np.asarray(self.form.coefficient(pb.points), dtype=np.float64).reshape(-1))
         self.point_batches.append(pb)
 
-    def _build_cell_items(self, point_rule):
-        """Cut cells and explicit cell rules: kind-1 items grouped by degree (Morton order)."""
+    def _build_cell_items(self, point_rule, extra=()):
+        """Cells on explicit point rules (moment-fitted cut cells, add_cell_quadrature!, sliver
+        points of subcell cut cells): kind-1 items grouped by degree (Morton order)."""
         space, D = self.space, self.D
-        if not point_rule:
+        items = sorted([(int(c), r[0], r[1]) for c, r in point_rule.items()] + list(extra), key=lambda t: t[0])
+        if not items:
             return
-        pos = np.array(sorted(point_rule), dtype=np.int64)
+        pos = np.array([t[0] for t in items], dtype=np.int64)
         degs = space.degrees[pos]
         for dsig in np.unique(degs, axis=0):
-            sel = pos[np.all(degs == dsig, axis=1)]
+            idx = [i for i in range(len(items)) if np.all(degs[i] == dsig)]
+            sel = pos[idx]
             pb = self._new_point_batch(L.GRICO_ITEM_CELL, sel, tuple(int(v) for v in dsig))
             det = np.prod(0.5 * pb.h, axis=1)
-            refs = [point_rule[int(c)][0] for c in sel]
-            wts = [point_rule[int(c)][1] * det[i] for i, c in enumerate(sel)]
+            refs = [items[i][1] for i in idx]
+            wts = [items[i][2] * det[k] for k, i in enumerate(idx)]
             self._finish_point_batch(pb, refs, wts)
+
+    def _build_subcell_items(self, groups):
+        """Cut cells of the candidate rule as octree subcells (GRICO_ITEM_SUBCELLS), one batch per
+        (degree, quadrature shape).  Returns the sliver fallback points as extra point rules."""
+        from .regions import FiniteCellExtension
+
+        space, domain, D = self.space, self.space.domain, self.D
+        extra = []
+        if not groups:
+            return extra
+        alpha = domain.cell_measure.alpha if isinstance(domain.cell_measure, FiniteCellExtension) else 0.0
+        for sel, deg, qsig in groups:
+            off, lev, pos, mask, ws, slivers = domain.subcell_quadrature(space.leaves[sel], qsig, _gauss)
+            nq = int(np.prod(qsig))
+            if alpha > 0.0:
+                # (1 - alpha) * physical + alpha * the full cell as one level-0 subcell per cell
+                counts = np.diff(off) + 1
+                first = np.concatenate([[0], np.cumsum(counts)])[:-1]
+                tot = int(counts.sum())
+                full = np.uint64((1 << nq) - 1) if nq < 64 else np.uint64(0xFFFFFFFFFFFFFFFF)
+                lev2 = np.zeros(tot, dtype=np.int32)
+                pos2 = np.zeros((tot, D), dtype=np.int32)
+                mask2 = np.full(tot, full, dtype=np.uint64)
+                ws2 = np.full(tot, alpha)
+                rest = np.ones(tot, dtype=bool)
+                rest[first] = False
+                lev2[rest], pos2[rest], mask2[rest], ws2[rest] = lev, pos, mask, (1.0 - alpha) * ws
+                off = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+                lev, pos, mask, ws = lev2, pos2, mask2, ws2
+                slivers = {c: (p, (1.0 - alpha) * w) for c, (p, w) in slivers.items()}
+            pb = self._new_point_batch(L.GRICO_ITEM_SUBCELLS, sel, deg)
+            pb.q = qsig
+            pb.subcell_offsets = off
+            pb.subcell_level = np.ascontiguousarray(lev, dtype=np.int32)
+            pb.subcell_pos = np.ascontiguousarray(pos, dtype=np.int32)
+            pb.subcell_mask = np.ascontiguousarray(mask, dtype=np.uint64)
+            pb.subcell_weight = np.ascontiguousarray(ws, dtype=np.float64)
+            pb.point_offsets = None
+            pb.ref_points = pb.weights = pb.normals = pb.eta = None
+            pb.kappa_points = None
+            if self.form.coefficient is not None and len(lev):
+                pb.kappa_points = np.ascontiguousarray(np.concatenate([
+                    np.asarray(self.form.coefficient(X), dtype=np.float64).reshape(-1)
+                    for X, _, _, _ in _subcell_point_chunks(pb)]))
+            self.point_batches.append(pb)
+            for c, (p, w) in slivers.items():
+                extra.append((int(sel[c]), p, w))
+        return extra
 
     def _build_nitsche_items(self, problem):
         """Boundary-face items (integration.jl:2230-2256) and embedded-surface items
@@ -598,6 +695,14 @@ class AssemblyPlan:
             d.tail_index = L.ptr(b.tail_index, C.c_int32)
             d.tail_coef = L.ptr(b.tail_coef, C.c_double)
             d.cell_size = L.ptr(b.h, C.c_double)
+            if b.kind == L.GRICO_ITEM_SUBCELLS:
+                for a in range(3):
+                    d.qpoints[a] = b.q[a] if a < self.D else 1
+                d.subcell_offsets = L.ptr(b.subcell_offsets, C.c_int64)
+                d.subcell_level = L.ptr(b.subcell_level, C.c_int32)
+                d.subcell_pos = L.ptr(b.subcell_pos, C.c_int32)
+                d.subcell_mask = L.ptr(b.subcell_mask, C.c_uint64)
+                d.subcell_weight = L.ptr(b.subcell_weight, C.c_double)
             d.point_offsets = L.ptr(b.point_offsets, C.c_int64)
             d.ref_points = L.ptr(b.ref_points, C.c_double)
             d.weights = L.ptr(b.weights, C.c_double)
@@ -723,7 +828,18 @@ def _source_points(plan, problem=None):
         else:
             arrays.append(None)
     for b in plan.point_batches:
-        if b.kind == L.GRICO_ITEM_CELL:
+        if b.kind == L.GRICO_ITEM_SUBCELLS:
+            if problem.rhs_operators:
+                parts = []
+                for X, _, _, _ in _subcell_point_chunks(b):
+                    f = np.zeros(X.shape[0])
+                    for op in problem.rhs_operators:
+                        f += np.asarray(op.source(X), dtype=np.float64).reshape(-1)
+                    parts.append(f)
+                arrays.append(np.ascontiguousarray(np.concatenate(parts)) if parts else None)
+            else:
+                arrays.append(None)
+        elif b.kind == L.GRICO_ITEM_CELL:
             if problem.rhs_operators:
                 f = np.zeros(b.points.shape[0])
                 for op in problem.rhs_operators:
@@ -821,35 +937,59 @@ def solve(plan_or_problem, solver=None, relative_tolerance=None, absolute_tolera
     return State(plan, expand_reduced(plan, x), rep)
 
 
-def _quadrature_sets(plan):
-    """(weights, physical points) of every cell rule: tensor batches and cell point items."""
-    out = []
-    for b in plan.batches:
-        out.append((_point_weights(plan, b).reshape(-1), b.points.reshape(-1, plan.D)))
+def _quadrature_chunks(plan, full_values=None):
+    """(weights, physical points, u at the points or None) over every cell rule: tensor batches,
+    cell point items and subcell items (verification.jl:201-230 integrates over the same rules)."""
+    x = None if full_values is None else np.asarray(full_values, dtype=np.float64)
+    D = plan.D
+    vals = _point_values(plan, x) if x is not None else [None] * len(plan.batches)
+    for b, u in zip(plan.batches, vals):
+        yield _point_weights(plan, b).reshape(-1), b.points.reshape(-1, D), None if u is None else u.reshape(-1)
     for b in plan.point_batches:
         if b.kind == L.GRICO_ITEM_CELL:
-            out.append((b.weights, b.points))
-    return out
+            u = None
+            if x is not None:
+                loc = _local_coefficients(b, x)
+                item = np.repeat(np.arange(len(b.cells)), np.diff(b.point_offsets))
+                u = _eval_at(b, loc, item, b.ref_points)
+            yield b.weights, b.points, u
+        elif b.kind == L.GRICO_ITEM_SUBCELLS:
+            loc = _local_coefficients(b, x) if x is not None else None
+            for X, w, item, xi in _subcell_point_chunks(b):
+                yield w, X, (_eval_at(b, loc, item, xi) if loc is not None else None)
+
+
+def _eval_at(b, loc, item, ref):
+    """u at reference points `ref` of the items `item` from their local coefficients."""
+    D = ref.shape[1]
+    phi = np.ones((ref.shape[0], 1))
+    for a in range(D):
+        va, _ = fe_basis_table(ref[:, a], b.degree[a])
+        # box index axis 1 fastest: new = old + stride * m_a
+        phi = (va[:, :, None] * phi[:, None, :]).reshape(phi.shape[0], -1)
+    return np.einsum("pm,pm->p", phi, loc[item])
+
+
+def _quadrature_sets(plan):
+    """(weights, physical points) of every cell rule."""
+    return [(w, X) for w, X, _ in _quadrature_chunks(plan)]
 
 
 def l2_error(state, exact):
     """Quadrature L2 error on the cell rules, cut-cell rules included (verification.jl:201-230,
     270-275)."""
-    plan = state.plan
     err2 = 0.0
-    values = _point_values(plan, state.coefficients) + _point_item_values(plan, state.coefficients)
-    for (w, pts), u in zip(_quadrature_sets(plan), values):
-        ex = np.asarray(exact(pts), dtype=np.float64).reshape(-1)
-        err2 += float(np.sum(w * (u.reshape(-1) - ex) ** 2))
+    for w, X, u in _quadrature_chunks(state.plan, state.coefficients):
+        ex = np.asarray(exact(X), dtype=np.float64).reshape(-1)
+        err2 += float(np.sum(w * (u - ex) ** 2))
     return math.sqrt(err2)
 
 
 def relative_l2_error(state, exact):
-    plan = state.plan
     num = l2_error(state, exact)
     den2 = 0.0
-    for w, pts in _quadrature_sets(plan):
-        ex = np.asarray(exact(pts), dtype=np.float64).reshape(-1)
+    for w, X, _ in _quadrature_chunks(state.plan):
+        ex = np.asarray(exact(X), dtype=np.float64).reshape(-1)
         den2 += float(np.sum(w * ex ** 2))
     return num / math.sqrt(den2) if den2 > 0 else num
 
@@ -867,26 +1007,6 @@ def _local_coefficients(b, x):
             lo, hi = b.tail_offsets[k], b.tail_offsets[k + 1]
             loc[r, c] = float(np.dot(b.tail_coef[lo:hi], x[b.tail_index[lo:hi]]))
     return loc
-
-
-def _point_item_values(plan, full_values):
-    """u at the points of every cell point item batch."""
-    x = np.asarray(full_values, dtype=np.float64)
-    D = plan.D
-    out = []
-    for b in plan.point_batches:
-        if b.kind != L.GRICO_ITEM_CELL:
-            continue
-        loc = _local_coefficients(b, x)
-        counts = np.diff(b.point_offsets)
-        item = np.repeat(np.arange(len(b.cells)), counts)
-        phi = np.ones((b.ref_points.shape[0], 1))
-        for a in range(D):
-            va, _ = fe_basis_table(b.ref_points[:, a], b.degree[a])
-            # box index axis 1 fastest: new = old + stride * m_a
-            phi = (va[:, :, None] * phi[:, None, :]).reshape(phi.shape[0], -1)
-        out.append(np.einsum("pm,pm->p", phi, loc[item]))
-    return out
 
 
 def _point_weights(plan, b):

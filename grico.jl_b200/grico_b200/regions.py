@@ -231,6 +231,93 @@ class PhysicalDomain:
         counts = np.bincount(c, minlength=n)
         return np.concatenate([[0], np.cumsum(counts)]).astype(np.int64), x[perm], w[perm]
 
+    def subcell_quadrature(self, cells, qshape, gauss, chunk=8192):
+        """The candidate rule of cut cells as octree subcells (the representation the subcell
+        kernel integrates by sum factorisation): per cell, in depth-first order, the inside
+        subcells and the terminal cut subcells with a keep mask over the qshape tensor points
+        (bit p, axis 1 fastest).  Returns (offsets [n+1], level [S], pos [S, D], mask [S] uint64,
+        weight factor [S] = 2^(-D level), slivers) where slivers maps a cell index to the
+        explicit (points, weights) of the sliver fallback (regions.jl:794-817)."""
+        cells = np.asarray(cells, dtype=np.int64)
+        D = self.D
+        nq = int(np.prod(qshape))
+        if nq > 64:
+            raise ValueError("subcell masks hold at most 64 points")
+        maxd = self.region.subdivision_depth
+        B = 1 << D
+        eta, _ = _tensor_rule(qshape, gauss)
+        bits = _corner_bits(D)
+        pw = (np.uint64(1) << np.arange(nq, dtype=np.uint64))
+        out_c, out_k, out_lev, out_pos, out_mask = [], [], [], [], []
+        slivers = {}
+        for s0 in range(0, len(cells), chunk):
+            cc = cells[s0:s0 + chunk]
+            n = len(cc)
+            cid = np.arange(n)
+            lower = -np.ones((n, D))
+            upper = np.ones((n, D))
+            key = np.zeros(n, dtype=np.int64)
+            for depth in range(maxd + 1):
+                if cid.size == 0:
+                    break
+                cls = self.classify(cc[cid], lower, upper)
+                terminal = depth >= maxd
+                center = 0.5 * (lower + upper)
+                half = 0.5 * (upper - lower)
+                emit = np.nonzero((cls == 1) | ((cls == 2) & terminal))[0]
+                if emit.size:
+                    keep = np.ones((emit.size, nq), dtype=bool)
+                    cut = np.nonzero(cls[emit] == 2)[0]
+                    if cut.size:
+                        xi = center[emit[cut], None, :] + half[emit[cut], None, :] * eta[None, :, :]
+                        X = self.map_from_biunit(np.repeat(cc[cid[emit[cut]]], nq), xi.reshape(-1, D))
+                        keep[cut] = (classifier_values(self.region.classifier, X) < 0.0).reshape(cut.size, nq)
+                    has = np.any(keep, axis=1)
+                    e2 = emit[has]
+                    out_c.append(cid[e2] + s0)
+                    out_k.append(key[e2])
+                    out_lev.append(np.full(e2.size, depth, dtype=np.int32))
+                    out_pos.append(np.rint((lower[e2] + 1.0) * (2.0 ** (depth - 1))).astype(np.int32))
+                    out_mask.append((keep[has].astype(np.uint64) * pw[None, :]).sum(axis=1, dtype=np.uint64))
+                    empty = emit[~has]
+                    if empty.size:
+                        blocks = []
+                        self._sliver_fallback(blocks, cc, cid[empty], key[empty], lower[empty], upper[empty])
+                        bc, _, _, bx, bw = blocks[0]
+                        for c in np.unique(bc):
+                            sel = bc == c
+                            prev = slivers.get(int(c) + s0)
+                            pts, wts = bx[sel], bw[sel]
+                            if prev is not None:
+                                pts, wts = np.concatenate([prev[0], pts]), np.concatenate([prev[1], wts])
+                            slivers[int(c) + s0] = (pts, wts)
+                split = np.nonzero((cls == 2) & (not terminal))[0]
+                if split.size == 0:
+                    break
+                mid = center[split]
+                weight = B ** (maxd - depth - 1)
+                lo = np.where(bits[None, :, :], mid[:, None, :], lower[split, None, :]).reshape(-1, D)
+                hi = np.where(bits[None, :, :], upper[split, None, :], mid[:, None, :]).reshape(-1, D)
+                key = (key[split, None] + np.arange(B)[None, :] * weight).reshape(-1)
+                cid = np.repeat(cid[split], B)
+                lower, upper = lo, hi
+        if out_c:
+            c = np.concatenate(out_c)
+            k = np.concatenate(out_k)
+            perm = np.lexsort((k, c))
+            lev = np.concatenate(out_lev)[perm]
+            pos = np.concatenate(out_pos)[perm].reshape(-1, D)
+            mask = np.concatenate(out_mask)[perm]
+            counts = np.bincount(c, minlength=len(cells))
+        else:
+            lev = np.zeros(0, dtype=np.int32)
+            pos = np.zeros((0, D), dtype=np.int32)
+            mask = np.zeros(0, dtype=np.uint64)
+            counts = np.zeros(len(cells), dtype=np.int64)
+        off = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+        ws = np.ldexp(1.0, -D * lev.astype(np.int64))
+        return off, lev, np.ascontiguousarray(pos, dtype=np.int32), mask, ws, slivers
+
     def _sliver_fallback(self, blocks, cells, cid, key, lower, upper):
         """regions.jl:794-817: centre then corners with negative values, weight vol/(2^D+1)."""
         D = self.D

@@ -125,6 +125,14 @@ typedef struct GricoCellBatchDesc {
  * (examples/annular_nitsche_fcm/driver.jl:52-62) with eta per item. */
 #define GRICO_ITEM_CELL 1
 #define GRICO_ITEM_NITSCHE 2
+/* Finite-cell cut cells as octree subcells (regions.jl:477-510): each subcell carries the
+ * cell's tensor rule of qpoints[a] Gauss points per axis mapped onto the subcell
+ * [-1 + 2 pos 2^-level, -1 + 2 (pos + 1) 2^-level] per axis, a keep mask over those
+ * prod(qpoints) <= 64 points (bit p, axis 1 fastest) and a weight factor (2^(-dim level) times
+ * the measure factor of FiniteCellExtension).  Uses the plan's mass/kappa form; the point
+ * arrays of the descriptor (point_offsets, ref_points, weights, normals, eta) are unused and
+ * kappa_points / rhs source values are given per subcell point [n_subcells * prod(qpoints)]. */
+#define GRICO_ITEM_SUBCELLS 3
 
 typedef struct GricoPointBatchDesc {
   int32_t n_items;
@@ -143,6 +151,13 @@ typedef struct GricoPointBatchDesc {
   const double* normals;      /* [n_points*dim] unit normals (GRICO_ITEM_NITSCHE)           */
   const double* eta;          /* [n_items] penalty (GRICO_ITEM_NITSCHE)                     */
   const double* kappa_points; /* [n_points] or NULL (GRICO_ITEM_CELL)                       */
+  /* GRICO_ITEM_SUBCELLS only */
+  int32_t qpoints[3];
+  const int64_t* subcell_offsets; /* [n_items+1]                                            */
+  const int32_t* subcell_level;   /* [n_subcells]                                           */
+  const int32_t* subcell_pos;     /* [n_subcells*dim]                                       */
+  const uint64_t* subcell_mask;   /* [n_subcells]                                           */
+  const double* subcell_weight;   /* [n_subcells]                                           */
 } GricoPointBatchDesc;
 
 typedef struct GricoPlanDesc {

@@ -157,9 +157,9 @@ def test_circle_quadrature_exact_and_oracle_mapping():
 
 def test_annulus_plan_structure():
     oplan, prob, plan, _ = fc_cases.annulus(device=False)
-    kinds = sorted(b.kind for b in plan.point_batches)
-    assert kinds == [gb._lib.GRICO_ITEM_CELL, gb._lib.GRICO_ITEM_NITSCHE]
-    n_cut = sum(len(b.cells) for b in plan.point_batches if b.kind == gb._lib.GRICO_ITEM_CELL)
+    kinds = {b.kind for b in plan.point_batches}
+    assert gb._lib.GRICO_ITEM_SUBCELLS in kinds and gb._lib.GRICO_ITEM_NITSCHE in kinds
+    n_cut = sum(len(b.cells) for b in plan.point_batches if b.kind == gb._lib.GRICO_ITEM_SUBCELLS)
     assert n_cut == plan.n_cut == len([c for c in oplan.cells if c["q"] is None])
     n_tensor = sum(len(b.cells) for b in plan.batches)
     assert n_tensor + n_cut == len(plan.space.leaves)
@@ -176,3 +176,44 @@ def test_unsupported_surface_forms():
     prob.surface_rhs_operators.append(gb.Nitsche(1.0))
     with pytest.raises(gb.GricoError):
         gb.compile(prob, device=False)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_subcell_representation_equals_candidate_rule(dim):
+    """The subcell records (inside subcells, masked terminal subcells, sliver points) list
+    exactly the candidate points and weights of regions.jl:477-510, bit for bit."""
+    if dim == 2:
+        lev = fc_cases.annulus_levelset(0.35, 1.0)
+        origin, extent, roots, refine, depth, q = (-1.0, -1.0), (2.0, 2.0), (2, 2), 1, 3, (3, 3)
+    else:
+        lev = fc_cases.shell_levelset((1.0, 1.0, 1.0), 0.4, 0.9)
+        origin, extent, roots, refine, depth, q = (0.0,) * 3, (2.0,) * 3, (1, 1, 1), 1, 2, (4, 4, 4)
+    bg = gb.Domain(origin, extent, roots)
+    gb.uniform_refine(bg, refine)
+    pd = gb.PhysicalDomain(bg, gb.ImplicitRegion(lev, subdivision_depth=depth))
+    leaves = bg.grid.active_leaves()
+    cut = leaves[pd.classify(leaves) == 2]
+    off, xi, w = pd.candidate_quadrature(cut, q, _gauss)
+    soff, slev, spos, smask, sws, slivers = pd.subcell_quadrature(cut, q, _gauss)
+    eta, ew = rg._tensor_rule(q, _gauss)
+    for i in range(len(cut)):
+        pts, wts = [], []
+        for s in range(soff[i], soff[i + 1]):
+            half = np.ldexp(1.0, -int(slev[s]))
+            c = -1.0 + (2.0 * spos[s] + 1.0) * half
+            keep = [(int(smask[s]) >> p) & 1 for p in range(len(ew))]
+            for p in range(len(ew)):
+                if keep[p]:
+                    pts.append(c + half * eta[p])
+                    wts.append(ew[p] * sws[s])
+        if i in slivers:
+            pts += list(slivers[i][0])
+            wts += list(slivers[i][1])
+        P = np.array(pts).reshape(-1, dim)
+        Wt = np.array(wts)
+        ref_p, ref_w = xi[off[i]:off[i + 1]], w[off[i]:off[i + 1]]
+        assert P.shape == ref_p.shape
+        o1 = np.lexsort(P.T[::-1])
+        o2 = np.lexsort(ref_p.T[::-1])
+        assert np.array_equal(P[o1], ref_p[o2])
+        assert np.array_equal(Wt[o1], ref_w[o2])
