@@ -208,6 +208,8 @@ def solve_legs(gb, L, plan, prob, target=1e-8):
     b = gb.reduced_rhs(plan)
     legs = {
         "fp64_cg_gmg_jacobi_v22 (reference method)": (GeometricMultigridPreconditioner(), 2000),
+        "fp64_cg_gmg_chebyshev3_v22 (plain FP64 GPU, no CUDA graph)": (
+            GeometricMultigridPreconditioner(smoother="chebyshev", pre_smoothing_steps=2, post_smoothing_steps=2), 500),
         "fp64_cg_gmg_chebyshev3_v22 (plain FP64 GPU)": (
             GeometricMultigridPreconditioner(smoother="chebyshev", pre_smoothing_steps=2, post_smoothing_steps=2), 500),
         "mixed_cg_fp64_gmg_chebyshev3_v22_fp32": (
@@ -228,8 +230,9 @@ def solve_legs(gb, L, plan, prob, target=1e-8):
             x = np.zeros(plan.n_reduced)
             so = L.GricoSolveOptions(rtol, 0.0, maxiter, L.GRICO_PRECOND_MULTIGRID, 30, 0)
             rep = L.GricoSolveReport()
+            flags = L.GRICO_FLAG_HOST_POINTERS | (L.GRICO_FLAG_NO_GRAPH if "no CUDA graph" in name else 0)
             rc = L.lib().grico_cg_solve(plan.handle, mg.handle, L.ptr(b, C.c_double), L.ptr(x, C.c_double),
-                                        C.byref(so), C.byref(rep), L.GRICO_FLAG_HOST_POINTERS)
+                                        C.byref(so), C.byref(rep), flags)
             err = gb.relative_l2_error(gb.State(plan, gb.expand_reduced(plan, x), rep), exact)
             tries.append({"rtol": rtol, "status": int(rc), "iterations": int(rep.iterations),
                           "solve_seconds": float(rep.seconds), "relative_l2_error": err})

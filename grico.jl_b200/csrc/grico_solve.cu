@@ -133,28 +133,58 @@ extern "C" int grico_cg_solve(GricoPlan* P, GricoMultigrid* mg, const double* b,
   rep.initial_residual = std::sqrt(rr);
   int it = 0;
   bool converged = rr <= tol * tol;
+  // One iteration as a fixed sequence of stream operations: operator apply, p.Ap, x/r update
+  // with ||r||^2, preconditioner with r.z, new direction.  It is replayed as one CUDA graph
+  // (the multigrid V-cycle alone is hundreds of small launches); after each replay the host
+  // reads p.Ap and ||r||^2 with a single copy.
+  auto iteration = [&](cudaStream_t s) -> int {
+    run_apply<double>(P, true, p, q, 1, s);
+    dot_into(P, p, q, n, Scalars::PAP, s);
+    cg_update_xr<<<kRedBlocks, kRedThreads, 0, s>>>(xd, r, p, q, P->scalars.get<double>(), n, P->partial.get<double>());
+    reduce_final<<<1, kRedThreads, 0, s>>>(P->partial.get<double>(), kRedBlocks, P->scalars.get<double>() + Scalars::RR);
+    int prc = apply_preconditioner(P, mg, opts->preconditioner, r, z, s, Scalars::RZ_NEW);
+    if (prc) return prc;
+    cg_direction<<<kRedBlocks, kRedThreads, 0, s>>>(p, z, P->scalars.get<double>() + Scalars::RZ_NEW,
+                                                    P->scalars.get<double>() + Scalars::RZ, n);
+    cudaMemcpyAsync(P->scalars.get<double>() + Scalars::RZ, P->scalars.get<double>() + Scalars::RZ_NEW, sizeof(double),
+                    cudaMemcpyDeviceToDevice, s);
+    return GRICO_OK;
+  };
+  cudaGraphExec_t exec = nullptr;
+  if (!converged && !(flags & GRICO_FLAG_NO_GRAPH)) {
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      const int crc = iteration(st);
+      const cudaError_t ec = cudaStreamEndCapture(st, &graph);
+      if (crc == GRICO_OK && ec == cudaSuccess && graph &&
+          cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess)
+        exec = nullptr;
+      if (graph) cudaGraphDestroy(graph);
+    }
+    (void)cudaGetLastError();  // a failed capture falls back to direct launches
+  }
+  double hs[2] = {0.0, 0.0};  // p.Ap, ||r||^2 (adjacent scalar slots)
   while (!converged && it < opts->maxiter) {
     ++it;
-    run_apply<double>(P, true, p, q, 1, st);
-    dot_into(P, p, q, n, Scalars::PAP, st);
-    double pap = read_scalar(P, Scalars::PAP, st);
+    if (exec) {
+      if (cudaGraphLaunch(exec, st) != cudaSuccess) { status = GRICO_ERR_CUDA; set_error("CG graph launch failed"); break; }
+    } else {
+      rc = iteration(st);
+      if (rc) { status = rc; break; }
+    }
+    cudaMemcpyAsync(hs, P->scalars.get<double>() + Scalars::PAP, 2 * sizeof(double), cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    const double pap = hs[0];
     if (!(pap > 0.0)) {
       status = std::isfinite(pap) ? GRICO_ERR_BREAKDOWN : GRICO_ERR_NONFINITE;
       set_error("CG encountered a non-positive operator direction");
       break;
     }
-    cg_update_xr<<<kRedBlocks, kRedThreads, 0, st>>>(xd, r, p, q, P->scalars.get<double>(), n, P->partial.get<double>());
-    reduce_final<<<1, kRedThreads, 0, st>>>(P->partial.get<double>(), kRedBlocks, P->scalars.get<double>() + Scalars::RR);
-    rc = apply_preconditioner(P, mg, opts->preconditioner, r, z, st, Scalars::RZ_NEW);
-    if (rc) { status = rc; break; }
-    rr = read_scalar(P, Scalars::RR, st);
+    rr = hs[1];
     if (!std::isfinite(rr)) { status = GRICO_ERR_NONFINITE; set_error("CG residual is not finite"); break; }
     if (rr <= tol * tol) { converged = true; break; }
-    cg_direction<<<kRedBlocks, kRedThreads, 0, st>>>(p, z, P->scalars.get<double>() + Scalars::RZ_NEW,
-                                                    P->scalars.get<double>() + Scalars::RZ, n);
-    cudaMemcpyAsync(P->scalars.get<double>() + Scalars::RZ, P->scalars.get<double>() + Scalars::RZ_NEW, sizeof(double),
-                    cudaMemcpyDeviceToDevice, st);
   }
+  if (exec) cudaGraphExecDestroy(exec);
   cudaEventRecord(e1, st);
   cudaEventSynchronize(e1);
   float ms = 0;

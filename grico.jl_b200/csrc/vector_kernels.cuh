@@ -46,6 +46,10 @@ static __global__ void cg_update_xr(double* __restrict__ x, double* __restrict__
                              const double* __restrict__ q, const double* __restrict__ scal, int64_t n,
                              double* __restrict__ partial) {
   __shared__ double sh[32];
+  if (!(scal[1] > 0.0)) {  // breakdown: keep x and r, the host reports it
+    if (threadIdx.x == 0) partial[blockIdx.x] = 0.0;
+    return;
+  }
   const double alpha = scal[0] / scal[1];  // rz / pAp
   double s = 0.0;
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {

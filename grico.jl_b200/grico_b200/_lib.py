@@ -35,6 +35,7 @@ SUBCELL_SHAPES = {3: {(2, 2), (2, 3), (3, 3), (2, 4), (3, 4), (4, 4)},
 GRICO_PREC_FP64 = 0
 GRICO_PREC_FP32 = 1
 GRICO_FLAG_HOST_POINTERS = 1
+GRICO_FLAG_NO_GRAPH = 2
 GRICO_PRECOND_IDENTITY = 0
 GRICO_PRECOND_JACOBI = 1
 GRICO_PRECOND_MULTIGRID = 2

@@ -911,8 +911,9 @@ class State:
 
 
 def solve(plan_or_problem, solver=None, relative_tolerance=None, absolute_tolerance=0.0, maxiter=None,
-          initial_solution=None):
-    """solve(plan; solver=CGSolver(...)) on the reduced system (solve.jl:229-276)."""
+          initial_solution=None, graph=True):
+    """solve(plan; solver=CGSolver(...)) on the reduced system (solve.jl:229-276).  `graph=False`
+    launches each CG iteration op by op instead of replaying it as a CUDA graph."""
     from .multigrid import GeometricMultigridPreconditioner, build_multigrid
 
     plan = plan_or_problem if isinstance(plan_or_problem, AssemblyPlan) else compile(plan_or_problem)
@@ -933,7 +934,8 @@ def solve(plan_or_problem, solver=None, relative_tolerance=None, absolute_tolera
     rep = L.GricoSolveReport()
     fn = L.lib().grico_cg_solve if isinstance(solver, CGSolver) else L.lib().grico_fgmres_solve
     L.check(fn(plan.handle, mg.handle if mg is not None else None, L.ptr(b, C.c_double), L.ptr(x, C.c_double),
-               C.byref(opts), C.byref(rep), L.GRICO_FLAG_HOST_POINTERS), "solve")
+               C.byref(opts), C.byref(rep), L.GRICO_FLAG_HOST_POINTERS | (0 if graph else L.GRICO_FLAG_NO_GRAPH)),
+            "solve")
     return State(plan, expand_reduced(plan, x), rep)
 
 

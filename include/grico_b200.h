@@ -53,6 +53,7 @@ extern "C" {
 #define GRICO_PREC_FP32 1 /* vectors float, arithmetic float (mixed-precision path) */
 
 #define GRICO_FLAG_HOST_POINTERS 1 /* vector arguments are host memory: copy in/out */
+#define GRICO_FLAG_NO_GRAPH 2      /* Krylov solves: launch each iteration op by op, no CUDA graph */
 
 /* ================================================================================
  * Host space compile (native replacement of the Julia-side HpSpace construction)

@@ -114,3 +114,17 @@ def test_mixed_precision_cg_gmg_reaches_fp64_accuracy(cuda):
                    relative_tolerance=1e-12)
     assert rel_err(s32.coefficients, s64.coefficients) <= 1e-10
     assert s32.report.iterations <= s64.report.iterations + 3
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_graph_replayed_cg_matches_direct_launches(cuda, precision):
+    """Replaying each CG iteration as one CUDA graph runs the same operations in the same order
+    as launching them one by one: same iteration count, same iterate to rounding."""
+    D = 3
+    src = lambda x: np.prod(np.sin(np.pi * x), axis=1) * (1.0 + D * np.pi ** 2)
+    _, plan = _pair("3d_p2", source=src)
+    pre = GeometricMultigridPreconditioner(smoother="chebyshev", precision=precision)
+    sg = gb.solve(plan, solver=gb.CGSolver(pre), relative_tolerance=1e-11, graph=True)
+    sd = gb.solve(plan, solver=gb.CGSolver(pre), relative_tolerance=1e-11, graph=False)
+    assert sg.report.iterations == sd.report.iterations
+    assert rel_err(sg.coefficients, sd.coefficients) <= 1e-12
