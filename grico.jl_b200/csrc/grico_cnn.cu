@@ -1,0 +1,118 @@
+// C ABI of the learned-smoother network primitives: 3x3x3 convolutions (forward, backward
+// data, backward weight), ReLU backward, masked mean squared error and Adam.  All pointers are
+// device pointers; every call is asynchronous on the given stream (NULL: the legacy stream).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <string>
+
+#include "cnn_kernels.cuh"
+#include "grico_host.h"
+#include "vector_kernels.cuh"
+
+using namespace grico;
+
+namespace {
+
+cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+
+bool conv_args_ok(int B, int Ci, int Co, int Z, int Y, int X) {
+  return B > 0 && Ci > 0 && Co > 0 && Z > 0 && Y > 0 && X > 0 && B <= 65535 && Co <= 65535 * kConvCo;
+}
+
+dim3 conv_grid(int B, int Co, int Z, int Y, int X) {
+  const int tiles = ((X + kConvTile - 1) / kConvTile) * ((Y + kConvTile - 1) / kConvTile) *
+                    ((Z + kConvTile - 1) / kConvTile);
+  return dim3(tiles, (Co + kConvCo - 1) / kConvCo, B);
+}
+
+int launch_status(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return GRICO_ERR_CUDA;
+  }
+  return GRICO_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int grico_conv3d_forward(const void* x, int x_bf16, const float* w, const float* bias, void* y, int y_bf16, int B,
+                         int Ci, int Co, int Z, int Y, int X, int relu, void* stream) {
+  if (!x || !w || !y || !conv_args_ok(B, Ci, Co, Z, Y, X)) {
+    set_error("grico_conv3d_forward: invalid argument");
+    return GRICO_ERR_INVALID;
+  }
+  const dim3 grid = conv_grid(B, Co, Z, Y, X);
+  cudaStream_t st = as_stream(stream);
+  if (!x_bf16 && !y_bf16)
+    conv3d_fwd<float, float><<<grid, 512, 0, st>>>(static_cast<const float*>(x), w, bias, static_cast<float*>(y), Ci, Co, Z, Y, X, relu);
+  else if (!x_bf16 && y_bf16)
+    conv3d_fwd<float, __nv_bfloat16><<<grid, 512, 0, st>>>(static_cast<const float*>(x), w, bias,
+                                                           static_cast<__nv_bfloat16*>(y), Ci, Co, Z, Y, X, relu);
+  else if (x_bf16 && y_bf16)
+    conv3d_fwd<__nv_bfloat16, __nv_bfloat16><<<grid, 512, 0, st>>>(static_cast<const __nv_bfloat16*>(x), w, bias,
+                                                                   static_cast<__nv_bfloat16*>(y), Ci, Co, Z, Y, X, relu);
+  else
+    conv3d_fwd<__nv_bfloat16, float><<<grid, 512, 0, st>>>(static_cast<const __nv_bfloat16*>(x), w, bias,
+                                                           static_cast<float*>(y), Ci, Co, Z, Y, X, relu);
+  return launch_status("grico_conv3d_forward");
+}
+
+// gx = conv^T(gy, w); wt: caller scratch of Co*Ci*27 floats for the flipped, transposed weights
+int grico_conv3d_backward_data(const float* gy, const float* w, float* wt, float* gx, int B, int Ci, int Co, int Z,
+                               int Y, int X, void* stream) {
+  if (!gy || !w || !wt || !gx || !conv_args_ok(B, Co, Ci, Z, Y, X)) {
+    set_error("grico_conv3d_backward_data: invalid argument");
+    return GRICO_ERR_INVALID;
+  }
+  cudaStream_t st = as_stream(stream);
+  conv3d_flip_transpose<<<64, 256, 0, st>>>(w, wt, Ci, Co);
+  conv3d_fwd<float, float><<<conv_grid(B, Ci, Z, Y, X), 512, 0, st>>>(gy, wt, nullptr, gx, Co, Ci, Z, Y, X, 0);
+  return launch_status("grico_conv3d_backward_data");
+}
+
+int grico_conv3d_backward_weight(const float* x, const float* gy, float* gw, float* gb, int B, int Ci, int Co, int Z,
+                                 int Y, int X, void* stream) {
+  if (!x || !gy || !gw || !conv_args_ok(B, Ci, Co, Z, Y, X) || Ci > 65535) {
+    set_error("grico_conv3d_backward_weight: invalid argument");
+    return GRICO_ERR_INVALID;
+  }
+  conv3d_bwd_weight<<<dim3(Ci, Co), 256, 0, as_stream(stream)>>>(x, gy, gw, gb, B, Ci, Co, Z, Y, X);
+  return launch_status("grico_conv3d_backward_weight");
+}
+
+int grico_relu_backward(const float* y, float* g, int64_t n, void* stream) {
+  if (!y || !g || n < 0) return GRICO_ERR_INVALID;
+  if (n == 0) return GRICO_OK;
+  relu_backward<<<int(std::min<int64_t>((n + 255) / 256, 148 * 16)), 256, 0, as_stream(stream)>>>(y, g, n);
+  return launch_status("grico_relu_backward");
+}
+
+// g = d/dp of sum(m (p - t)^2) / count; loss (device double) = that sum / count.
+// partial: caller scratch of kRedBlocks doubles.
+int grico_mse_grad(const float* p, const float* t, const float* mask, float* g, int64_t n, double count,
+                   double* partial, double* loss, void* stream) {
+  if (!p || !t || !g || !partial || !loss || n <= 0 || !(count > 0)) return GRICO_ERR_INVALID;
+  cudaStream_t st = as_stream(stream);
+  mse_grad<<<kRedBlocks, 256, 0, st>>>(p, t, mask, g, n, float(1.0 / count), partial);
+  reduce_final<<<1, kRedThreads, 0, st>>>(partial, kRedBlocks, loss);
+  scale_scalar<<<1, 1, 0, st>>>(loss, 1.0 / count);
+  return launch_status("grico_mse_grad");
+}
+
+int grico_adam_step(float* w, const float* g, float* m, float* v, int64_t n, float lr, float beta1, float beta2,
+                    int step, float eps, void* stream) {
+  if (!w || !g || !m || !v || n < 0 || step < 1) return GRICO_ERR_INVALID;
+  if (n == 0) return GRICO_OK;
+  const float c1 = 1.0f - std::pow(beta1, float(step));
+  const float c2 = 1.0f - std::pow(beta2, float(step));
+  adam_step<<<int(std::min<int64_t>((n + 255) / 256, 148 * 16)), 256, 0, as_stream(stream)>>>(w, g, m, v, n, lr, beta1,
+                                                                                            beta2, c1, c2, eps);
+  return launch_status("grico_adam_step");
+}
+
+}  // extern "C"

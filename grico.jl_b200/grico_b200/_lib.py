@@ -188,6 +188,13 @@ SIGNATURES = {
     "grico_mg_destroy": (C.c_int, [P]),
     "grico_mg_vcycle": (C.c_int, [P, f64p, f64p, C.c_int]),
     "grico_mg_lambda_max": (C.c_double, [P, C.c_int]),
+    "grico_conv3d_forward": (C.c_int, [P, C.c_int, P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                       C.c_int, C.c_int, P]),
+    "grico_conv3d_backward_data": (C.c_int, [P, P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P]),
+    "grico_conv3d_backward_weight": (C.c_int, [P, P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P]),
+    "grico_relu_backward": (C.c_int, [P, P, C.c_int64, P]),
+    "grico_mse_grad": (C.c_int, [P, P, P, P, C.c_int64, C.c_double, P, P, P]),
+    "grico_adam_step": (C.c_int, [P, P, P, P, C.c_int64, C.c_float, C.c_float, C.c_float, C.c_int, C.c_float, P]),
     "grico_last_error": (C.c_char_p, []),
 }
 

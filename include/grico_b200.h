@@ -291,6 +291,26 @@ double grico_mg_lambda_max(GricoMultigrid* mg, int level);
 
 const char* grico_last_error(void);
 
+/* ---- learned smoother: network primitives (device pointers, asynchronous on `stream`) ----
+ * No reference counterpart: the learned smoother is an addition of this library.  Tensors are
+ * [batch][channel][z][y][x]; convolutions are 3x3x3, stride 1, zero padding; weights
+ * [out][in][27] FP32; activations FP32 or BF16 (x_bf16 / y_bf16), FP32 arithmetic. */
+int grico_conv3d_forward(const void* x, int x_bf16, const float* w, const float* bias, void* y, int y_bf16, int B,
+                         int Ci, int Co, int Z, int Y, int X, int relu, void* stream);
+/* gx = transposed convolution of gy; wt: scratch of Co*Ci*27 floats */
+int grico_conv3d_backward_data(const float* gy, const float* w, float* wt, float* gx, int B, int Ci, int Co, int Z,
+                               int Y, int X, void* stream);
+/* gw = d loss / d w, gb = d loss / d bias (NULL: skipped); overwrites, does not accumulate */
+int grico_conv3d_backward_weight(const float* x, const float* gy, float* gw, float* gb, int B, int Ci, int Co, int Z,
+                                 int Y, int X, void* stream);
+int grico_relu_backward(const float* y, float* g, int64_t n, void* stream);
+/* masked mean squared error sum(m (p - t)^2) / count into *loss (device double) and its
+ * gradient g; partial: scratch of 592 doubles */
+int grico_mse_grad(const float* p, const float* t, const float* mask, float* g, int64_t n, double count,
+                   double* partial, double* loss, void* stream);
+int grico_adam_step(float* w, const float* g, float* m, float* v, int64_t n, float lr, float beta1, float beta2,
+                    int step, float eps, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
