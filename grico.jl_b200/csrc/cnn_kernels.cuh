@@ -176,4 +176,46 @@ static __global__ void adam_step(float* __restrict__ w, const float* __restrict_
   }
 }
 
+// dst[g] = src[idx[g]] * scale * (scale_dev ? *scale_dev : 1) for idx[g] >= 0, else 0
+template <typename TS, typename TD>
+__global__ void grid_gather(const int64_t* __restrict__ idx, int64_t n_grid, const TS* __restrict__ src, float scale,
+                            const double* __restrict__ scale_dev, TD* __restrict__ dst) {
+  const float s = scale * (scale_dev ? float(*scale_dev) : 1.0f);
+  for (int64_t g = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; g < n_grid; g += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t i = idx[g];
+    dst[g] = from_f<TD>(i >= 0 ? float(src[i]) * s : 0.0f);
+  }
+}
+
+// dst[idx[g]] += src[g] * scale * (scale_dev ? *scale_dev : 1) (each dof appears once in the grid)
+template <typename TS, typename TD>
+__global__ void grid_scatter_add(const int64_t* __restrict__ idx, int64_t n_grid, const TS* __restrict__ src,
+                                 float scale, const double* __restrict__ scale_dev, TD* __restrict__ dst) {
+  const float s = scale * (scale_dev ? float(*scale_dev) : 1.0f);
+  for (int64_t g = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; g < n_grid; g += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t i = idx[g];
+    if (i >= 0) dst[i] += TD(to_f(src[g]) * s);
+  }
+}
+
+// out = w (r - ar); partial sums of w (r - ar)^2
+template <typename T>
+__global__ void weighted_residual(const T* __restrict__ r, const T* __restrict__ ar, const T* __restrict__ w,
+                                  T* __restrict__ out, int64_t n, double* __restrict__ partial) {
+  __shared__ double sh[256];
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    const double d = double(r[i]) - double(ar[i]);
+    out[i] = T(double(w[i]) * d);
+    s += double(w[i]) * d * d;
+  }
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = sh[0];
+}
+
 }  // namespace grico

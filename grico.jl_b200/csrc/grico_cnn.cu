@@ -115,4 +115,33 @@ int grico_adam_step(float* w, const float* g, float* m, float* v, int64_t n, flo
   return launch_status("grico_adam_step");
 }
 
+// grid <- reduced vector (idx[g] = reduced dof of grid point g or -1), FP32
+int grico_grid_gather(const int64_t* idx, int64_t n_grid, const float* src, float scale, float* dst, void* stream) {
+  if (!idx || !src || !dst || n_grid < 0) return GRICO_ERR_INVALID;
+  if (n_grid == 0) return GRICO_OK;
+  grid_gather<float, float><<<int(std::min<int64_t>((n_grid + 255) / 256, 148 * 16)), 256, 0, as_stream(stream)>>>(
+      idx, n_grid, src, scale, nullptr, dst);
+  return launch_status("grico_grid_gather");
+}
+
+// reduced vector += scale * grid, FP32
+int grico_grid_scatter_add(const int64_t* idx, int64_t n_grid, const float* src, float scale, float* dst,
+                           void* stream) {
+  if (!idx || !src || !dst || n_grid < 0) return GRICO_ERR_INVALID;
+  if (n_grid == 0) return GRICO_OK;
+  grid_scatter_add<float, float><<<int(std::min<int64_t>((n_grid + 255) / 256, 148 * 16)), 256, 0, as_stream(stream)>>>(
+      idx, n_grid, src, scale, nullptr, dst);
+  return launch_status("grico_grid_scatter_add");
+}
+
+// out = w (r - ar), *sum = sum w (r - ar)^2 (device double); partial: scratch of 592 doubles
+int grico_weighted_residual(const float* r, const float* ar, const float* w, float* out, int64_t n, double* partial,
+                            double* sum, void* stream) {
+  if (!r || !ar || !w || !out || !partial || !sum || n <= 0) return GRICO_ERR_INVALID;
+  cudaStream_t st = as_stream(stream);
+  weighted_residual<float><<<kRedBlocks, 256, 0, st>>>(r, ar, w, out, n, partial);
+  reduce_final<<<1, kRedThreads, 0, st>>>(partial, kRedBlocks, sum);
+  return launch_status("grico_weighted_residual");
+}
+
 }  // extern "C"

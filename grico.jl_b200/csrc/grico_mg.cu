@@ -24,6 +24,7 @@
 #include "grico_mg_internal.h"
 #include "grico_plan_internal.h"
 #include "vector_kernels.cuh"
+#include "cnn_kernels.cuh"
 
 struct GricoMultigrid {
   struct Transfer {
@@ -43,6 +44,19 @@ struct GricoMultigrid {
   GricoMGOptions opts{};
   cudaStream_t stream = nullptr;
   grico::DevBuf io_r, io_z;
+  // learned smoother sweep on one level (see learned_sweep)
+  struct Learned {
+    int level = -1;
+    int nx = 0, ny = 0, nz = 0;
+    int64_t n_grid = 0;
+    double omega = 1.0;
+    std::vector<int> ch;                 // channels at each layer boundary
+    std::vector<grico::DevBuf> w, bias;  // FP32 weights [co][ci][27] and biases per layer
+    grico::DevBuf idx;                   // grid point -> reduced dof (or -1)
+    grico::DevBuf in, act0, act1;        // BF16 network input (channel 1: log coefficient) and activations
+    grico::DevBuf out;                   // FP32 network output grid
+    grico::DevBuf xn, tn, z;             // candidate iterate, its operator image, D^-1 r (level precision)
+  } learned;
 };
 
 namespace grico {
@@ -214,6 +228,73 @@ void coarse_solve(GricoMultigrid* mg, float* x, const float* b, cudaStream_t st)
   cast_kernel<double, float><<<blocks(n), 256, 0, st>>>(mg->coarse_x.get<double>(), x, n);
 }
 
+// s[1] = sqrt(s[0] / n) (the D^-1-weighted residual scale), s[2] = 1 / s[1] (0 if s[1] == 0)
+__global__ void residual_scale(double* s, int64_t n) {
+  const double sig = sqrt(s[0] / double(n > 0 ? n : 1));
+  s[1] = sig;
+  s[2] = sig > 0.0 ? 1.0 / sig : 0.0;
+}
+
+// accept the candidate iterate when its weighted residual norm is smaller
+template <typename T>
+__global__ void select_iterate(T* __restrict__ x, const T* __restrict__ xn, int64_t n, const double* __restrict__ s_old,
+                               const double* __restrict__ s_new) {
+  if (!(*s_new < *s_old)) return;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    x[i] = xn[i];
+}
+
+template <typename T>
+T* lbuf(grico::DevBuf& b) { return b.get<T>(); }
+
+// One learned smoother sweep on level l: r = b - A x, c = sigma * N(D^-1 r / sigma, log a) on the
+// level's grid, x_new = x + omega c, kept only if ||b - A x_new||_{D^-1} < ||r||_{D^-1}, so the
+// true residual judges every sweep and the plain iterate is the fallback.
+template <typename T>
+void learned_sweep(GricoMultigrid* mg, int l, T* x, const T* b, cudaStream_t st) {
+  using B = LevelBufs<T>;
+  auto& L = mg->learned;
+  const int64_t n = mg->levels[l]->n_red;
+  T* t = B::t(mg, l);
+  T* r = B::r(mg, l);
+  const T* dinv = B::dinv(mg, l);
+  double* sc = mg->levels[l]->scalars.get<double>() + 8;  // [0] old norm^2, [1] sigma, [2] 1/sigma, [3] new norm^2
+  double* partial = mg->levels[l]->partial.get<double>();
+  level_apply<T>(mg, l, x, t, st);
+  weighted_residual<T><<<kRedBlocks, 256, 0, st>>>(b, t, dinv, lbuf<T>(L.z), n, partial);  // z = D^-1 r
+  reduce_final<<<1, kRedThreads, 0, st>>>(partial, kRedBlocks, sc);
+  residual_scale<<<1, 1, 0, st>>>(sc, n);
+  const int gb = int(std::min<int64_t>((L.n_grid + 255) / 256, 148 * 16));
+  __nv_bfloat16* in = L.in.get<__nv_bfloat16>();
+  grid_gather<T, __nv_bfloat16><<<gb, 256, 0, st>>>(L.idx.get<int64_t>(), L.n_grid, lbuf<T>(L.z), 1.0f, sc + 2, in);
+  const int nl = int(L.w.size());
+  const __nv_bfloat16* src = in;
+  for (int k = 0; k < nl; ++k) {
+    const int ci = L.ch[k], co = L.ch[k + 1];
+    const int tiles = ((L.nx + kConvTile - 1) / kConvTile) * ((L.ny + kConvTile - 1) / kConvTile) *
+                      ((L.nz + kConvTile - 1) / kConvTile);
+    const dim3 grid(tiles, (co + kConvCo - 1) / kConvCo, 1);
+    if (k + 1 < nl) {
+      __nv_bfloat16* dst = (k % 2 == 0) ? L.act0.get<__nv_bfloat16>() : L.act1.get<__nv_bfloat16>();
+      conv3d_fwd<__nv_bfloat16, __nv_bfloat16><<<grid, 512, 0, st>>>(src, L.w[k].get<float>(), L.bias[k].get<float>(),
+                                                                     dst, ci, co, L.nz, L.ny, L.nx, 1);
+      src = dst;
+    } else {
+      conv3d_fwd<__nv_bfloat16, float><<<grid, 512, 0, st>>>(src, L.w[k].get<float>(), L.bias[k].get<float>(),
+                                                             L.out.get<float>(), ci, co, L.nz, L.ny, L.nx, 0);
+    }
+  }
+  T* xn = lbuf<T>(L.xn);
+  cudaMemcpyAsync(xn, x, sizeof(T) * n, cudaMemcpyDeviceToDevice, st);
+  grid_scatter_add<float, T><<<gb, 256, 0, st>>>(L.idx.get<int64_t>(), L.n_grid, L.out.get<float>(), float(L.omega),
+                                                 sc + 1, xn);
+  T* tn = lbuf<T>(L.tn);
+  level_apply<T>(mg, l, xn, tn, st);
+  weighted_residual<T><<<kRedBlocks, 256, 0, st>>>(b, tn, dinv, lbuf<T>(L.z), n, partial);
+  reduce_final<<<1, kRedThreads, 0, st>>>(partial, kRedBlocks, sc + 3);
+  select_iterate<T><<<blocks(n), 256, 0, st>>>(x, xn, n, sc, sc + 3);
+}
+
 template <typename T>
 void vcycle(GricoMultigrid* mg, int l, T* x, const T* b, cudaStream_t st) {
   using B = LevelBufs<T>;
@@ -223,7 +304,13 @@ void vcycle(GricoMultigrid* mg, int l, T* x, const T* b, cudaStream_t st) {
     return;
   }
   cudaMemsetAsync(x, 0, sizeof(T) * n, st);
-  smooth<T>(mg, l, x, b, mg->opts.pre_steps, st);
+  if (mg->learned.level == l) {
+    // the learned sweep replaces the last pre-smoothing step on its level
+    smooth<T>(mg, l, x, b, std::max(mg->opts.pre_steps - 1, 0), st);
+    learned_sweep<T>(mg, l, x, b, st);
+  } else {
+    smooth<T>(mg, l, x, b, mg->opts.pre_steps, st);
+  }
   T* t = B::t(mg, l);
   T* r = B::r(mg, l);
   level_apply<T>(mg, l, x, t, st);
@@ -466,6 +553,61 @@ int grico_mg_vcycle(GricoMultigrid* mg, const double* r, double* z, int flags) {
   if (rc) return rc;
   if (flags & GRICO_FLAG_HOST_POINTERS) cudaMemcpyAsync(z, zd, 8 * n, cudaMemcpyDeviceToHost, st);
   return cuda_ok(cudaStreamSynchronize(st), "vcycle") ? GRICO_OK : GRICO_ERR_CUDA;
+}
+
+int grico_mg_set_learned(GricoMultigrid* mg, const GricoLearnedDesc* d) {
+  if (!mg) return GRICO_ERR_INVALID;
+  if (!d) {
+    mg->learned = GricoMultigrid::Learned{};
+    return GRICO_OK;
+  }
+  const int nlev = int(mg->levels.size());
+  if (d->level < 1 || d->level >= nlev || d->nx < 1 || d->ny < 1 || d->nz < 1 || d->n_layers < 1 || !d->channels ||
+      !d->weights || !d->biases || !d->grid_index || !d->grid_log_coefficient) {
+    set_error("grico_mg_set_learned: invalid descriptor (the level must be a smoothed level, 1..levels-1)");
+    return GRICO_ERR_INVALID;
+  }
+  if (d->channels[0] != 2 || d->channels[d->n_layers] != 1) {
+    set_error("grico_mg_set_learned: the network maps 2 input channels (residual, log coefficient) to 1");
+    return GRICO_ERR_INVALID;
+  }
+  const int64_t ng = int64_t(d->nx) * d->ny * d->nz;
+  const int64_t n = mg->levels[d->level]->n_red;
+  for (int64_t g = 0; g < ng; ++g)
+    if (d->grid_index[g] < -1 || d->grid_index[g] >= n) {
+      set_error("grico_mg_set_learned: grid index out of range");
+      return GRICO_ERR_INVALID;
+    }
+  GricoMultigrid::Learned L;
+  L.level = d->level;
+  L.nx = d->nx;
+  L.ny = d->ny;
+  L.nz = d->nz;
+  L.n_grid = ng;
+  L.omega = d->omega;
+  int maxc = 1;
+  for (int k = 0; k <= d->n_layers; ++k) {
+    if (d->channels[k] < 1 || d->channels[k] > 1024) { set_error("grico_mg_set_learned: bad channel count"); return GRICO_ERR_INVALID; }
+    L.ch.push_back(d->channels[k]);
+    maxc = std::max(maxc, d->channels[k]);
+  }
+  bool ok = L.idx.upload(d->grid_index, size_t(ng));
+  L.w.resize(d->n_layers);
+  L.bias.resize(d->n_layers);
+  for (int k = 0; k < d->n_layers && ok; ++k)
+    ok = L.w[k].upload(d->weights[k], size_t(L.ch[k + 1]) * L.ch[k] * 27) && L.bias[k].upload(d->biases[k], size_t(L.ch[k + 1]));
+  std::vector<__nv_bfloat16> coef(ng);
+  for (int64_t g = 0; g < ng; ++g) coef[g] = __float2bfloat16(d->grid_log_coefficient[g]);
+  const size_t vb = (mg->opts.precision == GRICO_PREC_FP32 ? 4 : 8) * size_t(std::max<int64_t>(n, 1));
+  ok = ok && L.in.alloc(2 * sizeof(__nv_bfloat16) * ng) && L.act0.alloc(sizeof(__nv_bfloat16) * maxc * ng) &&
+       L.act1.alloc(sizeof(__nv_bfloat16) * maxc * ng) && L.out.alloc(sizeof(float) * ng) && L.xn.alloc(vb) &&
+       L.tn.alloc(vb) && L.z.alloc(vb);
+  if (!ok) return GRICO_ERR_CUDA;
+  cudaMemcpyAsync(L.in.get<__nv_bfloat16>() + ng, coef.data(), sizeof(__nv_bfloat16) * ng, cudaMemcpyHostToDevice,
+                  mg->stream);
+  if (!cuda_ok(cudaStreamSynchronize(mg->stream), "set learned")) return GRICO_ERR_CUDA;
+  mg->learned = std::move(L);
+  return GRICO_OK;
 }
 
 double grico_mg_lambda_max(GricoMultigrid* mg, int level) {

@@ -163,6 +163,22 @@ class GricoMGOptions(C.Structure):
 
 
 # name -> (restype, argtypes); every symbol include/grico_b200.h declares
+class GricoLearnedDesc(C.Structure):
+    _fields_ = [
+        ("level", C.c_int32),
+        ("nx", C.c_int32),
+        ("ny", C.c_int32),
+        ("nz", C.c_int32),
+        ("grid_index", i64p),
+        ("grid_log_coefficient", C.POINTER(C.c_float)),
+        ("n_layers", C.c_int32),
+        ("channels", i32p),
+        ("weights", C.POINTER(C.POINTER(C.c_float))),
+        ("biases", C.POINTER(C.POINTER(C.c_float))),
+        ("omega", C.c_double),
+    ]
+
+
 SIGNATURES = {
     "grico_space_build": (C.c_int, [C.c_int, i64p, C.c_int64, i32p, i64p, i32p, C.c_int, C.c_int, C.c_int, C.POINTER(P)]),
     "grico_space_destroy": (C.c_int, [P]),
@@ -188,6 +204,7 @@ SIGNATURES = {
     "grico_mg_destroy": (C.c_int, [P]),
     "grico_mg_vcycle": (C.c_int, [P, f64p, f64p, C.c_int]),
     "grico_mg_lambda_max": (C.c_double, [P, C.c_int]),
+    "grico_mg_set_learned": (C.c_int, [P, C.POINTER(GricoLearnedDesc)]),
     "grico_conv3d_forward": (C.c_int, [P, C.c_int, P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                        C.c_int, C.c_int, P]),
     "grico_conv3d_backward_data": (C.c_int, [P, P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P]),
@@ -195,6 +212,9 @@ SIGNATURES = {
     "grico_relu_backward": (C.c_int, [P, P, C.c_int64, P]),
     "grico_mse_grad": (C.c_int, [P, P, P, P, C.c_int64, C.c_double, P, P, P]),
     "grico_adam_step": (C.c_int, [P, P, P, P, C.c_int64, C.c_float, C.c_float, C.c_float, C.c_int, C.c_float, P]),
+    "grico_grid_gather": (C.c_int, [P, C.c_int64, P, C.c_float, P, P]),
+    "grico_grid_scatter_add": (C.c_int, [P, C.c_int64, P, C.c_float, P, P]),
+    "grico_weighted_residual": (C.c_int, [P, P, P, P, C.c_int64, P, P, P]),
     "grico_last_error": (C.c_char_p, []),
 }
 

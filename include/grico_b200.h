@@ -291,6 +291,26 @@ double grico_mg_lambda_max(GricoMultigrid* mg, int level);
 
 const char* grico_last_error(void);
 
+/* ---- learned smoother sweep inside the V-cycle (no reference counterpart) ----
+ * On `level` (a smoothed level whose free dofs sit on an nx x ny x nz grid, e.g. the degree-1
+ * level of a uniform mesh), the sweep computes r = b - A x, feeds (D^-1 r / sigma, log a) to
+ * the network (3x3x3 convolutions, ReLU between layers, BF16 activations, FP32 weights),
+ * scatters sigma * omega * output onto x and keeps the new iterate only if its D^-1-weighted
+ * residual norm is smaller.  It replaces the last pre-smoothing step on that level. */
+typedef struct GricoLearnedDesc {
+  int32_t level;
+  int32_t nx, ny, nz;
+  const int64_t* grid_index;            /* [nz*ny*nx] (x fastest): reduced dof or -1        */
+  const float* grid_log_coefficient;    /* [nz*ny*nx] second input channel                 */
+  int32_t n_layers;
+  const int32_t* channels;              /* [n_layers+1], channels[0] = 2, last = 1          */
+  const float* const* weights;          /* per layer [co][ci][27]                          */
+  const float* const* biases;           /* per layer [co]                                  */
+  double omega;                         /* correction scale                               */
+} GricoLearnedDesc;
+/* NULL desc removes the sweep.  Host arrays are copied. */
+int grico_mg_set_learned(GricoMultigrid* mg, const GricoLearnedDesc* desc);
+
 /* ---- learned smoother: network primitives (device pointers, asynchronous on `stream`) ----
  * No reference counterpart: the learned smoother is an addition of this library.  Tensors are
  * [batch][channel][z][y][x]; convolutions are 3x3x3, stride 1, zero padding; weights
@@ -310,6 +330,13 @@ int grico_mse_grad(const float* p, const float* t, const float* mask, float* g, 
                    double* partial, double* loss, void* stream);
 int grico_adam_step(float* w, const float* g, float* m, float* v, int64_t n, float lr, float beta1, float beta2,
                     int step, float eps, void* stream);
+/* grid <-> reduced vector: idx[g] is the reduced dof of grid point g, or -1 (FP32) */
+int grico_grid_gather(const int64_t* idx, int64_t n_grid, const float* src, float scale, float* dst, void* stream);
+int grico_grid_scatter_add(const int64_t* idx, int64_t n_grid, const float* src, float scale, float* dst,
+                           void* stream);
+/* out = w (r - ar) and *sum = sum w (r - ar)^2 (device double); partial: scratch of 592 doubles */
+int grico_weighted_residual(const float* r, const float* ar, const float* w, float* out, int64_t n, double* partial,
+                            double* sum, void* stream);
 
 #ifdef __cplusplus
 }
