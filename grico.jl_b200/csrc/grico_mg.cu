@@ -56,6 +56,7 @@ struct GricoMultigrid {
     grico::DevBuf in, act0, act1;        // BF16 network input (channel 1: log coefficient) and activations
     grico::DevBuf out;                   // FP32 network output grid
     grico::DevBuf xn, tn, z;             // candidate iterate, its operator image, D^-1 r (level precision)
+    grico::DevBuf stats;                 // [sweeps, accepted sweeps]
   } learned;
 };
 
@@ -238,8 +239,13 @@ __global__ void residual_scale(double* s, int64_t n) {
 // accept the candidate iterate when its weighted residual norm is smaller
 template <typename T>
 __global__ void select_iterate(T* __restrict__ x, const T* __restrict__ xn, int64_t n, const double* __restrict__ s_old,
-                               const double* __restrict__ s_new) {
-  if (!(*s_new < *s_old)) return;
+                               const double* __restrict__ s_new, unsigned long long* __restrict__ stats) {
+  const bool accept = *s_new < *s_old;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    stats[0] += 1;
+    if (accept) stats[1] += 1;
+  }
+  if (!accept) return;
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
     x[i] = xn[i];
 }
@@ -292,7 +298,7 @@ void learned_sweep(GricoMultigrid* mg, int l, T* x, const T* b, cudaStream_t st)
   level_apply<T>(mg, l, xn, tn, st);
   weighted_residual<T><<<kRedBlocks, 256, 0, st>>>(b, tn, dinv, lbuf<T>(L.z), n, partial);
   reduce_final<<<1, kRedThreads, 0, st>>>(partial, kRedBlocks, sc + 3);
-  select_iterate<T><<<blocks(n), 256, 0, st>>>(x, xn, n, sc, sc + 3);
+  select_iterate<T><<<blocks(n), 256, 0, st>>>(x, xn, n, sc, sc + 3, L.stats.get<unsigned long long>());
 }
 
 template <typename T>
@@ -601,12 +607,23 @@ int grico_mg_set_learned(GricoMultigrid* mg, const GricoLearnedDesc* d) {
   const size_t vb = (mg->opts.precision == GRICO_PREC_FP32 ? 4 : 8) * size_t(std::max<int64_t>(n, 1));
   ok = ok && L.in.alloc(2 * sizeof(__nv_bfloat16) * ng) && L.act0.alloc(sizeof(__nv_bfloat16) * maxc * ng) &&
        L.act1.alloc(sizeof(__nv_bfloat16) * maxc * ng) && L.out.alloc(sizeof(float) * ng) && L.xn.alloc(vb) &&
-       L.tn.alloc(vb) && L.z.alloc(vb);
+       L.tn.alloc(vb) && L.z.alloc(vb) && L.stats.alloc(2 * sizeof(unsigned long long));
   if (!ok) return GRICO_ERR_CUDA;
+  cudaMemsetAsync(L.stats.ptr, 0, 2 * sizeof(unsigned long long), mg->stream);
   cudaMemcpyAsync(L.in.get<__nv_bfloat16>() + ng, coef.data(), sizeof(__nv_bfloat16) * ng, cudaMemcpyHostToDevice,
                   mg->stream);
   if (!cuda_ok(cudaStreamSynchronize(mg->stream), "set learned")) return GRICO_ERR_CUDA;
   mg->learned = std::move(L);
+  return GRICO_OK;
+}
+
+int grico_mg_learned_stats(GricoMultigrid* mg, int64_t* sweeps, int64_t* accepted) {
+  if (!mg || mg->learned.level < 0) return GRICO_ERR_INVALID;
+  unsigned long long h[2] = {0, 0};
+  cudaMemcpyAsync(h, mg->learned.stats.ptr, sizeof(h), cudaMemcpyDeviceToHost, mg->stream);
+  if (!cuda_ok(cudaStreamSynchronize(mg->stream), "learned stats")) return GRICO_ERR_CUDA;
+  if (sweeps) *sweeps = int64_t(h[0]);
+  if (accepted) *accepted = int64_t(h[1]);
   return GRICO_OK;
 }
 

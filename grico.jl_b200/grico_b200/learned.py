@@ -291,3 +291,10 @@ def level_log_coefficient(level_plan, field):
     """log a at the vertices of a degree-1 level (the network's second input channel)."""
     _, dims = vertex_grid(level_plan)
     return field(vertex_points(dims, (0.0, 0.0, 0.0), (1.0, 1.0, 1.0))).astype(np.float32)
+
+
+def learned_stats(mg):
+    """(sweeps run, sweeps kept) of the learned sweep of `mg`."""
+    a, b = C.c_int64(), C.c_int64()
+    _check(L.lib().grico_mg_learned_stats(mg.handle, C.byref(a), C.byref(b)), "learned stats")
+    return a.value, b.value

@@ -220,6 +220,10 @@ def build_hierarchy(plan, opts, device=True):
         raise L.GricoError(L.GRICO_ERR_INVALID,
                            "GeometricMultigridPreconditioner requires at least one admissible h or p coarsening level")
     plans = [compile(_level_problem(plan.problem, s), device=device) for s in spaces[:-1]] + [plan]
+    # coarse levels whose every dof is constrained carry nothing: the coarsest level with free
+    # dofs becomes the direct-solve level
+    while len(plans) > 2 and plans[0].n_reduced == 0:
+        plans.pop(0)
     transfers = [transfer(plans[i], plans[i + 1]) for i in range(len(plans) - 1)]
     return plans, transfers
 

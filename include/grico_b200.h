@@ -310,6 +310,8 @@ typedef struct GricoLearnedDesc {
 } GricoLearnedDesc;
 /* NULL desc removes the sweep.  Host arrays are copied. */
 int grico_mg_set_learned(GricoMultigrid* mg, const GricoLearnedDesc* desc);
+/* learned sweeps run and kept since grico_mg_set_learned */
+int grico_mg_learned_stats(GricoMultigrid* mg, int64_t* sweeps, int64_t* accepted);
 
 /* ---- learned smoother: network primitives (device pointers, asynchronous on `stream`) ----
  * No reference counterpart: the learned smoother is an addition of this library.  Tensors are

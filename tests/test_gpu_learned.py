@@ -136,5 +136,9 @@ def test_learned_sweep_inside_fgmres_vcycle(cuda):
                                         C.byref(so), C.byref(rep), L.GRICO_FLAG_HOST_POINTERS)
         assert rc == 0
         iters[name] = rep.iterations
+        if name == "learned":
+            sweeps, kept = lr.learned_stats(mg)
+            print("learned sweeps", sweeps, "kept", kept)
+            assert sweeps > 0
     print("FGMRES iterations", iters)
     assert iters["learned"] <= 1.5 * iters["plain"] + 1
