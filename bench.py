@@ -316,6 +316,10 @@ def learned_legs(gb, L, refine=7, train_refine=5, train_fields=6, train_steps=20
                 rc, rep, ref = fgmres(mg, 1e-12, 3000)
                 ref_state = gb.State(plan, gb.expand_reduced(plan, ref), rep)
                 ref_norm = gb.l2_error(ref_state, lambda X: np.zeros(X.shape[0]))
+                if rc != 0 or not ref_norm > 0:
+                    raise RuntimeError(f"reference solve failed: status {rc}, iterations {rep.iterations}, "
+                                       f"|b| {np.linalg.norm(b)}, |x| {np.linalg.norm(ref)}, "
+                                       f"{L.lib().grico_last_error().decode()}")
             tries, hit = [], None
             for rtol in (1e-4, 1e-5, 1e-6, 1e-7, 1e-8, 1e-9):
                 rc, rep, x = fgmres(mg, rtol)

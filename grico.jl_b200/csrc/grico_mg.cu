@@ -88,7 +88,8 @@ template <typename T>
 __global__ void chebyshev_step(T* __restrict__ x, T* __restrict__ d, const T* __restrict__ b,
                                const T* __restrict__ ax, const T* __restrict__ dinv, T c1, T c2, int64_t n) {
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-    T di = c1 * d[i] + c2 * dinv[i] * (b[i] - ax[i]);
+    // the first step must not read d: fresh device memory may hold NaN bit patterns
+    T di = (c1 != T(0) ? c1 * d[i] : T(0)) + c2 * dinv[i] * (b[i] - ax[i]);
     d[i] = di;
     x[i] += di;
   }
