@@ -344,6 +344,59 @@ def learned_legs(gb, L, refine=7, train_refine=5, train_fields=6, train_steps=20
         "legs": results, "target_relative_l2": target}
 
 
+def batched_legs(gb, L, max_level=7, nrhs=32, rtol=1e-10):
+    """Adaptive hp L-shape (hanging nodes, degrees 2..7) with 32 Gaussian-bump loads: 32 single
+    CG solves one after another vs one lockstep solve (FP64, and FP32 inside FP64 refinement);
+    device seconds of the solves, tiles autotuned per batch first."""
+    import ctypes as C
+
+    import torch
+
+    from grico_b200 import batched as bt
+
+    t0 = time.perf_counter()
+    plan = gb.compile(bt.lshape_problem(max_level=max_level))
+    setup = time.perf_counter() - t0
+    tiles = {p: bt.autotune(plan, nrhs=nrhs, precision=p, reps=5).tolist() for p in ("fp64", "fp32")}
+    B = bt.reduced_rhs_many(plan, bt.gaussian_bumps(nrhs, seed=0))
+    # single-right-hand-side solves, one after another
+    single_s, single_it = 0.0, []
+    for s in range(nrhs):
+        x = np.zeros(plan.n_reduced)
+        so = L.GricoSolveOptions(rtol, 0.0, 100000, L.GRICO_PRECOND_JACOBI, 30, 0)
+        rep = L.GricoSolveReport()
+        L.check(L.lib().grico_cg_solve(plan.handle, None, L.ptr(B[s], C.c_double), L.ptr(x, C.c_double),
+                                       C.byref(so), C.byref(rep), L.GRICO_FLAG_HOST_POINTERS), "cg")
+        single_s += rep.seconds
+        single_it.append(rep.iterations)
+    out = {"dofs": plan.n_full, "reduced_dofs": plan.n_reduced, "cells": int(len(plan.space.leaves)),
+           "batches": [[int(b.degree[0]), len(b.cells)] for b in plan.batches], "nrhs": nrhs, "rtol": rtol,
+           "host_setup_seconds": setup, "tiles": tiles,
+           "single_cg_fp64": {"seconds": single_s, "iterations_max": max(single_it)}}
+    for name, mixed in (("lockstep_cg_fp64", False), ("lockstep_cg_fp32_in_fp64_refinement", True)):
+        X, reps = bt.solve_many(plan, B, relative_tolerance=rtol, mixed=mixed)
+        out[name] = {"seconds": reps[0].seconds, "iterations_max": max(r.iterations for r in reps),
+                     "status": sorted({int(r.status) for r in reps})}
+    # operator throughput, 1 vs nrhs right-hand sides (FP64 and FP32)
+    for prec, dt in ((L.GRICO_PREC_FP64, torch.float64), (L.GRICO_PREC_FP32, torch.float32)):
+        for k in (1, nrhs):
+            xv = torch.ones(k * plan.n_reduced, dtype=dt, device="cuda")
+            yv = torch.empty_like(xv)
+            st = torch.cuda.Stream()
+            for _ in range(3):
+                L.lib().grico_reduced_apply(plan.handle, xv.data_ptr(), yv.data_ptr(), k, prec, 0, st.cuda_stream)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(20):
+                L.lib().grico_reduced_apply(plan.handle, xv.data_ptr(), yv.data_ptr(), k, prec, 0, st.cuda_stream)
+            e1.record(st)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / 20
+            out[f"apply_{'fp64' if prec == L.GRICO_PREC_FP64 else 'fp32'}_nrhs{k}"] = {
+                "ms": ms, "dofs_per_s": k * plan.n_reduced / (ms * 1e-3)}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -354,7 +407,8 @@ def main():
     ap.add_argument("--soak", type=float, default=1.5, help="seconds of untimed load while clocks are sampled")
     ap.add_argument("--no-solve", action="store_true", help="skip the CG+GMG time-to-tolerance legs")
     ap.add_argument("--workload", default="poisson64",
-                    choices=["poisson64", "fcm_shell64", "fcm_shell32", "grf_learned128", "grf_learned64"],
+                    choices=["poisson64", "fcm_shell64", "fcm_shell32", "grf_learned128", "grf_learned64",
+                             "lshape_hp32"],
                     help="poisson64: 3-D Poisson 64^3 p=4 (default); fcm_shell*: finite-cell shell with Nitsche")
     ap.add_argument("--fp32", action="store_true", help="time the FP32 apply instead of FP64")
     args = ap.parse_args()
@@ -377,6 +431,17 @@ def main():
     import grico_b200 as gb
     from grico_b200 import _lib as L
 
+    if args.workload == "lshape_hp32":
+        out = batched_legs(gb, L)
+        if rank == 0:
+            print(json.dumps({"metric": "time to rtol 1e-10 for 32 right-hand sides (adaptive hp L-shape)",
+                              "value": out["lockstep_cg_fp32_in_fp64_refinement"]["seconds"], "unit": "s",
+                              "n_gpus": world, "steps": 1, "warmup": 0, "higher_is_better": False,
+                              "scaling": "weak", "vs_baseline": None, "dtype": "f64/f32",
+                              "data": "synthetic (seeded Gaussian bumps)",
+                              "config": {"workload": "lshape_hp32", "levels": "2..7", "degrees": "2..7"},
+                              "batched": out}), flush=True)
+        return
     if args.workload.startswith("grf_learned"):
         out = learned_legs(gb, L, refine=7 if args.workload.endswith("128") else 6)
         leg = out["legs"]

@@ -142,15 +142,25 @@ bool launch_fused(int dim, const DevBatch& bt, const BatchView& v, const T* x, T
                   int mode, const double* src, int nrhs, cudaStream_t st) {
   if (v.n_cells == 0) return true;
   const int N = bt.n[0], Q = bt.q[0];
-#define GRICO_L3(NN, QQ)                                                                                     \
-  if (N == NN && Q == QQ) {                                                                                  \
-    constexpr int CPB = (256 / (QQ * QQ)) > 0 ? (256 / (QQ * QQ)) : 1;                                       \
-    const size_t smem = size_t(3) * CPB * ((QQ * QQ * QQ) | 1) * sizeof(T);                                  \
-    auto kern = cell_apply_3d<NN, QQ, CPB, T>;                                                              \
-    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)); \
-    dim3 block(QQ * QQ, CPB), grid((v.n_cells + CPB - 1) / CPB, nrhs);                                       \
-    kern<<<grid, block, smem, st>>>(v, make_tables<NN, QQ, T>(bt), x, y, nvec, mass, kappa, mode, src);     \
-    return true;                                                                                             \
+  const int var = bt.tile[sizeof(T) == 4 ? 1 : 0];
+#define GRICO_L3_CPB(NN, QQ, CPB_)                                                                             \
+  {                                                                                                            \
+    constexpr int CPB = CPB_;                                                                                  \
+    const size_t smem = size_t(3) * CPB * ((QQ * QQ * QQ) | 1) * sizeof(T);                                    \
+    auto kern = cell_apply_3d<NN, QQ, CPB, T>;                                                                \
+    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));   \
+    dim3 block(QQ * QQ, CPB), grid((v.n_cells + CPB - 1) / CPB, nrhs);                                         \
+    kern<<<grid, block, smem, st>>>(v, make_tables<NN, QQ, T>(bt), x, y, nvec, mass, kappa, mode, src);       \
+    return true;                                                                                               \
+  }
+#define GRICO_L3(NN, QQ)                                                                                       \
+  if (N == NN && Q == QQ) {                                                                                    \
+    constexpr int C1 = (256 / (QQ * QQ)) > 0 ? (256 / (QQ * QQ)) : 1;                                          \
+    constexpr int C0 = C1 / 2 > 0 ? C1 / 2 : 1;                                                                \
+    constexpr int C2 = (2 * C1 * QQ * QQ <= 1024) ? 2 * C1 : C1;                                               \
+    if (var == 0) GRICO_L3_CPB(NN, QQ, C0)                                                                     \
+    if (var == 2) GRICO_L3_CPB(NN, QQ, C2)                                                                     \
+    GRICO_L3_CPB(NN, QQ, C1)                                                                                   \
   }
 #define GRICO_L2(NN, QQ)                                                                                     \
   if (N == NN && Q == QQ) {                                                                                  \
@@ -167,6 +177,7 @@ bool launch_fused(int dim, const DevBatch& bt, const BatchView& v, const T* x, T
     GRICO_L2(9, 9) GRICO_L2(2, 3) GRICO_L2(3, 4) GRICO_L2(4, 5) GRICO_L2(5, 6)
   }
 #undef GRICO_L3
+#undef GRICO_L3_CPB
 #undef GRICO_L2
   return false;
 }
@@ -1097,4 +1108,54 @@ extern "C" int grico_reduced_rhs_static(GricoPlan* P, const double* const* sourc
   project_reduced<<<grid_for(P->n_full), 256, 0, st>>>(P->red_off.get<int64_t>(), P->red_idx.get<int64_t>(),
                                                         P->red_coef.get<double>(), full, b_reduced, P->n_full);
   return cuda_ok(cudaGetLastError(), "grico_reduced_rhs_static") ? GRICO_OK : GRICO_ERR_CUDA;
+}
+
+namespace {
+
+template <typename T>
+int autotune_typed(GricoPlan* P, int nrhs, int reps, int* chosen) {
+  cudaStream_t st = P->stream;
+  const int64_t n = P->n_red;
+  DevBuf xb, yb;
+  if (!xb.alloc(sizeof(T) * std::max<int64_t>(n, 1) * nrhs) || !yb.alloc(sizeof(T) * std::max<int64_t>(n, 1) * nrhs))
+    return GRICO_ERR_CUDA;
+  fill_kernel<T><<<grid_for(n * nrhs), 256, 0, st>>>(xb.get<T>(), n * nrhs, T(1));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int slot = sizeof(T) == 4 ? 1 : 0;
+  for (size_t bi = 0; bi < P->batches.size(); ++bi) {
+    DevBatch& b = P->batches[bi];
+    int best = 1;
+    if (P->dim == 3 && b.isotropic && b.q[0] >= b.n[0] && b.n_cells > 0) {
+      float best_ms = 1e30f;
+      for (int var = 0; var < 3; ++var) {
+        b.tile[slot] = var;
+        launch_batch<T>(*P, b, true, xb.get<T>(), yb.get<T>(), n, 0, nullptr, nrhs, st);  // warm-up
+        cudaEventRecord(e0, st);
+        for (int r = 0; r < reps; ++r) launch_batch<T>(*P, b, true, xb.get<T>(), yb.get<T>(), n, 0, nullptr, nrhs, st);
+        cudaEventRecord(e1, st);
+        cudaEventSynchronize(e1);
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) { best_ms = ms; best = var; }
+      }
+    }
+    b.tile[slot] = best;
+    if (chosen) chosen[bi] = best;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return cuda_ok(cudaStreamSynchronize(st), "autotune") ? GRICO_OK : GRICO_ERR_CUDA;
+}
+
+}  // namespace
+
+extern "C" int grico_plan_autotune(GricoPlan* P, int nrhs, int precision, int reps, int* chosen) {
+  if (!P || nrhs < 1 || reps < 1 || (precision != GRICO_PREC_FP64 && precision != GRICO_PREC_FP32)) {
+    set_error("grico_plan_autotune: invalid argument");
+    return GRICO_ERR_INVALID;
+  }
+  return precision == GRICO_PREC_FP64 ? autotune_typed<double>(P, nrhs, reps, chosen)
+                                      : autotune_typed<float>(P, nrhs, reps, chosen);
 }

@@ -74,6 +74,8 @@ struct DevBatch {
   DevBuf h, kappa, B, G, W, D;
   DevBuf skip;  // uint8 per cell: hanging cells whose diagonal is added from the host
   std::vector<double> hB, hD, hW;  // axis-0 tables on the host (kernel parameters)
+  int tile[2] = {1, 1};  // cells-per-block variant of the 3-D tensor kernel per precision (0: FP64, 1: FP32):
+                         // 0 = half, 1 = default, 2 = double the default; chosen by grico_plan_autotune
 };
 
 struct DevPointBatch {

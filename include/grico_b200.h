@@ -54,6 +54,7 @@ extern "C" {
 
 #define GRICO_FLAG_HOST_POINTERS 1 /* vector arguments are host memory: copy in/out */
 #define GRICO_FLAG_NO_GRAPH 2      /* Krylov solves: launch each iteration op by op, no CUDA graph */
+#define GRICO_FLAG_MIXED 4         /* grico_cg_solve_multi: FP64 refinement around FP32 inner CG */
 
 /* ================================================================================
  * Host space compile (native replacement of the Julia-side HpSpace construction)
@@ -194,6 +195,12 @@ typedef struct GricoPlan GricoPlan;
 /* Copies every descriptor array to the device; the caller may free them afterwards.  The plan
  * owns its workspaces and one CUDA stream.  Calls on one plan are serialised. */
 int grico_plan_create(const GricoPlanDesc* desc, GricoPlan** out);
+/* Per-batch tile autotuner (no reference counterpart): times the cells-per-block variants
+ * (half, default, double) of the 3-D tensor-cell kernel on this plan's batches for `nrhs`
+ * right-hand sides in `precision`, keeps the fastest per batch for later applies of that
+ * precision, and writes the choice per cell batch to `chosen` (may be NULL; 0 = half, 1 =
+ * default, 2 = double).  Allocates scratch; call before any stream capture. */
+int grico_plan_autotune(GricoPlan* plan, int nrhs, int precision, int reps, int* chosen);
 int grico_plan_destroy(GricoPlan* plan);
 /* n_full, n_reduced */
 int grico_plan_sizes(const GricoPlan* plan, int64_t* n_full, int64_t* n_reduced);
@@ -254,6 +261,14 @@ typedef struct GricoMultigrid GricoMultigrid;
 
 int grico_cg_solve(GricoPlan* plan, GricoMultigrid* mg, const double* b, double* x,
                    const GricoSolveOptions* opts, GricoSolveReport* report, int flags);
+/* nrhs systems A x_s = b_s (B, X: [nrhs][n_reduced]) solved by lockstep CG, one operator apply
+ * for all systems per iteration, identity or Jacobi preconditioning, each with the reference's
+ * stopping rule; with GRICO_FLAG_MIXED the CG runs in FP32 inside FP64 iterative refinement
+ * (FP64 residuals and updates).  reports: [nrhs] or NULL.  No reference counterpart for the
+ * batching. */
+int grico_cg_solve_multi(GricoPlan* plan, const double* B, double* X, int nrhs, const GricoSolveOptions* opts,
+                         GricoSolveReport* reports, int flags);
+
 int grico_fgmres_solve(GricoPlan* plan, GricoMultigrid* mg, const double* b, double* x,
                        const GricoSolveOptions* opts, GricoSolveReport* report, int flags);
 

@@ -1,0 +1,61 @@
+"""Many right-hand sides per solve (lockstep CG, FP64 and FP32-inside-FP64 refinement) and the
+per-batch tile autotuner, on the adaptive hp L-shaped workload with hanging nodes."""
+import numpy as np
+import pytest
+
+import grico_b200 as gb
+from grico_b200 import batched as bt
+from cases import rel_err, sample_vector
+
+pytestmark = pytest.mark.gpu
+
+
+def _case(max_level=4, nrhs=4):
+    plan = gb.compile(bt.lshape_problem(max_level=max_level))
+    B = bt.reduced_rhs_many(plan, bt.gaussian_bumps(nrhs, seed=3))
+    return plan, B
+
+
+def test_lockstep_cg_matches_single_solves(cuda):
+    plan, B = _case()
+    X, reps = bt.solve_many(plan, B, relative_tolerance=1e-11)
+    for s in range(B.shape[0]):
+        x = np.zeros(plan.n_reduced)
+        import ctypes as C
+        from grico_b200 import _lib as L
+        so = L.GricoSolveOptions(1e-11, 0.0, 100000, L.GRICO_PRECOND_JACOBI, 30, 0)
+        rep = L.GricoSolveReport()
+        assert L.lib().grico_cg_solve(plan.handle, None, L.ptr(B[s], C.c_double), L.ptr(x, C.c_double),
+                                      C.byref(so), C.byref(rep), L.GRICO_FLAG_HOST_POINTERS) == 0
+        assert reps[s].status == 0
+        assert abs(reps[s].iterations - rep.iterations) <= 2
+        assert rel_err(X[s], x) <= 1e-9
+
+
+def test_mixed_refinement_reaches_fp64_accuracy(cuda):
+    plan, B = _case()
+    X64, _ = bt.solve_many(plan, B, relative_tolerance=1e-11)
+    X32, reps = bt.solve_many(plan, B, relative_tolerance=1e-11, mixed=True)
+    assert all(r.status == 0 for r in reps)
+    for s in range(B.shape[0]):
+        assert rel_err(X32[s], X64[s]) <= 1e-8
+
+
+def test_graph_and_direct_launches_agree(cuda):
+    plan, B = _case(nrhs=3)
+    Xg, rg = bt.solve_many(plan, B, relative_tolerance=1e-10, graph=True)
+    Xd, rd = bt.solve_many(plan, B, relative_tolerance=1e-10, graph=False)
+    assert [r.iterations for r in rg] == [r.iterations for r in rd]
+    assert rel_err(Xg, Xd) <= 1e-12
+
+
+def test_autotuned_tiles_keep_results(cuda):
+    plan, _ = _case()
+    x = sample_vector(plan.n_full, seed=9)
+    y0 = gb.apply(plan, x)
+    for prec in ("fp64", "fp32"):
+        chosen = bt.autotune(plan, nrhs=4, precision=prec, reps=3)
+        assert len(chosen) == len(plan.batches) and set(chosen.tolist()) <= {0, 1, 2}
+    assert rel_err(gb.apply(plan, x), y0) <= 1e-12
+    y32 = gb.apply(plan, x.astype(np.float32))
+    assert rel_err(y32, y0) <= 2e-5
