@@ -26,12 +26,30 @@ def needs_build() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compiles every source to an object in parallel (one nvcc per source), then links."""
     if not force and not needs_build():
         return OUT
-    cmd = [NVCC, *FLAGS, "-o", OUT] + [os.path.join(CSRC, s) for s in SOURCES]
-    if verbose:
-        print(" ".join(cmd), file=sys.stderr)
-    subprocess.run(cmd, check=True)
+    import tempfile
+    from concurrent.futures import ThreadPoolExecutor
+
+    compile_flags = [f for f in FLAGS if f not in ("-shared", "-lcudart")]
+    with tempfile.TemporaryDirectory(prefix="grico_build_") as tmp:
+        objs = [os.path.join(tmp, os.path.splitext(s)[0] + ".o") for s in SOURCES]
+        cmds = [[NVCC, *compile_flags, "-c", os.path.join(CSRC, s), "-o", o] for s, o in zip(SOURCES, objs)]
+        if verbose:
+            for c in cmds:
+                print(" ".join(c), file=sys.stderr)
+        with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+            results = list(ex.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds))
+        for c, r in zip(cmds, results):
+            if r.returncode != 0:
+                sys.stderr.write(r.stdout + r.stderr)
+                raise subprocess.CalledProcessError(r.returncode, c)
+        link = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", OUT + ".tmp", *objs, "-lcudart"]
+        if verbose:
+            print(" ".join(link), file=sys.stderr)
+        subprocess.run(link, check=True)
+        os.replace(OUT + ".tmp", OUT)
     return OUT
 
 

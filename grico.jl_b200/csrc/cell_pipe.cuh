@@ -1,0 +1,465 @@
+// Persistent, software-pipelined 3-D tensor-cell apply with bank-conflict-free line
+// assignment (operator apply of cell_apply_3d, same contraction schedule and results up to
+// rounding).
+//
+// A block of NT = Q*Q*CPB threads walks groups of CPB cells (group g, g + gridDim.x, ...).
+// While it computes group g, cp.async copies of x[map[e]] for the next group land in the
+// other shared stage and the map entries of the group after that are in flight into
+// registers, so the gather's two dependent global round trips overlap a whole group's
+// contractions.  Entries with a coefficient, a tail expansion or no dof are gathered
+// synchronously.
+//
+// Every contraction step gives each thread one whole line of a cell's Q^3 point box (x-, y- or
+// z-line), as in cell_apply_3d.  Which line a thread takes is not tied to its own cell: for each
+// of the three line shapes the host computes a lane -> (cell, line) table so that the 16 lanes
+// of every half warp (8-byte elements; 32 lanes for 4-byte elements) touch 16 different
+// shared-memory bank pairs, with the per-cell buffer pitch chosen by the same search.  With
+// the plain (cell-own) assignment every other shared-memory access of a 5^3 cell replays once.
+// With a constant coefficient the pointwise flux scaling is folded into the x and y derivative
+// steps.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "cell_kernels.cuh"
+
+namespace grico {
+
+// Asynchronous global -> shared copies of one element (cp.async, sm_80+): the copy runs while
+// the issuing thread goes on; cp.async.wait_group makes the thread's own copies complete.
+template <int BYTES>
+__device__ __forceinline__ void cp_async_elem(void* smem_dst, const void* gsrc) {
+  const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(dst), "l"(gsrc), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int PENDING>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(PENDING) : "memory");
+}
+
+// Returns v through an opaque register move: the compiler keeps the value in a register (or
+// spills it) rather than recomputing it from its operands.
+__device__ __forceinline__ int keep_reg(int v) {
+  asm volatile("mov.b32 %0, %0;" : "+r"(v));
+  return v;
+}
+__device__ __forceinline__ double keep_reg(double v) {
+  asm volatile("mov.b64 %0, %0;" : "+d"(v));
+  return v;
+}
+__device__ __forceinline__ float keep_reg(float v) {
+  asm volatile("mov.b32 %0, %0;" : "+f"(v));
+  return v;
+}
+
+// Line shapes of a Q^3 box stored x fastest (element (ix, iy, iz) at ix + Q iy + Q^2 iz):
+// z-lines are indexed by (a, b) = (x, y), y-lines by (x, z), x-lines by (y, z).
+enum LineShape { kLineX = 0, kLineY = 1, kLineZ = 2 };
+
+// Lane -> line table of one kernel shape: v[shape][lane] = cell | a << 7 | b << 11; bp = element
+// pitch between the three per-cell work buffers, sp = pitch between staged cells.
+template <int NT>
+struct LaneLines {
+  int bp, sp;
+  uint16_t v[3][NT];
+};
+
+namespace lanes_detail {
+
+inline int line_offset(int shape, int a, int b, int Q) {
+  return shape == kLineZ ? a + Q * b : shape == kLineY ? a + Q * Q * b : Q * a + Q * Q * b;
+}
+
+// Shared-memory wavefronts of one access step: lanes grouped in windows of W, each window
+// costs the largest number of distinct addresses that share one bank residue.
+inline int window_cost(const std::vector<long>& addr, const std::vector<char>& active, int W) {
+  int total = 0;
+  const int n = int(addr.size());
+  for (int w0 = 0; w0 < n; w0 += W) {
+    std::vector<std::vector<long>> by(W);
+    for (int l = w0; l < std::min(n, w0 + W); ++l)
+      if (active[l]) {
+        auto& v = by[size_t(addr[l] % W)];
+        if (std::find(v.begin(), v.end(), addr[l]) == v.end()) v.push_back(addr[l]);
+      }
+    size_t worst = 0;
+    for (auto& v : by) worst = std::max(worst, v.size());
+    total += int(worst);
+  }
+  return total;
+}
+
+// Greedy assignment of all CPB*Q*Q lines of one shape to lanes: each window takes lines of
+// distinct residues, the residue with most lines left first.  Returns the assignment (line
+// ids c*Q*Q + a + Q*b) and its cost.
+inline int assign_shape(int shape, int Q, int CPB, int bp, int W, std::vector<int>& out) {
+  const int T = Q * Q, NT = T * CPB;
+  std::vector<std::vector<int>> pool(W);
+  for (int c = CPB - 1; c >= 0; --c)
+    for (int t = T - 1; t >= 0; --t) {
+      const long a = long(3) * c * bp + line_offset(shape, t % Q, t / Q, Q);
+      pool[size_t(a % W)].push_back(c * T + t);
+    }
+  out.assign(size_t(NT), 0);
+  int cost = 0;
+  for (int w0 = 0; w0 < NT; w0 += W) {
+    std::vector<char> used(size_t(W), 0);
+    std::vector<int> count(size_t(W), 0);
+    for (int l = w0; l < std::min(NT, w0 + W); ++l) {
+      int best = -1;
+      for (int pass = 0; pass < 2 && best < 0; ++pass)
+        for (int r = 0; r < W; ++r)
+          if (!pool[size_t(r)].empty() && (pass == 1 || !used[size_t(r)]) &&
+              (best < 0 || pool[size_t(r)].size() > pool[size_t(best)].size()))
+            best = r;
+      out[size_t(l)] = pool[size_t(best)].back();
+      pool[size_t(best)].pop_back();
+      used[size_t(best)] = 1;
+      ++count[size_t(best)];
+    }
+    cost += *std::max_element(count.begin(), count.end());
+  }
+  return cost;
+}
+
+}  // namespace lanes_detail
+
+// Builds the lane tables for (N, Q, CPB) and element size `elem` (4 or 8 bytes): searches the
+// buffer pitch bp in [Q^3, Q^3 + 2W) and stage pitch sp in [N^3, N^3 + W) for the fewest
+// wavefronts (W = 128 / elem lanes per window).  v: [3][Q*Q*CPB].
+inline void build_lane_lines(int N, int Q, int CPB, int elem, int* bp_out, int* sp_out, uint16_t* v) {
+  using namespace lanes_detail;
+  const int W = 128 / elem, T = Q * Q, NT = Q * Q * CPB;
+  int best_cost = -1;
+  std::vector<std::vector<int>> tmp(3), keep(3);
+  for (int bp = Q * Q * Q; bp < Q * Q * Q + 2 * W; ++bp) {
+    int cost = 0;
+    for (int s = 0; s < 3; ++s) cost += assign_shape(s, Q, CPB, bp, W, tmp[size_t(s)]);
+    if (best_cost < 0 || cost < best_cost) {
+      best_cost = cost;
+      *bp_out = bp;
+      keep = tmp;
+    }
+  }
+  // stage pitch: step 1 reads N staged modes along each active z-line
+  const std::vector<int>& zl = keep[2];
+  int best_sp = N * N * N, sp_cost = -1;
+  std::vector<long> addr(size_t(NT), 0);
+  std::vector<char> act(size_t(NT), 0);
+  for (int sp = N * N * N; sp < N * N * N + W; ++sp) {
+    for (int l = 0; l < NT; ++l) {
+      const int id = zl[size_t(l)];
+      const int c = id / T, a = (id % T) % Q, b = (id % T) / Q;
+      addr[size_t(l)] = static_cast<long>(c) * sp + a + N * b;
+      act[size_t(l)] = static_cast<char>(a < N && b < N);
+    }
+    const int cost = window_cost(addr, act, W);
+    if (sp_cost < 0 || cost < sp_cost) {
+      sp_cost = cost;
+      best_sp = sp;
+    }
+  }
+  *sp_out = best_sp;
+  for (int s = 0; s < 3; ++s)
+    for (int l = 0; l < NT; ++l) {
+      const int id = keep[size_t(s)][size_t(l)];
+      const int c = id / T, a = (id % T) % Q, b = (id % T) / Q;
+      v[s * NT + l] = static_cast<uint16_t>(c | (a << 7) | (b << 11));
+    }
+}
+
+template <int NT>
+LaneLines<NT> make_lane_lines(int N, int Q, int CPB, int elem) {
+  LaneLines<NT> L{};
+  build_lane_lines(N, Q, CPB, elem, &L.bp, &L.sp, &L.v[0][0]);
+  return L;
+}
+
+// Shared-memory bytes of cell_apply_3d_pipe: two stages of cell sizes (4 doubles per cell), the
+// per-cell flux scales (4 doubles), three work buffers of bp elements per cell and two stages
+// of sp staged modes per cell.
+inline size_t pipe_smem_bytes(int CPB, int bp, int sp, int elem) {
+  return size_t(2) * CPB * 4 * 8 + size_t(CPB) * 4 * 8 + size_t(3) * CPB * bp * elem + size_t(2) * CPB * sp * elem;
+}
+
+// Minimum resident blocks per SM asked of the compiler: caps registers near 80 per thread so
+// that several groups overlap on an SM.
+constexpr int pipe_min_blocks(int threads) {
+  return (65536 / (80 * ((threads + 31) / 32 * 32))) > 0 ? 65536 / (80 * ((threads + 31) / 32 * 32)) : 1;
+}
+
+template <int N, int Q, int CPB, typename T>
+__global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB))
+    cell_apply_3d_pipe(BatchView b, const Tables1D<N, Q, T> tab, const LaneLines<Q * Q * CPB> lanes,
+                       const T* __restrict__ x, T* __restrict__ y, int64_t n_vec, T mass, T kappa) {
+  constexpr int Q2 = Q * Q;
+  constexpr int Q3 = Q * Q * Q;
+  constexpr int NB = N * N * N;
+  const int BP = lanes.bp, SP = lanes.sp;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* hst = reinterpret_cast<double*>(smem_raw);   // [2][CPB][4] staged cell sizes
+  double* scl = hst + 2 * CPB * 4;                      // [CPB][4] detJ sx^2, detJ sy^2, detJ sz^2, detJ
+  T* work = reinterpret_cast<T*>(scl + CPB * 4);        // [CPB][3][BP]
+  T* stage = work + 3 * CPB * BP;                       // [2][CPB][SP]
+  const int tid = threadIdx.x;
+  x += blockIdx.y * n_vec;
+  y += blockIdx.y * n_vec;
+  const int64_t n_groups = (int64_t(b.n_cells) + CPB - 1) / CPB;
+  const int64_t G = gridDim.x;
+  const bool fuse = b.kappa_pts == nullptr;
+
+  // This thread's lines: cell and in-cell position per shape.  The table sits in the
+  // parameter bank and is indexed per lane; every derived value goes through keep_reg so that
+  // the compiler holds it in a register instead of re-reading the bank (a divergent constant
+  // load) inside the group loop.
+  int lc[3], la[3], lb[3];
+#pragma unroll
+  for (int s = 0; s < 3; ++s) {
+    const int v = lanes.v[s][tid];
+    lc[s] = v & 127;
+    la[s] = (v >> 7) & 15;
+    lb[s] = (v >> 11) & 15;
+  }
+  const int baseX = keep_reg(3 * lc[kLineX] * BP + Q * la[kLineX] + Q2 * lb[kLineX]);  // x-line (y, z)
+  const int baseY = keep_reg(3 * lc[kLineY] * BP + la[kLineY] + Q2 * lb[kLineY]);      // y-line (x, z)
+  const int baseZ = keep_reg(3 * lc[kLineZ] * BP + la[kLineZ] + Q * lb[kLineZ]);       // z-line (x, y)
+  const int stZ = keep_reg(lc[kLineZ] * SP + la[kLineZ] + N * lb[kLineZ]);
+  const int cX = keep_reg(lc[kLineX]), cY = keep_reg(lc[kLineY]), cZ = keep_reg(lc[kLineZ]);
+  const int pZ = keep_reg(la[kLineZ] + Q * lb[kLineZ]);   // z-line's point offset in the cell box
+  const int mZ = keep_reg(la[kLineZ] + N * lb[kLineZ]);   // z-line's mode offset in the cell box
+  const bool zmodes = keep_reg(int(la[kLineZ] < N && lb[kLineZ] < N)) != 0;  // z-line through modes
+  const bool ymodes = keep_reg(int(la[kLineY] < N)) != 0;
+  const T wX = keep_reg(tab.W[la[kLineX]] * tab.W[lb[kLineX]]);
+  const T wY = keep_reg(tab.W[la[kLineY]] * tab.W[lb[kLineY]]);
+  const T wZ = keep_reg(tab.W[la[kLineZ]] * tab.W[lb[kLineZ]]);
+
+  // cp.async issue layout: thread (c, ta, tb) = its own cell's z-line
+  const int ic = tid / Q2, ita = (tid % Q2) % Q, itb = (tid % Q2) / Q;
+  const bool igather = ita < N && itb < N;
+  int mv[N];
+  auto load_map = [&](int64_t g) {
+    const int64_t cell = g * CPB + ic;
+    const bool ok = igather && g < n_groups && cell < b.n_cells;
+#pragma unroll
+    for (int k = 0; k < N; ++k) mv[k] = ok ? __ldg(b.map + cell * NB + ita + N * (itb + N * k)) : -1;
+  };
+  auto issue = [&](int64_t g, int s) {
+    const int64_t cell = g * CPB + ic;
+    if (g < n_groups && cell < b.n_cells) {
+      T* st = stage + (s * CPB + ic) * SP;
+      if (igather) {
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+          const int e = ita + N * (itb + N * k);
+          if (mv[k] >= 0 && b.coef == nullptr)
+            cp_async_elem<sizeof(T)>(st + e, x + mv[k]);
+          else
+            st[e] = gather_entry<T>(b, cell * NB + e, x);
+        }
+      }
+      if (tid % Q2 < 3) cp_async_elem<8>(hst + (s * CPB + ic) * 4 + tid % Q2, b.h + cell * 3 + tid % Q2);
+    }
+    cp_async_commit();  // every thread commits one group per issue, possibly empty
+  };
+
+  int64_t g = blockIdx.x;
+  load_map(g);
+  issue(g, 0);
+  load_map(g + G);
+  T line[Q], out[Q];
+  for (int s = 0; g < n_groups; g += G, s ^= 1) {
+    issue(g + G, s ^ 1);
+    load_map(g + 2 * G);
+    cp_async_wait<1>();
+    __syncthreads();  // staged modes and sizes of group g visible; previous group fully done
+    if (tid % Q2 == 0) {
+      const double* hc = hst + (s * CPB + ic) * 4;
+      const bool ok = g * CPB + ic < b.n_cells;
+      const double h0 = ok ? hc[0] : 1.0, h1 = ok ? hc[1] : 1.0, h2 = ok ? hc[2] : 1.0;
+      const double detJ = h0 * h1 * h2 * 0.125;
+      scl[ic * 4 + 0] = detJ * (2.0 / h0) * (2.0 / h0);
+      scl[ic * 4 + 1] = detJ * (2.0 / h1) * (2.0 / h1);
+      scl[ic * 4 + 2] = detJ * (2.0 / h2) * (2.0 / h2);
+      scl[ic * 4 + 3] = detJ;
+    }
+    const T* st = stage + s * CPB * SP;
+    // 1. z interpolation on z-lines through mode positions, from the staged modes
+    if (zmodes) {
+      const bool act = g * CPB + cZ < b.n_cells;
+      T in[N];
+#pragma unroll
+      for (int k = 0; k < N; ++k) in[k] = act ? st[stZ + N * N * k] : T(0);
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        T v = T(0);
+#pragma unroll
+        for (int k = 0; k < N; ++k) v += tab.B[k * Q + q] * in[k];
+        work[baseZ + Q2 * q] = v;
+      }
+    }
+    __syncthreads();
+    // 2. y interpolation on y-lines with x < N
+    if (ymodes) {
+#pragma unroll
+      for (int j = 0; j < N; ++j) line[j] = work[baseY + Q * j];
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        T v = T(0);
+#pragma unroll
+        for (int j = 0; j < N; ++j) v += tab.B[j * Q + q] * line[j];
+        out[q] = v;
+      }
+#pragma unroll
+      for (int q = 0; q < Q; ++q) work[baseY + Q * q] = out[q];
+    }
+    __syncthreads();
+    // 3. x interpolation and x derivative on x-lines; flux scaling folded in
+    {
+      const T cx = fuse ? wX * kappa * T(scl[cX * 4 + 0]) : T(1);
+#pragma unroll
+      for (int i = 0; i < N; ++i) line[i] = work[baseX + i];
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        T v = T(0);
+#pragma unroll
+        for (int i = 0; i < N; ++i) v += tab.B[i * Q + q] * line[i];
+        out[q] = v;
+      }
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        T v = T(0);
+#pragma unroll
+        for (int l = 0; l < Q; ++l) v += tab.D[q * Q + l] * out[l];
+        work[baseX + q] = out[q];
+        work[baseX + 2 * BP + q] = fuse ? v * (cx * tab.W[q]) : v;
+      }
+    }
+    __syncthreads();
+    // 4. y derivative on y-lines
+    {
+      const T cy = fuse ? wY * kappa * T(scl[cY * 4 + 1]) : T(1);
+#pragma unroll
+      for (int l = 0; l < Q; ++l) line[l] = work[baseY + Q * l];
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        T v = T(0);
+#pragma unroll
+        for (int l = 0; l < Q; ++l) v += tab.D[q * Q + l] * line[l];
+        work[baseY + BP + Q * q] = fuse ? v * (cy * tab.W[q]) : v;
+      }
+    }
+    __syncthreads();
+    // 5. z derivative, pointwise flux and transposed z derivative on z-lines
+    {
+      const double* sc = scl + cZ * 4;
+      const T wz = wZ * T(sc[3]);            // W_a W_b detJ
+      const T kz = wZ * kappa * T(sc[2]);    // W_a W_b kappa detJ sz^2
+      T u[Q], dz[Q];
+#pragma unroll
+      for (int l = 0; l < Q; ++l) u[l] = work[baseZ + Q2 * l];
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        T v = T(0);
+#pragma unroll
+        for (int l = 0; l < Q; ++l) v += tab.D[q * Q + l] * u[l];
+        dz[q] = v;
+      }
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        const T w = wz * tab.W[q];
+        if (fuse) {
+          dz[q] *= kz * tab.W[q];
+        } else {
+          const int64_t cell = g * CPB + cZ;
+          const int p = pZ + Q2 * q;
+          const T k = cell < b.n_cells ? T(b.kappa_pts[cell * Q3 + p]) : T(0);
+          const T wk = wZ * tab.W[q] * kappa * k;
+          work[baseZ + 2 * BP + Q2 * q] *= wk * T(sc[0]);
+          work[baseZ + BP + Q2 * q] *= wk * T(sc[1]);
+          dz[q] *= wk * T(sc[2]);
+        }
+        u[q] *= w * mass;
+      }
+#pragma unroll
+      for (int l = 0; l < Q; ++l) {
+        T v = u[l];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) v += tab.D[q * Q + l] * dz[q];
+        work[baseZ + Q2 * l] = v;
+      }
+    }
+    __syncthreads();
+    // 6. transposed y derivative on y-lines
+    {
+#pragma unroll
+      for (int q = 0; q < Q; ++q) line[q] = work[baseY + BP + Q * q];
+#pragma unroll
+      for (int l = 0; l < Q; ++l) {
+        T v = work[baseY + Q * l];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) v += tab.D[q * Q + l] * line[q];
+        work[baseY + Q * l] = v;
+      }
+    }
+    __syncthreads();
+    // 7. transposed x derivative and transposed x interpolation on x-lines
+    {
+#pragma unroll
+      for (int l = 0; l < Q; ++l) out[l] = work[baseX + l];
+#pragma unroll
+      for (int q = 0; q < Q; ++q) line[q] = work[baseX + 2 * BP + q];
+#pragma unroll
+      for (int l = 0; l < Q; ++l) {
+        T v = out[l];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) v += tab.D[q * Q + l] * line[q];
+        out[l] = v;
+      }
+#pragma unroll
+      for (int i = 0; i < N; ++i) {
+        T v = T(0);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) v += tab.B[i * Q + q] * out[q];
+        work[baseX + i] = v;
+      }
+    }
+    __syncthreads();
+    // 8. transposed y interpolation on y-lines with x < N
+    if (ymodes) {
+#pragma unroll
+      for (int q = 0; q < Q; ++q) line[q] = work[baseY + Q * q];
+#pragma unroll
+      for (int j = 0; j < N; ++j) {
+        T v = T(0);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) v += tab.B[j * Q + q] * line[q];
+        work[baseY + Q * j] = v;
+      }
+    }
+    __syncthreads();
+    // 9. transposed z interpolation on z-lines through mode positions and scatter (the next
+    // group writes the work buffers only after the barrier at its start)
+    if (zmodes) {
+      const int64_t cell = g * CPB + cZ;
+      if (cell < b.n_cells) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) line[q] = work[baseZ + Q2 * q];
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+          T v = T(0);
+#pragma unroll
+          for (int q = 0; q < Q; ++q) v += tab.B[k * Q + q] * line[q];
+          scatter_entry<T>(b, cell * NB + mZ + N * N * k, v, y);
+        }
+      }
+    }
+  }
+  cp_async_wait<0>();
+}
+
+}  // namespace grico

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "cell_kernels.cuh"
+#include "cell_pipe.cuh"
 #include "grico_host.h"
 #include "grico_plan_internal.h"
 #include "vector_kernels.cuh"
@@ -137,6 +138,32 @@ Tables1D<N, Q, T> make_tables(const DevBatch& b) {
   return t;
 }
 
+int sm_count() {
+  static const int n = [] {
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    return v > 0 ? v : 1;
+  }();
+  return n;
+}
+
+// Resident blocks per SM of a persistent kernel (0 when it cannot launch, e.g. too much shared
+// memory); raises the kernel's dynamic shared-memory limit first when it needs more than 48 KB.
+int persistent_blocks_per_sm(const void* kern, int threads, size_t smem) {
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, threads, smem) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
 template <typename T>
 bool launch_fused(int dim, const DevBatch& bt, const BatchView& v, const T* x, T* y, int64_t nvec, T mass, T kappa,
                   int mode, const double* src, int nrhs, cudaStream_t st) {
@@ -153,13 +180,31 @@ bool launch_fused(int dim, const DevBatch& bt, const BatchView& v, const T* x, T
     kern<<<grid, block, smem, st>>>(v, make_tables<NN, QQ, T>(bt), x, y, nvec, mass, kappa, mode, src);       \
     return true;                                                                                               \
   }
+#define GRICO_L3_PIPE(NN, QQ, CPB_)                                                                            \
+  if (mode == 0) {                                                                                             \
+    constexpr int CPB = CPB_;                                                                                  \
+    constexpr int NT = QQ * QQ * CPB;                                                                          \
+    static const LaneLines<NT> lanes = make_lane_lines<NT>(NN, QQ, CPB, int(sizeof(T)));                      \
+    static const size_t smem = pipe_smem_bytes(CPB, lanes.bp, lanes.sp, int(sizeof(T)));                      \
+    auto kern = cell_apply_3d_pipe<NN, QQ, CPB, T>;                                                           \
+    static const int per_sm = persistent_blocks_per_sm(reinterpret_cast<const void*>(kern), NT, smem);        \
+    if (per_sm > 0) {                                                                                          \
+      const int64_t groups = (int64_t(v.n_cells) + CPB - 1) / CPB;                                             \
+      dim3 grid(unsigned(std::min<int64_t>(groups, int64_t(per_sm) * sm_count())), nrhs);                      \
+      kern<<<grid, NT, smem, st>>>(v, make_tables<NN, QQ, T>(bt), lanes, x, y, nvec, mass, kappa);             \
+      return true;                                                                                             \
+    }                                                                                                          \
+  }
 #define GRICO_L3(NN, QQ)                                                                                       \
   if (N == NN && Q == QQ) {                                                                                    \
     constexpr int C1 = (256 / (QQ * QQ)) > 0 ? (256 / (QQ * QQ)) : 1;                                          \
     constexpr int C0 = C1 / 2 > 0 ? C1 / 2 : 1;                                                                \
     constexpr int C2 = (2 * C1 * QQ * QQ <= 1024) ? 2 * C1 : C1;                                               \
-    if (var == 0) GRICO_L3_CPB(NN, QQ, C0)                                                                     \
-    if (var == 2) GRICO_L3_CPB(NN, QQ, C2)                                                                     \
+    if (var == 3) GRICO_L3_PIPE(NN, QQ, C0)                                                                    \
+    if (var == 4) GRICO_L3_PIPE(NN, QQ, C1)                                                                    \
+    if (var == 5) GRICO_L3_PIPE(NN, QQ, C2)                                                                    \
+    if (var % 3 == 0) GRICO_L3_CPB(NN, QQ, C0)                                                                 \
+    if (var % 3 == 2) GRICO_L3_CPB(NN, QQ, C2)                                                                 \
     GRICO_L3_CPB(NN, QQ, C1)                                                                                   \
   }
 #define GRICO_L2(NN, QQ)                                                                                     \
@@ -177,6 +222,7 @@ bool launch_fused(int dim, const DevBatch& bt, const BatchView& v, const T* x, T
     GRICO_L2(9, 9) GRICO_L2(2, 3) GRICO_L2(3, 4) GRICO_L2(4, 5) GRICO_L2(5, 6)
   }
 #undef GRICO_L3
+#undef GRICO_L3_PIPE
 #undef GRICO_L3_CPB
 #undef GRICO_L2
   return false;
@@ -1129,7 +1175,7 @@ int autotune_typed(GricoPlan* P, int nrhs, int reps, int* chosen) {
     int best = 1;
     if (P->dim == 3 && b.isotropic && b.q[0] >= b.n[0] && b.n_cells > 0) {
       float best_ms = 1e30f;
-      for (int var = 0; var < 3; ++var) {
+      for (int var = 0; var < kTileVariants; ++var) {
         b.tile[slot] = var;
         launch_batch<T>(*P, b, true, xb.get<T>(), yb.get<T>(), n, 0, nullptr, nrhs, st);  // warm-up
         cudaEventRecord(e0, st);
@@ -1158,4 +1204,20 @@ extern "C" int grico_plan_autotune(GricoPlan* P, int nrhs, int precision, int re
   }
   return precision == GRICO_PREC_FP64 ? autotune_typed<double>(P, nrhs, reps, chosen)
                                       : autotune_typed<float>(P, nrhs, reps, chosen);
+}
+
+extern "C" int grico_plan_set_tiles(GricoPlan* P, int precision, const int* tiles, int n_batches) {
+  if (!P || !tiles || (precision != GRICO_PREC_FP64 && precision != GRICO_PREC_FP32) ||
+      n_batches != int(P->batches.size())) {
+    set_error("grico_plan_set_tiles: invalid argument (tiles must hold one entry per cell batch)");
+    return GRICO_ERR_INVALID;
+  }
+  for (int i = 0; i < n_batches; ++i)
+    if (tiles[i] < 0 || tiles[i] >= kTileVariants) {
+      set_error("grico_plan_set_tiles: tile variant out of range");
+      return GRICO_ERR_INVALID;
+    }
+  const int slot = precision == GRICO_PREC_FP32 ? 1 : 0;
+  for (int i = 0; i < n_batches; ++i) P->batches[size_t(i)].tile[slot] = tiles[i];
+  return GRICO_OK;
 }

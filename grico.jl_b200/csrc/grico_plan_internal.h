@@ -60,6 +60,8 @@ struct DevBuf {
   bool upload(const std::vector<T>& v) { return upload(v.data(), v.size()); }
 };
 
+constexpr int kTileVariants = 6;
+
 struct DevMap {
   DevBuf map, coef, toff, tidx, tcoef;
 };
@@ -74,8 +76,10 @@ struct DevBatch {
   DevBuf h, kappa, B, G, W, D;
   DevBuf skip;  // uint8 per cell: hanging cells whose diagonal is added from the host
   std::vector<double> hB, hD, hW;  // axis-0 tables on the host (kernel parameters)
-  int tile[2] = {1, 1};  // cells-per-block variant of the 3-D tensor kernel per precision (0: FP64, 1: FP32):
-                         // 0 = half, 1 = default, 2 = double the default; chosen by grico_plan_autotune
+  int tile[2] = {1, 1};  // 3-D tensor-kernel variant per precision (0: FP64, 1: FP32): cells per block
+                         // half (0), default (1) or double (2) the default, one block per cell group;
+                         // 3..5 the same sizes in the persistent cp.async-pipelined apply kernel;
+                         // chosen by grico_plan_autotune or set by grico_plan_set_tiles
 };
 
 struct DevPointBatch {

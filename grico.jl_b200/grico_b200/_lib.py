@@ -207,6 +207,7 @@ SIGNATURES = {
     "grico_mg_lambda_max": (C.c_double, [P, C.c_int]),
     "grico_mg_set_learned": (C.c_int, [P, C.POINTER(GricoLearnedDesc)]),
     "grico_plan_autotune": (C.c_int, [P, C.c_int, C.c_int, C.c_int, i32p]),
+    "grico_plan_set_tiles": (C.c_int, [P, C.c_int, i32p, C.c_int]),
     "grico_cg_solve_multi": (C.c_int, [P, f64p, f64p, C.c_int, C.POINTER(GricoSolveOptions), C.POINTER(GricoSolveReport), C.c_int]),
     "grico_mg_learned_stats": (C.c_int, [P, i64p, i64p]),
     "grico_conv3d_forward": (C.c_int, [P, C.c_int, P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,

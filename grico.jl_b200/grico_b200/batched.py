@@ -16,11 +16,19 @@ from . import _lib as L
 
 
 def autotune(plan, nrhs=1, precision="fp64", reps=5):
-    """Per cell batch: 0 = half, 1 = default, 2 = double cells per block."""
+    """Per cell batch: 0 = half, 1 = default, 2 = double cells per block (one block per cell
+    group); 3, 4, 5 = the same sizes in the persistent pipelined apply kernel."""
     chosen = np.zeros(max(len(plan.batches), 1), dtype=np.int32)
     prec = L.GRICO_PREC_FP64 if precision == "fp64" else L.GRICO_PREC_FP32
     L.check(L.lib().grico_plan_autotune(plan.handle, int(nrhs), prec, int(reps), L.ptr(chosen, C.c_int32)), "autotune")
     return chosen[:len(plan.batches)]
+
+
+def set_tiles(plan, tiles, precision="fp64"):
+    """Replay a kernel-variant choice (as returned by `autotune`) without timing."""
+    t = np.ascontiguousarray(tiles, dtype=np.int32)
+    prec = L.GRICO_PREC_FP64 if precision == "fp64" else L.GRICO_PREC_FP32
+    L.check(L.lib().grico_plan_set_tiles(plan.handle, prec, L.ptr(t, C.c_int32), int(t.size)), "set_tiles")
 
 
 def solve_many(plan, B, relative_tolerance=1e-10, absolute_tolerance=0.0, maxiter=None, jacobi=True, mixed=False,

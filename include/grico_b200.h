@@ -195,12 +195,18 @@ typedef struct GricoPlan GricoPlan;
 /* Copies every descriptor array to the device; the caller may free them afterwards.  The plan
  * owns its workspaces and one CUDA stream.  Calls on one plan are serialised. */
 int grico_plan_create(const GricoPlanDesc* desc, GricoPlan** out);
-/* Per-batch tile autotuner (no reference counterpart): times the cells-per-block variants
- * (half, default, double) of the 3-D tensor-cell kernel on this plan's batches for `nrhs`
- * right-hand sides in `precision`, keeps the fastest per batch for later applies of that
- * precision, and writes the choice per cell batch to `chosen` (may be NULL; 0 = half, 1 =
- * default, 2 = double).  Allocates scratch; call before any stream capture. */
+/* Per-batch tile autotuner (no reference counterpart): times the variants of the 3-D
+ * tensor-cell kernel on this plan's batches for `nrhs` right-hand sides in `precision`, keeps
+ * the fastest per batch for later applies of that precision, and writes the choice per cell
+ * batch to `chosen` (may be NULL).  Variants: 0, 1, 2 = half, default, double cells per block
+ * with one block per cell group; 3, 4, 5 = the same sizes in the persistent kernel that
+ * prefetches the next cell group's gather with asynchronous copies.  Batches without a 3-D
+ * isotropic tensor kernel report 1.  Allocates scratch; call before any stream capture. */
 int grico_plan_autotune(GricoPlan* plan, int nrhs, int precision, int reps, int* chosen);
+/* Sets the kernel variant of every cell batch for `precision` (tiles[n_batches], values as
+ * reported by grico_plan_autotune), e.g. to replay a stored tuning without timing again.
+ * No reference counterpart. */
+int grico_plan_set_tiles(GricoPlan* plan, int precision, const int* tiles, int n_batches);
 int grico_plan_destroy(GricoPlan* plan);
 /* n_full, n_reduced */
 int grico_plan_sizes(const GricoPlan* plan, int64_t* n_full, int64_t* n_reduced);

@@ -56,7 +56,7 @@ def test_autotuned_tiles_keep_results(cuda):
     y0 = gb.apply(plan, x)
     for prec in ("fp64", "fp32"):
         chosen = bt.autotune(plan, nrhs=4, precision=prec, reps=3)
-        assert len(chosen) == len(plan.batches) and set(chosen.tolist()) <= {0, 1, 2}
+        assert len(chosen) == len(plan.batches) and set(chosen.tolist()) <= set(range(6))
     assert rel_err(gb.apply(plan, x), y0) <= 1e-12
     y32 = gb.apply(plan, x.astype(np.float32))
     assert rel_err(y32, y0) <= 2e-5
