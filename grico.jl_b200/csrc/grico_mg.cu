@@ -6,6 +6,9 @@
 //   * damped Jacobi x += w D^-1 (b - A x)   — the reference's SPD smoother (multigrid.jl:943-956)
 //   * Chebyshev-Jacobi of a given degree on [lambda_max*lower, 1.2*lambda_max] of D^-1 A, with
 //     lambda_max from a power iteration at set-up — no reference counterpart.
+//   * fixed-step right-Jacobi-preconditioned GMRES (multigrid.jl:963-1056) for non-SPD levels:
+//     Arnoldi with modified Gram-Schmidt, Givens rotations and the back substitution run on the
+//     device (one thread for the small Hessenberg work), so the V-cycle needs no host round trip.
 // The coarsest level is solved in FP64 with the dense Cholesky factor of its reduced matrix
 // (common.jl:272-330); the factor is inverted once on the host and applied as a dense
 // matrix-vector product.
@@ -44,6 +47,10 @@ struct GricoMultigrid {
   GricoMGOptions opts{};
   cudaStream_t stream = nullptr;
   grico::DevBuf io_r, io_z;
+  // GMRES smoother: per smoothed level the Krylov basis V [(m+1) x n] and the preconditioned
+  // directions Z [m x n] in the working precision; one small FP64 workspace shared by all levels
+  std::vector<grico::DevBuf> gm_v, gm_z;
+  grico::DevBuf gm_ws;
   // learned smoother sweep on one level (see learned_sweep)
   struct Learned {
     int level = -1;
@@ -183,12 +190,19 @@ void level_apply(GricoMultigrid* mg, int l, const T* x, T* y, cudaStream_t st) {
 }
 
 template <typename T>
+void smooth_gmres(GricoMultigrid* mg, int l, T* x, const T* b, int steps, cudaStream_t st);
+
+template <typename T>
 void smooth(GricoMultigrid* mg, int l, T* x, const T* b, int steps, cudaStream_t st) {
   using B = LevelBufs<T>;
   const int64_t n = mg->levels[l]->n_red;
   T* t = B::t(mg, l);
   const T* dinv = B::dinv(mg, l);
   if (steps <= 0) return;
+  if (mg->opts.smoother == GRICO_SMOOTHER_GMRES) {
+    smooth_gmres<T>(mg, l, x, b, steps, st);
+    return;
+  }
   if (mg->opts.smoother == GRICO_SMOOTHER_JACOBI) {
     for (int s = 0; s < steps; ++s) {
       level_apply<T>(mg, l, x, t, st);
@@ -214,6 +228,155 @@ void smooth(GricoMultigrid* mg, int l, T* x, const T* b, int steps, cudaStream_t
       }
     }
   }
+}
+
+// ---- GMRES smoother (multigrid.jl:963-1056) ----
+// Small FP64 workspace: scalars, then H ((m+1) x m, column-major), g (m+1), cs, sn, y (m each).
+enum GmresScalar { kGmBeta = 0, kGmNrm2 = 1, kGmNrm = 2, kGmStop = 3, kGmInner = 4, kGmSingular = 5, kGmScalars = 8 };
+inline size_t gmres_ws_doubles(int m) { return size_t(kGmScalars) + size_t(m + 1) * m + size_t(m + 1) + 3 * size_t(m); }
+
+// ws[kGmBeta] holds ||r||^2 on entry and beta = ||r|| on exit: g = (beta, 0, ...), H = 0; stop
+// when beta == 0 (the smoother then leaves x unchanged, multigrid.jl:972)
+__global__ void gm_start(double* ws, int m) {
+  double* H = ws + kGmScalars;
+  double* g = H + (m + 1) * m;
+  for (int i = threadIdx.x; i < (m + 1) * m; i += blockDim.x) H[i] = 0.0;
+  for (int i = threadIdx.x; i < m + 1; i += blockDim.x) g[i] = 0.0;
+  if (threadIdx.x == 0) {
+    const double beta = sqrt(ws[kGmBeta]);
+    g[0] = beta;
+    ws[kGmStop] = beta > 0.0 ? 0.0 : 1.0;
+    ws[kGmInner] = 0.0;
+    ws[kGmBeta] = beta;
+  }
+}
+
+// ws[kGmNrm] = ||w|| from ws[kGmNrm2]
+__global__ void gm_sqrt_into(double* ws) { ws[kGmNrm] = sqrt(ws[kGmNrm2]); }
+
+// dst = src / *s (0 when *s == 0); the reference divides element by element
+template <typename T>
+__global__ void gm_divide(const T* __restrict__ src, T* __restrict__ dst, const double* __restrict__ s, int64_t n) {
+  const double d = *s;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    dst[i] = d > 0.0 ? T(double(src[i]) / d) : T(0);
+}
+
+// w -= c v with c a device scalar (modified Gram-Schmidt step)
+template <typename T>
+__global__ void gm_axpy_neg(T* __restrict__ w, const T* __restrict__ v, const double* __restrict__ c, int64_t n) {
+  const T a = T(*c);
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    w[i] -= a * v[i];
+}
+
+// H[j+1, j] = ||w||, then the previous rotations, the new rotation of column j and its action
+// on g (solve.jl:544-576); records the inner count and stops after a zero norm
+__global__ void gm_givens(double* ws, int m, int j) {
+  if (ws[kGmStop] != 0.0) return;
+  double* H = ws + kGmScalars;
+  double* g = H + (m + 1) * m;
+  double* cs = g + (m + 1);
+  double* sn = cs + m;
+  double* col = H + size_t(m + 1) * j;
+  const double nrm = ws[kGmNrm];
+  col[j + 1] = nrm;
+  for (int i = 0; i < j; ++i) {
+    const double a = col[i], b = col[i + 1];
+    col[i] = cs[i] * a + sn[i] * b;
+    col[i + 1] = -sn[i] * a + cs[i] * b;
+  }
+  const double scale = hypot(col[j], col[j + 1]);
+  const double c = scale == 0.0 ? 1.0 : col[j] / scale, s = scale == 0.0 ? 0.0 : col[j + 1] / scale;
+  cs[j] = c;
+  sn[j] = s;
+  const double a = col[j], b = col[j + 1];
+  col[j] = c * a + s * b;
+  col[j + 1] = -s * a + c * b;
+  const double ga = g[j], gb = g[j + 1];
+  g[j] = c * ga + s * gb;
+  g[j + 1] = -s * ga + c * gb;
+  ws[kGmInner] = double(j + 1);
+  if (nrm == 0.0) ws[kGmStop] = 1.0;
+}
+
+// back substitution of the rotated Hessenberg system; a zero or non-finite diagonal (the
+// reference's ArgumentError, multigrid.jl:1048-1051) counts in ws[kGmSingular] and skips the update
+__global__ void gm_solve(double* ws, int m) {
+  double* H = ws + kGmScalars;
+  double* g = H + (m + 1) * m;
+  double* y = g + (m + 1) + 2 * m;
+  const int inner = int(ws[kGmInner]);
+  for (int row = inner - 1; row >= 0; --row) {
+    double v = g[row];
+    for (int col = row + 1; col < inner; ++col) v -= H[size_t(m + 1) * col + row] * y[col];
+    const double d = H[size_t(m + 1) * row + row];
+    if (!isfinite(d) || d == 0.0) {
+      ws[kGmSingular] += 1.0;
+      ws[kGmInner] = 0.0;
+      return;
+    }
+    y[row] = v / d;
+  }
+}
+
+// x += omega y_j z_j for j < inner, one column after the other
+template <typename T>
+__global__ void gm_update(T* __restrict__ x, const T* __restrict__ Z, const double* __restrict__ ws, int m, double omega,
+                          int64_t n) {
+  const double* y = ws + kGmScalars + (m + 1) * m + (m + 1) + 2 * m;
+  const int inner = int(ws[kGmInner]);
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    T xi = x[i];
+    for (int j = 0; j < inner; ++j) {
+      const T a = T(omega * y[j]);
+      if (a != T(0)) xi += a * Z[size_t(j) * n + i];
+    }
+    x[i] = xi;
+  }
+}
+
+template <typename T>
+void smooth_gmres(GricoMultigrid* mg, int l, T* x, const T* b, int steps, cudaStream_t st) {
+  using B = LevelBufs<T>;
+  const int64_t n = mg->levels[l]->n_red;
+  const int m = mg->opts.smoother_restart;
+  const int count = int(std::min<int64_t>(std::min(steps, m), n));
+  if (count <= 0) return;
+  T* t = B::t(mg, l);
+  T* r = B::r(mg, l);
+  const T* dinv = B::dinv(mg, l);
+  T* V = mg->gm_v[l].get<T>();
+  T* Z = mg->gm_z[l].get<T>();
+  double* ws = mg->gm_ws.get<double>();
+  double* H = ws + kGmScalars;
+  double* partial = mg->levels[l]->partial.get<double>();
+  level_apply<T>(mg, l, x, t, st);
+  residual_kernel<T><<<blocks(n), 256, 0, st>>>(r, b, t, n);
+  dot_partial<T><<<kRedBlocks, kRedThreads, 0, st>>>(r, r, n, partial);
+  reduce_final<<<1, kRedThreads, 0, st>>>(partial, kRedBlocks, ws + kGmBeta);
+  gm_start<<<1, 128, 0, st>>>(ws, m);
+  gm_divide<T><<<blocks(n), 256, 0, st>>>(r, V, ws + kGmBeta, n);
+  for (int j = 0; j < count; ++j) {
+    T* vj = V + size_t(j) * n;
+    T* zj = Z + size_t(j) * n;
+    scale_kernel<T><<<blocks(n), 256, 0, st>>>(dinv, vj, zj, n);  // z = D^-1 v
+    level_apply<T>(mg, l, zj, t, st);                              // w = A z
+    for (int i = 0; i <= j; ++i) {
+      const T* vi = V + size_t(i) * n;
+      double* hij = H + size_t(m + 1) * j + i;
+      dot_partial<T><<<kRedBlocks, kRedThreads, 0, st>>>(t, vi, n, partial);
+      reduce_final<<<1, kRedThreads, 0, st>>>(partial, kRedBlocks, hij);
+      gm_axpy_neg<T><<<blocks(n), 256, 0, st>>>(t, vi, hij, n);
+    }
+    dot_partial<T><<<kRedBlocks, kRedThreads, 0, st>>>(t, t, n, partial);
+    reduce_final<<<1, kRedThreads, 0, st>>>(partial, kRedBlocks, ws + kGmNrm2);
+    gm_sqrt_into<<<1, 1, 0, st>>>(ws);
+    gm_divide<T><<<blocks(n), 256, 0, st>>>(t, V + size_t(j + 1) * n, ws + kGmNrm, n);
+    gm_givens<<<1, 1, 0, st>>>(ws, m, j);
+  }
+  gm_solve<<<1, 1, 0, st>>>(ws, m);
+  gm_update<T><<<blocks(n), 256, 0, st>>>(x, Z, ws, m, mg->opts.jacobi_omega, n);
 }
 
 void coarse_solve(GricoMultigrid* mg, double* x, const double* b, cudaStream_t st) {
@@ -349,6 +512,8 @@ int mg_vcycle_device(GricoMultigrid* mg, const double* r, double* z, cudaStream_
   return cuda_ok(cudaGetLastError(), "vcycle") ? GRICO_OK : GRICO_ERR_CUDA;
 }
 
+int mg_smoother(const GricoMultigrid* mg) { return mg ? mg->opts.smoother : -1; }
+
 int prepare_jacobi(GricoPlan* P, cudaStream_t st);
 
 }  // namespace grico
@@ -363,8 +528,17 @@ int grico_mg_create(GricoPlan* const* levels, int nlevels, const GricoTransferDe
     set_error("grico_mg_create: invalid argument");
     return GRICO_ERR_INVALID;
   }
-  if (opts->smoother != GRICO_SMOOTHER_JACOBI && opts->smoother != GRICO_SMOOTHER_CHEBYSHEV) {
+  if (opts->smoother != GRICO_SMOOTHER_JACOBI && opts->smoother != GRICO_SMOOTHER_CHEBYSHEV &&
+      opts->smoother != GRICO_SMOOTHER_GMRES) {
     set_error("grico_mg_create: unknown smoother");
+    return GRICO_ERR_INVALID;
+  }
+  if (opts->smoother == GRICO_SMOOTHER_GMRES &&
+      (opts->smoother_restart < 1 || opts->smoother_restart > 64 ||
+       opts->smoother_restart < std::max(opts->pre_steps, opts->post_steps))) {
+    // multigrid.jl:352-358
+    set_error("grico_mg_create: the GMRES smoother needs 1 <= smoother_restart <= 64 and smoother_restart >= "
+              "max(pre_steps, post_steps)");
     return GRICO_ERR_INVALID;
   }
   if (opts->smoother == GRICO_SMOOTHER_CHEBYSHEV && (opts->chebyshev_degree < 1 || !(opts->chebyshev_lower > 0.0 && opts->chebyshev_lower < 1.0))) {
@@ -499,6 +673,20 @@ int grico_mg_create(GricoPlan* const* levels, int nlevels, const GricoTransferDe
       for (int64_t i = 0; i < n0; ++i) inv[i * n0 + j] = col[i];
     }
     if (!mg->coarse_inv.upload(inv)) return GRICO_ERR_CUDA;
+  }
+  // GMRES smoother workspaces (multigrid.jl:163-176, 360-365)
+  if (opts->smoother == GRICO_SMOOTHER_GMRES) {
+    const int m = opts->smoother_restart;
+    const size_t es = fp32 ? sizeof(float) : sizeof(double);
+    mg->gm_v.resize(size_t(nlevels));
+    mg->gm_z.resize(size_t(nlevels));
+    for (int l = 1; l < nlevels; ++l) {
+      const size_t n = size_t(std::max<int64_t>(levels[l]->n_red, 1));
+      if (!mg->gm_v[size_t(l)].alloc(es * n * size_t(m + 1)) || !mg->gm_z[size_t(l)].alloc(es * n * size_t(m)))
+        return GRICO_ERR_CUDA;
+    }
+    if (!mg->gm_ws.alloc(sizeof(double) * gmres_ws_doubles(m))) return GRICO_ERR_CUDA;
+    cudaMemsetAsync(mg->gm_ws.ptr, 0, sizeof(double) * gmres_ws_doubles(m), st);
   }
   // Chebyshev: lambda_max(D^-1 A) per smoothed level by power iteration
   if (opts->smoother == GRICO_SMOOTHER_CHEBYSHEV) {

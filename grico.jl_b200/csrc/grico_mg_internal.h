@@ -7,4 +7,6 @@
 namespace grico {
 // z = V-cycle(r) on the finest level of mg, on stream st (multigrid.jl:858-889)
 int mg_vcycle_device(GricoMultigrid* mg, const double* r, double* z, cudaStream_t st);
+// GRICO_SMOOTHER_* of mg
+int mg_smoother(const GricoMultigrid* mg);
 }  // namespace grico

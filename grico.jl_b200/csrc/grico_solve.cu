@@ -87,6 +87,11 @@ extern "C" int grico_cg_solve(GricoPlan* P, GricoMultigrid* mg, const double* b,
                               const GricoSolveOptions* opts, GricoSolveReport* report, int flags) {
   if (!P || !b || !x || !opts) { set_error("cg: invalid argument"); return GRICO_ERR_INVALID; }
   if (opts->preconditioner == GRICO_PRECOND_MULTIGRID && !mg) { set_error("cg: multigrid preconditioner missing"); return GRICO_ERR_INVALID; }
+  if (opts->preconditioner == GRICO_PRECOND_MULTIGRID && mg_smoother(mg) == GRICO_SMOOTHER_GMRES) {
+    // multigrid.jl:253-255: the GMRES smoother makes the V-cycle nonlinear and nonsymmetric
+    set_error("cg: the GMRES multigrid smoother needs FGMRES");
+    return GRICO_ERR_INVALID;
+  }
   if (opts->maxiter < 1) { set_error("maxiter must be positive"); return GRICO_ERR_INVALID; }
   if (!(opts->relative_tolerance >= 0) || !(opts->absolute_tolerance >= 0)) { set_error("tolerances must be non-negative"); return GRICO_ERR_INVALID; }
   cudaStream_t st = P->stream;

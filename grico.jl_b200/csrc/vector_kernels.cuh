@@ -89,11 +89,12 @@ static __global__ void fill_kernel(T* __restrict__ y, int64_t n, T v) {
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) y[i] = v;
 }
 
-// y = a*x + b*y
+// y = a*x + b*y; with b == 0, y is not read (it may be fresh memory holding NaN bit patterns,
+// and 0 * NaN is NaN)
 template <typename T>
 static __global__ void axpby_kernel(T a, const T* __restrict__ x, T b, T* __restrict__ y, int64_t n) {
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
-    y[i] = a * x[i] + b * y[i];
+    y[i] = b == T(0) ? a * x[i] : a * x[i] + b * y[i];
 }
 
 // z = w .* r

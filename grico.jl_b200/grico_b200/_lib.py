@@ -42,6 +42,7 @@ GRICO_PRECOND_JACOBI = 1
 GRICO_PRECOND_MULTIGRID = 2
 GRICO_SMOOTHER_JACOBI = 0
 GRICO_SMOOTHER_CHEBYSHEV = 1
+GRICO_SMOOTHER_GMRES = 2
 
 P = C.c_void_p
 i32p = C.POINTER(C.c_int32)
@@ -160,6 +161,7 @@ class GricoMGOptions(C.Structure):
         ("chebyshev_degree", C.c_int32),
         ("chebyshev_lower", C.c_double),
         ("precision", C.c_int32),
+        ("smoother_restart", C.c_int32),
     ]
 
 

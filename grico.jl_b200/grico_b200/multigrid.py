@@ -7,9 +7,12 @@ default, multigrid.jl:470-499), then h-coarsening one split frontier per level
 transfers come from libgrico_b200 (grico_transfer_build); the coarsest level is factorised
 by dense Cholesky (at most `coarse_direct_dof_limit` dofs, multigrid.jl:382-398).
 
-Smoothers: damped Jacobi (the reference's SPD smoother, multigrid.jl:943-956) and, with
-`smoother="chebyshev"`, Chebyshev-Jacobi of degree `chebyshev_degree` on
-[lambda_max/`chebyshev_range`, 1.2 lambda_max] of D^-1 A (no reference counterpart).
+Smoothers: damped Jacobi (the reference's SPD smoother, multigrid.jl:943-956), the fixed-step
+right-Jacobi GMRES smoother with `smoother_restart` Krylov columns for non-SPD problems
+(multigrid.jl:963-1056; `smoother="auto"` picks Jacobi for SPD problems and GMRES otherwise,
+multigrid.jl:347-350) and, with `smoother="chebyshev"`, Chebyshev-Jacobi of degree
+`chebyshev_degree` on [lambda_max/`chebyshev_range`, 1.2 lambda_max] of D^-1 A (no reference
+counterpart).
 """
 from __future__ import annotations
 
@@ -22,25 +25,43 @@ from . import _lib as L
 
 class GeometricMultigridPreconditioner:
     def __init__(self, min_degree=1, max_levels=16, p_sequence="bisect", pre_smoothing_steps=2,
-                 post_smoothing_steps=2, smoother_damping=0.8, smoother="auto", coarse_direct_dof_limit=512,
-                 chebyshev_degree=3, chebyshev_range=15.0, precision="fp64"):
+                 post_smoothing_steps=2, smoother_damping=0.8, smoother="auto", smoother_restart=8,
+                 coarse_direct_dof_limit=512, chebyshev_degree=3, chebyshev_range=15.0, precision="fp64"):
         if p_sequence not in ("bisect", "decrease_by_one", "go_to_one"):
             raise ValueError("p_sequence must be :bisect, :decrease_by_one, or :go_to_one")
-        if smoother not in ("auto", "jacobi", "chebyshev"):
-            raise ValueError("smoother must be :auto, :jacobi or :chebyshev (the GMRES smoother is for non-SPD problems)")
+        if smoother not in ("auto", "jacobi", "gmres", "chebyshev"):
+            raise ValueError("smoother must be :auto, :jacobi, :gmres or :chebyshev")
         if max_levels < 1 or pre_smoothing_steps < 0 or post_smoothing_steps < 0 or smoother_damping <= 0:
             raise ValueError("invalid multigrid options")
+        if int(smoother_restart) < 1:
+            raise ValueError("smoother_restart must be positive")
         self.min_degree = int(min_degree)
         self.max_levels = int(max_levels)
         self.p_sequence = p_sequence
         self.pre_smoothing_steps = int(pre_smoothing_steps)
         self.post_smoothing_steps = int(post_smoothing_steps)
         self.smoother_damping = float(smoother_damping)
-        self.smoother = "jacobi" if smoother == "auto" else smoother
+        self.smoother = smoother
+        self.smoother_restart = int(smoother_restart)
         self.coarse_direct_dof_limit = int(coarse_direct_dof_limit)
         self.chebyshev_degree = int(chebyshev_degree)
         self.chebyshev_range = float(chebyshev_range)
         self.precision = precision
+
+
+def resolved_smoother(opts, problem=None):
+    """multigrid.jl:347-358: `auto` is Jacobi for SPD problems and GMRES otherwise; GMRES needs
+    `smoother_restart >= max(pre, post)`."""
+    from .problem import SPD
+
+    sm = opts.smoother
+    if sm == "auto":
+        spd = problem is None or isinstance(getattr(problem, "operator_class", SPD()), SPD)
+        sm = "jacobi" if spd else "gmres"
+    if sm == "gmres" and max(opts.pre_smoothing_steps, opts.post_smoothing_steps) > opts.smoother_restart:
+        raise ValueError("GMRES multigrid smoother requires smoother_restart to be at least "
+                         "max(pre_smoothing_steps, post_smoothing_steps)")
+    return sm
 
 
 def _coarsened_degree(degree, lower, sequence):
@@ -167,6 +188,7 @@ class Multigrid:
         self.plans = plans
         self.transfers = transfers
         self.opts = opts
+        self.smoother = resolved_smoother(opts, getattr(plans[-1], "problem", None))
         if plans[0].n_reduced > opts.coarse_direct_dof_limit:
             raise L.GricoError(L.GRICO_ERR_INVALID,
                                f"coarse level has {plans[0].n_reduced} dofs > coarse_direct_dof_limit; "
@@ -180,7 +202,9 @@ class Multigrid:
             descs[i].col_index = L.ptr(col, C.c_int64)
             descs[i].values = L.ptr(val, C.c_double)
         mo = L.GricoMGOptions()
-        mo.smoother = L.GRICO_SMOOTHER_CHEBYSHEV if opts.smoother == "chebyshev" else L.GRICO_SMOOTHER_JACOBI
+        mo.smoother = {"jacobi": L.GRICO_SMOOTHER_JACOBI, "chebyshev": L.GRICO_SMOOTHER_CHEBYSHEV,
+                       "gmres": L.GRICO_SMOOTHER_GMRES}[self.smoother]
+        mo.smoother_restart = opts.smoother_restart
         mo.pre_steps = opts.pre_smoothing_steps
         mo.post_steps = opts.post_smoothing_steps
         mo.jacobi_omega = opts.smoother_damping

@@ -925,6 +925,15 @@ def solve(plan_or_problem, solver=None, relative_tolerance=None, absolute_tolera
     mg = None
     pre = solver.preconditioner
     if isinstance(pre, GeometricMultigridPreconditioner):
+        from .multigrid import resolved_smoother
+
+        if isinstance(solver, CGSolver):
+            if not isinstance(plan.problem.operator_class, SPD):
+                raise ValueError("CG with GeometricMultigridPreconditioner requires an SPD affine problem; "
+                                 "use FGMRESSolver")  # multigrid.jl:248-251
+            if resolved_smoother(pre, plan.problem) == "gmres":
+                raise ValueError("CG with GeometricMultigridPreconditioner requires the Jacobi smoother; "
+                                 "use FGMRESSolver for nonsymmetric smoother policies")  # multigrid.jl:253-255
         mg = build_multigrid(plan, pre)
         code = L.GRICO_PRECOND_MULTIGRID
     else:

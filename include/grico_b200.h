@@ -290,6 +290,8 @@ typedef struct GricoTransferDesc {
 
 #define GRICO_SMOOTHER_JACOBI 0     /* damped Jacobi, reference default (multigrid.jl:943-956) */
 #define GRICO_SMOOTHER_CHEBYSHEV 1  /* Chebyshev-Jacobi (no reference counterpart)            */
+#define GRICO_SMOOTHER_GMRES 2      /* fixed-step right-Jacobi GMRES (multigrid.jl:963-1056), for
+                                       non-SPD operators; not for CG (multigrid.jl:253-255)      */
 
 typedef struct GricoMGOptions {
   int32_t smoother;
@@ -298,6 +300,7 @@ typedef struct GricoMGOptions {
   int32_t chebyshev_degree;
   double chebyshev_lower;       /* fraction of lambda_max for the lower bound               */
   int32_t precision;            /* GRICO_PREC_FP64 or GRICO_PREC_FP32 for level applies     */
+  int32_t smoother_restart;     /* GMRES smoother Krylov columns, >= max(pre, post) (8)     */
 } GricoMGOptions;
 
 /* levels[0] is the coarsest; transfers[i] maps level i -> i+1.  coarse_matrix is the dense

@@ -1322,9 +1322,14 @@ class Multigrid:
     """V-cycle with damped Jacobi smoothing and a dense Cholesky coarse solve
     (multigrid.jl:858-956, common.jl:272-330)."""
 
-    def __init__(self, plans, pre=2, post=2, omega=0.8):
+    def __init__(self, plans, pre=2, post=2, omega=0.8, smoother="jacobi", restart=8):
         self.plans = plans
         self.pre, self.post, self.omega = pre, post, omega
+        if smoother not in ("jacobi", "gmres"):
+            raise ValueError("smoother must be jacobi or gmres")
+        if smoother == "gmres" and max(pre, post) > restart:
+            raise ValueError("GMRES smoother requires restart >= max(pre, post)")  # multigrid.jl:352-358
+        self.smoother, self.restart = smoother, restart
         self.transfers = [multigrid_transfer(plans[i], plans[i + 1]) for i in range(len(plans) - 1)]
         self.P = []
         for i, ent in enumerate(self.transfers):
@@ -1344,9 +1349,71 @@ class Multigrid:
 
     def smooth(self, level, x, b, steps):
         p = self.plans[level]
+        if self.smoother == "gmres":
+            return self.smooth_gmres(level, x, b, steps)
         for _ in range(steps):
             r = b - p.reduced_apply(x)
             x = x + self.omega * self.dinv[level] * r
+        return x
+
+    def smooth_gmres(self, level, x, b, steps):
+        """Fixed-step right-Jacobi-preconditioned GMRES smoother (multigrid.jl:963-1056):
+        `count` Arnoldi steps with modified Gram-Schmidt, Givens rotations on the Hessenberg
+        columns (solve.jl:544-576), back substitution, x += omega * Z y."""
+        if steps == 0:
+            return x
+        p = self.plans[level]
+        r = b - p.reduced_apply(x)
+        beta = math.sqrt(float(np.dot(r, r)))
+        if beta == 0.0:
+            return x
+        n = len(b)
+        count = min(steps, self.restart, n)
+        if count == 0:
+            return x
+        V = np.zeros((n, count + 1))
+        Z = np.zeros((n, count))
+        H = np.zeros((count + 1, count))
+        g = np.zeros(count + 1)
+        cs = np.zeros(count)
+        sn = np.zeros(count)
+        V[:, 0] = r / beta
+        g[0] = beta
+        inner = 0
+        for j in range(count):
+            inner = j + 1
+            Z[:, j] = self.dinv[level] * V[:, j]
+            w = p.reduced_apply(Z[:, j])
+            for i in range(j + 1):
+                H[i, j] = float(np.dot(w, V[:, i]))
+                w = w - H[i, j] * V[:, i]
+            nrm = math.sqrt(float(np.dot(w, w)))
+            H[j + 1, j] = nrm
+            if nrm > 0.0:
+                V[:, j + 1] = w / nrm
+            for i in range(j):
+                a, c = H[i, j], H[i + 1, j]
+                H[i, j] = cs[i] * a + sn[i] * c
+                H[i + 1, j] = -sn[i] * a + cs[i] * c
+            scale = math.hypot(H[j, j], H[j + 1, j])
+            cs[j], sn[j] = (1.0, 0.0) if scale == 0.0 else (H[j, j] / scale, H[j + 1, j] / scale)
+            a, c = H[j, j], H[j + 1, j]
+            H[j, j] = cs[j] * a + sn[j] * c
+            H[j + 1, j] = -sn[j] * a + cs[j] * c
+            a, c = g[j], g[j + 1]
+            g[j] = cs[j] * a + sn[j] * c
+            g[j + 1] = -sn[j] * a + cs[j] * c
+            if nrm == 0.0:
+                break
+        y = np.zeros(inner)
+        for row in range(inner - 1, -1, -1):
+            v = g[row] - sum(H[row, col] * y[col] for col in range(row + 1, inner))
+            if not math.isfinite(H[row, row]) or H[row, row] == 0.0:
+                raise ValueError("GMRES smoother: singular Krylov least-squares problem")
+            y[row] = v / H[row, row]
+        for j in range(inner):
+            if self.omega * y[j] != 0.0:
+                x = x + (self.omega * y[j]) * Z[:, j]
         return x
 
     def vcycle(self, level, b):

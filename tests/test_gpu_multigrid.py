@@ -130,3 +130,45 @@ def test_graph_replayed_cg_matches_direct_launches(cuda, precision):
     assert sg.report.iterations == sd.report.iterations
     # atomic scatter order differs run to run; in the FP32 V-cycle that shows at ~1e-12
     assert rel_err(sg.coefficients, sd.coefficients) <= (1e-12 if precision == "fp64" else 1e-10)
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("steps", [(2, 2), (1, 3)])
+def test_gmres_smoother_vcycle_matches_oracle(cuda, name, steps):
+    """V-cycle with the fixed-step right-Jacobi GMRES smoother (multigrid.jl:963-1056) against the
+    oracle's restatement, FP64, two successive V-cycles (the workspace is reused)."""
+    oplans, plan = _pair(name)
+    pre, post = steps
+    opts = GeometricMultigridPreconditioner(smoother="gmres", pre_smoothing_steps=pre, post_smoothing_steps=post,
+                                            smoother_restart=4)
+    mg = build_multigrid(plan, opts)
+    omg = go.Multigrid(oplans, pre=pre, post=post, smoother="gmres", restart=4)
+    rng = np.random.default_rng(9)
+    for _ in range(2):
+        r = rng.standard_normal(plan.n_reduced)
+        assert rel_err(mg.vcycle(r), omg.apply(r)) <= 1e-10
+
+
+def test_gmres_smoother_fgmres_solve(cuda):
+    """FGMRES(30) + V-cycle with the GMRES smoother solves to the requested tolerance, and its
+    solution equals the Jacobi-smoothed FGMRES solution; CG refuses the GMRES smoother."""
+    D = 2
+    src = lambda x: np.prod(np.sin(np.pi * x), axis=1) * (1.0 + D * np.pi ** 2)
+    _, plan = _pair("2d_p4", source=src)
+    s_gm = gb.solve(plan, solver=gb.FGMRESSolver(GeometricMultigridPreconditioner(smoother="gmres")),
+                    relative_tolerance=1e-11)
+    s_ja = gb.solve(plan, solver=gb.FGMRESSolver(GeometricMultigridPreconditioner()), relative_tolerance=1e-11)
+    assert s_gm.report.status == 0
+    assert rel_err(s_gm.coefficients, s_ja.coefficients) <= 1e-8
+    with pytest.raises(ValueError):
+        gb.solve(plan, solver=gb.CGSolver(GeometricMultigridPreconditioner(smoother="gmres")))
+
+
+def test_gmres_smoother_fp32_levels(cuda):
+    """FP32 working precision with the GMRES smoother: the V-cycle stays within FP32 rounding of
+    the FP64 V-cycle."""
+    _, plan = _pair("3d_p2")
+    r = np.random.default_rng(3).standard_normal(plan.n_reduced)
+    z64 = build_multigrid(plan, GeometricMultigridPreconditioner(smoother="gmres")).vcycle(r)
+    z32 = build_multigrid(plan, GeometricMultigridPreconditioner(smoother="gmres", precision="fp32")).vcycle(r)
+    assert rel_err(z32, z64) <= 1e-4

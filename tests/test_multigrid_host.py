@@ -96,3 +96,42 @@ def test_c2_shape_hierarchy_has_p_then_h_levels():
     assert len(plans) == 6
     assert sizes[0] == 3 ** 3 and sizes[-1] == 31 ** 3
     assert [p.space.degrees.max() for p in plans] == [1, 1, 1, 1, 2, 4]
+
+
+def test_smoother_policy():
+    """multigrid.jl:347-358: auto -> Jacobi for SPD problems, GMRES otherwise; GMRES needs
+    smoother_restart >= max(pre, post); CG refuses the GMRES smoother before any device work."""
+    from grico_b200.multigrid import resolved_smoother
+
+    d = gb.Domain((0.0, 0.0), (1.0, 1.0), (2, 2))
+    plan = _product_plan(d, 2, faces=[(1, 1)])
+    assert resolved_smoother(GeometricMultigridPreconditioner(), plan.problem) == "jacobi"
+    plan.problem.operator_class = gb.NonsymmetricOperator()
+    assert resolved_smoother(GeometricMultigridPreconditioner(), plan.problem) == "gmres"
+    with pytest.raises(ValueError):
+        resolved_smoother(GeometricMultigridPreconditioner(smoother="gmres", pre_smoothing_steps=9), plan.problem)
+    plan.problem.operator_class = gb.SPD()
+    with pytest.raises(ValueError):
+        gb.solve(plan, solver=gb.CGSolver(GeometricMultigridPreconditioner(smoother="gmres")))
+    with pytest.raises(ValueError):
+        go.Multigrid([], pre=3, post=1, smoother="gmres", restart=2)
+
+
+def test_oracle_gmres_smoother_reduces_residual():
+    """The oracle's GMRES smoother minimises ||b - A(x + Z y)|| over its Krylov space, so with
+    unit damping its residual is never larger than one damped-Jacobi step's."""
+    od = go.Domain((0.0, 0.0), (1.0, 1.0), (2, 2))
+    _refine_uniform(od.grid, 1)
+    oplans = _oracle_levels(od, 2, [(1, 1), (2, 2)])
+    fine = oplans[-1]
+    b = np.random.default_rng(1).standard_normal(len(fine.solve_dofs))
+    x0 = np.zeros_like(b)
+    mg_g = go.Multigrid(oplans, smoother="gmres", restart=4, omega=1.0)
+    mg_j = go.Multigrid(oplans, omega=0.8)
+    lv = len(oplans) - 1
+    for steps in (1, 2, 4):
+        xg = mg_g.smooth(lv, x0, b, steps)
+        xj = mg_j.smooth(lv, x0, b, 1)
+        rg = np.linalg.norm(b - fine.reduced_apply(xg))
+        assert rg <= np.linalg.norm(b - fine.reduced_apply(xj)) * (1 + 1e-12)
+        assert rg < np.linalg.norm(b)
