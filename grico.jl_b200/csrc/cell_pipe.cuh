@@ -6,8 +6,10 @@
 // While it computes group g, cp.async copies of x[map[e]] for the next group land in the
 // other shared stage and the map entries of the group after that are in flight into
 // registers, so the gather's two dependent global round trips overlap a whole group's
-// contractions.  Entries with a coefficient, a tail expansion or no dof are gathered
-// synchronously.
+// contractions.  The kernel serves plain maps only (every entry a dof or -1, no coefficients,
+// no tail expansions): the gather is branch-free (a zero-filling copy for -1 entries) and the
+// map entries are staged beside the modes, so the scatter reads them from shared memory.
+// Batches with hanging-node tails or coefficients use cell_apply_3d.
 //
 // Every contraction step gives each thread one whole line of a cell's Q^3 point box (x-, y- or
 // z-line), as in cell_apply_3d.  Which line a thread takes is not tied to its own cell: for each
@@ -35,6 +37,15 @@ template <int BYTES>
 __device__ __forceinline__ void cp_async_elem(void* smem_dst, const void* gsrc) {
   const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
   asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(dst), "l"(gsrc), "n"(BYTES) : "memory");
+}
+// Same with a source size of BYTES or 0: with 0 the destination is filled with zeros and the
+// source is not read.
+template <int BYTES>
+__device__ __forceinline__ void cp_async_zfill(void* smem_dst, const void* gsrc, bool read) {
+  const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  const unsigned src_bytes = read ? unsigned(BYTES) : 0u;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(dst), "l"(gsrc), "n"(BYTES), "r"(src_bytes)
+               : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int PENDING>
@@ -181,21 +192,25 @@ LaneLines<NT> make_lane_lines(int N, int Q, int CPB, int elem) {
 }
 
 // Shared-memory bytes of cell_apply_3d_pipe: two stages of cell sizes (4 doubles per cell), the
-// per-cell flux scales (4 doubles), three work buffers of bp elements per cell and two stages
-// of sp staged modes per cell.
+// per-cell flux scales (4 doubles), three work buffers of bp elements per cell, two stages of
+// sp staged modes per cell and two stages of sp staged map entries (int32) per cell.
 inline size_t pipe_smem_bytes(int CPB, int bp, int sp, int elem) {
-  return size_t(2) * CPB * 4 * 8 + size_t(CPB) * 4 * 8 + size_t(3) * CPB * bp * elem + size_t(2) * CPB * sp * elem;
+  return size_t(2) * CPB * 4 * 8 + size_t(CPB) * 4 * 8 + size_t(2) * CPB * sp * 4 + size_t(3) * CPB * bp * elem +
+         size_t(2) * CPB * sp * elem;
 }
 
-// Minimum resident blocks per SM asked of the compiler: caps registers near 100 per thread.
-// Measured on the 5^3 FP64 apply (125 threads): 96 registers, 5 blocks per SM, 0.345 ms;
-// 80 registers, 6 blocks, 0.410 ms; 64 registers spill (0.81 ms).
-constexpr int pipe_min_blocks(int threads) {
-  return (65536 / (100 * ((threads + 31) / 32 * 32))) > 0 ? 65536 / (100 * ((threads + 31) / 32 * 32)) : 1;
+// Minimum resident blocks per SM asked of the compiler, from a register target per thread:
+// 128 for boxes of 5^3 points and more, 100 below.  Measured on the 5^3 FP64 apply (125
+// threads, real 64^3 map): 116 registers, 4 blocks per SM, 0.340 ms; 96 registers (capped),
+// 5 blocks, 0.369 ms; an 80-register cap 0.410 ms; 64 registers spill heavily (0.81 ms).
+constexpr int pipe_min_blocks(int threads, int q) {
+  return (65536 / ((q >= 5 ? 128 : 100) * ((threads + 31) / 32 * 32))) > 0
+             ? 65536 / ((q >= 5 ? 128 : 100) * ((threads + 31) / 32 * 32))
+             : 1;
 }
 
 template <int N, int Q, int CPB, typename T>
-__global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB))
+__global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB, Q))
     cell_apply_3d_pipe(BatchView b, const Tables1D<N, Q, T> tab, const LaneLines<Q * Q * CPB> lanes,
                        const T* __restrict__ x, T* __restrict__ y, int64_t n_vec, T mass, T kappa) {
   constexpr int Q2 = Q * Q;
@@ -207,6 +222,7 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB))
   double* scl = hst + 2 * CPB * 4;                      // [CPB][4] detJ sx^2, detJ sy^2, detJ sz^2, detJ
   T* work = reinterpret_cast<T*>(scl + CPB * 4);        // [CPB][3][BP]
   T* stage = work + 3 * CPB * BP;                       // [2][CPB][SP]
+  int* smap = reinterpret_cast<int*>(stage + 2 * CPB * SP);  // [2][CPB][SP] staged map entries
   const int tid = threadIdx.x;
   x += blockIdx.y * n_vec;
   y += blockIdx.y * n_vec;
@@ -232,7 +248,6 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB))
   const int stZ = keep_reg(lc[kLineZ] * SP + la[kLineZ] + N * lb[kLineZ]);
   const int cX = keep_reg(lc[kLineX]), cY = keep_reg(lc[kLineY]), cZ = keep_reg(lc[kLineZ]);
   const int pZ = keep_reg(la[kLineZ] + Q * lb[kLineZ]);   // z-line's point offset in the cell box
-  const int mZ = keep_reg(la[kLineZ] + N * lb[kLineZ]);   // z-line's mode offset in the cell box
   const bool zmodes = keep_reg(int(la[kLineZ] < N && lb[kLineZ] < N)) != 0;  // z-line through modes
   const bool ymodes = keep_reg(int(la[kLineY] < N)) != 0;
   const T wX = keep_reg(tab.W[la[kLineX]] * tab.W[lb[kLineX]]);
@@ -249,21 +264,23 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB))
 #pragma unroll
     for (int k = 0; k < N; ++k) mv[k] = ok ? __ldg(b.map + cell * NB + ita + N * (itb + N * k)) : -1;
   };
+  // group g into stage s: modes (zeros for -1 entries and for cells past the end, whose map
+  // entries load_map set to -1), map entries and cell sizes
   auto issue = [&](int64_t g, int s) {
     const int64_t cell = g * CPB + ic;
-    if (g < n_groups && cell < b.n_cells) {
+    if (g < n_groups) {
       T* st = stage + (s * CPB + ic) * SP;
+      int* sm = smap + (s * CPB + ic) * SP;
       if (igather) {
 #pragma unroll
         for (int k = 0; k < N; ++k) {
           const int e = ita + N * (itb + N * k);
-          if (mv[k] >= 0 && b.coef == nullptr)
-            cp_async_elem<sizeof(T)>(st + e, x + mv[k]);
-          else
-            st[e] = gather_entry<T>(b, cell * NB + e, x);
+          cp_async_zfill<sizeof(T)>(st + e, x + (mv[k] >= 0 ? mv[k] : 0), mv[k] >= 0);
+          sm[e] = mv[k];
         }
       }
-      if (tid % Q2 < 3) cp_async_elem<8>(hst + (s * CPB + ic) * 4 + tid % Q2, b.h + cell * 3 + tid % Q2);
+      if (cell < b.n_cells && tid % Q2 < 3)
+        cp_async_elem<8>(hst + (s * CPB + ic) * 4 + tid % Q2, b.h + cell * 3 + tid % Q2);
     }
     cp_async_commit();  // every thread commits one group per issue, possibly empty
   };
@@ -274,10 +291,10 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB))
   load_map(g + G);
   T line[Q], out[Q];
   for (int s = 0; g < n_groups; g += G, s ^= 1) {
-    issue(g + G, s ^ 1);
-    load_map(g + 2 * G);
-    cp_async_wait<1>();
-    __syncthreads();  // staged modes and sizes of group g visible; previous group fully done
+    cp_async_wait<0>();
+    // Staged modes, map entries and sizes of group g visible; every thread is past the previous
+    // group, including its step 9, which read the staged map entries of stage s ^ 1.
+    __syncthreads();
     if (tid % Q2 == 0) {
       const double* hc = hst + (s * CPB + ic) * 4;
       const bool ok = g * CPB + ic < b.n_cells;
@@ -291,10 +308,9 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB))
     const T* st = stage + s * CPB * SP;
     // 1. z interpolation on z-lines through mode positions, from the staged modes
     if (zmodes) {
-      const bool act = g * CPB + cZ < b.n_cells;
       T in[N];
 #pragma unroll
-      for (int k = 0; k < N; ++k) in[k] = act ? st[stZ + N * N * k] : T(0);
+      for (int k = 0; k < N; ++k) in[k] = st[stZ + N * N * k];
 #pragma unroll
       for (int q = 0; q < Q; ++q) {
         T v = T(0);
@@ -303,6 +319,8 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB))
         work[baseZ + Q2 * q] = v;
       }
     }
+    // copies of the next group (stage s ^ 1 is free: every thread is past the previous group)
+    issue(g + G, s ^ 1);
     __syncthreads();
     // 2. y interpolation on y-lines with x < N
     if (ymodes) {
@@ -443,20 +461,24 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB))
       }
     }
     __syncthreads();
-    // 9. transposed z interpolation on z-lines through mode positions and scatter (the next
-    // group writes the work buffers only after the barrier at its start)
+    // map entries of the group after next, consumed by the next iteration's issue (loaded here
+    // to keep them out of the registers of steps 1-8)
+    load_map(g + 2 * G);
+    // 9. transposed z interpolation on z-lines through mode positions and scatter through the
+    // staged map entries (the next group writes the work buffers only after its first barrier)
     if (zmodes) {
-      const int64_t cell = g * CPB + cZ;
-      if (cell < b.n_cells) {
+      const int* sm = smap + s * CPB * SP + stZ;
 #pragma unroll
-        for (int q = 0; q < Q; ++q) line[q] = work[baseZ + Q2 * q];
+      for (int q = 0; q < Q; ++q) line[q] = work[baseZ + Q2 * q];
+      // kept rolled: unrolled, the compiler hoists every map load and output at once and spills
+      // (5^3 FP64: 0.37 ms rolled vs 0.50 ms unrolled)
+#pragma unroll 1
+      for (int k = 0; k < N; ++k) {
+        T v = T(0);
 #pragma unroll
-        for (int k = 0; k < N; ++k) {
-          T v = T(0);
-#pragma unroll
-          for (int q = 0; q < Q; ++q) v += tab.B[k * Q + q] * line[q];
-          scatter_entry<T>(b, cell * NB + mZ + N * N * k, v, y);
-        }
+        for (int q = 0; q < Q; ++q) v += tab.B[k * Q + q] * line[q];
+        const int dof = sm[N * N * k];
+        if (dof >= 0) atomicAdd(y + dof, v);
       }
     }
   }

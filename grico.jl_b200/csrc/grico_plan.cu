@@ -139,13 +139,14 @@ Tables1D<N, Q, T> make_tables(const DevBatch& b) {
 }
 
 // Default 3-D kernel variant by points per axis, from a sweep of all variants on uniform
-// 16-million-dof grids (B200, one apply, degrees 1..7 with q = p + 1): the pipelined kernel
-// with half-size cell groups wins in FP64 up to q = 5 (p = 2: 0.64 vs 0.98 ms, p = 3: 0.41
-// vs 0.71 ms), the default-size groups from q = 6; in FP32 the one-block-per-group kernel
-// with half-size groups is fastest for q <= 3.
+// 16-million-dof grids (B200, one apply, degrees 1..7 with q = p + 1, FP64 ms of the best
+// variant vs the one-block-per-group default): the pipelined kernel wins at every q — half-size
+// groups (3) for q = 2, 3, 5 (p = 4: 0.367 vs 0.495 ms), default-size groups (4) for q = 4 and
+// q >= 6 (p = 3: 0.374 vs 0.710 ms; p = 7: 0.500 vs 0.843 ms); in FP32 the one-block-per-group
+// kernel with half-size groups stays fastest for q = 2.
 int default_tile_3d(int q, bool fp32) {
-  if (fp32 && q <= 3) return 0;
-  return q <= 5 ? 3 : 4;
+  if (fp32 && q <= 2) return 0;
+  return (q == 4 || q >= 6) ? 4 : 3;
 }
 
 int sm_count() {
@@ -191,7 +192,7 @@ bool launch_fused(int dim, const DevBatch& bt, const BatchView& v, const T* x, T
     return true;                                                                                               \
   }
 #define GRICO_L3_PIPE(NN, QQ, CPB_)                                                                            \
-  if (mode == 0) {                                                                                             \
+  if (mode == 0 && v.coef == nullptr && v.tail_off == nullptr) {                                               \
     constexpr int CPB = CPB_;                                                                                  \
     constexpr int NT = QQ * QQ * CPB;                                                                          \
     static const LaneLines<NT> lanes = make_lane_lines<NT>(NN, QQ, CPB, int(sizeof(T)));                      \
