@@ -571,8 +571,26 @@ int run_apply(GricoPlan* P, bool reduced, const T* x, T* y, int nrhs, cudaStream
   const int64_t n = reduced ? P->n_red : P->n_full;
   if (nrhs < 1) return GRICO_ERR_INVALID;
   cudaMemsetAsync(y, 0, sizeof(T) * n * nrhs, st);
-  for (auto& b : P->batches) launch_batch<T>(*P, b, reduced, x, y, n, 0, nullptr, nrhs, st);
-  for (auto& pb : P->pbatches) launch_points<T>(*P, pb, reduced, x, y, n, 0, nullptr, nrhs, st);
+  for (size_t bi = 0; bi < P->batches.size(); ++bi) {
+    GricoPlan::BatchEvent ev{int(bi), nullptr, nullptr};
+    if (P->time_batches && cudaEventCreate(&ev.start) == cudaSuccess && cudaEventCreate(&ev.stop) == cudaSuccess)
+      cudaEventRecord(ev.start, st);
+    launch_batch<T>(*P, P->batches[bi], reduced, x, y, n, 0, nullptr, nrhs, st);
+    if (ev.stop) {
+      cudaEventRecord(ev.stop, st);
+      P->batch_events.push_back(ev);
+    }
+  }
+  for (size_t pi = 0; pi < P->pbatches.size(); ++pi) {
+    GricoPlan::BatchEvent ev{int(P->batches.size() + pi), nullptr, nullptr};
+    if (P->time_batches && cudaEventCreate(&ev.start) == cudaSuccess && cudaEventCreate(&ev.stop) == cudaSuccess)
+      cudaEventRecord(ev.start, st);
+    launch_points<T>(*P, P->pbatches[pi], reduced, x, y, n, 0, nullptr, nrhs, st);
+    if (ev.stop) {
+      cudaEventRecord(ev.stop, st);
+      P->batch_events.push_back(ev);
+    }
+  }
   if (!reduced && (P->n_fixed + P->n_rel) > 0) {
     dim3 grid(grid_for(P->n_fixed + P->n_rel), nrhs);
     constraint_action<T><<<grid, 256, 0, st>>>(P->fixed.get<int64_t>(), P->n_fixed, P->rel_piv.get<int64_t>(),
@@ -950,6 +968,10 @@ int grico_plan_create(const GricoPlanDesc* d, GricoPlan** out) {
 int grico_plan_destroy(GricoPlan* P) {
   if (!P) return GRICO_OK;
   cudaStreamSynchronize(P->stream);
+  for (auto& ev : P->batch_events) {
+    cudaEventDestroy(ev.start);
+    cudaEventDestroy(ev.stop);
+  }
   cudaStream_t st = P->stream;
   delete P;
   cudaStreamDestroy(st);
@@ -980,15 +1002,46 @@ static int apply_common(GricoPlan* P, bool reduced, const void* x, void* y, int 
     dx = P->host_x.ptr;
     dy = P->host_y.ptr;
   }
+  P->time_batches = (flags & GRICO_FLAG_TIME_BATCHES) != 0;
   int rc = precision == GRICO_PREC_FP64
                ? run_apply<double>(P, reduced, static_cast<const double*>(dx), static_cast<double*>(dy), nrhs, st)
                : run_apply<float>(P, reduced, static_cast<const float*>(dx), static_cast<float*>(dy), nrhs, st);
+  P->time_batches = false;
   if (rc != GRICO_OK) return rc;
   if (flags & GRICO_FLAG_HOST_POINTERS) {
     if (!cuda_ok(cudaMemcpyAsync(y, dy, bytes, cudaMemcpyDeviceToHost, st), "copy out")) return GRICO_ERR_CUDA;
     if (!cuda_ok(cudaStreamSynchronize(st), "apply")) return GRICO_ERR_CUDA;
   }
   return GRICO_OK;
+}
+
+int grico_plan_batch_times(GricoPlan* P, double* ms, int64_t* launches, int n_batches) {
+  const size_t nb = P ? P->batches.size() + P->pbatches.size() : 0;
+  if (!P || !ms || n_batches < 0 || size_t(n_batches) > nb) {
+    set_error("grico_plan_batch_times: invalid argument");
+    return GRICO_ERR_INVALID;
+  }
+  std::vector<double> total(nb, 0.0);
+  std::vector<int64_t> count(nb, 0);
+  int rc = GRICO_OK;
+  for (auto& ev : P->batch_events) {
+    float t = 0.0f;
+    if (rc == GRICO_OK && cuda_ok(cudaEventSynchronize(ev.stop), "batch timing") &&
+        cuda_ok(cudaEventElapsedTime(&t, ev.start, ev.stop), "batch timing")) {
+      total[size_t(ev.batch)] += t;
+      count[size_t(ev.batch)] += 1;
+    } else {
+      rc = GRICO_ERR_CUDA;
+    }
+    cudaEventDestroy(ev.start);
+    cudaEventDestroy(ev.stop);
+  }
+  P->batch_events.clear();
+  for (int i = 0; i < n_batches; ++i) {
+    ms[i] = count[size_t(i)] ? total[size_t(i)] / double(count[size_t(i)]) : 0.0;
+    if (launches) launches[i] = count[size_t(i)];
+  }
+  return rc;
 }
 
 int grico_apply(GricoPlan* P, const void* x, void* y, int nrhs, int precision, int flags, void* stream) {

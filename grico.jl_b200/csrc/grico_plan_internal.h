@@ -114,6 +114,12 @@ struct GricoPlan {
   int64_t n_hang = 0;
   grico::DevBuf partial, scalars;
   grico::DevBuf host_x, host_y;
+  // GRICO_FLAG_TIME_BATCHES: event pairs around cell-batch launches, (batch, start, stop)
+  struct BatchEvent { int batch; cudaEvent_t start, stop; };
+  bool time_batches = false;
+  std::vector<BatchEvent> batch_events;
+  std::vector<double> batch_ms;
+  std::vector<int64_t> batch_launches;
   // Krylov workspaces (allocated on first solve)
   grico::DevBuf w_r, w_z, w_p, w_q, w_x, w_b, w_dinv;
 };

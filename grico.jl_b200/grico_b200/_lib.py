@@ -37,6 +37,7 @@ GRICO_PREC_FP32 = 1
 GRICO_FLAG_HOST_POINTERS = 1
 GRICO_FLAG_NO_GRAPH = 2
 GRICO_FLAG_MIXED = 4
+GRICO_FLAG_TIME_BATCHES = 8
 GRICO_PRECOND_IDENTITY = 0
 GRICO_PRECOND_JACOBI = 1
 GRICO_PRECOND_MULTIGRID = 2
@@ -210,6 +211,7 @@ SIGNATURES = {
     "grico_mg_set_learned": (C.c_int, [P, C.POINTER(GricoLearnedDesc)]),
     "grico_plan_autotune": (C.c_int, [P, C.c_int, C.c_int, C.c_int, i32p]),
     "grico_plan_set_tiles": (C.c_int, [P, C.c_int, i32p, C.c_int]),
+    "grico_plan_batch_times": (C.c_int, [P, f64p, i64p, C.c_int]),
     "grico_cg_solve_multi": (C.c_int, [P, f64p, f64p, C.c_int, C.POINTER(GricoSolveOptions), C.POINTER(GricoSolveReport), C.c_int]),
     "grico_mg_learned_stats": (C.c_int, [P, i64p, i64p]),
     "grico_conv3d_forward": (C.c_int, [P, C.c_int, P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,

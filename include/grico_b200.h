@@ -55,6 +55,8 @@ extern "C" {
 #define GRICO_FLAG_HOST_POINTERS 1 /* vector arguments are host memory: copy in/out */
 #define GRICO_FLAG_NO_GRAPH 2      /* Krylov solves: launch each iteration op by op, no CUDA graph */
 #define GRICO_FLAG_MIXED 4         /* grico_cg_solve_multi: FP64 refinement around FP32 inner CG */
+#define GRICO_FLAG_TIME_BATCHES 8  /* grico_apply / grico_reduced_apply: record CUDA events around
+                                      every cell-batch kernel launch (grico_plan_batch_times)   */
 
 /* ================================================================================
  * Host space compile (native replacement of the Julia-side HpSpace construction)
@@ -207,6 +209,13 @@ int grico_plan_autotune(GricoPlan* plan, int nrhs, int precision, int reps, int*
  * reported by grico_plan_autotune), e.g. to replay a stored tuning without timing again.
  * No reference counterpart. */
 int grico_plan_set_tiles(GricoPlan* plan, int precision, const int* tiles, int n_batches);
+/* Average device time of each batch's kernel launch over the applies called with
+ * GRICO_FLAG_TIME_BATCHES since the last query (CUDA events recorded on the apply's stream
+ * around each launch).  Batches are numbered cell batches first, then point batches; the first
+ * n_batches are reported: ms[i] average milliseconds per launch, launches[i] (may be NULL)
+ * launches timed.  Synchronises with those events and resets the record.  No reference
+ * counterpart (measurement support). */
+int grico_plan_batch_times(GricoPlan* plan, double* ms, int64_t* launches, int n_batches);
 int grico_plan_destroy(GricoPlan* plan);
 /* n_full, n_reduced */
 int grico_plan_sizes(const GricoPlan* plan, int64_t* n_full, int64_t* n_reduced);

@@ -182,3 +182,28 @@ def test_every_kernel_variant_matches_oracle(cuda, name):
         for k in range(2):
             assert rel_err(yf[k], ref_full[k]) <= TOL, (var, k)
             assert rel_err(yr[k], ref_red[k]) <= TOL, (var, k)
+
+
+def test_batch_event_timing(cuda):
+    """GRICO_FLAG_TIME_BATCHES records one event pair per batch launch; the query averages them,
+    counts the launches, resets the record, and the flag leaves the result unchanged."""
+    import ctypes as C
+    from grico_b200 import _lib as L
+
+    oplan, prob = build("3d_p2_hanging", mu=0.7, kappa=1.3)
+    plan = gb.compile(prob)
+    x = sample_vector(plan.n_full, seed=4)
+    y0 = gb.apply(plan, x)
+    nb = len(plan.batches) + len(plan.point_batches)
+    y = np.zeros_like(x)
+    for _ in range(3):
+        assert L.lib().grico_apply(plan.handle, L.ptr(x, C.c_double), L.ptr(y, C.c_double), 1, L.GRICO_PREC_FP64,
+                                   L.GRICO_FLAG_HOST_POINTERS | L.GRICO_FLAG_TIME_BATCHES, None) == 0
+    assert rel_err(y, y0) <= TOL
+    ms = np.zeros(nb)
+    n = np.zeros(nb, dtype=np.int64)
+    assert L.lib().grico_plan_batch_times(plan.handle, L.ptr(ms, C.c_double), L.ptr(n, C.c_int64), nb) == 0
+    assert (n == 3).all() and (ms > 0).all()
+    assert L.lib().grico_plan_batch_times(plan.handle, L.ptr(ms, C.c_double), L.ptr(n, C.c_int64), nb) == 0
+    assert (n == 0).all() and (ms == 0).all()
+    assert L.lib().grico_plan_batch_times(plan.handle, L.ptr(ms, C.c_double), None, nb + 1) != 0
