@@ -544,6 +544,11 @@ struct PointView {
   const double* eta;       // [n_items] or null
   const double* kpts;      // [n_points] or null
   const uint8_t* skip;     // nullable: items excluded from the diagonal kernel (host computes them)
+  // GRICO_ITEM_INTERFACE: plus-side modes per axis, reference points, cell sizes, normal axis
+  int np[3];
+  const double* ref_p;     // [n_points*dim]
+  const double* h_p;       // [n_items*dim]
+  const int32_t* axis;     // [n_items]
 };
 
 constexpr int kPointChunk = 32;
@@ -737,6 +742,157 @@ __global__ void __launch_bounds__(kPointThreads) point_apply(PointView b, const 
   }
 #pragma unroll
   for (int k = 0; k < kMaxModes; ++k) {
+    const int i = threadIdx.x + k * blockDim.x;
+    if (i >= nb) break;
+    if (mode == 3) {
+      const int v = b.map[item * nb + i];
+      if (v >= 0) {
+        const T c = b.coef ? T(b.coef[item * nb + i]) : T(1);
+        atomicAdd(y + v, c * c * acc[k]);
+      }
+    } else {
+      scatter_entry<T>(bv, item * nb + i, acc[k], y);
+    }
+  }
+}
+
+constexpr int kIfaceModes = 8;  // modes per thread: minus + plus boxes <= 1024
+
+// value and normal derivative (along axis ax) of box mode mi at chunk point pp
+template <typename T, int D>
+__device__ __forceinline__ void mode_value_dn(const T* tv, const T* td, int nmax, int pp, const int* mi, int ax,
+                                              T& phi, T& dn) {
+  phi = T(1);
+  dn = T(1);
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    const T v = tv[(pp * D + a) * nmax + mi[a]];
+    phi *= v;
+    dn *= a == ax ? td[(pp * D + a) * nmax + mi[a]] : v;
+  }
+}
+
+// Symmetric interior-penalty interface items (GRICO_ITEM_INTERFACE; interface_apply!,
+// accumulators.jl:1576-1616, with the SIPG form of benchmark/sine_poisson_sipg.jl:54-95).
+// mode 0 apply, 3 local diagonal (interface_diagonal!, sine_poisson_sipg.jl:97-123); there is
+// no load term.  One block per interface: both cells' local coefficients are gathered into
+// shared memory, points are staged in chunks with 1-D tables of both sides, one warp per point
+// forms the two traces u-, u+, du-/dn, du+/dn, and one thread per mode projects
+//   minus test mode: w (sigma J - {du/dn}) phi + w (-J/2) dphi/dn,
+//   plus test mode: -w (sigma J - {du/dn}) phi + w (-J/2) dphi/dn,   J = u- - u+.
+template <typename T, int D>
+__global__ void __launch_bounds__(kPointThreads) interface_apply(PointView b, const T* __restrict__ x,
+                                                                 T* __restrict__ y, int64_t n_vec, int mode) {
+  extern __shared__ unsigned char smem_raw[];
+  const int nm[3] = {b.n[0], D > 1 ? b.n[1] : 1, D > 2 ? b.n[2] : 1};
+  const int npl[3] = {b.np[0], D > 1 ? b.np[1] : 1, D > 2 ? b.np[2] : 1};
+  const int nbm = nm[0] * nm[1] * nm[2], nbp = npl[0] * npl[1] * npl[2], nb = nbm + nbp;
+  const int nmax = max(max(nm[0], max(nm[1], nm[2])), max(npl[0], max(npl[1], npl[2])));
+  T* xl = reinterpret_cast<T*>(smem_raw);       // nb
+  T* tvm = xl + nb;                              // [chunk][D][nmax] minus values
+  T* tdm = tvm + kPointChunk * D * nmax;         // minus derivatives (physical)
+  T* tvp = tdm + kPointChunk * D * nmax;         // plus values
+  T* tdp = tvp + kPointChunk * D * nmax;         // plus derivatives (physical)
+  T* fl = tdp + kPointChunk * D * nmax;          // [chunk][2] value and normal-derivative coefficients
+  const int64_t item = blockIdx.x;
+  if (mode == 1 || (mode == 3 && b.skip && b.skip[item])) return;
+  x += blockIdx.y * n_vec;
+  y += blockIdx.y * n_vec;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int ax = b.axis[item];
+  T sm[D], sp[D];
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    sm[a] = T(2) / T(b.h[item * D + a]);
+    sp[a] = T(2) / T(b.h_p[item * D + a]);
+  }
+  const T sigma = T(b.eta[item]);
+  BatchView bv;
+  bv.n_cells = b.n_items;
+  bv.map = b.map;
+  bv.coef = b.coef;
+  bv.tail_off = b.tail_off;
+  bv.tail_idx = b.tail_idx;
+  bv.tail_coef = b.tail_coef;
+  if (mode == 0)
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) xl[i] = gather_entry<T>(bv, item * nb + i, x);
+  T acc[kIfaceModes];
+#pragma unroll
+  for (int k = 0; k < kIfaceModes; ++k) acc[k] = T(0);
+  const int64_t p_begin = b.pt_off[item], p_end = b.pt_off[item + 1];
+  for (int64_t p0 = p_begin; p0 < p_end; p0 += kPointChunk) {
+    const int cnt = int(p_end - p0 < int64_t(kPointChunk) ? p_end - p0 : int64_t(kPointChunk));
+    __syncthreads();
+    for (int t = threadIdx.x; t < 2 * cnt * D; t += blockDim.x) {
+      const int side = t / (cnt * D), r = t - side * cnt * D, pp = r / D, a = r - pp * D;
+      const int deg = (side ? npl[a] : nm[a]) - 1;
+      T* v = (side ? tvp : tvm) + (pp * D + a) * nmax;
+      T* d = (side ? tdp : tdm) + (pp * D + a) * nmax;
+      fe_basis_dev<T>(T((side ? b.ref_p : b.ref)[(p0 + pp) * D + a]), deg, v, d);
+      const T sc = side ? sp[a] : sm[a];
+      for (int i = 0; i <= deg; ++i) d[i] *= sc;
+    }
+    __syncthreads();
+    if (mode == 0) {
+      for (int pp = warp; pp < cnt; pp += kPointWarps) {
+        T um = T(0), dm = T(0), up = T(0), dp = T(0);
+        for (int i = lane; i < nb; i += 32) {
+          const bool plus = i >= nbm;
+          const int li = plus ? i - nbm : i;
+          const int* nn = plus ? npl : nm;
+          const int mi[3] = {li % nn[0], (li / nn[0]) % nn[1], li / (nn[0] * nn[1])};
+          T phi, dn;
+          mode_value_dn<T, D>(plus ? tvp : tvm, plus ? tdp : tdm, nmax, pp, mi, ax, phi, dn);
+          const T xi = xl[i];
+          if (plus) {
+            up += xi * phi;
+            dp += xi * dn;
+          } else {
+            um += xi * phi;
+            dm += xi * dn;
+          }
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+          um += __shfl_xor_sync(0xffffffffu, um, off);
+          dm += __shfl_xor_sync(0xffffffffu, dm, off);
+          up += __shfl_xor_sync(0xffffffffu, up, off);
+          dp += __shfl_xor_sync(0xffffffffu, dp, off);
+        }
+        if (lane == 0) {
+          const T w = T(b.w[p0 + pp]);
+          const T jump = um - up;
+          const T avg = T(0.5) * (dm + dp);
+          fl[pp * 2] = w * (sigma * jump - avg);
+          fl[pp * 2 + 1] = -T(0.5) * w * jump;
+        }
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int k = 0; k < kIfaceModes; ++k) {
+      const int i = threadIdx.x + k * blockDim.x;
+      if (i >= nb) break;
+      const bool plus = i >= nbm;
+      const int li = plus ? i - nbm : i;
+      const int* nn = plus ? npl : nm;
+      const int mi[3] = {li % nn[0], (li / nn[0]) % nn[1], li / (nn[0] * nn[1])};
+      T s = T(0);
+      for (int pp = 0; pp < cnt; ++pp) {
+        T phi, dn;
+        mode_value_dn<T, D>(plus ? tvp : tvm, plus ? tdp : tdm, nmax, pp, mi, ax, phi, dn);
+        if (mode == 3) {
+          const T w = T(b.w[p0 + pp]);
+          s += w * (sigma * phi * phi + (plus ? phi * dn : -phi * dn));
+        } else {
+          s += (plus ? -fl[pp * 2] : fl[pp * 2]) * phi + fl[pp * 2 + 1] * dn;
+        }
+      }
+      acc[k] += s;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kIfaceModes; ++k) {
     const int i = threadIdx.x + k * blockDim.x;
     if (i >= nb) break;
     if (mode == 3) {

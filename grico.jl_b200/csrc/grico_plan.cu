@@ -344,6 +344,27 @@ void launch_points(const GricoPlan& P, const DevPointBatch& pb, bool reduced, co
   v.kpts = pb.kpts.get<double>();
   v.skip = reduced ? pb.skip.get<uint8_t>() : nullptr;
   const int D = P.dim;
+  if (pb.kind == GRICO_ITEM_INTERFACE) {
+    if (mode == 1) return;  // no load term on interior interfaces
+    for (int a = 0; a < 3; ++a) v.np[a] = pb.np[a];
+    v.ref_p = pb.ref_p.get<double>();
+    v.h_p = pb.h_p.get<double>();
+    v.axis = pb.axis.get<int32_t>();
+    const int nbi = pb.n[0] * (D > 1 ? pb.n[1] : 1) * (D > 2 ? pb.n[2] : 1) +
+                    pb.np[0] * (D > 1 ? pb.np[1] : 1) * (D > 2 ? pb.np[2] : 1);
+    const int nmax = std::max(std::max(pb.n[0], std::max(D > 1 ? pb.n[1] : 1, D > 2 ? pb.n[2] : 1)),
+                              std::max(pb.np[0], std::max(D > 1 ? pb.np[1] : 1, D > 2 ? pb.np[2] : 1)));
+    const size_t smem = sizeof(T) * (size_t(nbi) + 4 * size_t(kPointChunk) * D * nmax + 2 * size_t(kPointChunk));
+    dim3 grid(pb.n_items, nrhs);
+    auto go = [&](auto kernel) {
+      if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+      kernel<<<grid, kPointThreads, smem, st>>>(v, x, y, nvec, mode);
+    };
+    if (D == 1) go(interface_apply<T, 1>);
+    else if (D == 2) go(interface_apply<T, 2>);
+    else go(interface_apply<T, 3>);
+    return;
+  }
   const int nb = pb.n[0] * (D > 1 ? pb.n[1] : 1) * (D > 2 ? pb.n[2] : 1);
   const int nmax = std::max(pb.n[0], std::max(D > 1 ? pb.n[1] : 1, D > 2 ? pb.n[2] : 1));
   const size_t smem = sizeof(T) * (size_t(nb) + 2 * size_t(kPointChunk) * D * nmax + size_t(kPointChunk) * (D + 1));
@@ -406,6 +427,61 @@ void accumulate_point_item_diagonal(const GricoPlanDesc& d, const GricoPointBatc
         }
         A[i * nb + j] += w * aij;
       }
+  }
+  std::map<int64_t, std::vector<std::pair<int64_t, double>>> by_dof;
+  for (int64_t i = 0; i < nb; ++i) {
+    const int32_t e = rmap[it * nb + i];
+    if (e >= 0) by_dof[e].emplace_back(i, rcoef[it * nb + i]);
+    else if (e <= -2) {
+      const int64_t k = -(int64_t(e) + 2);
+      for (int64_t t = toff[k]; t < toff[k + 1]; ++t) by_dof[tidx[t]].emplace_back(i, tcoef[t]);
+    }
+  }
+  for (auto& kv : by_dof) {
+    double s = 0.0;
+    for (auto& a : kv.second)
+      for (auto& b : kv.second) s += a.second * A[a.first * nb + b.first] * b.second;
+    out[kv.first] += s;
+  }
+}
+
+// The same for a two-sided interface item (local matrix of the SIPG form over the minus and plus
+// modes, test i trial j: -[phi_i]{dphi_j/dn} - {dphi_i/dn}[phi_j] + sigma [phi_i][phi_j]).
+void accumulate_interface_item_diagonal(const GricoPlanDesc& d, const GricoPointBatchDesc& pb, const int* nm,
+                                        const int* npl, int64_t it, int64_t nb, const std::vector<int32_t>& rmap,
+                                        const std::vector<double>& rcoef, const std::vector<int64_t>& toff,
+                                        const std::vector<int32_t>& tidx, const std::vector<double>& tcoef,
+                                        std::map<int64_t, double>& out) {
+  const int D = d.dim;
+  const int ax = pb.face_axis[it];
+  const int64_t nbm = box_count(D, nm);
+  std::vector<double> A(nb * nb, 0.0), jump(nb), avg(nb);
+  double v[3][17], dv[3][17];
+  for (int64_t p = pb.point_offsets[it]; p < pb.point_offsets[it + 1]; ++p) {
+    for (int side = 0; side < 2; ++side) {
+      const int* n = side ? npl : nm;
+      const double* ref = side ? pb.ref_points_plus : pb.ref_points;
+      const double* h = side ? pb.cell_size_plus : pb.cell_size;
+      for (int a = 0; a < D; ++a) {
+        fe_basis(ref[p * D + a], n[a] - 1, v[a], dv[a]);
+        for (int i = 0; i < n[a]; ++i) dv[a][i] *= 2.0 / h[it * D + a];
+      }
+      const int64_t cnt = box_count(D, n), off = side ? nbm : 0;
+      for (int64_t i = 0; i < cnt; ++i) {
+        const int mi[3] = {int(i % n[0]), int((i / n[0]) % n[1]), int(i / (n[0] * n[1]))};
+        double val = 1.0, dn = 1.0;
+        for (int a = 0; a < D; ++a) {
+          val *= v[a][mi[a]];
+          dn *= a == ax ? dv[a][mi[a]] : v[a][mi[a]];
+        }
+        jump[off + i] = side ? -val : val;
+        avg[off + i] = 0.5 * dn;
+      }
+    }
+    const double w = pb.weights[p], sigma = pb.eta[it];
+    for (int64_t i = 0; i < nb; ++i)
+      for (int64_t j = 0; j < nb; ++j)
+        A[i * nb + j] += w * (-jump[i] * avg[j] - avg[i] * jump[j] + sigma * jump[i] * jump[j]);
   }
   std::map<int64_t, std::vector<std::pair<int64_t, double>>> by_dof;
   for (int64_t i = 0; i < nb; ++i) {
@@ -670,7 +746,8 @@ static int validate_plan_desc(const GricoPlanDesc* d) {
   for (int bi = 0; bi < d->n_point_batches; ++bi) {
     const GricoPointBatchDesc& pb = d->point_batches[bi];
     const std::string tag = "point batch " + std::to_string(bi);
-    if (pb.kind != GRICO_ITEM_CELL && pb.kind != GRICO_ITEM_NITSCHE && pb.kind != GRICO_ITEM_SUBCELLS) {
+    if (pb.kind != GRICO_ITEM_CELL && pb.kind != GRICO_ITEM_NITSCHE && pb.kind != GRICO_ITEM_SUBCELLS &&
+        pb.kind != GRICO_ITEM_INTERFACE) {
       set_error(tag + ": unknown item kind");
       return GRICO_ERR_UNSUPPORTED_FORM;
     }
@@ -704,13 +781,24 @@ static int validate_plan_desc(const GricoPlanDesc* d) {
       }
     }
     if (pb.kind == GRICO_ITEM_NITSCHE && pb.n_items > 0 && (!pb.normals || !pb.eta)) { set_error(tag + ": Nitsche items need normals and eta"); return GRICO_ERR_INVALID; }
-    int n[3] = {1, 1, 1};
+    const bool iface = pb.kind == GRICO_ITEM_INTERFACE;
+    if (iface && pb.n_items > 0 && (!pb.eta || !pb.ref_points_plus || !pb.cell_size_plus || !pb.face_axis)) {
+      set_error(tag + ": interface items need eta, plus-side points and sizes, and face axes");
+      return GRICO_ERR_INVALID;
+    }
+    int n[3] = {1, 1, 1}, np_[3] = {1, 1, 1};
     for (int a = 0; a < d->dim; ++a) {
       n[a] = pb.degree[a] + 1;
       if (n[a] < 1 || n[a] > 16) { set_error(tag + ": degree out of range"); return GRICO_ERR_INVALID; }
+      if (iface) {
+        np_[a] = pb.degree_plus[a] + 1;
+        if (np_[a] < 1 || np_[a] > 16) { set_error(tag + ": plus-side degree out of range"); return GRICO_ERR_INVALID; }
+      }
     }
-    const int64_t nb = box_count(d->dim, n);
-    if (nb > int64_t(kMaxModes) * kPointThreads) { set_error(tag + ": too many local modes for point items"); return GRICO_ERR_INVALID; }
+    const int64_t nb = box_count(d->dim, n) + (iface ? box_count(d->dim, np_) : 0);
+    if (nb > int64_t(iface ? kIfaceModes : kMaxModes) * kPointThreads) { set_error(tag + ": too many local modes for point items"); return GRICO_ERR_INVALID; }
+    for (int64_t it = 0; iface && it < pb.n_items; ++it)
+      if (pb.face_axis[it] < 0 || pb.face_axis[it] >= d->dim) { set_error(tag + ": face axis out of range"); return GRICO_ERR_INVALID; }
     if (!sub && pb.point_offsets && pb.n_items > 0 && pb.point_offsets[0] != 0) { set_error(tag + ": point offsets must start at 0"); return GRICO_ERR_INVALID; }
     for (int64_t it = 0; !sub && it < pb.n_items; ++it)
       if (pb.point_offsets[it + 1] < pb.point_offsets[it]) { set_error(tag + ": point offsets must not decrease"); return GRICO_ERR_INVALID; }
@@ -867,7 +955,10 @@ int grico_plan_create(const GricoPlanDesc* d, GricoPlan** out) {
     pb.n_items = pd.n_items;
     pb.kind = pd.kind;
     for (int a = 0; a < d->dim; ++a) pb.n[a] = pd.degree[a] + 1;
-    const int64_t nb = box_count(d->dim, pb.n);
+    const bool iface = pd.kind == GRICO_ITEM_INTERFACE;
+    if (iface)
+      for (int a = 0; a < d->dim; ++a) pb.np[a] = pd.degree_plus[a] + 1;
+    const int64_t nb = box_count(d->dim, pb.n) + (iface ? box_count(d->dim, pb.np) : 0);
     const int64_t ne = int64_t(pd.n_items) * nb;
     bool ok = pb.full.map.upload(pd.map_index, size_t(ne)) && pb.h.upload(pd.cell_size, size_t(pd.n_items) * d->dim);
     if (pd.kind == GRICO_ITEM_SUBCELLS) {
@@ -898,6 +989,10 @@ int grico_plan_create(const GricoPlanDesc* d, GricoPlan** out) {
            pb.full.tcoef.upload(pd.tail_coef, size_t(pd.tail_offsets[pd.n_tail]));
     if (pd.kind == GRICO_ITEM_NITSCHE)
       ok = ok && pb.nrm.upload(pd.normals, size_t(pb.n_points) * d->dim) && pb.eta.upload(pd.eta, size_t(pd.n_items));
+    if (iface)
+      ok = ok && pb.eta.upload(pd.eta, size_t(pd.n_items)) &&
+           pb.ref_p.upload(pd.ref_points_plus, size_t(pb.n_points) * d->dim) &&
+           pb.h_p.upload(pd.cell_size_plus, size_t(pd.n_items) * d->dim) && pb.axis.upload(pd.face_axis, size_t(pd.n_items));
     if (pd.kappa_points) ok = ok && pb.kpts.upload(pd.kappa_points, size_t(pb.n_points));
     std::vector<int32_t> rmap, tidx;
     std::vector<double> rcoef, tcoef;
@@ -925,6 +1020,8 @@ int grico_plan_create(const GricoPlanDesc* d, GricoPlan** out) {
       ++hanging;
       if (pd.kind == GRICO_ITEM_SUBCELLS)
         accumulate_subcell_item_diagonal(*d, pd, pb.n, it, nb, rmap, rcoef, toff, tidx, tcoef, P->hang_diag);
+      else if (iface)
+        accumulate_interface_item_diagonal(*d, pd, pb.n, pb.np, it, nb, rmap, rcoef, toff, tidx, tcoef, P->hang_diag);
       else
         accumulate_point_item_diagonal(*d, pd, pb.n, it, it, nb, rmap, rcoef, toff, tidx, tcoef, P->hang_diag);
     }

@@ -94,6 +94,9 @@ struct DevPointBatch {
   int64_t n_sub = 0;
   DevBuf sub_off, sub_level, sub_pos, sub_mask, sub_w;
   std::vector<double> hEta, hW, hDm;  // Gauss points, weights, collocation derivative (q[0])
+  // GRICO_ITEM_INTERFACE: plus-side modes per axis, reference points, cell sizes, normal axis
+  int np[3] = {1, 1, 1};
+  DevBuf ref_p, h_p, axis;
 };
 
 }  // namespace grico

@@ -10,7 +10,8 @@ from .space import (AxisDegrees, ByLeafDegrees, DegreePlusQuadrature, FullTensor
                     StoredDegrees, TrunkBasis, UniformDegree, active_leaf_count, scalar_dof_count)
 from .problem import (SPD, AffineProblem, AssemblyPlan, BoundaryFace, CGSolver, Diffusion, Dirichlet, FGMRESSolver,
                       IdentityPreconditioner, JacobiPreconditioner, Load, Mass, MassDiffusion, Nitsche,
-                      NonsymmetricOperator, ScalarField, State, VariableDiffusion, add_boundary_accumulator,
+                      NonsymmetricOperator, SIPG, ScalarField, State, VariableDiffusion, add_boundary,
+                      add_boundary_accumulator, add_interface,
                       add_cell_accumulator, add_cell_quadrature, add_constraint, add_surface_accumulator,
                       add_surface_quadrature, apply, apply_, compile, expand_reduced, l2_error, reduced_apply,
                       reduced_diagonal, reduced_rhs, relative_l2_error, solve)

@@ -29,6 +29,7 @@ GRICO_FORM_MASS_DIFFUSION = 1
 GRICO_ITEM_CELL = 1
 GRICO_ITEM_NITSCHE = 2
 GRICO_ITEM_SUBCELLS = 3
+GRICO_ITEM_INTERFACE = 4
 # (modes per axis, points per axis) pairs the subcell kernel is compiled for, per dimension
 SUBCELL_SHAPES = {3: {(2, 2), (2, 3), (3, 3), (2, 4), (3, 4), (4, 4)},
                   2: {(n, q) for n in range(2, 9) for q in (n, n + 1) if q <= 8}}
@@ -91,6 +92,10 @@ class GricoPointBatchDesc(C.Structure):
         ("subcell_pos", i32p),
         ("subcell_mask", C.POINTER(C.c_uint64)),
         ("subcell_weight", f64p),
+        ("degree_plus", C.c_int32 * 3),
+        ("ref_points_plus", f64p),
+        ("cell_size_plus", f64p),
+        ("face_axis", i32p),
     ]
 
 

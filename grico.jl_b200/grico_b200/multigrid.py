@@ -157,6 +157,11 @@ def _level_problem(problem, space):
     p.cell_operators = list(problem.cell_operators)
     p.rhs_operators = list(problem.rhs_operators)
     p.dirichlet = [Dirichlet(u, c.boundary, c.value) for c in problem.dirichlet]
+    # face forms carry no field reference, so every level reuses them (multigrid.jl:309-345
+    # rediscretises every operator of the problem on each level)
+    p.boundary_operators = list(problem.boundary_operators)
+    p.boundary_rhs_operators = list(problem.boundary_rhs_operators)
+    p.interface_operators = list(getattr(problem, "interface_operators", []))
     return p
 
 

@@ -58,6 +58,21 @@ class Load:
         self.source = source
 
 
+class SIPG:
+    """Symmetric interior-penalty DG Poisson terms (benchmark/sine_poisson_sipg.jl:24-157), as an
+    interface operator (`add_interface`) and as a boundary operator (`add_boundary`):
+    interior  -{du/dn}[v] - {dv/dn}[u] + sigma [u][v],  [w] = w- - w+, n from minus to plus,
+              sigma = penalty (max(p-, p+) + 1)^2 / (2 h- h+ / (h- + h+)) along the face axis;
+    boundary  -v du/dn - u dv/dn + sigma u v,  sigma = penalty (p + 1)^2 / h, with the load
+              TestChannels(sigma g, -g n) when `data` is given (g = 0 otherwise)."""
+
+    def __init__(self, penalty, data=None):
+        self.penalty = float(penalty)
+        if not self.penalty >= 0.0:
+            raise ValueError("penalty must be non-negative")
+        self.data = data
+
+
 class Nitsche:
     """Symmetric Nitsche Dirichlet data u = g on boundary faces or embedded surfaces
     (examples/annular_nitsche_fcm/driver.jl:45-76): bilinear TestChannels(-du/dn + eta*u, -u*n),
@@ -115,7 +130,8 @@ class AffineProblem:
         self.dirichlet = []
         self.surface_operators = []        # bilinear Nitsche forms on embedded surfaces
         self.surface_rhs_operators = []
-        self.boundary_operators = []       # (BoundaryFace, Nitsche)
+        self.boundary_operators = []       # (BoundaryFace, Nitsche or SIPG)
+        self.interface_operators = []      # SIPG on every interior interface
         self.boundary_rhs_operators = []
         self.surfaces = []                 # SurfaceQuadrature attachments
         self.cell_quadratures = {}         # leaf -> (reference points, reference weights)
@@ -183,6 +199,30 @@ def add_boundary_accumulator(problem, boundary, test_field, *args):
         problem.boundary_rhs_operators.append((boundary, op))
     else:
         raise TypeError("add_boundary_accumulator(problem, boundary, test, trial, op) or (problem, boundary, test, op)")
+    return problem
+
+
+def add_interface(problem, op):
+    """add_interface!(problem, operator) (problem.jl): an operator on every interior interface of
+    the space (matching and hanging); the B200 plan supports the SIPG form."""
+    if not isinstance(op, SIPG):
+        raise L.GricoError(L.GRICO_ERR_UNSUPPORTED_FORM, f"interface form {type(op).__name__} is not supported by the GPU plan")
+    if problem.interface_operators:
+        raise L.GricoError(L.GRICO_ERR_UNSUPPORTED_FORM, "one interface form on the GPU plan")
+    problem.interface_operators.append(op)
+    return problem
+
+
+def add_boundary(problem, boundary, op):
+    """add_boundary!(problem, boundary, operator): the SIPG boundary operator (with its load when
+    op.data is given) or the symmetric Nitsche form on the boundary faces of `boundary`."""
+    if not isinstance(boundary, BoundaryFace):
+        raise TypeError("boundary must be a BoundaryFace")
+    if not isinstance(op, (SIPG, Nitsche)):
+        raise L.GricoError(L.GRICO_ERR_UNSUPPORTED_FORM, f"boundary form {type(op).__name__} is not supported by the GPU plan")
+    problem.boundary_operators.append((boundary, op))
+    if op.data is not None:
+        problem.boundary_rhs_operators.append((boundary, op))
     return problem
 
 
@@ -280,6 +320,31 @@ def _item_maps(space, cells, b):
         b.tail_offsets = b.tail_index = b.tail_coef = None
     b.map_index = np.ascontiguousarray(mp)
     b.map_coef = None if np.all(coef == 1.0) else np.ascontiguousarray(coef)
+
+
+def _concat_item_maps(a, b):
+    """a's item maps become [a's box modes, b's box modes] per item (interface items), with b's
+    tail expansions appended to a's tail table."""
+    n = len(a.map_index) // max(a.nbox, 1) if a.nbox else 0
+    ma = a.map_index.reshape(n, a.nbox)
+    mb = b.map_index.reshape(n, b.nbox).copy()
+    na_tail = 0 if a.tail_offsets is None else len(a.tail_offsets) - 1
+    tails = mb <= -2
+    mb[tails] -= na_tail  # tail k of b becomes tail na_tail + k: code -(k + 2) - na_tail
+    a.map_index = np.ascontiguousarray(np.concatenate([ma, mb], axis=1).reshape(-1).astype(np.int32))
+    ca = np.ones(ma.shape) if a.map_coef is None else a.map_coef.reshape(n, a.nbox)
+    cb = np.ones(mb.shape) if b.map_coef is None else b.map_coef.reshape(n, b.nbox)
+    coef = np.concatenate([ca, cb], axis=1).reshape(-1)
+    a.map_coef = None if np.all(coef == 1.0) else np.ascontiguousarray(coef)
+    if b.tail_offsets is not None:
+        if a.tail_offsets is None:
+            a.tail_offsets, a.tail_index, a.tail_coef = b.tail_offsets, b.tail_index, b.tail_coef
+        else:
+            base = a.tail_offsets[-1]
+            a.tail_offsets = np.concatenate([a.tail_offsets, base + b.tail_offsets[1:]]).astype(np.int64)
+            a.tail_index = np.concatenate([a.tail_index, b.tail_index]).astype(np.int32)
+            a.tail_coef = np.concatenate([a.tail_coef, b.tail_coef])
+    a.nbox_minus, a.nbox = a.nbox, a.nbox + b.nbox
 
 
 def fe_basis_table(x, p):
@@ -427,6 +492,7 @@ class AssemblyPlan:
         extra = self._build_subcell_items(sub_groups)
         self._build_cell_items(point_rule, extra)
         self._build_nitsche_items(problem)
+        self._build_interface_items(problem)
         # --- Dirichlet: fixed dofs are the dofs with a trace on a selected boundary face ---
         self._compile_dirichlet(problem)
         # --- reduced map ---
@@ -574,7 +640,8 @@ class AssemblyPlan:
             bops[key] = [op, None]
         for bf, op in problem.boundary_rhs_operators:
             key = (bf.axis - 1, bf.side - 1)
-            if key not in bops or bops[key][1] is not None or bops[key][0].penalty != op.penalty:
+            if key not in bops or bops[key][1] is not None or bops[key][0].penalty != op.penalty or \
+                    type(bops[key][0]) is not type(op):
                 raise L.GricoError(L.GRICO_ERR_UNSUPPORTED_FORM,
                                    "a Nitsche boundary load needs the matching Nitsche boundary form")
             bops[key][1] = op.data
@@ -598,17 +665,77 @@ class AssemblyPlan:
                 scale = 1.0 if D == 1 else math.ldexp(float(np.prod([h[a] for a in range(D) if a != ax])), -(D - 1))
                 nrm = np.zeros((ref.shape[0], D))
                 nrm[:, ax] = -1.0 if sd == 0 else 1.0
-                items.append((int(pos), ref, wref * scale, nrm, op.penalty, g))
+                # SIPG boundary penalty (sine_poisson_sipg.jl:42-46); Nitsche: penalty / min(h)
+                eta = (op.penalty * (int(space.degrees[pos][ax]) + 1) ** 2 / float(h[ax])
+                       if isinstance(op, SIPG) else None)
+                items.append((int(pos), ref, wref * scale, nrm, op.penalty, g, eta))
         if not items:
             return
         degs = np.array([space.degrees[it[0]] for it in items]).reshape(len(items), D)
         for dsig in np.unique(degs, axis=0):
             sel = [i for i in range(len(items)) if np.all(degs[i] == dsig)]
             pb = self._new_point_batch(L.GRICO_ITEM_NITSCHE, [items[i][0] for i in sel], tuple(int(v) for v in dsig))
-            eta = np.array([items[i][4] / float(np.min(pb.h[k])) for k, i in enumerate(sel)])
+            eta = np.array([items[i][6] if len(items[i]) > 6 and items[i][6] is not None
+                            else items[i][4] / float(np.min(pb.h[k])) for k, i in enumerate(sel)])
             pb.data = [items[i][5] for i in sel]
             self._finish_point_batch(pb, [items[i][1] for i in sel], [items[i][2] for i in sel],
                                      [items[i][3] for i in sel], eta)
+
+    def _build_interface_items(self, problem):
+        """Two-sided SIPG items on every interior interface (integration.jl:2262-2307): the shared
+        tangential patch is the intersection of the two faces with max(q-, q+) Gauss points per
+        tangential axis (integration.jl:2800-2841); one batch per (minus degree, plus degree,
+        point count) in enumeration order."""
+        if not problem.interface_operators:
+            return
+        op = problem.interface_operators[0]
+        space, domain, D = self.space, self.space.domain, self.D
+        i_m, i_p, i_a = space.interfaces
+        if len(i_m) == 0:
+            return
+        lower = domain.cell_lower(space.leaves)
+        size = domain.cell_size(space.leaves)
+        items = []
+        for m, pl, ax in zip(i_m.tolist(), i_p.tolist(), i_a.tolist()):
+            tang = [a for a in range(D) if a != ax]
+            lo = np.maximum(lower[m], lower[pl])
+            hi = np.minimum(lower[m] + size[m], lower[pl] + size[pl])
+            rules = [_gauss(int(max(space.qshape[m][a], space.qshape[pl][a]))) for a in tang]
+            npts = int(np.prod([len(r[0]) for r in rules])) if tang else 1
+            phys = np.zeros((npts, D))
+            w = np.ones(npts)
+            if tang:
+                grids = np.meshgrid(*[r[0] for r in rules], indexing="ij")
+                wg = np.meshgrid(*[r[1] for r in rules], indexing="ij")
+                for k, a in enumerate(tang):
+                    half = 0.5 * (hi[a] - lo[a])
+                    phys[:, a] = lo[a] + half * (1.0 + grids[k].reshape(-1, order="F"))
+                    w = w * wg[k].reshape(-1, order="F") * half
+            phys[:, ax] = lower[m][ax] + size[m][ax]
+            ref_m = (phys - (lower[m] + 0.5 * size[m])) / (0.5 * size[m])
+            ref_p = (phys - (lower[pl] + 0.5 * size[pl])) / (0.5 * size[pl])
+            ref_m[:, ax] = 1.0
+            ref_p[:, ax] = -1.0
+            hm, hp = float(size[m][ax]), float(size[pl][ax])
+            pmax = max(int(space.degrees[m][ax]), int(space.degrees[pl][ax]))
+            sigma = op.penalty * (pmax + 1) ** 2 / (2.0 * hm * hp / (hm + hp))
+            items.append((m, pl, ax, ref_m, ref_p, w, sigma))
+        sig = {}
+        for it in items:
+            key = (tuple(int(v) for v in space.degrees[it[0]]), tuple(int(v) for v in space.degrees[it[1]]), len(it[5]))
+            sig.setdefault(key, []).append(it)
+        for (dm, dp, _), its in sig.items():
+            pb = self._new_point_batch(L.GRICO_ITEM_INTERFACE, [it[0] for it in its], dm)
+            plus = _PointBatch()
+            _item_maps(space, np.array([it[1] for it in its], dtype=np.int64), plus)
+            _concat_item_maps(pb, plus)
+            pb.degree_plus = dp
+            pb.plus_cells = np.array([it[1] for it in its], dtype=np.int64)
+            pb.h_plus = np.ascontiguousarray(domain.cell_size(space.leaves[pb.plus_cells]))
+            pb.face_axis = np.array([it[2] for it in its], dtype=np.int32)
+            pb.ref_points_plus = np.ascontiguousarray(np.concatenate([it[4] for it in its]).reshape(-1, D))
+            self._finish_point_batch(pb, [it[3] for it in its], [it[5] for it in its],
+                                     eta=np.array([it[6] for it in its]))
 
     def _points(self, b):
         D = self.D
@@ -703,6 +830,12 @@ class AssemblyPlan:
                 d.subcell_pos = L.ptr(b.subcell_pos, C.c_int32)
                 d.subcell_mask = L.ptr(b.subcell_mask, C.c_uint64)
                 d.subcell_weight = L.ptr(b.subcell_weight, C.c_double)
+            if b.kind == L.GRICO_ITEM_INTERFACE:
+                for a in range(3):
+                    d.degree_plus[a] = b.degree_plus[a] if a < self.D else 0
+                d.ref_points_plus = L.ptr(b.ref_points_plus, C.c_double)
+                d.cell_size_plus = L.ptr(b.h_plus, C.c_double)
+                d.face_axis = L.ptr(b.face_axis, C.c_int32)
             d.point_offsets = L.ptr(b.point_offsets, C.c_int64)
             d.ref_points = L.ptr(b.ref_points, C.c_double)
             d.weights = L.ptr(b.weights, C.c_double)
@@ -847,6 +980,8 @@ def _source_points(plan, problem=None):
                 arrays.append(np.ascontiguousarray(f))
             else:
                 arrays.append(None)
+        elif b.kind == L.GRICO_ITEM_INTERFACE:
+            arrays.append(None)  # interior interfaces carry no load
         else:
             g = np.zeros(b.points.shape[0])
             any_data = False

@@ -137,6 +137,14 @@ typedef struct GricoCellBatchDesc {
  * arrays of the descriptor (point_offsets, ref_points, weights, normals, eta) are unused and
  * kappa_points / rhs source values are given per subcell point [n_subcells * prod(qpoints)]. */
 #define GRICO_ITEM_SUBCELLS 3
+/* Two-sided interface items (interface_apply!, accumulators.jl:1576-1616) with the symmetric
+ * interior-penalty form -{du/dn}[v] - {dv/dn}[u] + sigma [u][v] of
+ * benchmark/sine_poisson_sipg.jl:54-95: [w] = w(minus) - w(plus), {w} = average, n the unit
+ * normal e_axis from the minus to the plus cell, sigma = eta[item].  map_index holds the minus
+ * cell's box modes followed by the plus cell's (prod(degree+1) + prod(degree_plus+1) entries per
+ * item); ref_points / cell_size are the minus side's, ref_points_plus / cell_size_plus the plus
+ * side's, both on the shared tangential patch rule with physical `weights`.  No load term. */
+#define GRICO_ITEM_INTERFACE 4
 
 typedef struct GricoPointBatchDesc {
   int32_t n_items;
@@ -162,6 +170,11 @@ typedef struct GricoPointBatchDesc {
   const int32_t* subcell_pos;     /* [n_subcells*dim]                                       */
   const uint64_t* subcell_mask;   /* [n_subcells]                                           */
   const double* subcell_weight;   /* [n_subcells]                                           */
+  /* GRICO_ITEM_INTERFACE only */
+  int32_t degree_plus[3];
+  const double* ref_points_plus;  /* [n_points*dim]                                         */
+  const double* cell_size_plus;   /* [n_items*dim]                                          */
+  const int32_t* face_axis;       /* [n_items] 0-based normal axis                          */
 } GricoPointBatchDesc;
 
 typedef struct GricoPlanDesc {

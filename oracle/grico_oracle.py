@@ -709,11 +709,14 @@ class Plan:
     dirichlet: list of (axis, side, value) with constant values."""
 
     def __init__(self, space: Space, mu=0.0, kappa=1.0, kappa_fn=None, source=None, dirichlet=(),
-                 cell_rules=None, surface_items=()):
+                 cell_rules=None, surface_items=(), interface_penalty=None):
         """cell_rules: {leaf: (reference points [n, D], reference weights [n])} replacing the
         tensor rule of those leaves (finite-cell cut cells, add_cell_quadrature!);
         surface_items: [(leaf, reference points, physical weights, physical unit normals,
-        penalty, g)] symmetric Nitsche items (boundary faces or embedded surfaces)."""
+        penalty, g[, eta])] symmetric Nitsche items (boundary faces or embedded surfaces); eta
+        defaults to penalty / min(h);
+        interface_penalty: SIPG interior-penalty terms on every interface of the space
+        (benchmark/sine_poisson_sipg.jl:54-95) with this penalty."""
         cell_rules = cell_rules or {}
         self.space = space
         dom = space.domain
@@ -775,7 +778,7 @@ class Plan:
             self.cells.append(dict(leaf=leaf, modes=modes, terms=terms, w=w, pts=pts, vals=vals, grads=grads,
                                    axis_v=axis_v, axis_g=axis_g, q=q, degs=degs))
         self.surfaces = []
-        for (leaf, ref, wphys, nphys, penalty, g) in surface_items:
+        for (leaf, ref, wphys, nphys, penalty, g, *_) in surface_items:
             li = snap.leaf_to_index[leaf]
             c = self._point_item(li, leaf, ref)
             c["w"] = np.asarray(wphys, dtype=np.float64)
@@ -783,6 +786,13 @@ class Plan:
             c["eta"] = penalty / min(dom.cell_size(leaf, a) for a in range(D))
             c["g"] = g
             self.surfaces.append(c)
+        for k, it in enumerate(surface_items):
+            if len(it) > 6 and it[6] is not None:
+                self.surfaces[k]["eta"] = float(it[6])
+        self.interfaces = []
+        if interface_penalty is not None:
+            for (m, pl, ax1) in snap.interfaces:
+                self.interfaces.append(self._interface_item(m, pl, ax1 - 1, interface_penalty))
         self.colors = self._colour()
         self.fixed, self.fixed_values, self.rows = self._dirichlet(dirichlet)
         self.fixed_mask = np.zeros(self.ndofs + 1, dtype=bool)
@@ -791,6 +801,54 @@ class Plan:
         for (pivot, _, _, _) in self.rows:
             self.blocked[pivot] = True
         self._reduced_map()
+
+    def _interface_item(self, m, pl, ax, penalty):
+        """Shared tangential patch of the faces of leaves m (its upper face on axis ax) and pl,
+        with max(q-, q+) Gauss points per tangential axis (integration.jl:2279-2307, 2800-2841),
+        both sides' tables at the patch points, physical weights and the SIPG penalty
+        (sine_poisson_sipg.jl:28-40)."""
+        space, dom, D = self.space, self.space.domain, self.space.D
+        snap = space.snapshot
+        lm, lp = snap.leaf_to_index[m], snap.leaf_to_index[pl]
+        chm = [dom.center_half(m, a) for a in range(D)]
+        chp = [dom.center_half(pl, a) for a in range(D)]
+        tang = [a for a in range(D) if a != ax]
+        lo = {a: max(chm[a][0] - chm[a][1], chp[a][0] - chp[a][1]) for a in tang}
+        hi = {a: min(chm[a][0] + chm[a][1], chp[a][0] + chp[a][1]) for a in tang}
+        rules = [gauss_legendre_rule(max(space.qshape[lm][a], space.qshape[lp][a])) for a in tang]
+        shape = tuple(len(r[0]) - 1 for r in rules)
+        npts = int(np.prod([len(r[0]) for r in rules])) if tang else 1
+        ref_m = np.zeros((npts, D))
+        ref_p = np.zeros((npts, D))
+        w = np.ones(npts)
+        for p in range(npts):
+            idx = mode_from_linear(p, shape) if tang else ()
+            x = [0.0] * D
+            for k, a in enumerate(tang):
+                half = 0.5 * (hi[a] - lo[a])
+                x[a] = lo[a] + half * (1.0 + rules[k][0][idx[k]])
+                w[p] *= rules[k][1][idx[k]] * half
+            for a in tang:
+                ref_m[p, a] = (x[a] - chm[a][0]) / chm[a][1]
+                ref_p[p, a] = (x[a] - chp[a][0]) / chp[a][1]
+            ref_m[p, ax] = 1.0
+            ref_p[p, ax] = -1.0
+        hm, hp = dom.cell_size(m, ax), dom.cell_size(pl, ax)
+        pmax = max(space.degrees[lm][ax], space.degrees[lp][ax])
+        sigma = penalty * (pmax + 1) ** 2 / (2.0 * hm * hp / (hm + hp))
+        return dict(minus=self._point_item(lm, m, ref_m), plus=self._point_item(lp, pl, ref_p), w=w, axis=ax,
+                    sigma=sigma)
+
+    def interface_local_apply(self, it, xm, xp):
+        """-[v]{du/dn} - {dv/dn}[u] + sigma [v][u] at every patch point, [w] = w- - w+,
+        n = e_axis from minus to plus (sine_poisson_sipg.jl:54-95)."""
+        a = it["axis"]
+        mi, pi = it["minus"], it["plus"]
+        jump = mi["vals"].T @ xm - pi["vals"].T @ xp
+        avg = 0.5 * (mi["grads"][a].T @ xm + pi["grads"][a].T @ xp)
+        cv = it["w"] * (it["sigma"] * jump - avg)
+        cd = -0.5 * it["w"] * jump
+        return mi["vals"] @ cv + mi["grads"][a] @ cd, -(pi["vals"] @ cv) + pi["grads"][a] @ cd
 
     def _point_item(self, li, leaf, ref):
         """Full value/gradient tables of one leaf's modes at arbitrary reference points
@@ -1041,6 +1099,13 @@ class Plan:
                     if self.fixed_mask[d] or self.blocked[d]:
                         continue
                     y1[d] += cc * yloc[i]
+        for it in self.interfaces:
+            for side, yloc in zip(("minus", "plus"), self._interface_apply_sides(it, x1)):
+                for i, t in enumerate(it[side]["terms"]):
+                    for (d, cc) in t:
+                        if self.fixed_mask[d] or self.blocked[d]:
+                            continue
+                        y1[d] += cc * yloc[i]
         for d in self.fixed:
             y1[d] = x1[d]
         for (pivot, idx, co, _) in self.rows:
@@ -1049,6 +1114,11 @@ class Plan:
                 v -= c * x1[j]
             y1[pivot] = v
         return y1[1:]
+
+    def _interface_apply_sides(self, it, x1):
+        xm = np.array([sum(cc * x1[d] for (d, cc) in t) for t in it["minus"]["terms"]])
+        xp = np.array([sum(cc * x1[d] for (d, cc) in t) for t in it["plus"]["terms"]])
+        return self.interface_local_apply(it, xm, xp)
 
     def apply_physical(self, x):
         x1 = np.concatenate([[0.0], np.asarray(x, dtype=np.float64)])
@@ -1059,6 +1129,11 @@ class Plan:
             for i, t in enumerate(c["terms"]):
                 for (d, cc) in t:
                     y1[d] += cc * yloc[i]
+        for it in self.interfaces:
+            for side, yloc in zip(("minus", "plus"), self._interface_apply_sides(it, x1)):
+                for i, t in enumerate(it[side]["terms"]):
+                    for (d, cc) in t:
+                        y1[d] += cc * yloc[i]
         return y1[1:]
 
     def expand(self, xr, include_shift=False):
@@ -1097,11 +1172,19 @@ class Plan:
             for i, t in enumerate(c["terms"]):
                 for (d, cc) in t:
                     out[d] += cc * cc * diag[i]
+        for it in self.interfaces:  # interface_diagonal!, sine_poisson_sipg.jl:97-123
+            a = it["axis"]
+            for side, sign in (("minus", 1.0), ("plus", -1.0)):
+                c = it[side]
+                diag = (it["sigma"] * c["vals"] ** 2 - sign * c["vals"] * c["grads"][a]) @ it["w"]
+                for i, t in enumerate(c["terms"]):
+                    for (d, cc) in t:
+                        out[d] += cc * cc * diag[i]
         return out[1:]
 
     def reduced_diagonal(self):
         """Direct copy when the map is an injection, else None (assembly.jl:662-726)."""
-        for c in self.cells + self.surfaces:
+        for c in self.cells + self.surfaces + [it[s] for it in self.interfaces for s in ("minus", "plus")]:
             for t in c["terms"]:
                 if len(t) != 1:
                     return None
