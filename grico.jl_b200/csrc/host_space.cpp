@@ -925,6 +925,9 @@ extern "C" int grico_transfer_build(const GricoSpace* coarse_space, const GricoS
     std::vector<Triple> triples;
     std::vector<std::pair<int64_t, double>> source;
     std::vector<std::vector<std::pair<int64_t, double>>> local;
+    std::vector<std::pair<int, double>> nz[3][17];
+    std::vector<char> active;
+    std::vector<int> touched;
     auto add_to = [](std::vector<std::pair<int64_t, double>>& v, int64_t k, double x) {
       if (x == 0.0) return;
       for (auto& t : v)
@@ -962,7 +965,20 @@ extern "C" int grico_transfer_build(const GricoSpace* coarse_space, const GricoS
           if (fp.deg[a] < cp.deg[a]) { set_error("fine multigrid level must represent every coarse mode exactly"); return GRICO_ERR_INVALID; }
           M[a] = &matrix(cp.deg[a], fp.deg[a], delta, rel);
         }
-        local.assign(fp.box, {});
+        // nonzero 1-D restriction entries per axis and coarse digit: (fine digit, value); entries
+        // of O(eps) are rounding residues of exact zeros
+        for (int a = 0; a < D; ++a)
+          for (int c = 0; c <= cp.deg[a]; ++c) {
+            nz[a][c].clear();
+            for (int f = 0; f <= fp.deg[a]; ++f) {
+              const double m = (*M[a])[f * (cp.deg[a] + 1) + c];
+              if (std::fabs(m) > 4.0 * 2.220446049250313e-16) nz[a][c].emplace_back(f, m);
+            }
+          }
+        if (int(local.size()) < fp.box) local.resize(size_t(fp.box));
+        active.assign(size_t(fp.box), 0);
+        for (int fbox : fp.modes) active[size_t(fbox)] = 1;
+        touched.clear();
         for (int cbox : cp.modes) {
           int64_t ce = C->leaf_box_offset[cl] + cbox;
           if (C->term_offsets[ce] == C->term_offsets[ce + 1]) continue;
@@ -975,19 +991,31 @@ extern "C" int grico_transfer_build(const GricoSpace* coarse_space, const GricoS
           if (source.empty()) continue;
           int cm[3] = {0, 0, 0};
           for (int a = 0; a < D; ++a) cm[a] = mode_digit(cbox, cp.shape, a);
-          for (int fbox : fp.modes) {
-            double coef = 1.0;
-            for (int a = 0; a < D && coef != 0.0; ++a) {
-              const double m = (*M[a])[mode_digit(fbox, fp.shape, a) * (cp.deg[a] + 1) + cm[a]];
-              // 1-D restriction entries of O(eps) are rounding residues of exact zeros
-              coef *= std::fabs(m) <= 4.0 * 2.220446049250313e-16 ? 0.0 : m;
-            }
-            if (coef == 0.0) continue;
-            if (!std::isfinite(coef)) { set_error("multigrid transfer coefficient must be finite"); return GRICO_ERR_INVALID; }
-            for (auto& sp : source) add_to(local[fbox], sp.first, coef * sp.second);
-          }
+          static const std::vector<std::pair<int, double>> one{{0, 1.0}};
+          const auto& n0 = nz[0][cm[0]];
+          const auto& n1 = D > 1 ? nz[1][cm[1]] : one;
+          const auto& n2 = D > 2 ? nz[2][cm[2]] : one;
+          // fine modes in box order (axis 1 fastest), as the dense loop visited them
+          for (const auto& e2 : n2)
+            for (const auto& e1 : n1)
+              for (const auto& e0 : n0) {
+                const int fbox = e0.first + fp.shape[0] * (e1.first + (D > 1 ? fp.shape[1] : 1) * e2.first);
+                if (!active[size_t(fbox)]) continue;
+                double coef = e0.second;
+                if (D > 1) coef *= e1.second;
+                if (D > 2) coef *= e2.second;
+                if (coef == 0.0) continue;
+                if (!std::isfinite(coef)) { set_error("multigrid transfer coefficient must be finite"); return GRICO_ERR_INVALID; }
+                auto& lf = local[size_t(fbox)];
+                if (active[size_t(fbox)] == 1) {  // first contribution to this fine mode
+                  active[size_t(fbox)] = 2;
+                  touched.push_back(fbox);
+                }
+                for (auto& sp : source) add_to(lf, sp.first, coef * sp.second);
+              }
         }
-        for (int fbox = 0; fbox < fp.box; ++fbox) {
+        std::sort(touched.begin(), touched.end());
+        for (int fbox : touched) {
           if (local[fbox].empty()) continue;
           int64_t fe = F->leaf_box_offset[fl] + fbox;
           if (F->term_offsets[fe + 1] - F->term_offsets[fe] != 1) continue;
@@ -1000,11 +1028,26 @@ extern "C" int grico_transfer_build(const GricoSpace* coarse_space, const GricoS
             if (c != 0.0) triples.push_back({r, sp.first, c});
           }
         }
+        for (int fbox : touched) local[size_t(fbox)].clear();
       }
     }
-    std::stable_sort(triples.begin(), triples.end(), [](const Triple& a, const Triple& b) {
-      return a.fine != b.fine ? a.fine < b.fine : a.coarse < b.coarse;
-    });
+    // stable order by (fine, coarse): a counting sort by fine row keeps the emission order inside
+    // each row, then a stable sort of each (short) row by coarse column
+    {
+      std::vector<int64_t> start(size_t(n_fine_reduced) + 1, 0);
+      for (const Triple& t : triples) {
+        if (t.fine < 0 || t.fine >= n_fine_reduced) { set_error("multigrid transfer row out of range"); return GRICO_ERR_INVALID; }
+        ++start[size_t(t.fine) + 1];
+      }
+      for (int64_t r = 0; r < n_fine_reduced; ++r) start[size_t(r) + 1] += start[size_t(r)];
+      std::vector<Triple> sorted(triples.size());
+      std::vector<int64_t> fill(start.begin(), start.end() - 1);
+      for (const Triple& t : triples) sorted[size_t(fill[size_t(t.fine)]++)] = t;
+      for (int64_t r = 0; r < n_fine_reduced; ++r)
+        std::stable_sort(sorted.begin() + start[size_t(r)], sorted.begin() + start[size_t(r) + 1],
+                         [](const Triple& a, const Triple& b) { return a.coarse < b.coarse; });
+      triples.swap(sorted);
+    }
     std::vector<int64_t> row_count(n_fine_reduced, 0);
     std::vector<int64_t> cols;
     std::vector<double> vals;

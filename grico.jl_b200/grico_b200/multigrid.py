@@ -76,44 +76,54 @@ def _coarsened_degree(degree, lower, sequence):
 
 
 def _coarsened_degrees(degrees, cg, min_degree, sequence):
+    """_coarsened_degree on every entry (array form)."""
+    degrees = np.asarray(degrees)
     lower = np.minimum(degrees, max(min_degree, 1 if cg else 0))
-    out = degrees.copy()
-    for i in range(degrees.shape[0]):
-        for a in range(degrees.shape[1]):
-            out[i, a] = _coarsened_degree(int(degrees[i, a]), int(lower[i, a]), sequence)
-    return out
+    if sequence == "bisect":
+        c = np.maximum(degrees // 2, lower)
+    elif sequence == "decrease_by_one":
+        c = np.maximum(degrees - 1, lower)
+    else:
+        c = lower
+    return np.where(degrees <= lower, degrees, c).astype(degrees.dtype)
 
 
 def h_coarsening(grid, leaves, degrees):
     """Merge every expanded cell whose two children are both active leaves (multigrid.jl:514-586).
-    Returns (leaves, degrees) of the coarser level or None."""
+    Returns (leaves, degrees) of the coarser level or None.  The merged parent takes the place of
+    its first child in the leaf order and the smaller degree of its children per axis."""
     leaves = np.asarray(leaves, dtype=np.int64)
-    pos = {int(l): i for i, l in enumerate(leaves)}
-    parents = np.unique(grid.parent[leaves])
-    parents = parents[parents > 0]
-    cand = []
-    for p in parents:
-        f = int(grid.first_child[p])
-        if f in pos and (f + 1) in pos:
-            cand.append((int(p), f, f + 1))
-    if not cand:
+    degrees = np.asarray(degrees)
+    parent = np.asarray(grid.parent)[leaves]
+    first = np.asarray(grid.first_child)[np.maximum(parent, 0)]
+    is_first = (parent > 0) & (leaves == first)
+    is_second = (parent > 0) & (leaves == first + 1)
+    # a parent merges when both of its children are active leaves
+    order = np.argsort(leaves, kind="stable")
+    sorted_leaves = leaves[order]
+
+    def position(ids):
+        k = np.searchsorted(sorted_leaves, ids)
+        k = np.minimum(k, len(sorted_leaves) - 1)
+        found = sorted_leaves[k] == ids
+        return np.where(found, order[k], -1)
+
+    sib_of_first = position(np.where(is_first, leaves + 1, -1))
+    merge_first = is_first & (sib_of_first >= 0)
+    if not merge_first.any():
         return None
-    merged = {}
-    for p, a, b in cand:
-        merged[a] = p
-        merged[b] = p
-    new_leaves, new_deg, emitted = [], [], set()
-    parent_deg = {p: np.minimum(degrees[pos[a]], degrees[pos[b]]) for p, a, b in cand}
-    for i, l in enumerate(leaves):
-        p = merged.get(int(l))
-        if p is None:
-            new_leaves.append(int(l))
-            new_deg.append(degrees[i])
-        elif p not in emitted:
-            emitted.add(p)
-            new_leaves.append(p)
-            new_deg.append(parent_deg[p])
-    return np.array(new_leaves, dtype=np.int64), np.array(new_deg, dtype=np.int32)
+    sib_of_second = position(np.where(is_second, leaves - 1, -1))
+    merge_second = is_second & (sib_of_second >= 0)
+    pos_first = np.where(merge_first, np.arange(len(leaves)), np.where(merge_second, sib_of_second, -1))
+    merged = pos_first >= 0
+    # emit each merged parent once, at the position of whichever child comes first in the order
+    emit_pos = np.where(merged, np.minimum(np.arange(len(leaves)), np.where(merge_first, sib_of_first, sib_of_second)),
+                        np.arange(len(leaves)))
+    keep = (~merged) | (emit_pos == np.arange(len(leaves)))
+    new_leaves = np.where(merged, parent, leaves)[keep]
+    partner = np.where(merge_first, sib_of_first, np.where(merge_second, sib_of_second, np.arange(len(leaves))))
+    new_deg = np.where(merged[:, None], np.minimum(degrees, degrees[partner]), degrees)[keep]
+    return new_leaves.astype(np.int64), new_deg.astype(np.int32)
 
 
 def hp_multigrid_spaces(fine_space, opts):

@@ -263,7 +263,21 @@ def add_constraint(problem, constraint):
 # ---------------------------------------------------------------------------------------
 
 class _Batch:
-    pass
+    """A tensor-cell batch of the host plan.  `points` (physical quadrature points, n_cells x nq x
+    D) is built on first use: only right-hand sides, tabulated coefficients and error norms read
+    it, and at 64^3 cells, p = 4 it is 0.8 GB."""
+
+    def __getattr__(self, name):
+        if name == "points":
+            D = self.lower.shape[1]
+            grids = np.meshgrid(*[self.rules[a][0] for a in range(D)], indexing="ij")
+            # axis 1 fastest: flatten in Fortran order
+            ref = np.stack([g.reshape(-1, order="F") for g in grids], axis=1)  # [nq, D]
+            half = 0.5 * self.h
+            pts = (self.lower + half)[:, None, :] + ref[None, :, :] * half[:, None, :]
+            self.points = pts
+            return pts
+        raise AttributeError(name)
 
 
 def _gauss(n):
@@ -481,7 +495,6 @@ class AssemblyPlan:
                 b.lower = domain.cell_lower(b.leaves)
                 # reference points of the tensor rule, axis 1 fastest
                 b.rules = [_tables(b.degree[a], b.q[a]) for a in range(D)]
-                b.points = self._points(b)                           # [n_cells, nq, D]
                 b.kappa_points = None
                 if self.form.coefficient is not None:
                     vals = np.asarray(self.form.coefficient(b.points.reshape(-1, D)), dtype=np.float64)
@@ -747,50 +760,76 @@ class AssemblyPlan:
         return center[:, None, :] + ref[None, :, :] * half[:, None, :]
 
     def _compile_dirichlet(self, problem):
+        """Fixed dofs: every dof with a term on a mode of a selected boundary face; a vertex mode
+        with a single term takes the constraint's value (the last face in enumeration order wins
+        where faces with different values meet), every other fixed dof 0 (plans.jl:486-972 for
+        constant data).  Vectorised per (degrees, axis, side) group of boundary faces."""
         space = self.space
         D = self.D
-        fixed = {}
-        if problem.dirichlet:
-            b_leaf, b_axis, b_side = space.boundary_faces
-            sel = {}
-            for con in problem.dirichlet:
-                key = (con.boundary.axis - 1, con.boundary.side - 1)
-                if key in sel and sel[key] != con.value:
-                    raise ValueError("multiple Dirichlet constraints target the same boundary face")
-                sel[key] = con.value
-            matched = set()
-            for pos, ax, sd in zip(b_leaf, b_axis, b_side):
-                key = (int(ax), int(sd))
-                if key not in sel:
-                    continue
-                matched.add(key)
-                val = sel[key]
-                deg = space.degrees[pos]
-                shape = deg + 1
+        self.fixed_dofs = np.zeros(0, dtype=np.int64)
+        self.fixed_values = np.zeros(0, dtype=np.float64)
+        if not problem.dirichlet:
+            return
+        b_leaf, b_axis, b_side = space.boundary_faces
+        sel = {}
+        for con in problem.dirichlet:
+            key = (con.boundary.axis - 1, con.boundary.side - 1)
+            if key in sel and sel[key] != con.value:
+                raise ValueError("multiple Dirichlet constraints target the same boundary face")
+            sel[key] = con.value
+        b_leaf = np.asarray(b_leaf, dtype=np.int64)
+        b_axis = np.asarray(b_axis, dtype=np.int64)
+        b_side = np.asarray(b_side, dtype=np.int64)
+        face_ids = np.arange(len(b_leaf), dtype=np.int64)
+        dof_parts, val_parts, set_parts, order_parts = [], [], [], []
+        matched = set()
+        degs = space.degrees[b_leaf] if len(b_leaf) else np.zeros((0, D), dtype=np.int64)
+        for (ax, sd), val in sel.items():
+            mask = (b_axis == ax) & (b_side == sd)
+            if not mask.any():
+                continue
+            matched.add((ax, sd))
+            fsel = face_ids[mask]
+            for dsig in np.unique(degs[fsel], axis=0):
+                g = fsel[np.all(degs[fsel] == dsig, axis=1)]
+                shape = dsig + 1
                 nb = int(np.prod(shape))
                 box = np.arange(nb)
-                digits = []
-                rem = box.copy()
-                for a in range(D):
-                    digits.append(rem % shape[a])
-                    rem //= shape[a]
-                digits = np.stack(digits, axis=1)
-                on_face = digits[:, ax] == sd
-                vertex = np.all(digits <= 1, axis=1)
-                for m in np.nonzero(on_face)[0]:
-                    e = space.box_offsets[pos] + m
-                    for t in range(space.term_offsets[e], space.term_offsets[e + 1]):
-                        d = int(space.term_index[t])
-                        single_vertex = vertex[m] and (space.term_offsets[e + 1] - space.term_offsets[e] == 1)
-                        if d not in fixed:
-                            fixed[d] = 0.0
-                        if single_vertex and val != 0.0:
-                            fixed[d] = val
-            for key in sel:
-                if key not in matched:
-                    raise ValueError("Dirichlet constraint does not match any boundary face")
-        self.fixed_dofs = np.array(sorted(fixed), dtype=np.int64)
-        self.fixed_values = np.array([fixed[d] for d in self.fixed_dofs], dtype=np.float64)
+                digits = np.stack([(box // int(np.prod(shape[:a]))) % shape[a] for a in range(D)], axis=1)
+                modes = np.nonzero(digits[:, ax] == sd)[0]
+                vertex = np.all(digits[modes] <= 1, axis=1)
+                e = (space.box_offsets[b_leaf[g]][:, None] + modes[None, :]).reshape(-1)
+                lo = space.term_offsets[e]
+                cnt = space.term_offsets[e + 1] - lo
+                rep = np.repeat(np.arange(e.size), cnt)
+                t = np.repeat(lo - np.concatenate([[0], np.cumsum(cnt)[:-1]]), cnt) + np.arange(int(cnt.sum()))
+                dof_parts.append(space.term_index[t].astype(np.int64))
+                single_vertex = np.tile(vertex, len(g))[rep] & (cnt[rep] == 1)
+                set_parts.append(single_vertex & (val != 0.0))
+                val_parts.append(np.full(rep.size, float(val)))
+                # enumeration order: boundary face, then mode, then term
+                face_of = np.repeat(g, len(modes))[rep]
+                order_parts.append(face_of * (1 << 32) + np.arange(rep.size, dtype=np.int64) % (1 << 32))
+        for key in sel:
+            if key not in matched:
+                raise ValueError("Dirichlet constraint does not match any boundary face")
+        if not dof_parts:
+            return
+        dofs = np.concatenate(dof_parts)
+        setv = np.concatenate(set_parts)
+        vals = np.concatenate(val_parts)
+        order = np.concatenate(order_parts)
+        fixed = np.unique(dofs)
+        values = np.zeros(fixed.size)
+        if setv.any():
+            sd_, sv, so = dofs[setv], vals[setv], order[setv]
+            last = np.lexsort((so, sd_))          # by dof, then enumeration order
+            sd_, sv = sd_[last], sv[last]
+            keep = np.ones(sd_.size, dtype=bool)
+            keep[:-1] = sd_[1:] != sd_[:-1]        # last assignment per dof
+            values[np.searchsorted(fixed, sd_[keep])] = sv[keep]
+        self.fixed_dofs = fixed.astype(np.int64)
+        self.fixed_values = values
 
     def _create_device_plan(self):
         descs = (L.GricoCellBatchDesc * len(self.batches))()

@@ -58,10 +58,17 @@ class StoredDegrees:
     """Explicit per-leaf degrees aligned with an active-leaf list (used by multigrid levels)."""
 
     def __init__(self, leaves, degrees):
-        self.map = {int(l): tuple(int(x) for x in d) for l, d in zip(leaves, degrees)}
+        leaves = np.asarray(leaves, dtype=np.int64)
+        order = np.argsort(leaves, kind="stable")
+        self.sorted_leaves = leaves[order]
+        self.sorted_degrees = np.asarray(degrees, dtype=np.int32).reshape(len(leaves), -1)[order]
 
     def degrees(self, domain, leaves):
-        return np.array([self.map[int(l)] for l in leaves], dtype=np.int32)
+        leaves = np.asarray(leaves, dtype=np.int64)
+        k = np.searchsorted(self.sorted_leaves, leaves)
+        if np.any(k >= len(self.sorted_leaves)) or np.any(self.sorted_leaves[np.minimum(k, len(self.sorted_leaves) - 1)] != leaves):
+            raise KeyError("leaf without a stored degree")
+        return self.sorted_degrees[k].astype(np.int32)
 
 
 class DegreePlusQuadrature:
