@@ -38,6 +38,7 @@ struct BatchView {
   const double* W;           // [q]     reference Gauss weights
   const double* G;           // [n*q]   reference derivative table psi_i'(xi_p)
   const uint8_t* skip;       // nullable: cells excluded from the diagonal kernel
+  const double* mass_pts;    // nullable [n_cells*nq]: pointwise mass added to the constant mass
 };
 
 template <typename T>
@@ -207,7 +208,7 @@ __global__ void __launch_bounds__(Q* Q* CPB) cell_apply_3d(BatchView b, const Ta
         S2[p] = S2[p] * (wk * sx * sx);
         S1[p] = S1[p] * (wk * sy * sy);
         dz[q] *= wk * sz * sz;
-        u[q] *= w * mass;
+        u[q] *= w * (b.mass_pts && act ? mass + T(b.mass_pts[cell * Q3 + p]) : mass);
       }
 #pragma unroll
       for (int l = 0; l < Q; ++l) {
@@ -363,7 +364,7 @@ __global__ void __launch_bounds__(Q* CPB) cell_apply_2d(BatchView b, const T* __
     } else {
       T k = kappa;
       if (b.kappa_pts && act) k *= T(b.kappa_pts[cell * Q2 + tx + Q * q]);
-      r[q] = w * mass * u[q];
+      r[q] = w * (b.mass_pts && act ? mass + T(b.mass_pts[cell * Q2 + tx + Q * q]) : mass) * u[q];
       dx[q] *= w * k * sx * sx;
       dy[q] *= w * k * sy * sy;
     }
@@ -405,8 +406,9 @@ __global__ void __launch_bounds__(Q* CPB) cell_apply_2d(BatchView b, const T* __
 }
 
 // Generic tensor-table kernel for any dimension 1..3 and any (n, q) — one block per cell,
-// threads over points then over modes; O(n^D q^D D) per cell.  Used for 1-D, q < p+1 and as
-// the diagonal kernel (mode 3: local diagonal sum of squared shape products).
+// threads over points then over modes; O(n^D q^D D) per cell.  Used for 1-D, q < p+1, as the
+// diagonal kernel (mode 3: local diagonal sum of squared shape products) and to evaluate the
+// field at the quadrature points (mode 4: y[cell * nq + p] = u(x_p), nothing projected).
 template <typename T>
 __global__ void cell_apply_generic(BatchView b, int dim, int n0, int n1, int n2, int q0, int q1, int q2,
                                    const T* __restrict__ x, T* __restrict__ y, int64_t n_vec, T mass, T kappa,
@@ -433,7 +435,7 @@ __global__ void cell_apply_generic(BatchView b, int dim, int n0, int n1, int n2,
   auto Bv = [&](int a, int i, int p) { return T(b.B[a * nmax * qmax + i * q[a] + p]); };
   auto Gv = [&](int a, int i, int p) { return T(b.G[a * nmax * qmax + i * q[a] + p]) * (T(2) / hs[a]); };
   auto Wv = [&](int a, int p) { return T(b.W[a * qmax + p]); };
-  if (mode == 0) {
+  if (mode == 0 || mode == 4) {
     for (int i = threadIdx.x; i < nb; i += blockDim.x) xl[i] = gather_entry<T>(b, cell * nb + i, x);
     __syncthreads();
   }
@@ -461,13 +463,18 @@ __global__ void cell_apply_generic(BatchView b, int dim, int n0, int n1, int n2,
           g[a] += xl[i] * gg;
         }
       }
+      if (mode == 4) {  // u at the point
+        y[cell * nq + p] = uval;
+        continue;
+      }
       T k = kappa;
       if (b.kappa_pts) k *= T(b.kappa_pts[cell * nq + p]);
-      flux[p] = w * mass * uval;
+      flux[p] = w * (b.mass_pts ? mass + T(b.mass_pts[cell * nq + p]) : mass) * uval;
       for (int a = 0; a < dim; ++a) flux[(a + 1) * nq + p] = w * k * g[a];
     }
     __syncthreads();
   }
+  if (mode == 4) return;
   for (int i = threadIdx.x; i < nb; i += blockDim.x) {
     int mi[3] = {i % n0, (i / n0) % n1, i / (n0 * n1)};
     T acc = 0;
@@ -481,7 +488,7 @@ __global__ void cell_apply_generic(BatchView b, int dim, int n0, int n1, int n2,
         for (int a = 0; a < dim; ++a) w *= Wv(a, pi[a]);
         T k = kappa;
         if (b.kappa_pts) k *= T(b.kappa_pts[cell * nq + p]);
-        T s = mass * prod * prod;
+        T s = (b.mass_pts ? mass + T(b.mass_pts[cell * nq + p]) : mass) * prod * prod;
         for (int a = 0; a < dim; ++a) {
           T gg = Gv(a, mi[a], pi[a]);
           for (int e = 0; e < dim; ++e)

@@ -402,7 +402,12 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB, Q))
           work[baseZ + BP + Q2 * q] *= wk * T(sc[1]);
           dz[q] *= wk * T(sc[2]);
         }
-        u[q] *= w * mass;
+        T m = mass;
+        if (b.mass_pts) {
+          const int64_t cm = g * CPB + cZ;
+          if (cm < b.n_cells) m += T(b.mass_pts[cm * Q3 + pZ + Q2 * q]);
+        }
+        u[q] *= w * m;
       }
 #pragma unroll
       for (int l = 0; l < Q; ++l) {

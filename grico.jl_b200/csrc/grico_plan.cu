@@ -127,6 +127,7 @@ void fill_view(BatchView& v, const DevBatch& b, bool reduced) {
   v.W = b.W.get<double>();
   v.G = b.G.get<double>();
   v.skip = reduced ? b.skip.get<uint8_t>() : nullptr;
+  v.mass_pts = b.mass_pts.get<double>();
 }
 
 template <int N, int Q, typename T>
@@ -245,7 +246,7 @@ void launch_batch(const GricoPlan& P, const DevBatch& b, bool reduced, const T* 
   BatchView v;
   fill_view(v, b, reduced);
   const int dim = P.dim;
-  if (mode != 3 && b.isotropic && b.q[0] >= b.n[0] &&
+  if (mode != 3 && mode != 4 && b.isotropic && b.q[0] >= b.n[0] &&
       launch_fused<T>(dim, b, v, x, y, nvec, T(P.mass), T(P.kappa), mode, src, nrhs, st))
     return;
   int n[3] = {1, 1, 1}, q[3] = {1, 1, 1};
@@ -1110,6 +1111,69 @@ static int apply_common(GricoPlan* P, bool reduced, const void* x, void* y, int 
     if (!cuda_ok(cudaStreamSynchronize(st), "apply")) return GRICO_ERR_CUDA;
   }
   return GRICO_OK;
+}
+
+int grico_plan_set_mass_points(GricoPlan* P, const double* const* mass_points, int flags) {
+  if (!P) { set_error("grico_plan_set_mass_points: invalid argument"); return GRICO_ERR_INVALID; }
+  if (mass_points && !P->pbatches.empty()) {
+    set_error("grico_plan_set_mass_points: plans with point-quadrature items are not supported");
+    return GRICO_ERR_UNSUPPORTED_FORM;
+  }
+  const cudaMemcpyKind kind = (flags & GRICO_FLAG_HOST_POINTERS) ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  for (size_t bi = 0; bi < P->batches.size(); ++bi) {
+    DevBatch& b = P->batches[bi];
+    if (!mass_points || !mass_points[bi]) {
+      b.mass_pts.alloc(0);
+      continue;
+    }
+    const size_t n = size_t(b.n_cells) * size_t(b.q[0]) * size_t(P->dim > 1 ? b.q[1] : 1) *
+                     size_t(P->dim > 2 ? b.q[2] : 1);
+    if (!b.mass_pts.ensure(sizeof(double) * n)) return GRICO_ERR_CUDA;
+    if (n && !cuda_ok(cudaMemcpyAsync(b.mass_pts.ptr, mass_points[bi], sizeof(double) * n, kind, P->stream),
+                      "mass points"))
+      return GRICO_ERR_CUDA;
+  }
+  return cuda_ok(cudaStreamSynchronize(P->stream), "mass points") ? GRICO_OK : GRICO_ERR_CUDA;
+}
+
+int grico_eval_points(GricoPlan* P, const double* u, int reduced, double* const* values, int flags) {
+  if (!P || !u || !values) { set_error("grico_eval_points: invalid argument"); return GRICO_ERR_INVALID; }
+  cudaStream_t st = P->stream;
+  const int64_t n = reduced ? P->n_red : P->n_full;
+  const bool host = (flags & GRICO_FLAG_HOST_POINTERS) != 0;
+  const double* du = u;
+  DevBuf ub, vb;
+  if (host) {
+    if (!ub.alloc(sizeof(double) * std::max<int64_t>(n, 1))) return GRICO_ERR_CUDA;
+    cudaMemcpyAsync(ub.ptr, u, sizeof(double) * n, cudaMemcpyHostToDevice, st);
+    du = ub.get<double>();
+  }
+  for (size_t bi = 0; bi < P->batches.size(); ++bi) {
+    if (!values[bi]) continue;
+    const DevBatch& b = P->batches[bi];
+    int nn[3] = {1, 1, 1}, q[3] = {1, 1, 1};
+    for (int a = 0; a < P->dim; ++a) { nn[a] = b.n[a]; q[a] = b.q[a]; }
+    const size_t nq = size_t(q[0]) * q[1] * q[2], count = size_t(b.n_cells) * nq;
+    double* out = values[bi];
+    if (host) {
+      if (!vb.ensure(sizeof(double) * std::max<size_t>(count, 1))) return GRICO_ERR_CUDA;
+      out = vb.get<double>();
+    }
+    if (b.n_cells > 0) {
+      BatchView v;
+      fill_view(v, b, reduced != 0);
+      const size_t smem = sizeof(double) * (size_t(nn[0]) * nn[1] * nn[2] + (P->dim + 1) * nq);
+      if (smem > 48 * 1024)
+        cudaFuncSetAttribute(cell_apply_generic<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+      cell_apply_generic<double><<<dim3(b.n_cells, 1), 128, smem, st>>>(v, P->dim, nn[0], nn[1], nn[2], q[0], q[1],
+                                                                        q[2], du, out, 0, 0.0, 0.0, 4, nullptr);
+    }
+    if (host && count &&
+        !cuda_ok(cudaMemcpyAsync(values[bi], out, sizeof(double) * count, cudaMemcpyDeviceToHost, st), "values"))
+      return GRICO_ERR_CUDA;
+    if (host && !cuda_ok(cudaStreamSynchronize(st), "eval points")) return GRICO_ERR_CUDA;
+  }
+  return cuda_ok(cudaStreamSynchronize(st), "eval points") ? GRICO_OK : GRICO_ERR_CUDA;
 }
 
 int grico_plan_batch_times(GricoPlan* P, double* ms, int64_t* launches, int n_batches) {

@@ -75,6 +75,7 @@ struct DevBatch {
   DevMap full, red;
   DevBuf h, kappa, B, G, W, D;
   DevBuf skip;  // uint8 per cell: hanging cells whose diagonal is added from the host
+  DevBuf mass_pts;  // optional pointwise mass [n_cells * nq] added to the form's mass (grico_plan_set_mass_points)
   std::vector<double> hB, hD, hW;  // axis-0 tables on the host (kernel parameters)
   int tile[2] = {1, 1};  // 3-D tensor-kernel variant per precision (0: FP64, 1: FP32): cells per block
                          // half (0), default (1) or double (2) the default, one block per cell group;

@@ -18,3 +18,5 @@ from .problem import (SPD, AffineProblem, AssemblyPlan, BoundaryFace, CGSolver, 
 from .regions import (FiniteCellExtension, ImplicitRegion, PhysicalDomain, PhysicalMeasure, SurfaceQuadrature,
                       finite_cell_quadrature, sphere_surface_quadrature)
 from .multigrid import GeometricMultigridPreconditioner
+from .nonlinear import ExpReaction, ResidualProblem, add_residual_accumulator, newton_solve
+from .nonlinear import compile as compile_residual

@@ -217,6 +217,8 @@ SIGNATURES = {
     "grico_plan_autotune": (C.c_int, [P, C.c_int, C.c_int, C.c_int, i32p]),
     "grico_plan_set_tiles": (C.c_int, [P, C.c_int, i32p, C.c_int]),
     "grico_plan_batch_times": (C.c_int, [P, f64p, i64p, C.c_int]),
+    "grico_plan_set_mass_points": (C.c_int, [P, C.POINTER(f64p), C.c_int]),
+    "grico_eval_points": (C.c_int, [P, f64p, C.c_int, C.POINTER(f64p), C.c_int]),
     "grico_cg_solve_multi": (C.c_int, [P, f64p, f64p, C.c_int, C.POINTER(GricoSolveOptions), C.POINTER(GricoSolveReport), C.c_int]),
     "grico_mg_learned_stats": (C.c_int, [P, i64p, i64p]),
     "grico_conv3d_forward": (C.c_int, [P, C.c_int, P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,

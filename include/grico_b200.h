@@ -222,6 +222,18 @@ int grico_plan_autotune(GricoPlan* plan, int nrhs, int precision, int reps, int*
  * reported by grico_plan_autotune), e.g. to replay a stored tuning without timing again.
  * No reference counterpart. */
 int grico_plan_set_tiles(GricoPlan* plan, int precision, const int* tiles, int n_batches);
+/* Pointwise mass coefficients c(x_q) added to the form's mass at the quadrature points of every
+ * cell batch: mass_points[b] = [n_cells*prod(q)] for batch b (points axis 1 fastest, as the
+ * load arrays), NULL entry or NULL array = none.  This is how a Newton tangent
+ * (tangent_apply!, assembly.jl:1050-1083) with a state-dependent reaction term (e.g.
+ * lambda exp(u), examples/nonlinear_bratu/driver.jl) runs through the ordinary apply, reduced
+ * apply and diagonal kernels.  Plans with point-quadrature items are refused.  Arrays are
+ * copied (device pointers, or host with GRICO_FLAG_HOST_POINTERS). */
+int grico_plan_set_mass_points(GricoPlan* plan, const double* const* mass_points, int flags);
+/* u at the quadrature points of every cell batch: values[b] = [n_cells*prod(q)] (NULL entries are
+ * skipped), u on the full layout (reduced = 0) or the reduced one (reduced = 1).  The state
+ * evaluation of residual!/tangent_apply! (assembly.jl:997-1083). */
+int grico_eval_points(GricoPlan* plan, const double* u, int reduced, double* const* values, int flags);
 /* Average device time of each batch's kernel launch over the applies called with
  * GRICO_FLAG_TIME_BATCHES since the last query (CUDA events recorded on the apply's stream
  * around each launch).  Batches are numbered cell batches first, then point batches; the first

@@ -1269,6 +1269,70 @@ def cg_solve(apply_fn, b, precond=None, rtol=1e-10, atol=0.0, maxiter=10000):
     raise ValueError("CG did not converge")
 
 
+def bratu_residual(plan: Plan, x_full, lam, source=None):
+    """Full-layout residual of the accumulator of examples/nonlinear_bratu/driver.jl:39-45:
+    value channel lam exp(u) - f, gradient channel kappa grad u, on every cell rule; constraint
+    rows are not written (the reduced residual projects them away)."""
+    D = plan.space.D
+    x1 = np.concatenate([[0.0], np.asarray(x_full, dtype=np.float64)])
+    y1 = np.zeros(plan.ndofs + 1)
+    for c in plan.cells:
+        xloc = np.array([sum(cc * x1[d] for (d, cc) in t) for t in c["terms"]])
+        u = c["vals"].T @ xloc
+        g = [c["grads"][a].T @ xloc for a in range(D)]
+        f = np.array([source(tuple(p)) for p in c["pts"]]) if source else 0.0
+        yloc = c["vals"] @ (c["w"] * (lam * np.exp(u) - f)) + sum(c["grads"][a] @ (c["w"] * plan.kappa * g[a])
+                                                                for a in range(D))
+        for i, t in enumerate(c["terms"]):
+            for (d, cc) in t:
+                y1[d] += cc * yloc[i]
+    return y1[1:]
+
+
+def bratu_tangent(plan: Plan, x_full, dx_full, lam):
+    """Tangent action of the same accumulator (driver.jl:48-54): value channel lam exp(u) du,
+    gradient channel kappa grad du."""
+    D = plan.space.D
+    x1 = np.concatenate([[0.0], np.asarray(x_full, dtype=np.float64)])
+    d1 = np.concatenate([[0.0], np.asarray(dx_full, dtype=np.float64)])
+    y1 = np.zeros(plan.ndofs + 1)
+    for c in plan.cells:
+        xloc = np.array([sum(cc * x1[d] for (d, cc) in t) for t in c["terms"]])
+        dloc = np.array([sum(cc * d1[d] for (d, cc) in t) for t in c["terms"]])
+        u = c["vals"].T @ xloc
+        du = c["vals"].T @ dloc
+        g = [c["grads"][a].T @ dloc for a in range(D)]
+        yloc = c["vals"] @ (c["w"] * lam * np.exp(u) * du) + sum(c["grads"][a] @ (c["w"] * plan.kappa * g[a])
+                                                                  for a in range(D))
+        for i, t in enumerate(c["terms"]):
+            for (d, cc) in t:
+                y1[d] += cc * yloc[i]
+    return y1[1:]
+
+
+def bratu_newton(plan: Plan, lam, source=None, rtol=1e-10, atol=1e-10, maxiter=10):
+    """Newton on the reduced space with exact (dense) tangent solves (solve.jl:277-333)."""
+    n = len(plan.solve_dofs)
+    ur = np.zeros(n)
+    r0 = None
+    for it in range(maxiter + 1):
+        x = plan.expand(ur, include_shift=True)
+        r = plan.project(bratu_residual(plan, x, lam, source))
+        rn = float(np.linalg.norm(r))
+        r0 = rn if r0 is None else r0
+        if rn <= max(atol, rtol * r0):
+            return ur, it
+        if it == maxiter:
+            break
+        J = np.zeros((n, n))
+        for j in range(n):
+            e = np.zeros(n)
+            e[j] = 1.0
+            J[:, j] = plan.project(bratu_tangent(plan, x, plan.expand(e), lam))
+        ur = ur + np.linalg.solve(J, -r)
+    raise ValueError("Newton solve did not converge")
+
+
 def l2_error(plan: Plan, full_values, exact):
     """Cell quadrature L2 error (verification.jl:201-230)."""
     x1 = np.concatenate([[0.0], np.asarray(full_values)])
