@@ -1070,6 +1070,11 @@ int grico_plan_destroy(GricoPlan* P) {
     cudaEventDestroy(ev.start);
     cudaEventDestroy(ev.stop);
   }
+  for (auto& sl : P->stage)
+    if (sl.done) {
+      cudaEventSynchronize(sl.done);
+      cudaEventDestroy(sl.done);
+    }
   cudaStream_t st = P->stream;
   delete P;
   cudaStreamDestroy(st);
@@ -1094,7 +1099,23 @@ static int apply_common(GricoPlan* P, bool reduced, const void* x, void* y, int 
   const size_t bytes = es * size_t(n) * nrhs;
   const void* dx = x;
   void* dy = y;
-  if (flags & GRICO_FLAG_HOST_POINTERS) {
+  const bool async = (flags & GRICO_FLAG_HOST_POINTERS) && (flags & GRICO_FLAG_ASYNC);
+  GricoPlan::Stage* slot = nullptr;
+  if (async) {
+    slot = &P->stage[P->stage_next];
+    P->stage_next ^= 1;
+    if (!slot->done && !cuda_ok(cudaEventCreateWithFlags(&slot->done, cudaEventDisableTiming), "stage event"))
+      return GRICO_ERR_CUDA;
+    // the slot's previous call (on any stream) must have copied its result out first
+    if (slot->used && !cuda_ok(cudaStreamWaitEvent(st, slot->done, 0), "stage wait")) return GRICO_ERR_CUDA;
+    if (bytes > slot->x.bytes || bytes > slot->y.bytes) {
+      if (slot->used) cudaEventSynchronize(slot->done);
+      if (!slot->x.ensure(bytes) || !slot->y.ensure(bytes)) return GRICO_ERR_CUDA;
+    }
+    if (!cuda_ok(cudaMemcpyAsync(slot->x.ptr, x, bytes, cudaMemcpyHostToDevice, st), "copy in")) return GRICO_ERR_CUDA;
+    dx = slot->x.ptr;
+    dy = slot->y.ptr;
+  } else if (flags & GRICO_FLAG_HOST_POINTERS) {
     if (!P->host_x.ensure(bytes) || !P->host_y.ensure(bytes)) return GRICO_ERR_CUDA;
     if (!cuda_ok(cudaMemcpyAsync(P->host_x.ptr, x, bytes, cudaMemcpyHostToDevice, st), "copy in")) return GRICO_ERR_CUDA;
     dx = P->host_x.ptr;
@@ -1108,6 +1129,10 @@ static int apply_common(GricoPlan* P, bool reduced, const void* x, void* y, int 
   if (rc != GRICO_OK) return rc;
   if (flags & GRICO_FLAG_HOST_POINTERS) {
     if (!cuda_ok(cudaMemcpyAsync(y, dy, bytes, cudaMemcpyDeviceToHost, st), "copy out")) return GRICO_ERR_CUDA;
+    if (async) {
+      slot->used = true;
+      return cuda_ok(cudaEventRecord(slot->done, st), "stage event") ? GRICO_OK : GRICO_ERR_CUDA;
+    }
     if (!cuda_ok(cudaStreamSynchronize(st), "apply")) return GRICO_ERR_CUDA;
   }
   return GRICO_OK;

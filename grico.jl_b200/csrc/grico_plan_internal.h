@@ -118,6 +118,11 @@ struct GricoPlan {
   int64_t n_hang = 0;
   grico::DevBuf partial, scalars;
   grico::DevBuf host_x, host_y;
+  // GRICO_FLAG_ASYNC staging ring: device copies of x and y per slot, and the event that marks
+  // the end of the slot's last copy out
+  struct Stage { grico::DevBuf x, y; cudaEvent_t done = nullptr; bool used = false; };
+  Stage stage[2];
+  int stage_next = 0;
   // GRICO_FLAG_TIME_BATCHES: event pairs around cell-batch launches, (batch, start, stop)
   struct BatchEvent { int batch; cudaEvent_t start, stop; };
   bool time_batches = false;

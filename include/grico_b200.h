@@ -57,6 +57,11 @@ extern "C" {
 #define GRICO_FLAG_MIXED 4         /* grico_cg_solve_multi: FP64 refinement around FP32 inner CG */
 #define GRICO_FLAG_TIME_BATCHES 8  /* grico_apply / grico_reduced_apply: record CUDA events around
                                       every cell-batch kernel launch (grico_plan_batch_times)   */
+#define GRICO_FLAG_ASYNC 16        /* grico_apply / grico_reduced_apply with host pointers: enqueue
+                                      the copy in, the kernels and the copy out on `stream` and
+                                      return; the caller synchronises the stream before reading y
+                                      or changing x.  Two calls may be in flight per plan (two
+                                      staging slots; a third waits for the first on the device) */
 
 /* ================================================================================
  * Host space compile (native replacement of the Julia-side HpSpace construction)

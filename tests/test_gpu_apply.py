@@ -207,3 +207,24 @@ def test_batch_event_timing(cuda):
     assert L.lib().grico_plan_batch_times(plan.handle, L.ptr(ms, C.c_double), L.ptr(n, C.c_int64), nb) == 0
     assert (n == 0).all() and (ms == 0).all()
     assert L.lib().grico_plan_batch_times(plan.handle, L.ptr(ms, C.c_double), None, nb + 1) != 0
+
+
+def test_async_host_pointer_applies(cuda):
+    """GRICO_FLAG_ASYNC: three applies with different inputs in flight on two streams (the third
+    reuses the first staging slot) give the synchronous results once the streams are drained."""
+    import ctypes as C
+    import torch
+    from grico_b200 import _lib as L
+
+    _, prob = build("3d_p4", mu=0.7, kappa=1.3)
+    plan = gb.compile(prob)
+    xs = [torch.tensor(sample_vector(plan.n_full, seed=s)).pin_memory() for s in (21, 22, 23)]
+    ys = [torch.zeros(plan.n_full, dtype=torch.float64).pin_memory() for _ in range(3)]
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    for k in range(3):
+        assert L.lib().grico_apply(plan.handle, xs[k].data_ptr(), ys[k].data_ptr(), 1, L.GRICO_PREC_FP64,
+                                   L.GRICO_FLAG_HOST_POINTERS | L.GRICO_FLAG_ASYNC, streams[k % 2].cuda_stream) == 0
+    for s in streams:
+        s.synchronize()
+    for k in range(3):
+        assert rel_err(ys[k].numpy(), gb.apply(plan, xs[k].numpy())) <= TOL
