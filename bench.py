@@ -207,18 +207,15 @@ def solve_legs(gb, L, plan, prob, target=1e-8):
     exact = lambda X: np.prod(np.sin(np.pi * X), axis=1)
     prob.rhs_operators = [gb.Load(lambda X: 3.0 * np.pi ** 2 * exact(X))]
     b = gb.reduced_rhs(plan)
+    cheb = lambda deg, steps, prec="fp64": GeometricMultigridPreconditioner(
+        smoother="chebyshev", chebyshev_degree=deg, pre_smoothing_steps=steps, post_smoothing_steps=steps,
+        precision=prec)
     legs = {
         "fp64_cg_gmg_jacobi_v22 (reference method)": (GeometricMultigridPreconditioner(), 2000),
-        "fp64_cg_gmg_chebyshev3_v22 (plain FP64 GPU, no CUDA graph)": (
-            GeometricMultigridPreconditioner(smoother="chebyshev", pre_smoothing_steps=2, post_smoothing_steps=2), 500),
-        "fp64_cg_gmg_chebyshev3_v22 (plain FP64 GPU)": (
-            GeometricMultigridPreconditioner(smoother="chebyshev", pre_smoothing_steps=2, post_smoothing_steps=2), 500),
-        "mixed_cg_fp64_gmg_chebyshev3_v22_fp32": (
-            GeometricMultigridPreconditioner(smoother="chebyshev", pre_smoothing_steps=2, post_smoothing_steps=2,
-                                             precision="fp32"), 500),
-        "mixed_cg_fp64_gmg_chebyshev3_v11_fp32": (
-            GeometricMultigridPreconditioner(smoother="chebyshev", pre_smoothing_steps=1, post_smoothing_steps=1,
-                                             precision="fp32"), 500),
+        "fp64_cg_gmg_chebyshev2_v22 (plain FP64 GPU, no CUDA graph)": (cheb(2, 2), 500),
+        "fp64_cg_gmg_chebyshev2_v22 (plain FP64 GPU)": (cheb(2, 2), 500),
+        "mixed_cg_fp64_gmg_chebyshev2_v22_fp32": (cheb(2, 2, "fp32"), 500),
+        "mixed_cg_fp64_gmg_chebyshev3_v22_fp32": (cheb(3, 2, "fp32"), 500),
     }
     out = {}
     for name, (opts, maxiter) in legs.items():

@@ -9,7 +9,7 @@
 // contractions.  The kernel serves plain maps only (every entry a dof or -1, no coefficients,
 // no tail expansions): the gather is branch-free (a zero-filling copy for -1 entries) and the
 // map entries are staged beside the modes, so the scatter reads them from shared memory.
-// Batches with hanging-node tails or coefficients use cell_apply_3d.
+// Batches with hanging-node tails, coefficients or pointwise mass use cell_apply_3d.
 //
 // Every contraction step gives each thread one whole line of a cell's Q^3 point box (x-, y- or
 // z-line), as in cell_apply_3d.  Which line a thread takes is not tied to its own cell: for each
@@ -402,12 +402,7 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB, Q))
           work[baseZ + BP + Q2 * q] *= wk * T(sc[1]);
           dz[q] *= wk * T(sc[2]);
         }
-        T m = mass;
-        if (b.mass_pts) {
-          const int64_t cm = g * CPB + cZ;
-          if (cm < b.n_cells) m += T(b.mass_pts[cm * Q3 + pZ + Q2 * q]);
-        }
-        u[q] *= w * m;
+        u[q] *= w * mass;
       }
 #pragma unroll
       for (int l = 0; l < Q; ++l) {

@@ -193,7 +193,7 @@ bool launch_fused(int dim, const DevBatch& bt, const BatchView& v, const T* x, T
     return true;                                                                                               \
   }
 #define GRICO_L3_PIPE(NN, QQ, CPB_)                                                                            \
-  if (mode == 0 && v.coef == nullptr && v.tail_off == nullptr) {                                               \
+  if (mode == 0 && v.coef == nullptr && v.tail_off == nullptr && v.mass_pts == nullptr) {                      \
     constexpr int CPB = CPB_;                                                                                  \
     constexpr int NT = QQ * QQ * CPB;                                                                          \
     static const LaneLines<NT> lanes = make_lane_lines<NT>(NN, QQ, CPB, int(sizeof(T)));                      \

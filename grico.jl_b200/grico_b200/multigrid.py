@@ -26,7 +26,7 @@ from . import _lib as L
 class GeometricMultigridPreconditioner:
     def __init__(self, min_degree=1, max_levels=16, p_sequence="bisect", pre_smoothing_steps=2,
                  post_smoothing_steps=2, smoother_damping=0.8, smoother="auto", smoother_restart=8,
-                 coarse_direct_dof_limit=512, chebyshev_degree=3, chebyshev_range=15.0, precision="fp64"):
+                 coarse_direct_dof_limit=512, chebyshev_degree=2, chebyshev_range=15.0, precision="fp64"):
         if p_sequence not in ("bisect", "decrease_by_one", "go_to_one"):
             raise ValueError("p_sequence must be :bisect, :decrease_by_one, or :go_to_one")
         if smoother not in ("auto", "jacobi", "gmres", "chebyshev"):

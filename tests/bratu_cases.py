@@ -10,13 +10,15 @@ import grico_b200 as gb
 
 
 def bratu(roots=(2, 2), degree=2, lam=0.5, amplitude=0.1, device=True):
-    exact = lambda X: amplitude * np.sin(math.pi * X[:, 0]) * np.sin(math.pi * X[:, 1])
-    source = lambda X: 2.0 * math.pi ** 2 * exact(X) + lam * np.exp(exact(X))
-    od = go.Domain((0.0, 0.0), (1.0, 1.0), roots)
+    """The example in 2-D (len(roots) = 2) or its 3-D analogue u_e = A prod sin(pi x_i)."""
+    D = len(roots)
+    exact = lambda X: amplitude * np.prod(np.sin(math.pi * X[:, :D]), axis=1)
+    source = lambda X: D * math.pi ** 2 * exact(X) + lam * np.exp(exact(X))
+    od = go.Domain((0.0,) * D, (1.0,) * D, roots)
     osp = go.Space(od, degree, basis="full")
-    faces = [(a, s) for a in (1, 2) for s in (go.LOWER, go.UPPER)]
+    faces = [(a, s) for a in range(1, D + 1) for s in (go.LOWER, go.UPPER)]
     oplan = go.Plan(osp, mu=0.0, kappa=1.0, dirichlet=[(a, s, 0.0) for a, s in faces])
-    d = gb.Domain((0.0, 0.0), (1.0, 1.0), roots)
+    d = gb.Domain((0.0,) * D, (1.0,) * D, roots)
     sp = gb.HpSpace(d, gb.SpaceOptions(basis=gb.FullTensorBasis(), degree=gb.UniformDegree(degree)))
     u = gb.ScalarField(sp)
     prob = gb.ResidualProblem(u)

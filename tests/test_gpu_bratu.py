@@ -18,7 +18,8 @@ def _state(oplan, seed):
     return 0.1 * np.random.default_rng(seed).standard_normal(n)
 
 
-@pytest.mark.parametrize("cfg", [dict(), dict(roots=(3, 2), degree=4, lam=1.0, amplitude=0.2)])
+@pytest.mark.parametrize("cfg", [dict(), dict(roots=(3, 2), degree=4, lam=1.0, amplitude=0.2),
+                                 dict(roots=(2, 2, 2), degree=4, lam=1.0, amplitude=0.2)])
 def test_residual_tangent_diagonal_match_oracle(cuda, cfg):
     oplan, plan, c = bratu(**cfg)
     ur = _state(oplan, 1)
