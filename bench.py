@@ -222,6 +222,15 @@ def solve_legs(gb, L, plan, prob, target=1e-8):
         t0 = time.perf_counter()
         mg = build_multigrid(plan, opts)
         setup = time.perf_counter() - t0
+        # one loose solve first: it captures the iteration graph that the plan keeps for the
+        # timed solves with this hierarchy; its time (capture included) is reported beside them
+        x = np.zeros(plan.n_reduced)
+        so = L.GricoSolveOptions(1e-2, 0.0, maxiter, L.GRICO_PRECOND_MULTIGRID, 30, 0)
+        rep = L.GricoSolveReport()
+        flags = L.GRICO_FLAG_HOST_POINTERS | (L.GRICO_FLAG_NO_GRAPH if "no CUDA graph" in name else 0)
+        L.lib().grico_cg_solve(plan.handle, mg.handle, L.ptr(b, C.c_double), L.ptr(x, C.c_double),
+                               C.byref(so), C.byref(rep), flags)
+        first = {"rtol": 1e-2, "iterations": int(rep.iterations), "solve_seconds": float(rep.seconds)}
         tries = []
         hit = None
         for rtol in (1e-4, 1e-5, 1e-6, 1e-7, 1e-8, 1e-9, 1e-10):
@@ -241,7 +250,8 @@ def solve_legs(gb, L, plan, prob, target=1e-8):
                 break
         out[name] = {"time_to_target_seconds": hit["solve_seconds"] if hit else None,
                      "iterations": hit["iterations"] if hit else None, "target_relative_l2": target,
-                     "host_setup_seconds": setup, "levels": len(mg.plans), "tries": tries}
+                     "host_setup_seconds": setup, "levels": len(mg.plans), "first_solve": first,
+                     "tries": tries}
         del mg
     return out
 

@@ -19,6 +19,7 @@
 // iteration owns them) and the coarsest solve stays FP64.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <memory>
 #include <vector>
@@ -47,6 +48,7 @@ struct GricoMultigrid {
   GricoMGOptions opts{};
   cudaStream_t stream = nullptr;
   grico::DevBuf io_r, io_z;
+  uint64_t identity = 0;  // see mg_identity
   // GMRES smoother: per smoothed level the Krylov basis V [(m+1) x n] and the preconditioned
   // directions Z [m x n] in the working precision; one small FP64 workspace shared by all levels
   std::vector<grico::DevBuf> gm_v, gm_z;
@@ -514,6 +516,18 @@ int mg_vcycle_device(GricoMultigrid* mg, const double* r, double* z, cudaStream_
 
 int mg_smoother(const GricoMultigrid* mg) { return mg ? mg->opts.smoother : -1; }
 
+namespace {
+std::atomic<uint64_t> g_mg_identity{1};
+}
+uint64_t mg_identity(const GricoMultigrid* mg) { return mg ? mg->identity : 0; }
+
+uint64_t mg_epoch(const GricoMultigrid* mg) {
+  uint64_t e = 0;
+  if (mg)
+    for (const GricoPlan* L : mg->levels) e += L->epoch;
+  return e;
+}
+
 int prepare_jacobi(GricoPlan* P, cudaStream_t st);
 
 }  // namespace grico
@@ -551,6 +565,7 @@ int grico_mg_create(GricoPlan* const* levels, int nlevels, const GricoTransferDe
   }
   std::unique_ptr<GricoMultigrid> mg(new GricoMultigrid());
   mg->opts = *opts;
+  mg->identity = g_mg_identity.fetch_add(1);
   const bool fp32 = opts->precision == GRICO_PREC_FP32;
   mg->stream = levels[nlevels - 1]->stream;
   cudaStream_t st = mg->stream;
@@ -751,6 +766,7 @@ int grico_mg_vcycle(GricoMultigrid* mg, const double* r, double* z, int flags) {
 }
 
 int grico_mg_set_learned(GricoMultigrid* mg, const GricoLearnedDesc* d) {
+  if (mg) mg->identity = g_mg_identity.fetch_add(1);  // the V-cycle changes
   if (!mg) return GRICO_ERR_INVALID;
   if (!d) {
     mg->learned = GricoMultigrid::Learned{};

@@ -9,4 +9,8 @@ namespace grico {
 int mg_vcycle_device(GricoMultigrid* mg, const double* r, double* z, cudaStream_t st);
 // GRICO_SMOOTHER_* of mg
 int mg_smoother(const GricoMultigrid* mg);
+// identity of mg's current V-cycle: unique per multigrid object, renewed when the cycle changes
+uint64_t mg_identity(const GricoMultigrid* mg);
+// sum of the level plans' epochs (changes when a level's kernels or their arguments change)
+uint64_t mg_epoch(const GricoMultigrid* mg);
 }  // namespace grico

@@ -1075,6 +1075,7 @@ int grico_plan_destroy(GricoPlan* P) {
       cudaEventSynchronize(sl.done);
       cudaEventDestroy(sl.done);
     }
+  if (P->cg_exec) cudaGraphExecDestroy(P->cg_exec);
   cudaStream_t st = P->stream;
   delete P;
   cudaStreamDestroy(st);
@@ -1145,6 +1146,7 @@ int grico_plan_set_mass_points(GricoPlan* P, const double* const* mass_points, i
     return GRICO_ERR_UNSUPPORTED_FORM;
   }
   const cudaMemcpyKind kind = (flags & GRICO_FLAG_HOST_POINTERS) ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  ++P->epoch;  // kernel arguments baked into a kept solver graph change
   for (size_t bi = 0; bi < P->batches.size(); ++bi) {
     DevBatch& b = P->batches[bi];
     if (!mass_points || !mass_points[bi]) {
@@ -1456,6 +1458,7 @@ extern "C" int grico_plan_autotune(GricoPlan* P, int nrhs, int precision, int re
     set_error("grico_plan_autotune: invalid argument");
     return GRICO_ERR_INVALID;
   }
+  ++P->epoch;
   return precision == GRICO_PREC_FP64 ? autotune_typed<double>(P, nrhs, reps, chosen)
                                       : autotune_typed<float>(P, nrhs, reps, chosen);
 }
@@ -1473,5 +1476,6 @@ extern "C" int grico_plan_set_tiles(GricoPlan* P, int precision, const int* tile
     }
   const int slot = precision == GRICO_PREC_FP32 ? 1 : 0;
   for (int i = 0; i < n_batches; ++i) P->batches[size_t(i)].tile[slot] = tiles[i];
+  ++P->epoch;  // kernels baked into a kept solver graph change
   return GRICO_OK;
 }

@@ -129,6 +129,14 @@ struct GricoPlan {
   std::vector<BatchEvent> batch_events;
   std::vector<double> batch_ms;
   std::vector<int64_t> batch_launches;
+  // CG iteration graph kept across solves; replayed while its key (multigrid identity,
+  // preconditioner, solution buffer, plan epoch) matches.  The epoch changes whenever kernel
+  // choices or per-point data baked into launches change.
+  cudaGraphExec_t cg_exec = nullptr;
+  uint64_t cg_key_mg = 0, cg_key_epoch = 0;
+  int cg_key_pc = -1;
+  const void* cg_key_x = nullptr;
+  uint64_t epoch = 1;
   // Krylov workspaces (allocated on first solve)
   grico::DevBuf w_r, w_z, w_p, w_q, w_x, w_b, w_dinv;
 };

@@ -155,18 +155,38 @@ extern "C" int grico_cg_solve(GricoPlan* P, GricoMultigrid* mg, const double* b,
                     cudaMemcpyDeviceToDevice, s);
     return GRICO_OK;
   };
+  // The graph is kept on the plan and replayed by later solves with the same multigrid cycle,
+  // preconditioner, solution buffer and plan epochs (every other buffer it touches belongs to the
+  // plan or the multigrid object; an epoch changes with the kernels or arguments of a plan).
   cudaGraphExec_t exec = nullptr;
   if (!converged && !(flags & GRICO_FLAG_NO_GRAPH)) {
-    cudaGraph_t graph = nullptr;
-    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
-      const int crc = iteration(st);
-      const cudaError_t ec = cudaStreamEndCapture(st, &graph);
-      if (crc == GRICO_OK && ec == cudaSuccess && graph &&
-          cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess)
-        exec = nullptr;
-      if (graph) cudaGraphDestroy(graph);
+    const bool use_mg = opts->preconditioner == GRICO_PRECOND_MULTIGRID;
+    const uint64_t mg_key = use_mg ? mg_identity(mg) : 0;
+    const uint64_t epoch = P->epoch + (use_mg ? mg_epoch(mg) : 0);
+    if (P->cg_exec && P->cg_key_mg == mg_key && P->cg_key_pc == opts->preconditioner && P->cg_key_x == xd &&
+        P->cg_key_epoch == epoch) {
+      exec = P->cg_exec;
+    } else {
+      if (P->cg_exec) cudaGraphExecDestroy(P->cg_exec);
+      P->cg_exec = nullptr;
+      cudaGraph_t graph = nullptr;
+      if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        const int crc = iteration(st);
+        const cudaError_t ec = cudaStreamEndCapture(st, &graph);
+        if (crc == GRICO_OK && ec == cudaSuccess && graph &&
+            cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess)
+          exec = nullptr;
+        if (graph) cudaGraphDestroy(graph);
+      }
+      (void)cudaGetLastError();  // a failed capture falls back to direct launches
+      if (exec) {
+        P->cg_exec = exec;
+        P->cg_key_mg = mg_key;
+        P->cg_key_pc = opts->preconditioner;
+        P->cg_key_x = xd;
+        P->cg_key_epoch = epoch;
+      }
     }
-    (void)cudaGetLastError();  // a failed capture falls back to direct launches
   }
   double hs[2] = {0.0, 0.0};  // p.Ap, ||r||^2 (adjacent scalar slots)
   while (!converged && it < opts->maxiter) {
@@ -189,7 +209,6 @@ extern "C" int grico_cg_solve(GricoPlan* P, GricoMultigrid* mg, const double* b,
     if (!std::isfinite(rr)) { status = GRICO_ERR_NONFINITE; set_error("CG residual is not finite"); break; }
     if (rr <= tol * tol) { converged = true; break; }
   }
-  if (exec) cudaGraphExecDestroy(exec);
   cudaEventRecord(e1, st);
   cudaEventSynchronize(e1);
   float ms = 0;

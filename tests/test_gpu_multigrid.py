@@ -172,3 +172,39 @@ def test_gmres_smoother_fp32_levels(cuda):
     z64 = build_multigrid(plan, GeometricMultigridPreconditioner(smoother="gmres")).vcycle(r)
     z32 = build_multigrid(plan, GeometricMultigridPreconditioner(smoother="gmres", precision="fp32")).vcycle(r)
     assert rel_err(z32, z64) <= 1e-4
+
+
+def test_kept_cg_graph_replays_across_solves(cuda):
+    """The iteration graph captured by one solve is kept on the plan and replayed by the next
+    solve with the same hierarchy, preconditioner and solution buffer; a new hierarchy or a
+    changed kernel choice captures a new one.  Every solve matches a direct-launch solve."""
+    import ctypes as C
+
+    from grico_b200 import _lib as L
+    from grico_b200.batched import set_tiles
+
+    D = 3
+    src = lambda x: np.prod(np.sin(np.pi * x), axis=1) * (1.0 + D * np.pi ** 2)
+    _, plan = _pair("3d_p2", source=src)
+    pre = GeometricMultigridPreconditioner(smoother="chebyshev")
+    mg = build_multigrid(plan, pre)
+    rng = np.random.default_rng(12)
+
+    def run(b, flags):
+        x = np.zeros(plan.n_reduced)
+        opts = L.GricoSolveOptions(1e-11, 0.0, 200, L.GRICO_PRECOND_MULTIGRID, 30, 0)
+        rep = L.GricoSolveReport()
+        L.check(L.lib().grico_cg_solve(plan.handle, mg.handle, L.ptr(b, C.c_double), L.ptr(x, C.c_double),
+                                       C.byref(opts), C.byref(rep), L.GRICO_FLAG_HOST_POINTERS | flags), "cg")
+        return x, rep.iterations
+
+    for step in range(4):
+        if step == 2:
+            set_tiles(plan, [1] * len(plan.batches))
+        if step == 3:
+            mg = build_multigrid(plan, pre)
+        b = rng.standard_normal(plan.n_reduced)
+        xg, ig = run(b, 0)
+        xd, id_ = run(b, L.GRICO_FLAG_NO_GRAPH)
+        assert ig == id_
+        assert rel_err(xg, xd) <= 1e-12
