@@ -8,7 +8,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "grico_b200", "libgrico_b200.so")
-SOURCES = ["host_space.cpp", "grico_plan.cu", "grico_solve.cu", "grico_mg.cu", "grico_cnn.cu", "grico_multi.cu"]
+SOURCES = ["host_space.cpp", "grico_plan.cu", "grico_solve.cu", "grico_mg.cu", "grico_cnn.cu", "grico_multi.cu", "grico_shard.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
          "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", "-shared", "-lcudart"]

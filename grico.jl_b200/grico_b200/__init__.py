@@ -20,3 +20,4 @@ from .regions import (FiniteCellExtension, ImplicitRegion, PhysicalDomain, Physi
 from .multigrid import GeometricMultigridPreconditioner
 from .nonlinear import ExpReaction, ResidualProblem, add_residual_accumulator, newton_solve
 from .nonlinear import compile as compile_residual
+from .sharded import ShardedOperator, ShardGroup, ShardPlan, sharded_cg

@@ -232,6 +232,14 @@ SIGNATURES = {
     "grico_grid_gather": (C.c_int, [P, C.c_int64, P, C.c_float, P, P]),
     "grico_grid_scatter_add": (C.c_int, [P, C.c_int64, P, C.c_float, P, P]),
     "grico_weighted_residual": (C.c_int, [P, P, P, P, C.c_int64, P, P, P]),
+    "grico_halo_pack": (C.c_int, [P, P, P, C.c_int64, P, C.c_int64, P]),
+    "grico_halo_unpack": (C.c_int, [P, P, P, C.c_int64, P, P]),
+    "grico_vec_dot": (C.c_int, [C.c_int64, P, P, P, P, P]),
+    "grico_vec_axpby": (C.c_int, [C.c_int64, C.c_double, P, C.c_double, P, P]),
+    "grico_vec_invert": (C.c_int, [C.c_int64, P, P, P]),
+    "grico_cg_update_xr": (C.c_int, [C.c_int64, C.c_int64, P, P, P, P, P, P, P]),
+    "grico_cg_precondition": (C.c_int, [C.c_int64, C.c_int64, P, P, P, P, P, P]),
+    "grico_cg_direction": (C.c_int, [C.c_int64, P, P, P, P]),
     "grico_last_error": (C.c_char_p, []),
 }
 

@@ -1,0 +1,398 @@
+"""Sharded plans: the cells of one compiled plan split over ranks, with the partition-surface
+halo sum of every apply.
+
+The reference runs in one shared-memory process (its backend seam, `src/common.jl:8-18`, has
+the single `_SharedMemoryCPUBackend`); here a job spread over several GPUs splits the cells.
+They are cut into contiguous ranges of the Morton order (the active-leaf order of
+`topology.jl:250-268`), balanced by the work of a cell, prod(p+1) * prod(q).  A rank compiles
+the plan of its cells over a local numbering of the dofs they touch.  A reduced dof touched by
+several ranks is shared: the lowest of them owns it, the others hold it as a ghost.  The local
+reduced vector lists owned dofs first and ghosts after them, so a sum over owned entries (a dot
+product) is a sum over a prefix.
+
+One sharded apply is the local reduced apply followed by the halo sum: each rank packs its
+contributions to the shared dofs into a buffer indexed by global halo slot, the buffers are
+summed over ranks (one all-reduce), and each rank unpacks the sums.  Vectors stay consistent:
+every rank holds the same value of a shared dof.  CG (`solve.jl:376-431`) then needs two more
+all-reduces per iteration: p.Ap, and (r.r, r.z) together.
+
+`ShardGroup` is the collective: `torch.distributed` across processes (NCCL between GPUs) and,
+for several shards held by one process, a sum over them first.
+"""
+from __future__ import annotations
+
+import copy
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _lib as L
+from .problem import AssemblyPlan, reduced_rhs
+
+
+def cell_ranks(plan, parts):
+    """Part of every active leaf (Morton position): contiguous ranges balanced by the per-cell
+    work prod(p+1) * prod(q); each leaf goes to the part holding the middle of its share."""
+    if parts < 1:
+        raise ValueError("parts must be positive")
+    space = plan.space
+    w = np.prod(space.degrees.astype(np.float64) + 1.0, axis=1) * np.prod(space.qshape.astype(np.float64), axis=1)
+    if len(w) < parts:
+        raise ValueError(f"{len(w)} cells cannot be split into {parts} parts")
+    c = np.cumsum(w)
+    mid = (c - 0.5 * w) / c[-1]
+    rank = np.minimum((mid * parts).astype(np.int64), parts - 1)
+    if np.unique(rank).size != parts:
+        raise ValueError(f"a part of the {parts}-way split holds no cell")
+    return rank.astype(np.int32)
+
+
+def _entry_dofs(b, sel):
+    """Full dofs touched by the cells `sel` of batch b: single-term entries and tail rows."""
+    nb = b.nbox
+    m = b.map_index.reshape(-1, nb)[sel].reshape(-1)
+    out = [m[m >= 0]]
+    if b.tail_offsets is not None:
+        k = -m[m <= -2] - 2
+        if k.size:
+            lo, hi = b.tail_offsets[k], b.tail_offsets[k + 1]
+            out.append(b.tail_index[np.concatenate([np.arange(a, z) for a, z in zip(lo, hi)])])
+    return np.concatenate(out)
+
+
+def _touched(plan, rank, r):
+    t = np.zeros(plan.n_full, dtype=bool)
+    for b in plan.batches:
+        sel = np.nonzero(rank[b.cells] == r)[0]
+        if sel.size:
+            t[_entry_dofs(b, sel)] = True
+    return t
+
+
+def _local_batch(b, sel, glob):
+    """Batch b restricted to its cells `sel`, map entries renumbered to local full dofs (glob:
+    sorted global ids of the local dofs) and tail rows renumbered in order of use."""
+    lb = copy.copy(b)
+    nb = b.nbox
+    lb.__dict__.pop("points", None)
+    lb.cells = b.cells[sel]
+    lb.leaves = b.leaves[sel]
+    lb.h = np.ascontiguousarray(b.h[sel])
+    lb.lower = b.lower[sel]
+    lb.kappa_points = None if b.kappa_points is None else np.ascontiguousarray(b.kappa_points[sel])
+    m = b.map_index.reshape(-1, nb)[sel].reshape(-1).copy()
+    single = m >= 0
+    m[single] = np.searchsorted(glob, m[single]).astype(np.int32)
+    lb.map_coef = None if b.map_coef is None else np.ascontiguousarray(b.map_coef.reshape(-1, nb)[sel].reshape(-1))
+    multi = np.nonzero(m <= -2)[0]
+    if multi.size:
+        k = -m[multi] - 2
+        lo, hi = b.tail_offsets[k], b.tail_offsets[k + 1]
+        cnt = hi - lo
+        src = np.concatenate([np.arange(a, z) for a, z in zip(lo, hi)])
+        lb.tail_offsets = np.concatenate([[0], np.cumsum(cnt)]).astype(np.int64)
+        lb.tail_index = np.searchsorted(glob, b.tail_index[src]).astype(np.int32)
+        lb.tail_coef = np.ascontiguousarray(b.tail_coef[src])
+        m[multi] = -(np.arange(multi.size, dtype=np.int32) + 2)
+    else:
+        lb.tail_offsets = lb.tail_index = lb.tail_coef = None
+    lb.map_index = np.ascontiguousarray(m.astype(np.int32))
+    return lb
+
+
+class ShardPlan:
+    """Rank r's share of `plan` split `parts` ways.
+
+    Attributes: `plan` (an AssemblyPlan over the local dofs: apply, rhs and diagonal work on it
+    unchanged), `n_owned` (owned reduced dofs: local reduced ids 0..n_owned-1), `global_reduced`
+    (global reduced id of every local reduced dof), `halo_local` / `halo_slot` (the local reduced
+    ids of shared dofs and their global halo slots) and `n_halo` (global halo slots)."""
+
+    def __init__(self, plan, rank, parts, device=True, cell_rank=None):
+        if plan.point_batches:
+            raise L.GricoError(L.GRICO_ERR_UNSUPPORTED_FORM, "sharded plans support tensor cells only")
+        if not 0 <= rank < parts:
+            raise ValueError("rank out of range")
+        self.rank, self.parts = int(rank), int(parts)
+        cr = cell_ranks(plan, parts) if cell_rank is None else cell_rank
+        self.cell_rank = cr
+        # ranks touching every full dof: how many, and the lowest
+        count = np.zeros(plan.n_full, dtype=np.int32)
+        first = np.full(plan.n_full, -1, dtype=np.int32)
+        mine = None
+        for r in range(parts):
+            t = _touched(plan, cr, r)
+            count += t
+            first[(first < 0) & t] = r
+            if r == rank:
+                mine = t
+        free = plan.reduced_index >= 0
+        shared = free & (count >= 2)
+        halo_global = np.nonzero(shared)[0]                      # full ids, sorted: slot order
+        self.n_halo = int(halo_global.size)
+        # local numbering
+        glob = np.nonzero(mine)[0]
+        lfree = free[glob]
+        owned = lfree & (first[glob] == rank)
+        ghost = lfree & ~owned
+        order = np.concatenate([np.nonzero(owned)[0], np.nonzero(ghost)[0]])   # local full ids
+        self.n_owned = int(owned.sum())
+        n_red = int(order.size)
+        red_of_local = np.full(glob.size, -1, dtype=np.int64)
+        red_of_local[order] = np.arange(n_red)
+        self.global_full = glob
+        self.global_reduced = plan.reduced_index[glob[order]]
+        sh = shared[glob[order]]
+        self.halo_local = np.ascontiguousarray(np.nonzero(sh)[0].astype(np.int32))
+        self.halo_slot = np.ascontiguousarray(np.searchsorted(halo_global, glob[order][sh]).astype(np.int32))
+        # the local plan: same problem and form, local cells and dofs
+        lp = object.__new__(AssemblyPlan)
+        lp.problem, lp.form, lp.space, lp.D = plan.problem, plan.form, plan.space, plan.D
+        lp.n_full = int(glob.size)
+        lp.n_cut = 0
+        lp.point_batches = []
+        lp.batches = []
+        for b in plan.batches:
+            sel = np.nonzero(cr[b.cells] == rank)[0]
+            if sel.size:
+                lp.batches.append(_local_batch(b, sel, glob))
+        fixed_local = np.nonzero(~lfree)[0]
+        lp.fixed_dofs = fixed_local.astype(np.int64)
+        lp.fixed_values = np.ascontiguousarray(plan.shift[glob[fixed_local]])
+        lp.solve_dofs = order.astype(np.int64)
+        lp.n_reduced = n_red
+        lp.reduced_index = red_of_local
+        lp.red_offsets = np.concatenate([[0], np.cumsum(lfree.astype(np.int64))]).astype(np.int64)
+        lp.red_index = np.ascontiguousarray(red_of_local[np.nonzero(lfree)[0]])
+        lp.red_coef = np.ones(n_red)
+        lp.shift = np.ascontiguousarray(plan.shift[glob])
+        lp.handle = None
+        if device:
+            lp._create_device_plan()
+        self.plan = lp
+
+    @property
+    def n_reduced(self):
+        return self.plan.n_reduced
+
+    def scatter(self, global_reduced_vector):
+        """This rank's local reduced vector from a global one."""
+        return np.ascontiguousarray(np.asarray(global_reduced_vector)[self.global_reduced])
+
+
+class ShardGroup:
+    """Sum over all shards of a job: first over the shards this process holds (a list; one in a
+    job with one process per GPU), then across processes with torch.distributed (`group`, or
+    the default group when it is initialised with more than one rank)."""
+
+    def __init__(self, group=None):
+        import torch.distributed as dist
+
+        self.group = group
+        self.dist = dist if dist.is_available() and dist.is_initialized() and dist.get_world_size(group) > 1 else None
+
+    def allreduce(self, views):
+        """Sum the same-shaped tensors `views` (one per local shard) over every shard of the job;
+        every view receives the sum."""
+        head = views[0]
+        for v in views[1:]:
+            head.add_(v)
+        if self.dist is not None:
+            self.dist.all_reduce(head, group=self.group)
+        for v in views[1:]:
+            v.copy_(head)
+
+
+def _ptr(t, offset=0):
+    return C.c_void_p(t.data_ptr() + 8 * offset)
+
+
+class _DeviceOps:
+    """The sharded path's device work: libgrico_b200 calls on torch CUDA tensors (FP64), all on
+    torch's current stream, so the collectives order behind them."""
+
+    def __init__(self):
+        import torch
+
+        from .problem import torch_stream_handle
+
+        self.torch = torch
+        self.stream = C.c_void_p(torch_stream_handle())
+
+    def vector(self, n):
+        return self.torch.zeros(max(int(n), 1), dtype=self.torch.float64, device="cuda")
+
+    def upload(self, a):
+        return self.torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64)).to("cuda")
+
+    def index(self, a):
+        return self.torch.as_tensor(np.ascontiguousarray(a, dtype=np.int32)).to("cuda")
+
+    def apply(self, shard, x, y):
+        L.check(L.lib().grico_reduced_apply(shard.plan.handle, _ptr(x), _ptr(y), 1, L.GRICO_PREC_FP64, 0,
+                                            self.stream), "sharded apply")
+
+    def pack(self, shard, idx, y, buf):
+        loc, slot = idx
+        L.check(L.lib().grico_halo_pack(_ptr(y), _ptr(loc), _ptr(slot), int(shard.halo_local.size), _ptr(buf),
+                                        int(shard.n_halo), self.stream), "halo pack")
+
+    def unpack(self, shard, idx, buf, y):
+        loc, slot = idx
+        L.check(L.lib().grico_halo_unpack(_ptr(y), _ptr(loc), _ptr(slot), int(shard.halo_local.size), _ptr(buf),
+                                          self.stream), "halo unpack")
+
+    def dot(self, n, x, y, out, slot, partial):
+        L.check(L.lib().grico_vec_dot(int(n), _ptr(x), _ptr(y), _ptr(out, slot), _ptr(partial), self.stream), "dot")
+
+    def diagonal(self, shard, d):
+        self.torch.cuda.current_stream().synchronize()
+        L.check(L.lib().grico_reduced_diagonal(shard.plan.handle, C.cast(_ptr(d), L.f64p), 0), "diagonal")
+
+    def invert(self, n, d, dinv):
+        L.check(L.lib().grico_vec_invert(int(n), _ptr(d), _ptr(dinv), self.stream), "Jacobi")
+
+    def update_xr(self, n, n_sum, x, r, p, q, s, partial):
+        L.check(L.lib().grico_cg_update_xr(int(n), int(n_sum), _ptr(x), _ptr(r), _ptr(p), _ptr(q), _ptr(s),
+                                           _ptr(partial), self.stream), "cg update")
+
+    def precondition(self, n, n_sum, dinv, r, z, s, partial):
+        L.check(L.lib().grico_cg_precondition(int(n), int(n_sum), None if dinv is None else _ptr(dinv), _ptr(r),
+                                              _ptr(z), _ptr(s), _ptr(partial), self.stream), "cg precondition")
+
+    def direction(self, n, p, z, s):
+        L.check(L.lib().grico_cg_direction(int(n), _ptr(p), _ptr(z), _ptr(s), self.stream), "cg direction")
+
+    def copy(self, src, dst):
+        L.check(L.lib().grico_vec_axpby(int(src.numel()), 1.0, _ptr(src), 0.0, _ptr(dst), self.stream), "copy")
+
+    def host(self, t):
+        return t.cpu().numpy()
+
+
+class ShardedOperator:
+    """The sharded reduced operator of the shards this process holds (one per process in a
+    multi-GPU job; several on one device to run a split on a single GPU)."""
+
+    def __init__(self, shards, group=None, ops=None):
+        self.shards = list(shards)
+        self.group = group or ShardGroup()
+        self.ops = ops or _DeviceOps()
+        o = self.ops
+        self._idx = [(o.index(s.halo_local), o.index(s.halo_slot)) for s in self.shards]
+        self._buf = [o.vector(s.n_halo) for s in self.shards]
+
+    def halo_sum(self, ys):
+        """Sum the shards' contributions to every shared dof; each shard's entries become the sums."""
+        o = self.ops
+        if self.shards[0].n_halo == 0:
+            return
+        for s, idx, y, buf in zip(self.shards, self._idx, ys, self._buf):
+            o.pack(s, idx, y, buf)
+        self.group.allreduce([b[: self.shards[0].n_halo] for b in self._buf])
+        for s, idx, y, buf in zip(self.shards, self._idx, ys, self._buf):
+            o.unpack(s, idx, buf, y)
+
+    def apply(self, xs, ys):
+        """ys[k] = (A x)_local of shard k, consistent on shared dofs."""
+        for s, x, y in zip(self.shards, xs, ys):
+            self.ops.apply(s, x, y)
+        self.halo_sum(ys)
+
+    def rhs(self):
+        """Local reduced right-hand sides, consistent on shared dofs."""
+        bs = [self.ops.upload(reduced_rhs(s.plan)) if s.n_reduced else self.ops.vector(0) for s in self.shards]
+        self.halo_sum(bs)
+        return bs
+
+    def inverse_diagonal(self):
+        o = self.ops
+        ds = [o.vector(s.n_reduced) for s in self.shards]
+        for s, d in zip(self.shards, ds):
+            o.diagonal(s, d)
+        self.halo_sum(ds)
+        out = [o.vector(s.n_reduced) for s in self.shards]
+        for s, d, di in zip(self.shards, ds, out):
+            o.invert(s.n_reduced, d, di)
+        return out
+
+
+class ShardedReport:
+    def __init__(self, iterations, status, initial_residual, final_residual):
+        self.iterations = iterations
+        self.status = status
+        self.initial_residual = initial_residual
+        self.final_residual = final_residual
+
+
+def sharded_cg(op, bs, relative_tolerance=None, absolute_tolerance=0.0, maxiter=1000, jacobi=True):
+    """Preconditioned CG on the sharded reduced system (solve.jl:376-431: stop when
+    ||r|| <= max(atol, rtol ||b||), Jacobi or identity preconditioner).  `bs`: consistent local
+    right-hand sides (ShardedOperator.rhs).  Returns (local solutions, report)."""
+    o = op.ops
+    shards = op.shards
+    rtol = math.sqrt(np.finfo(np.float64).eps) if relative_tolerance is None else float(relative_tolerance)
+    n = [s.n_reduced for s in shards]
+    no = [s.n_owned for s in shards]
+    dinv = op.inverse_diagonal() if jacobi else [None] * len(shards)
+    xs = [o.vector(k) for k in n]
+    rs = [o.vector(k) for k in n]
+    zs = [o.vector(k) for k in n]
+    ps = [o.vector(k) for k in n]
+    qs = [o.vector(k) for k in n]
+    ss = [o.vector(8) for _ in shards]      # rz, pAp, rr, rz_new, bb
+    part = [o.vector(592) for _ in shards]
+    for k in range(len(shards)):
+        o.copy(bs[k], rs[k])
+        o.dot(no[k], bs[k], bs[k], ss[k], 4, part[k])
+        o.precondition(n[k], no[k], dinv[k], rs[k], zs[k], ss[k], part[k])  # s3 = r.z
+        o.copy(zs[k], ps[k])
+    op.group.allreduce([s[3:5] for s in ss])                                  # r.z, b.b
+    for s in ss:
+        s[0:1].copy_(s[3:4])
+        s[2:3].copy_(s[4:5])                                                   # r = b: r.r = b.b
+    h = o.host(ss[0])
+    bnorm = math.sqrt(h[4])
+    tol = max(float(absolute_tolerance), rtol * bnorm)
+    rr = h[2]
+    init = math.sqrt(rr)
+    it = 0
+    status = L.GRICO_OK
+    converged = rr <= tol * tol
+    while not converged and it < maxiter:
+        it += 1
+        op.apply(ps, qs)
+        for k in range(len(shards)):
+            o.dot(no[k], ps[k], qs[k], ss[k], 1, part[k])
+        op.group.allreduce([s[1:2] for s in ss])                               # p.Ap
+        for k in range(len(shards)):
+            o.update_xr(n[k], no[k], xs[k], rs[k], ps[k], qs[k], ss[k], part[k])
+            o.precondition(n[k], no[k], dinv[k], rs[k], zs[k], ss[k], part[k])
+        op.group.allreduce([s[2:4] for s in ss])                               # r.r, r.z
+        h = o.host(ss[0])
+        pap, rr = h[1], h[2]
+        if not pap > 0.0:
+            status = L.GRICO_ERR_BREAKDOWN if math.isfinite(pap) else L.GRICO_ERR_NONFINITE
+            break
+        if not math.isfinite(rr):
+            status = L.GRICO_ERR_NONFINITE
+            break
+        if rr <= tol * tol:
+            converged = True
+            break
+        for k in range(len(shards)):
+            o.direction(n[k], ps[k], zs[k], ss[k])
+    if status == L.GRICO_OK and not converged:
+        status = L.GRICO_ERR_NOT_CONVERGED
+    return xs, ShardedReport(it, status, init, math.sqrt(rr) if math.isfinite(rr) else rr)
+
+
+def gather_reduced(shards, xs, n_reduced, ops=None):
+    """Global reduced vector from the owned entries of the shards (host arrays; for one process
+    holding every shard, or rank 0 after gathering)."""
+    out = np.zeros(n_reduced)
+    for s, x in zip(shards, xs):
+        hx = ops.host(x) if ops is not None else np.asarray(x)
+        out[s.global_reduced[: s.n_owned]] = hx[: s.n_owned]
+    return out

@@ -280,6 +280,35 @@ int grico_reduced_diagonal(GricoPlan* plan, double* diag, int flags);
 /* Reconstruct the full vector u = shift + P u_red (assembly.jl:965-970). */
 int grico_expand_reduced(GricoPlan* plan, const double* u_red, double* u_full, int flags);
 
+/* ---- sharded reduced solves (no reference counterpart: the reference runs in one process) ----
+ * A rank holds the plan of its cells with a local reduced numbering: the dofs it owns first,
+ * the ghost dofs it shares with other ranks after them.  All pointers are device pointers; the
+ * work is enqueued on `stream` (NULL = default stream) and nothing synchronises. */
+/* buf[0 .. n_slots) = 0, then buf[slot[i]] = y[local[i]] for i < n: the halo contribution of
+ * this rank, summed over ranks by the caller's collective */
+int grico_halo_pack(const double* y, const int32_t* local, const int32_t* slot, int64_t n, double* buf,
+                    int64_t n_slots, void* stream);
+/* y[local[i]] = buf[slot[i]] for i < n */
+int grico_halo_unpack(double* y, const int32_t* local, const int32_t* slot, int64_t n, const double* buf,
+                      void* stream);
+/* *out = sum_{i<n} x_i y_i (deterministic two-stage sum); partial: scratch of 592 doubles */
+int grico_vec_dot(int64_t n, const double* x, const double* y, double* out, double* partial, void* stream);
+/* y = a x + b y (y is not read when b == 0) */
+int grico_vec_axpby(int64_t n, double a, const double* x, double b, double* y, void* stream);
+/* dinv = 1 / d; synchronises `stream` and returns GRICO_ERR_NONFINITE if an entry of d is zero
+ * or not finite (solve.jl:740-748) */
+int grico_vec_invert(int64_t n, const double* d, double* dinv, void* stream);
+/* CG steps on device scalars s = scalars[0..3] = (r.z, p.Ap, r.r, r.z new) (solve.jl:376-431):
+ * update_xr: x += (s0/s1) p, r -= (s0/s1) q on n entries (nothing when s1 <= 0), s2 = sum of
+ *            r*r over the first n_sum entries;
+ * precondition: z = dinv .* r (dinv NULL: z = r), s3 = sum of r*z over the first n_sum entries;
+ * direction: p = z + (s3/s0) p, then s0 = s3. */
+int grico_cg_update_xr(int64_t n, int64_t n_sum, double* x, double* r, const double* p, const double* q,
+                       double* scalars, double* partial, void* stream);
+int grico_cg_precondition(int64_t n, int64_t n_sum, const double* dinv, const double* r, double* z, double* scalars,
+                          double* partial, void* stream);
+int grico_cg_direction(int64_t n, double* p, const double* z, double* scalars, void* stream);
+
 /* ---- Krylov solvers on the reduced system ---- */
 #define GRICO_PRECOND_IDENTITY 0
 #define GRICO_PRECOND_JACOBI 1
