@@ -25,6 +25,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <cmath>
 #include <vector>
 
 #include "cell_kernels.cuh"
@@ -199,6 +200,166 @@ inline size_t pipe_smem_bytes(int CPB, int bp, int sp, int elem) {
          size_t(2) * CPB * sp * elem;
 }
 
+// Even-odd form of the 1-D contractions.  Gauss points are mirrored (xi_{Q-1-q} = -xi_q), the
+// integrated Legendre modes k >= 2 have parity (-1)^k, the two vertex modes map onto each other
+// (psi_0(-x) = psi_1(x)), and the collocation derivative is centro-antisymmetric
+// (D[Q-1-q][Q-1-l] = -D[q][l]).  So a line splits into its symmetric and antisymmetric halves:
+// modes into the even set {psi_0 + psi_1 (as (psi_0+psi_1)/2 with coefficient c0 + c1),
+// psi_2, psi_4, ...} and the odd set {(psi_1-psi_0)/2 with coefficient c1 - c0, psi_3, ...};
+// points into sums and differences of mirrored pairs.  Each half is a contraction over half the
+// points, so an N x Q contraction costs about N*Q/2 FMAs plus Q adds, and its dependent chains
+// are half as long.  (Kopriva's even-odd decomposition; the reference contracts directly,
+// integration.jl:995-1136.)
+template <int N, int Q, typename T>
+struct TablesEO {
+  static constexpr int QH = (Q + 1) / 2;   // points of the left half, centre included
+  static constexpr int QL = Q / 2;         // mirrored pairs
+  static constexpr int NE = 1 + (N - 1) / 2;  // even modes: vertex sum, psi_2, psi_4, ...
+  static constexpr int NO = 1 + (N - 2) / 2;  // odd modes: vertex difference, psi_3, ...
+  T BE[NE * QH];  // BE[e*QH+q]: even mode e at point q (vertex sum: (psi_0 + psi_1) / 2)
+  T BO[NO * QL];  // BO[o*QL+q]: odd mode o at point q (vertex difference: (psi_1 - psi_0) / 2)
+  T DS[QL * QH];  // derivative rows q < QL on pair sums: (D[q][l] + D[q][Q-1-l]) / 2, centre D[q][c]
+  T DD[QH * QL];  // derivative rows q < QH on pair differences: (D[q][l] - D[q][Q-1-l]) / 2
+  T TS[QL * QH];  // the same for the transposed derivative D^T
+  T TD[QH * QL];
+};
+
+// Even-odd tables from the plain ones; false when the tables lack the symmetry (then the plain
+// contractions run).
+template <int N, int Q, typename T>
+bool make_eo_tables(const double* B, const double* D, TablesEO<N, Q, T>& t) {
+  using E = TablesEO<N, Q, T>;
+  constexpr int QH = E::QH, QL = E::QL;
+  double scale = 0.0;
+  for (int i = 0; i < N * Q; ++i) scale = std::max(scale, std::abs(B[i]));
+  for (int i = 0; i < Q * Q; ++i) scale = std::max(scale, std::abs(D[i]));
+  const double tol = 1e-13 * std::max(scale, 1.0);
+  for (int q = 0; q < Q; ++q) {
+    if (N < 2 || std::abs(B[0 * Q + Q - 1 - q] - B[1 * Q + q]) > tol) return false;
+    for (int k = 2; k < N; ++k)
+      if (std::abs(B[k * Q + Q - 1 - q] - ((k & 1) ? -1.0 : 1.0) * B[k * Q + q]) > tol) return false;
+    for (int l = 0; l < Q; ++l)
+      if (std::abs(D[(Q - 1 - q) * Q + Q - 1 - l] + D[q * Q + l]) > tol) return false;
+  }
+  for (int q = 0; q < QH; ++q) {
+    t.BE[q] = T(0.5 * (B[0 * Q + q] + B[1 * Q + q]));
+    for (int k = 2; k < N; k += 2) t.BE[(k / 2) * QH + q] = T(B[k * Q + q]);
+  }
+  for (int q = 0; q < QL; ++q) {
+    t.BO[q] = T(0.5 * (B[1 * Q + q] - B[0 * Q + q]));
+    for (int k = 3; k < N; k += 2) t.BO[((k - 1) / 2) * QL + q] = T(B[k * Q + q]);
+  }
+  auto split = [&](auto at, T* S, T* Dd) {
+    for (int q = 0; q < QL; ++q)
+      for (int l = 0; l < QH; ++l)
+        S[q * QH + l] = T(l < QL ? 0.5 * (at(q, l) + at(q, Q - 1 - l)) : at(q, l));
+    for (int q = 0; q < QH; ++q)
+      for (int l = 0; l < QL; ++l) Dd[q * QL + l] = T(0.5 * (at(q, l) - at(q, Q - 1 - l)));
+  };
+  split([&](int q, int l) { return D[q * Q + l]; }, t.DS, t.DD);
+  split([&](int q, int l) { return D[l * Q + q]; }, t.TS, t.TD);
+  return true;
+}
+
+// out[q] = sum_k psi_k(xi_q) in[k]
+template <int N, int Q, typename T>
+__device__ __forceinline__ void eo_interp(const TablesEO<N, Q, T>& t, const T (&in)[N], T (&out)[Q]) {
+  using E = TablesEO<N, Q, T>;
+  constexpr int QH = E::QH, QL = E::QL, NE = E::NE, NO = E::NO;
+  T ev[NE], od[NO];
+  ev[0] = in[0] + in[1];
+  od[0] = in[1] - in[0];
+#pragma unroll
+  for (int k = 2; k < N; ++k) {  // even k: ev[k/2]; odd k: od[(k-1)/2] (both in range for any k < N)
+    if (k & 1) od[(k - 1) / 2] = in[k];
+    else ev[k / 2] = in[k];
+  }
+  T e[QH];
+#pragma unroll
+  for (int q = 0; q < QH; ++q) {
+    T v = T(0);
+#pragma unroll
+    for (int i = 0; i < NE; ++i) v += t.BE[i * QH + q] * ev[i];
+    e[q] = v;
+  }
+#pragma unroll
+  for (int q = 0; q < QL; ++q) {
+    T v = T(0);
+#pragma unroll
+    for (int i = 0; i < NO; ++i) v += t.BO[i * QL + q] * od[i];
+    out[q] = e[q] + v;
+    out[Q - 1 - q] = e[q] - v;
+  }
+  if constexpr ((Q & 1) != 0) out[QL] = e[QL];
+}
+
+// out[k] = sum_q psi_k(xi_q) in[q]
+template <int N, int Q, typename T>
+__device__ __forceinline__ void eo_interp_t(const TablesEO<N, Q, T>& t, const T (&in)[Q], T (&out)[N]) {
+  using E = TablesEO<N, Q, T>;
+  constexpr int QH = E::QH, QL = E::QL, NE = E::NE, NO = E::NO;
+  T sm[QH], df[QL > 0 ? QL : 1];
+#pragma unroll
+  for (int q = 0; q < QL; ++q) {
+    sm[q] = in[q] + in[Q - 1 - q];
+    df[q] = in[q] - in[Q - 1 - q];
+  }
+  if constexpr ((Q & 1) != 0) sm[QL] = in[QL];
+  T ev[NE], od[NO];
+#pragma unroll
+  for (int i = 0; i < NE; ++i) {
+    T v = T(0);
+#pragma unroll
+    for (int q = 0; q < QH; ++q) v += t.BE[i * QH + q] * sm[q];
+    ev[i] = v;
+  }
+#pragma unroll
+  for (int i = 0; i < NO; ++i) {
+    T v = T(0);
+#pragma unroll
+    for (int q = 0; q < QL; ++q) v += t.BO[i * QL + q] * df[q];
+    od[i] = v;
+  }
+  out[0] = ev[0] - od[0];
+  out[1] = ev[0] + od[0];
+#pragma unroll
+  for (int k = 2; k < N; ++k) {
+    if (k & 1) out[k] = od[(k - 1) / 2];
+    else out[k] = ev[k / 2];
+  }
+}
+
+// out[q] = sum_l M[q][l] in[l] for the centro-antisymmetric M whose split tables are S, Dd
+// (M = D with t.DS, t.DD; M = D^T with t.TS, t.TD)
+template <int Q, typename T>
+__device__ __forceinline__ void eo_deriv(const T* S, const T* Dd, const T (&in)[Q], T (&out)[Q]) {
+  constexpr int QH = (Q + 1) / 2, QL = Q / 2;
+  T sm[QH], df[QL > 0 ? QL : 1];
+#pragma unroll
+  for (int l = 0; l < QL; ++l) {
+    sm[l] = in[l] + in[Q - 1 - l];
+    df[l] = in[l] - in[Q - 1 - l];
+  }
+  if constexpr ((Q & 1) != 0) sm[QL] = in[QL];
+  T b[QH];
+#pragma unroll
+  for (int q = 0; q < QH; ++q) {
+    T v = T(0);
+#pragma unroll
+    for (int l = 0; l < QL; ++l) v += Dd[q * QL + l] * df[l];
+    b[q] = v;
+  }
+#pragma unroll
+  for (int q = 0; q < QL; ++q) {
+    T a = T(0);
+#pragma unroll
+    for (int l = 0; l < QH; ++l) a += S[q * QH + l] * sm[l];
+    out[q] = b[q] + a;
+    out[Q - 1 - q] = b[q] - a;
+  }
+  if constexpr ((Q & 1) != 0) out[QL] = b[QL];
+}
+
 // Minimum resident blocks per SM asked of the compiler, from a register target per thread:
 // 128 for boxes of 5^3 points and more, 100 below.  Measured on the 5^3 FP64 apply (125
 // threads, real 64^3 map): 116 registers, 4 blocks per SM, 0.340 ms; 96 registers (capped),
@@ -209,10 +370,12 @@ constexpr int pipe_min_blocks(int threads, int q) {
              : 1;
 }
 
-template <int N, int Q, int CPB, typename T>
+// EO: the contractions in even-odd form (tables `eo`); otherwise directly on `tab`.
+template <int N, int Q, int CPB, typename T, bool EO>
 __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB, Q))
-    cell_apply_3d_pipe(BatchView b, const Tables1D<N, Q, T> tab, const LaneLines<Q * Q * CPB> lanes,
-                       const T* __restrict__ x, T* __restrict__ y, int64_t n_vec, T mass, T kappa) {
+    cell_apply_3d_pipe(BatchView b, const Tables1D<N, Q, T> tab, const TablesEO<N, Q, T> eo,
+                       const LaneLines<Q * Q * CPB> lanes, const T* __restrict__ x, T* __restrict__ y,
+                       int64_t n_vec, T mass, T kappa) {
   constexpr int Q2 = Q * Q;
   constexpr int Q3 = Q * Q * Q;
   constexpr int NB = N * N * N;
@@ -311,12 +474,18 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB, Q))
       T in[N];
 #pragma unroll
       for (int k = 0; k < N; ++k) in[k] = st[stZ + N * N * k];
+      if constexpr (EO) {
+        eo_interp(eo, in, out);
 #pragma unroll
-      for (int q = 0; q < Q; ++q) {
-        T v = T(0);
+        for (int q = 0; q < Q; ++q) work[baseZ + Q2 * q] = out[q];
+      } else {
 #pragma unroll
-        for (int k = 0; k < N; ++k) v += tab.B[k * Q + q] * in[k];
-        work[baseZ + Q2 * q] = v;
+        for (int q = 0; q < Q; ++q) {
+          T v = T(0);
+#pragma unroll
+          for (int k = 0; k < N; ++k) v += tab.B[k * Q + q] * in[k];
+          work[baseZ + Q2 * q] = v;
+        }
       }
     }
     // copies of the next group (stage s ^ 1 is free: every thread is past the previous group)
@@ -324,14 +493,21 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB, Q))
     __syncthreads();
     // 2. y interpolation on y-lines with x < N
     if (ymodes) {
+      if constexpr (EO) {
+        T in[N];
 #pragma unroll
-      for (int j = 0; j < N; ++j) line[j] = work[baseY + Q * j];
+        for (int j = 0; j < N; ++j) in[j] = work[baseY + Q * j];
+        eo_interp(eo, in, out);
+      } else {
 #pragma unroll
-      for (int q = 0; q < Q; ++q) {
-        T v = T(0);
+        for (int j = 0; j < N; ++j) line[j] = work[baseY + Q * j];
 #pragma unroll
-        for (int j = 0; j < N; ++j) v += tab.B[j * Q + q] * line[j];
-        out[q] = v;
+        for (int q = 0; q < Q; ++q) {
+          T v = T(0);
+#pragma unroll
+          for (int j = 0; j < N; ++j) v += tab.B[j * Q + q] * line[j];
+          out[q] = v;
+        }
       }
 #pragma unroll
       for (int q = 0; q < Q; ++q) work[baseY + Q * q] = out[q];
@@ -340,22 +516,35 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB, Q))
     // 3. x interpolation and x derivative on x-lines; flux scaling folded in
     {
       const T cx = fuse ? wX * kappa * T(scl[cX * 4 + 0]) : T(1);
+      if constexpr (EO) {
+        T in[N];
 #pragma unroll
-      for (int i = 0; i < N; ++i) line[i] = work[baseX + i];
+        for (int i = 0; i < N; ++i) in[i] = work[baseX + i];
+        eo_interp(eo, in, out);
+        eo_deriv<Q>(eo.DS, eo.DD, out, line);
 #pragma unroll
-      for (int q = 0; q < Q; ++q) {
-        T v = T(0);
+        for (int q = 0; q < Q; ++q) {
+          work[baseX + q] = out[q];
+          work[baseX + 2 * BP + q] = fuse ? line[q] * (cx * tab.W[q]) : line[q];
+        }
+      } else {
 #pragma unroll
-        for (int i = 0; i < N; ++i) v += tab.B[i * Q + q] * line[i];
-        out[q] = v;
-      }
+        for (int i = 0; i < N; ++i) line[i] = work[baseX + i];
 #pragma unroll
-      for (int q = 0; q < Q; ++q) {
-        T v = T(0);
+        for (int q = 0; q < Q; ++q) {
+          T v = T(0);
 #pragma unroll
-        for (int l = 0; l < Q; ++l) v += tab.D[q * Q + l] * out[l];
-        work[baseX + q] = out[q];
-        work[baseX + 2 * BP + q] = fuse ? v * (cx * tab.W[q]) : v;
+          for (int i = 0; i < N; ++i) v += tab.B[i * Q + q] * line[i];
+          out[q] = v;
+        }
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+          T v = T(0);
+#pragma unroll
+          for (int l = 0; l < Q; ++l) v += tab.D[q * Q + l] * out[l];
+          work[baseX + q] = out[q];
+          work[baseX + 2 * BP + q] = fuse ? v * (cx * tab.W[q]) : v;
+        }
       }
     }
     __syncthreads();
@@ -364,12 +553,18 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB, Q))
       const T cy = fuse ? wY * kappa * T(scl[cY * 4 + 1]) : T(1);
 #pragma unroll
       for (int l = 0; l < Q; ++l) line[l] = work[baseY + Q * l];
+      if constexpr (EO) {
+        eo_deriv<Q>(eo.DS, eo.DD, line, out);
 #pragma unroll
-      for (int q = 0; q < Q; ++q) {
-        T v = T(0);
+        for (int q = 0; q < Q; ++q) work[baseY + BP + Q * q] = fuse ? out[q] * (cy * tab.W[q]) : out[q];
+      } else {
 #pragma unroll
-        for (int l = 0; l < Q; ++l) v += tab.D[q * Q + l] * line[l];
-        work[baseY + BP + Q * q] = fuse ? v * (cy * tab.W[q]) : v;
+        for (int q = 0; q < Q; ++q) {
+          T v = T(0);
+#pragma unroll
+          for (int l = 0; l < Q; ++l) v += tab.D[q * Q + l] * line[l];
+          work[baseY + BP + Q * q] = fuse ? v * (cy * tab.W[q]) : v;
+        }
       }
     }
     __syncthreads();
@@ -381,12 +576,16 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB, Q))
       T u[Q], dz[Q];
 #pragma unroll
       for (int l = 0; l < Q; ++l) u[l] = work[baseZ + Q2 * l];
+      if constexpr (EO) {
+        eo_deriv<Q>(eo.DS, eo.DD, u, dz);
+      } else {
 #pragma unroll
-      for (int q = 0; q < Q; ++q) {
-        T v = T(0);
+        for (int q = 0; q < Q; ++q) {
+          T v = T(0);
 #pragma unroll
-        for (int l = 0; l < Q; ++l) v += tab.D[q * Q + l] * u[l];
-        dz[q] = v;
+          for (int l = 0; l < Q; ++l) v += tab.D[q * Q + l] * u[l];
+          dz[q] = v;
+        }
       }
 #pragma unroll
       for (int q = 0; q < Q; ++q) {
@@ -404,12 +603,18 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB, Q))
         }
         u[q] *= w * mass;
       }
+      if constexpr (EO) {
+        eo_deriv<Q>(eo.TS, eo.TD, dz, out);
 #pragma unroll
-      for (int l = 0; l < Q; ++l) {
-        T v = u[l];
+        for (int l = 0; l < Q; ++l) work[baseZ + Q2 * l] = u[l] + out[l];
+      } else {
 #pragma unroll
-        for (int q = 0; q < Q; ++q) v += tab.D[q * Q + l] * dz[q];
-        work[baseZ + Q2 * l] = v;
+        for (int l = 0; l < Q; ++l) {
+          T v = u[l];
+#pragma unroll
+          for (int q = 0; q < Q; ++q) v += tab.D[q * Q + l] * dz[q];
+          work[baseZ + Q2 * l] = v;
+        }
       }
     }
     __syncthreads();
@@ -417,12 +622,18 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB, Q))
     {
 #pragma unroll
       for (int q = 0; q < Q; ++q) line[q] = work[baseY + BP + Q * q];
+      if constexpr (EO) {
+        eo_deriv<Q>(eo.TS, eo.TD, line, out);
 #pragma unroll
-      for (int l = 0; l < Q; ++l) {
-        T v = work[baseY + Q * l];
+        for (int l = 0; l < Q; ++l) work[baseY + Q * l] += out[l];
+      } else {
 #pragma unroll
-        for (int q = 0; q < Q; ++q) v += tab.D[q * Q + l] * line[q];
-        work[baseY + Q * l] = v;
+        for (int l = 0; l < Q; ++l) {
+          T v = work[baseY + Q * l];
+#pragma unroll
+          for (int q = 0; q < Q; ++q) v += tab.D[q * Q + l] * line[q];
+          work[baseY + Q * l] = v;
+        }
       }
     }
     __syncthreads();
@@ -432,19 +643,29 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB, Q))
       for (int l = 0; l < Q; ++l) out[l] = work[baseX + l];
 #pragma unroll
       for (int q = 0; q < Q; ++q) line[q] = work[baseX + 2 * BP + q];
+      if constexpr (EO) {
+        T t[Q], m[N];
+        eo_deriv<Q>(eo.TS, eo.TD, line, t);
 #pragma unroll
-      for (int l = 0; l < Q; ++l) {
-        T v = out[l];
+        for (int l = 0; l < Q; ++l) out[l] += t[l];
+        eo_interp_t(eo, out, m);
 #pragma unroll
-        for (int q = 0; q < Q; ++q) v += tab.D[q * Q + l] * line[q];
-        out[l] = v;
-      }
+        for (int i = 0; i < N; ++i) work[baseX + i] = m[i];
+      } else {
 #pragma unroll
-      for (int i = 0; i < N; ++i) {
-        T v = T(0);
+        for (int l = 0; l < Q; ++l) {
+          T v = out[l];
 #pragma unroll
-        for (int q = 0; q < Q; ++q) v += tab.B[i * Q + q] * out[q];
-        work[baseX + i] = v;
+          for (int q = 0; q < Q; ++q) v += tab.D[q * Q + l] * line[q];
+          out[l] = v;
+        }
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+          T v = T(0);
+#pragma unroll
+          for (int q = 0; q < Q; ++q) v += tab.B[i * Q + q] * out[q];
+          work[baseX + i] = v;
+        }
       }
     }
     __syncthreads();
@@ -452,12 +673,19 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB, Q))
     if (ymodes) {
 #pragma unroll
       for (int q = 0; q < Q; ++q) line[q] = work[baseY + Q * q];
+      if constexpr (EO) {
+        T m[N];
+        eo_interp_t(eo, line, m);
 #pragma unroll
-      for (int j = 0; j < N; ++j) {
-        T v = T(0);
+        for (int j = 0; j < N; ++j) work[baseY + Q * j] = m[j];
+      } else {
 #pragma unroll
-        for (int q = 0; q < Q; ++q) v += tab.B[j * Q + q] * line[q];
-        work[baseY + Q * j] = v;
+        for (int j = 0; j < N; ++j) {
+          T v = T(0);
+#pragma unroll
+          for (int q = 0; q < Q; ++q) v += tab.B[j * Q + q] * line[q];
+          work[baseY + Q * j] = v;
+        }
       }
     }
     __syncthreads();
@@ -470,15 +698,25 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB, Q))
       const int* sm = smap + s * CPB * SP + stZ;
 #pragma unroll
       for (int q = 0; q < Q; ++q) line[q] = work[baseZ + Q2 * q];
-      // kept rolled: unrolled, the compiler hoists every map load and output at once and spills
-      // (5^3 FP64: 0.37 ms rolled vs 0.50 ms unrolled)
-#pragma unroll 1
-      for (int k = 0; k < N; ++k) {
-        T v = T(0);
+      if constexpr (EO) {
+        T m[N];
+        eo_interp_t(eo, line, m);
 #pragma unroll
-        for (int q = 0; q < Q; ++q) v += tab.B[k * Q + q] * line[q];
-        const int dof = sm[N * N * k];
-        if (dof >= 0) atomicAdd(y + dof, v);
+        for (int k = 0; k < N; ++k) {
+          const int dof = sm[N * N * k];
+          if (dof >= 0) atomicAdd(y + dof, m[k]);
+        }
+      } else {
+        // kept rolled: unrolled, the compiler hoists every map load and output at once and
+        // spills (5^3 FP64: 0.37 ms rolled vs 0.50 ms unrolled)
+#pragma unroll 1
+        for (int k = 0; k < N; ++k) {
+          T v = T(0);
+#pragma unroll
+          for (int q = 0; q < Q; ++q) v += tab.B[k * Q + q] * line[q];
+          const int dof = sm[N * N * k];
+          if (dof >= 0) atomicAdd(y + dof, v);
+        }
       }
     }
   }

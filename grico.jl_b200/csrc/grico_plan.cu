@@ -139,15 +139,20 @@ Tables1D<N, Q, T> make_tables(const DevBatch& b) {
   return t;
 }
 
-// Default 3-D kernel variant by points per axis, from a sweep of all variants on uniform
-// 16-million-dof grids (B200, one apply, degrees 1..7 with q = p + 1, FP64 ms of the best
-// variant vs the one-block-per-group default): the pipelined kernel wins at every q — half-size
-// groups (3) for q = 2, 3, 5 (p = 4: 0.367 vs 0.495 ms), default-size groups (4) for q = 4 and
-// q >= 6 (p = 3: 0.374 vs 0.710 ms; p = 7: 0.500 vs 0.843 ms); in FP32 the one-block-per-group
-// kernel with half-size groups stays fastest for q = 2.
+// Default 3-D kernel variant by points per axis.  A sweep of all variants on uniform
+// 16-million-dof grids (B200, one apply, degrees 1..7 with q = p + 1) found the pipelined kernel
+// fastest at every q (p = 4: 0.367 vs 0.495 ms for the one-block-per-group kernel; p = 3: 0.374
+// vs 0.710 ms; p = 7: 0.500 vs 0.843 ms), with half-size groups for q = 2, 3, 5 and default-size
+// groups for q = 4 and q >= 6; in FP32 the one-block-per-group kernel with half-size groups stays
+// fastest for q = 2.  A second sweep (4-million-dof grids, q = p + 1 and p + 2, ms per apply)
+// compared its even-odd and direct contractions: even-odd wins by 7 % at q = 5 (FP64 0.095 vs
+// 0.102), 12-20 % at q = 6, 7 and 1.5-1.8x at q = 8, 9; at q = 4 the direct form with
+// default-size groups is 4 % faster in FP64 (0.108 vs 0.112), the even-odd form with half-size
+// groups in FP32.
 int default_tile_3d(int q, bool fp32) {
   if (fp32 && q <= 2) return 0;
-  return (q == 4 || q >= 6) ? 4 : 3;
+  if (q == 4) return fp32 ? 3 : 7;
+  return q >= 6 ? 4 : 3;
 }
 
 int sm_count() {
@@ -192,29 +197,36 @@ bool launch_fused(int dim, const DevBatch& bt, const BatchView& v, const T* x, T
     kern<<<grid, block, smem, st>>>(v, make_tables<NN, QQ, T>(bt), x, y, nvec, mass, kappa, mode, src);       \
     return true;                                                                                               \
   }
-#define GRICO_L3_PIPE(NN, QQ, CPB_)                                                                            \
-  if (mode == 0 && v.coef == nullptr && v.tail_off == nullptr && v.mass_pts == nullptr) {                      \
+#define GRICO_L3_PIPE_EO(NN, QQ, CPB_, EO_)                                                                   \
+  {                                                                                                            \
     constexpr int CPB = CPB_;                                                                                  \
     constexpr int NT = QQ * QQ * CPB;                                                                          \
     static const LaneLines<NT> lanes = make_lane_lines<NT>(NN, QQ, CPB, int(sizeof(T)));                      \
     static const size_t smem = pipe_smem_bytes(CPB, lanes.bp, lanes.sp, int(sizeof(T)));                      \
-    auto kern = cell_apply_3d_pipe<NN, QQ, CPB, T>;                                                           \
+    auto kern = cell_apply_3d_pipe<NN, QQ, CPB, T, EO_>;                                                      \
     static const int per_sm = persistent_blocks_per_sm(reinterpret_cast<const void*>(kern), NT, smem);        \
     if (per_sm > 0) {                                                                                          \
       const int64_t groups = (int64_t(v.n_cells) + CPB - 1) / CPB;                                             \
       dim3 grid(unsigned(std::min<int64_t>(groups, int64_t(per_sm) * sm_count())), nrhs);                      \
-      kern<<<grid, NT, smem, st>>>(v, make_tables<NN, QQ, T>(bt), lanes, x, y, nvec, mass, kappa);             \
+      kern<<<grid, NT, smem, st>>>(v, make_tables<NN, QQ, T>(bt), eo, lanes, x, y, nvec, mass, kappa);         \
       return true;                                                                                             \
     }                                                                                                          \
+  }
+// variants 3-5: even-odd contractions (when the tables have the symmetry), 6-8: direct ones
+#define GRICO_L3_PIPE(NN, QQ, CPB_, WANT_EO)                                                                   \
+  if (mode == 0 && v.coef == nullptr && v.tail_off == nullptr && v.mass_pts == nullptr) {                      \
+    TablesEO<NN, QQ, T> eo{};                                                                                  \
+    if (WANT_EO && make_eo_tables<NN, QQ, T>(bt.hB.data(), bt.hD.data(), eo)) GRICO_L3_PIPE_EO(NN, QQ, CPB_, true) \
+    GRICO_L3_PIPE_EO(NN, QQ, CPB_, false)                                                                      \
   }
 #define GRICO_L3(NN, QQ)                                                                                       \
   if (N == NN && Q == QQ) {                                                                                    \
     constexpr int C1 = (256 / (QQ * QQ)) > 0 ? (256 / (QQ * QQ)) : 1;                                          \
     constexpr int C0 = C1 / 2 > 0 ? C1 / 2 : 1;                                                                \
     constexpr int C2 = (2 * C1 * QQ * QQ <= 1024) ? 2 * C1 : C1;                                               \
-    if (var == 3) GRICO_L3_PIPE(NN, QQ, C0)                                                                    \
-    if (var == 4) GRICO_L3_PIPE(NN, QQ, C1)                                                                    \
-    if (var == 5) GRICO_L3_PIPE(NN, QQ, C2)                                                                    \
+    if (var == 3 || var == 6) GRICO_L3_PIPE(NN, QQ, C0, var == 3)                                              \
+    if (var == 4 || var == 7) GRICO_L3_PIPE(NN, QQ, C1, var == 4)                                              \
+    if (var == 5 || var == 8) GRICO_L3_PIPE(NN, QQ, C2, var == 5)                                              \
     if (var % 3 == 0) GRICO_L3_CPB(NN, QQ, C0)                                                                 \
     if (var % 3 == 2) GRICO_L3_CPB(NN, QQ, C2)                                                                 \
     GRICO_L3_CPB(NN, QQ, C1)                                                                                   \
@@ -235,6 +247,7 @@ bool launch_fused(int dim, const DevBatch& bt, const BatchView& v, const T* x, T
   }
 #undef GRICO_L3
 #undef GRICO_L3_PIPE
+#undef GRICO_L3_PIPE_EO
 #undef GRICO_L3_CPB
 #undef GRICO_L2
   return false;

@@ -60,7 +60,7 @@ struct DevBuf {
   bool upload(const std::vector<T>& v) { return upload(v.data(), v.size()); }
 };
 
-constexpr int kTileVariants = 6;
+constexpr int kTileVariants = 9;
 
 struct DevMap {
   DevBuf map, coef, toff, tidx, tcoef;
@@ -79,7 +79,8 @@ struct DevBatch {
   std::vector<double> hB, hD, hW;  // axis-0 tables on the host (kernel parameters)
   int tile[2] = {1, 1};  // 3-D tensor-kernel variant per precision (0: FP64, 1: FP32): cells per block
                          // half (0), default (1) or double (2) the default, one block per cell group;
-                         // 3..5 the same sizes in the persistent cp.async-pipelined apply kernel;
+                         // 3..5 the same sizes in the persistent cp.async-pipelined apply kernel
+                         // with even-odd contractions, 6..8 that kernel with direct contractions;
                          // chosen by grico_plan_autotune or set by grico_plan_set_tiles
 };
 

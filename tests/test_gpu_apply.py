@@ -162,8 +162,9 @@ def test_cg_not_converged_status(cuda):
 
 @pytest.mark.parametrize("name", ["3d_p4", "3d_p2_hanging", "3d_p3_trunk", "3d_p1", "3d_p4_kappa"])
 def test_every_kernel_variant_matches_oracle(cuda, name):
-    """All six 3-D tensor-kernel variants (three cells-per-block sizes, one block per cell group
-    or the persistent pipelined kernel) against the oracle: mass + diffusion, hanging-node tails,
+    """All nine 3-D tensor-kernel variants (three cells-per-block sizes; one block per cell group,
+    or the persistent pipelined kernel with even-odd or direct contractions) against the oracle:
+    mass + diffusion, hanging-node tails,
     trunk (inactive) modes, tabulated coefficients; full and reduced layouts; 2 right-hand sides."""
     from grico_b200 import batched as bt
 
@@ -175,7 +176,9 @@ def test_every_kernel_variant_matches_oracle(cuda, name):
     xr = np.stack([sample_vector(plan.n_reduced, seed=s) for s in (7, 8)])
     ref_full = [oplan.apply(v) for v in xs]
     ref_red = [oplan.reduced_apply(v) for v in xr]
-    for var in range(6):
+    from grico_b200 import _lib as L
+
+    for var in range(L.TILE_VARIANTS):
         bt.set_tiles(plan, [var] * len(plan.batches))
         yf = gb.apply(plan, xs.reshape(-1), nrhs=2).reshape(2, -1)
         yr = gb.reduced_apply(plan, xr.reshape(-1), nrhs=2).reshape(2, -1)
@@ -228,3 +231,36 @@ def test_async_host_pointer_applies(cuda):
         s.synchronize()
     for k in range(3):
         assert rel_err(ys[k].numpy(), gb.apply(plan, xs[k].numpy())) <= TOL
+
+
+@pytest.mark.parametrize("p,extra", [(1, 1), (2, 1), (3, 1), (4, 1), (5, 1), (6, 1), (7, 1), (8, 1),
+                                     (1, 2), (2, 2), (3, 2), (4, 2)])
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_even_odd_pipelined_kernel_matches_oracle(cuda, p, extra, prec):
+    """The pipelined kernel with even-odd contractions (variants 3-5) and with direct ones
+    (6-8) on plain maps (uniform mesh, homogeneous Dirichlet, constant coefficients) against the
+    oracle's C tensor schedule, every isotropic shape q = p + 1 and q = p + 2."""
+    from grico_b200 import _lib as L
+    from grico_b200 import batched as bt
+    from sharded_cases import full_apply
+
+    d = gb.Domain((0.0, 0.0, 0.0), (1.0, 1.0, 1.0), (4, 4, 4))
+    gb.uniform_refine(d, 1)
+    s = gb.HpSpace(d, gb.SpaceOptions(basis=gb.FullTensorBasis(), degree=gb.UniformDegree(p),
+                                      quadrature=gb.DegreePlusQuadrature(extra)))
+    u = gb.ScalarField(s)
+    prob = gb.AffineProblem(u)
+    gb.add_cell_accumulator(prob, u, u, gb.MassDiffusion(0.7, 1.3))
+    for a in (1, 2, 3):
+        for side in (gb.LOWER, gb.UPPER):
+            gb.add_constraint(prob, gb.Dirichlet(u, gb.BoundaryFace(a, side), 0.0))
+    plan = gb.compile(prob)
+    x = sample_vector(plan.n_full, seed=3)
+    ref = full_apply(plan, x)
+    ref[plan.fixed_dofs] = x[plan.fixed_dofs]
+    xv = x.astype(np.float32) if prec == "fp32" else x
+    tol = 2e-5 if prec == "fp32" else TOL
+    for var in range(3, L.TILE_VARIANTS):
+        bt.set_tiles(plan, [var] * len(plan.batches), precision=prec)
+        y = gb.apply(plan, xv)
+        assert rel_err(y.astype(np.float64), ref) <= tol, var

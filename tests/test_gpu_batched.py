@@ -4,6 +4,7 @@ import numpy as np
 import pytest
 
 import grico_b200 as gb
+from grico_b200 import _lib as L
 from grico_b200 import batched as bt
 from cases import rel_err, sample_vector
 
@@ -56,7 +57,7 @@ def test_autotuned_tiles_keep_results(cuda):
     y0 = gb.apply(plan, x)
     for prec in ("fp64", "fp32"):
         chosen = bt.autotune(plan, nrhs=4, precision=prec, reps=3)
-        assert len(chosen) == len(plan.batches) and set(chosen.tolist()) <= set(range(6))
+        assert len(chosen) == len(plan.batches) and set(chosen.tolist()) <= set(range(L.TILE_VARIANTS))
     assert rel_err(gb.apply(plan, x), y0) <= 1e-12
     y32 = gb.apply(plan, x.astype(np.float32))
     assert rel_err(y32, y0) <= 2e-5
