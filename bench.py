@@ -194,7 +194,7 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def solve_legs(gb, L, plan, prob, target=1e-8):
+def solve_legs(gb, L, plan, prob, target=1e-8, only=None):
     """Time to relative L2 error <= `target` on the same workload with f = 3 pi^2 prod sin(pi x_i)
     (exact u = prod sin): each method solves with ||r|| <= rtol ||b|| for rtol = 1e-6, 1e-7, ...
     and reports the first solve whose relative L2 error (verification.jl:297-304) meets the
@@ -210,15 +210,21 @@ def solve_legs(gb, L, plan, prob, target=1e-8):
     cheb = lambda deg, steps, prec="fp64": GeometricMultigridPreconditioner(
         smoother="chebyshev", chebyshev_degree=deg, pre_smoothing_steps=steps, post_smoothing_steps=steps,
         precision=prec)
+    # name: (short id, preconditioner, maxiter); every solve of a leg runs inside an NVTX range
+    # named by the short id (profilers filter on it)
     legs = {
-        "fp64_cg_gmg_jacobi_v22 (reference method)": (GeometricMultigridPreconditioner(), 2000),
-        "fp64_cg_gmg_chebyshev2_v22 (plain FP64 GPU, no CUDA graph)": (cheb(2, 2), 500),
-        "fp64_cg_gmg_chebyshev2_v22 (plain FP64 GPU)": (cheb(2, 2), 500),
-        "mixed_cg_fp64_gmg_chebyshev2_v22_fp32": (cheb(2, 2, "fp32"), 500),
-        "mixed_cg_fp64_gmg_chebyshev3_v22_fp32": (cheb(3, 2, "fp32"), 500),
+        "fp64_cg_gmg_jacobi_v22 (reference method)": ("ref_jacobi", GeometricMultigridPreconditioner(), 2000),
+        "fp64_cg_gmg_chebyshev2_v22 (plain FP64 GPU, no CUDA graph)": ("fp64_nograph", cheb(2, 2), 500),
+        "fp64_cg_gmg_chebyshev2_v22 (plain FP64 GPU)": ("fp64", cheb(2, 2), 500),
+        "mixed_cg_fp64_gmg_chebyshev2_v22_fp32": ("mixed2", cheb(2, 2, "fp32"), 500),
+        "mixed_cg_fp64_gmg_chebyshev3_v22_fp32": ("mixed3", cheb(3, 2, "fp32"), 500),
     }
+    import torch
+
     out = {}
-    for name, (opts, maxiter) in legs.items():
+    for name, (sid, opts, maxiter) in legs.items():
+        if only and sid not in only:
+            continue
         t0 = time.perf_counter()
         mg = build_multigrid(plan, opts)
         setup = time.perf_counter() - t0
@@ -238,8 +244,10 @@ def solve_legs(gb, L, plan, prob, target=1e-8):
             so = L.GricoSolveOptions(rtol, 0.0, maxiter, L.GRICO_PRECOND_MULTIGRID, 30, 0)
             rep = L.GricoSolveReport()
             flags = L.GRICO_FLAG_HOST_POINTERS | (L.GRICO_FLAG_NO_GRAPH if "no CUDA graph" in name else 0)
+            torch.cuda.nvtx.range_push(sid)
             rc = L.lib().grico_cg_solve(plan.handle, mg.handle, L.ptr(b, C.c_double), L.ptr(x, C.c_double),
                                         C.byref(so), C.byref(rep), flags)
+            torch.cuda.nvtx.range_pop()
             err = gb.relative_l2_error(gb.State(plan, gb.expand_reduced(plan, x), rep), exact)
             tries.append({"rtol": rtol, "status": int(rc), "iterations": int(rep.iterations),
                           "solve_seconds": float(rep.seconds), "relative_l2_error": err})
@@ -464,6 +472,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--soak", type=float, default=1.5, help="seconds of untimed load while clocks are sampled")
     ap.add_argument("--no-solve", action="store_true", help="skip the CG+GMG time-to-tolerance legs")
+    ap.add_argument("--solve-legs", default="", help="comma-separated short ids of the solve legs to run "
+                    "(ref_jacobi, fp64_nograph, fp64, mixed2, mixed3); default: all")
     ap.add_argument("--workload", default="poisson64",
                     choices=["poisson64", "fcm_shell64", "fcm_shell32", "grf_learned128", "grf_learned64",
                              "lshape_hp32"],
@@ -610,7 +620,7 @@ def main():
 
     solve_info = None
     if not args.no_solve:
-        solve_info = solve_legs(gb, L, plan, prob)
+        solve_info = solve_legs(gb, L, plan, prob, only=[v for v in args.solve_legs.split(",") if v])
 
     if rank == 0:
         peak, peak_kind = load_peaks()
