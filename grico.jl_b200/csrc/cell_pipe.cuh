@@ -370,7 +370,8 @@ constexpr int pipe_min_blocks(int threads, int q) {
              : 1;
 }
 
-// EO: the contractions in even-odd form (tables `eo`); otherwise directly on `tab`.
+// EO: the contractions in even-odd form (tables `eo`), constant coefficients only (the launch
+// sends batches with tabulated coefficients to EO = false); otherwise directly on `tab`.
 template <int N, int Q, int CPB, typename T, bool EO>
 __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB, Q))
     cell_apply_3d_pipe(BatchView b, const Tables1D<N, Q, T> tab, const TablesEO<N, Q, T> eo,
@@ -453,6 +454,10 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB, Q))
   issue(g, 0);
   load_map(g + G);
   T line[Q], out[Q];
+  // EO kernels serve constant coefficients only: the x- and y-fluxes stay in registers from
+  // the step that forms them (3, 4) to the step that reads them back (7, 6), on the same line
+  // of the same thread, instead of a round trip through shared memory
+  T fx[EO ? Q : 1], fy[EO ? Q : 1];
   for (int s = 0; g < n_groups; g += G, s ^= 1) {
     cp_async_wait<0>();
     // Staged modes, map entries and sizes of group g visible; every thread is past the previous
@@ -521,11 +526,11 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB, Q))
 #pragma unroll
         for (int i = 0; i < N; ++i) in[i] = work[baseX + i];
         eo_interp(eo, in, out);
-        eo_deriv<Q>(eo.DS, eo.DD, out, line);
+        eo_deriv<Q>(eo.DS, eo.DD, out, fx);
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
           work[baseX + q] = out[q];
-          work[baseX + 2 * BP + q] = fuse ? line[q] * (cx * tab.W[q]) : line[q];
+          fx[q] *= cx * tab.W[q];
         }
       } else {
 #pragma unroll
@@ -554,9 +559,9 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB, Q))
 #pragma unroll
       for (int l = 0; l < Q; ++l) line[l] = work[baseY + Q * l];
       if constexpr (EO) {
-        eo_deriv<Q>(eo.DS, eo.DD, line, out);
+        eo_deriv<Q>(eo.DS, eo.DD, line, fy);
 #pragma unroll
-        for (int q = 0; q < Q; ++q) work[baseY + BP + Q * q] = fuse ? out[q] * (cy * tab.W[q]) : out[q];
+        for (int q = 0; q < Q; ++q) fy[q] *= cy * tab.W[q];
       } else {
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
@@ -590,7 +595,7 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB, Q))
 #pragma unroll
       for (int q = 0; q < Q; ++q) {
         const T w = wz * tab.W[q];
-        if (fuse) {
+        if (EO || fuse) {
           dz[q] *= kz * tab.W[q];
         } else {
           const int64_t cell = g * CPB + cZ;
@@ -620,13 +625,13 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB, Q))
     __syncthreads();
     // 6. transposed y derivative on y-lines
     {
-#pragma unroll
-      for (int q = 0; q < Q; ++q) line[q] = work[baseY + BP + Q * q];
       if constexpr (EO) {
-        eo_deriv<Q>(eo.TS, eo.TD, line, out);
+        eo_deriv<Q>(eo.TS, eo.TD, fy, out);
 #pragma unroll
         for (int l = 0; l < Q; ++l) work[baseY + Q * l] += out[l];
       } else {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) line[q] = work[baseY + BP + Q * q];
 #pragma unroll
         for (int l = 0; l < Q; ++l) {
           T v = work[baseY + Q * l];
@@ -641,17 +646,17 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB, Q))
     {
 #pragma unroll
       for (int l = 0; l < Q; ++l) out[l] = work[baseX + l];
-#pragma unroll
-      for (int q = 0; q < Q; ++q) line[q] = work[baseX + 2 * BP + q];
       if constexpr (EO) {
         T t[Q], m[N];
-        eo_deriv<Q>(eo.TS, eo.TD, line, t);
+        eo_deriv<Q>(eo.TS, eo.TD, fx, t);
 #pragma unroll
         for (int l = 0; l < Q; ++l) out[l] += t[l];
         eo_interp_t(eo, out, m);
 #pragma unroll
         for (int i = 0; i < N; ++i) work[baseX + i] = m[i];
       } else {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) line[q] = work[baseX + 2 * BP + q];
 #pragma unroll
         for (int l = 0; l < Q; ++l) {
           T v = out[l];

@@ -142,17 +142,16 @@ Tables1D<N, Q, T> make_tables(const DevBatch& b) {
 // Default 3-D kernel variant by points per axis.  A sweep of all variants on uniform
 // 16-million-dof grids (B200, one apply, degrees 1..7 with q = p + 1) found the pipelined kernel
 // fastest at every q (p = 4: 0.367 vs 0.495 ms for the one-block-per-group kernel; p = 3: 0.374
-// vs 0.710 ms; p = 7: 0.500 vs 0.843 ms), with half-size groups for q = 2, 3, 5 and default-size
-// groups for q = 4 and q >= 6; in FP32 the one-block-per-group kernel with half-size groups stays
-// fastest for q = 2.  A second sweep (4-million-dof grids, q = p + 1 and p + 2, ms per apply)
-// compared its even-odd and direct contractions: even-odd wins by 7 % at q = 5 (FP64 0.095 vs
-// 0.102), 12-20 % at q = 6, 7 and 1.5-1.8x at q = 8, 9; at q = 4 the direct form with
-// default-size groups is 4 % faster in FP64 (0.108 vs 0.112), the even-odd form with half-size
-// groups in FP32.
+// vs 0.710 ms; p = 7: 0.500 vs 0.843 ms).  A second sweep (4-million-dof grids, q = p + 1 and
+// p + 2, ms per apply) compared its even-odd form (fluxes kept in registers) with the direct
+// one: even-odd wins at every shape, by 9-12 % at p = 1..4 and 1.3-1.7x at p = 6..8 in FP64
+// (p = 4, q = 5: 0.091 vs 0.102 ms; FP32 0.064 vs 0.073), and in FP32 it also beats the
+// one-block-per-group kernel at q = 2 (0.150 vs 0.159 ms).  Group sizes: half size (3) except
+// default size (4) for FP64 q = 4, 8 and FP32 q >= 6.
 int default_tile_3d(int q, bool fp32) {
-  if (fp32 && q <= 2) return 0;
-  if (q == 4) return fp32 ? 3 : 7;
-  return q >= 6 ? 4 : 3;
+  if (q <= 5) return (q == 4 && !fp32) ? 4 : 3;
+  if (fp32) return 4;
+  return q == 8 ? 4 : 3;
 }
 
 int sm_count() {
@@ -212,11 +211,13 @@ bool launch_fused(int dim, const DevBatch& bt, const BatchView& v, const T* x, T
       return true;                                                                                             \
     }                                                                                                          \
   }
-// variants 3-5: even-odd contractions (when the tables have the symmetry), 6-8: direct ones
+// variants 3-5: even-odd contractions (constant coefficients, tables with the symmetry), 6-8:
+// direct ones
 #define GRICO_L3_PIPE(NN, QQ, CPB_, WANT_EO)                                                                   \
   if (mode == 0 && v.coef == nullptr && v.tail_off == nullptr && v.mass_pts == nullptr) {                      \
     TablesEO<NN, QQ, T> eo{};                                                                                  \
-    if (WANT_EO && make_eo_tables<NN, QQ, T>(bt.hB.data(), bt.hD.data(), eo)) GRICO_L3_PIPE_EO(NN, QQ, CPB_, true) \
+    if (WANT_EO && v.kappa_pts == nullptr && make_eo_tables<NN, QQ, T>(bt.hB.data(), bt.hD.data(), eo))       \
+      GRICO_L3_PIPE_EO(NN, QQ, CPB_, true)                                                                     \
     GRICO_L3_PIPE_EO(NN, QQ, CPB_, false)                                                                      \
   }
 #define GRICO_L3(NN, QQ)                                                                                       \
