@@ -240,6 +240,11 @@ extern "C" int grico_cg_solve_multi(GricoPlan* P, const double* B, double* X, in
     set_error("cg multi: invalid options");
     return GRICO_ERR_INVALID;
   }
+  if (P->n_red == 0) {  // every dof fixed: solved before the first iteration
+    if (reports)
+      for (int r = 0; r < nrhs; ++r) reports[r] = GricoSolveReport{};
+    return GRICO_OK;
+  }
   cudaStream_t st = P->stream;
   const int64_t n = P->n_red;
   const int64_t nn = n * nrhs;

@@ -83,6 +83,17 @@ int prepare_jacobi(GricoPlan* P, cudaStream_t st) {
 
 using namespace grico;
 
+namespace {
+
+// An empty reduced system (every dof fixed) is solved before the first iteration: ||b|| = 0
+// meets the stopping rule of solve.jl:407-421 at once.
+int empty_system(GricoSolveReport* report) {
+  if (report) *report = GricoSolveReport{};
+  return GRICO_OK;
+}
+
+}  // namespace
+
 extern "C" int grico_cg_solve(GricoPlan* P, GricoMultigrid* mg, const double* b, double* x,
                               const GricoSolveOptions* opts, GricoSolveReport* report, int flags) {
   if (!P || !b || !x || !opts) { set_error("cg: invalid argument"); return GRICO_ERR_INVALID; }
@@ -94,6 +105,7 @@ extern "C" int grico_cg_solve(GricoPlan* P, GricoMultigrid* mg, const double* b,
   }
   if (opts->maxiter < 1) { set_error("maxiter must be positive"); return GRICO_ERR_INVALID; }
   if (!(opts->relative_tolerance >= 0) || !(opts->absolute_tolerance >= 0)) { set_error("tolerances must be non-negative"); return GRICO_ERR_INVALID; }
+  if (P->n_red == 0) return empty_system(report);
   cudaStream_t st = P->stream;
   const int64_t n = P->n_red;
   const size_t bytes = sizeof(double) * std::max<int64_t>(n, 1);
@@ -238,6 +250,7 @@ extern "C" int grico_fgmres_solve(GricoPlan* P, GricoMultigrid* mg, const double
   if (opts->restart < 1) { set_error("restart must be positive"); return GRICO_ERR_INVALID; }
   if (opts->maxiter < 1) { set_error("maxiter must be positive"); return GRICO_ERR_INVALID; }
   if (opts->preconditioner == GRICO_PRECOND_MULTIGRID && !mg) { set_error("fgmres: multigrid preconditioner missing"); return GRICO_ERR_INVALID; }
+  if (P->n_red == 0) return empty_system(report);
   cudaStream_t st = P->stream;
   const int64_t n = P->n_red;
   const int m = int(std::min<int64_t>(opts->restart, std::max<int64_t>(n, 1)));

@@ -264,3 +264,48 @@ def test_even_odd_pipelined_kernel_matches_oracle(cuda, p, extra, prec):
         bt.set_tiles(plan, [var] * len(plan.batches), precision=prec)
         y = gb.apply(plan, xv)
         assert rel_err(y.astype(np.float64), ref) <= tol, var
+
+
+@pytest.mark.parametrize("roots", [(1, 1, 1), (7, 1, 1), (3, 2, 2), (11, 3, 1)])
+@pytest.mark.parametrize("p", [2, 4])
+def test_pipelined_kernel_ragged_cell_groups(cuda, roots, p):
+    """Cell counts below one group and with a ragged last group (1, 7, 12, 33 cells; groups of
+    3..56 cells): every variant against the oracle's C tensor schedule, no constraints (every
+    map entry a dof)."""
+    from grico_b200 import _lib as L
+    from grico_b200 import batched as bt
+    from sharded_cases import full_apply
+
+    d = gb.Domain((0.0, 0.0, 0.0), (1.0, 0.5, 2.0), roots)
+    s = gb.HpSpace(d, gb.SpaceOptions(basis=gb.FullTensorBasis(), degree=gb.UniformDegree(p)))
+    u = gb.ScalarField(s)
+    prob = gb.AffineProblem(u)
+    gb.add_cell_accumulator(prob, u, u, gb.MassDiffusion(0.3, 1.1))
+    plan = gb.compile(prob)
+    x = sample_vector(plan.n_full, seed=21)
+    ref = full_apply(plan, x)
+    for prec, tol in (("fp64", TOL), ("fp32", 2e-5)):
+        xv = x.astype(np.float32) if prec == "fp32" else x
+        for var in range(L.TILE_VARIANTS):
+            bt.set_tiles(plan, [var] * len(plan.batches), precision=prec)
+            assert rel_err(gb.apply(plan, xv).astype(np.float64), ref) <= tol, (prec, var)
+
+
+def test_all_dofs_fixed(cuda):
+    """A single p=1 cell with Dirichlet data on every face: no free dof.  The reduced system is
+    empty; the full apply writes the constraint rows (y = x) and CG returns at once."""
+    d = gb.Domain((0.0, 0.0, 0.0), (1.0, 1.0, 1.0), (1, 1, 1))
+    s = gb.HpSpace(d, gb.SpaceOptions(basis=gb.FullTensorBasis(), degree=gb.UniformDegree(1)))
+    u = gb.ScalarField(s)
+    prob = gb.AffineProblem(u)
+    gb.add_cell_accumulator(prob, u, u, gb.Diffusion(1.0))
+    for a in (1, 2, 3):
+        for side in (gb.LOWER, gb.UPPER):
+            gb.add_constraint(prob, gb.Dirichlet(u, gb.BoundaryFace(a, side), 0.0))
+    plan = gb.compile(prob)
+    assert plan.n_reduced == 0 and plan.n_full == 8
+    x = sample_vector(8, seed=2)
+    assert np.array_equal(gb.apply(plan, x), x)
+    state = gb.solve(plan, solver=gb.CGSolver(gb.JacobiPreconditioner()))
+    assert state.report.iterations == 0
+    assert np.array_equal(state.coefficients, np.zeros(8))
