@@ -662,11 +662,20 @@ int run_apply(GricoPlan* P, bool reduced, const T* x, T* y, int nrhs, cudaStream
   const int64_t n = reduced ? P->n_red : P->n_full;
   if (nrhs < 1) return GRICO_ERR_INVALID;
   cudaMemsetAsync(y, 0, sizeof(T) * n * nrhs, st);
+  // several batches: round-robin over the branch streams (not while timing batches, whose
+  // event pairs need one stream)
+  const bool fork = P->n_branches > 1 && !P->time_batches;
+  if (fork) {
+    cudaEventRecord(P->fork_ev, st);
+    for (int k = 0; k < P->n_branches; ++k) cudaStreamWaitEvent(P->branch[k], P->fork_ev, 0);
+  }
+  int launched = 0;
+  auto stream_for = [&]() { return fork ? P->branch[launched++ % P->n_branches] : st; };
   for (size_t bi = 0; bi < P->batches.size(); ++bi) {
     GricoPlan::BatchEvent ev{int(bi), nullptr, nullptr};
     if (P->time_batches && cudaEventCreate(&ev.start) == cudaSuccess && cudaEventCreate(&ev.stop) == cudaSuccess)
       cudaEventRecord(ev.start, st);
-    launch_batch<T>(*P, P->batches[bi], reduced, x, y, n, 0, nullptr, nrhs, st);
+    launch_batch<T>(*P, P->batches[bi], reduced, x, y, n, 0, nullptr, nrhs, stream_for());
     if (ev.stop) {
       cudaEventRecord(ev.stop, st);
       P->batch_events.push_back(ev);
@@ -676,12 +685,17 @@ int run_apply(GricoPlan* P, bool reduced, const T* x, T* y, int nrhs, cudaStream
     GricoPlan::BatchEvent ev{int(P->batches.size() + pi), nullptr, nullptr};
     if (P->time_batches && cudaEventCreate(&ev.start) == cudaSuccess && cudaEventCreate(&ev.stop) == cudaSuccess)
       cudaEventRecord(ev.start, st);
-    launch_points<T>(*P, P->pbatches[pi], reduced, x, y, n, 0, nullptr, nrhs, st);
+    launch_points<T>(*P, P->pbatches[pi], reduced, x, y, n, 0, nullptr, nrhs, stream_for());
     if (ev.stop) {
       cudaEventRecord(ev.stop, st);
       P->batch_events.push_back(ev);
     }
   }
+  if (fork)
+    for (int k = 0; k < P->n_branches; ++k) {
+      cudaEventRecord(P->join_ev[k], P->branch[k]);
+      cudaStreamWaitEvent(st, P->join_ev[k], 0);
+    }
   if (!reduced && (P->n_fixed + P->n_rel) > 0) {
     dim3 grid(grid_for(P->n_fixed + P->n_rel), nrhs);
     constraint_action<T><<<grid, 256, 0, st>>>(P->fixed.get<int64_t>(), P->n_fixed, P->rel_piv.get<int64_t>(),
@@ -1073,6 +1087,26 @@ int grico_plan_create(const GricoPlanDesc* d, GricoPlan** out) {
   ok = ok && P->partial.alloc(sizeof(double) * (kRedBlocks + 8)) && P->scalars.alloc(sizeof(double) * 16);
   if (!ok) return GRICO_ERR_CUDA;
   if (!cuda_ok(cudaStreamSynchronize(P->stream), "plan upload")) return GRICO_ERR_CUDA;
+  const int n_launch = int(P->batches.size() + P->pbatches.size());
+  if (n_launch > 1) {
+    const int nbr = std::min(n_launch, int(GricoPlan::kBranches));
+    bool made = cudaEventCreateWithFlags(&P->fork_ev, cudaEventDisableTiming) == cudaSuccess;
+    int k = 0;
+    for (; made && k < nbr; ++k) {
+      if (cudaStreamCreateWithFlags(&P->branch[k], cudaStreamNonBlocking) != cudaSuccess) { made = false; break; }
+      if (cudaEventCreateWithFlags(&P->join_ev[k], cudaEventDisableTiming) != cudaSuccess) {
+        cudaStreamDestroy(P->branch[k]);
+        made = false;
+        break;
+      }
+    }
+    P->n_branches = k;  // streams and events made so far (destroyed with the plan)
+    if (!made) {
+      set_error("plan: branch streams");
+      grico_plan_destroy(P.release());
+      return GRICO_ERR_CUDA;
+    }
+  }
   *out = P.release();
   return GRICO_OK;
 }
@@ -1090,6 +1124,12 @@ int grico_plan_destroy(GricoPlan* P) {
       cudaEventDestroy(sl.done);
     }
   if (P->cg_exec) cudaGraphExecDestroy(P->cg_exec);
+  for (int k = 0; k < P->n_branches; ++k) {
+    cudaStreamSynchronize(P->branch[k]);
+    cudaStreamDestroy(P->branch[k]);
+    cudaEventDestroy(P->join_ev[k]);
+  }
+  if (P->fork_ev) cudaEventDestroy(P->fork_ev);
   cudaStream_t st = P->stream;
   delete P;
   cudaStreamDestroy(st);

@@ -138,6 +138,13 @@ struct GricoPlan {
   int cg_key_pc = -1;
   const void* cg_key_x = nullptr;
   uint64_t epoch = 1;
+  // The cell and point batches of one apply run concurrently on these streams, forked from and
+  // joined back to the launching stream (the scatter is atomic, so their order is free); made
+  // when the plan has more than one batch
+  static constexpr int kBranches = 4;
+  int n_branches = 0;
+  cudaStream_t branch[kBranches] = {};
+  cudaEvent_t fork_ev = nullptr, join_ev[kBranches] = {};
   // Krylov workspaces (allocated on first solve)
   grico::DevBuf w_r, w_z, w_p, w_q, w_x, w_b, w_dinv;
 };
