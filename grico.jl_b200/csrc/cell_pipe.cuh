@@ -74,17 +74,18 @@ __device__ __forceinline__ float keep_reg(float v) {
 enum LineShape { kLineX = 0, kLineY = 1, kLineZ = 2 };
 
 // Lane -> line table of one kernel shape: v[shape][lane] = cell | a << 7 | b << 11; bp = element
-// pitch between the three per-cell work buffers, sp = pitch between staged cells.
+// pitch of a per-cell work buffer, sp = pitch between staged cells, pz = pitch between the
+// z-planes of a cell's point box in the work buffer (Q*Q, or padded).
 template <int NT>
 struct LaneLines {
-  int bp, sp;
+  int bp, sp, pz;
   uint16_t v[3][NT];
 };
 
 namespace lanes_detail {
 
-inline int line_offset(int shape, int a, int b, int Q) {
-  return shape == kLineZ ? a + Q * b : shape == kLineY ? a + Q * Q * b : Q * a + Q * Q * b;
+inline int line_offset(int shape, int a, int b, int Q, int pz) {
+  return shape == kLineZ ? a + Q * b : shape == kLineY ? a + pz * b : Q * a + pz * b;
 }
 
 // Shared-memory wavefronts of one access step: lanes grouped in windows of W, each window
@@ -109,12 +110,12 @@ inline int window_cost(const std::vector<long>& addr, const std::vector<char>& a
 // Greedy assignment of all CPB*Q*Q lines of one shape to lanes: each window takes lines of
 // distinct residues, the residue with most lines left first.  Returns the assignment (line
 // ids c*Q*Q + a + Q*b) and its cost.
-inline int assign_shape(int shape, int Q, int CPB, int bp, int W, std::vector<int>& out) {
+inline int assign_shape(int shape, int Q, int pz, int CPB, int pitch, int W, std::vector<int>& out) {
   const int T = Q * Q, NT = T * CPB;
   std::vector<std::vector<int>> pool(W);
   for (int c = CPB - 1; c >= 0; --c)
     for (int t = T - 1; t >= 0; --t) {
-      const long a = long(3) * c * bp + line_offset(shape, t % Q, t / Q, Q);
+      const long a = long(c) * pitch + line_offset(shape, t % Q, t / Q, Q, pz);
       pool[size_t(a % W)].push_back(c * T + t);
     }
   out.assign(size_t(NT), 0);
@@ -141,23 +142,32 @@ inline int assign_shape(int shape, int Q, int CPB, int bp, int W, std::vector<in
 
 }  // namespace lanes_detail
 
-// Builds the lane tables for (N, Q, CPB) and element size `elem` (4 or 8 bytes): searches the
-// buffer pitch bp in [Q^3, Q^3 + 2W) and stage pitch sp in [N^3, N^3 + W) for the fewest
-// wavefronts (W = 128 / elem lanes per window).  v: [3][Q*Q*CPB].
-inline void build_lane_lines(int N, int Q, int CPB, int elem, int* bp_out, int* sp_out, uint16_t* v) {
+// Builds the lane tables for (N, Q, CPB) and element size `elem` (4 or 8 bytes) for the fewest
+// wavefronts (W = 128 / elem lanes per window): the stage pitch sp in [N^3, N^3 + W) and, with
+// three work buffers per cell (cell pitch 3 bp), the buffer pitch bp in [Q^3, Q^3 + 2W) at the
+// plain plane pitch pz = Q^2; with one work buffer per cell (`single`), also the plane pitch pz in
+// [Q^2, Q^2 + W), bp in [pz Q, pz Q + 2W).  The padded plane pitch spreads the cells' lines over
+// all banks where the plain box cannot: e.g. FP32 q = 4 / 5 / 8 need 12 / 13 / 24 wavefronts for
+// the three line shapes instead of 15 / 15 / 40.  The search takes 15-230 ms per shape on the
+// host, once per process.  v: [3][Q*Q*CPB].
+inline void build_lane_lines(int N, int Q, int CPB, int elem, bool single, int* bp_out, int* sp_out, int* pz_out,
+                             uint16_t* v) {
   using namespace lanes_detail;
   const int W = 128 / elem, T = Q * Q, NT = Q * Q * CPB;
   int best_cost = -1;
   std::vector<std::vector<int>> tmp(3), keep(3);
-  for (int bp = Q * Q * Q; bp < Q * Q * Q + 2 * W; ++bp) {
-    int cost = 0;
-    for (int s = 0; s < 3; ++s) cost += assign_shape(s, Q, CPB, bp, W, tmp[size_t(s)]);
-    if (best_cost < 0 || cost < best_cost) {
-      best_cost = cost;
-      *bp_out = bp;
-      keep = tmp;
+  const int pz_end = single ? Q * Q + W : Q * Q + 1;
+  for (int pz = Q * Q; pz < pz_end; ++pz)
+    for (int bp = pz * Q; bp < pz * Q + 2 * W; ++bp) {
+      int cost = 0;
+      for (int s = 0; s < 3; ++s) cost += assign_shape(s, Q, pz, CPB, single ? bp : 3 * bp, W, tmp[size_t(s)]);
+      if (best_cost < 0 || cost < best_cost) {
+        best_cost = cost;
+        *bp_out = bp;
+        *pz_out = pz;
+        keep = tmp;
+      }
     }
-  }
   // stage pitch: step 1 reads N staged modes along each active z-line
   const std::vector<int>& zl = keep[2];
   int best_sp = N * N * N, sp_cost = -1;
@@ -186,18 +196,19 @@ inline void build_lane_lines(int N, int Q, int CPB, int elem, int* bp_out, int* 
 }
 
 template <int NT>
-LaneLines<NT> make_lane_lines(int N, int Q, int CPB, int elem) {
+LaneLines<NT> make_lane_lines(int N, int Q, int CPB, int elem, bool single) {
   LaneLines<NT> L{};
-  build_lane_lines(N, Q, CPB, elem, &L.bp, &L.sp, &L.v[0][0]);
+  build_lane_lines(N, Q, CPB, elem, single, &L.bp, &L.sp, &L.pz, &L.v[0][0]);
   return L;
 }
 
 // Shared-memory bytes of cell_apply_3d_pipe: two stages of cell sizes (4 doubles per cell), the
-// per-cell flux scales (4 doubles), three work buffers of bp elements per cell, two stages of
-// sp staged modes per cell and two stages of sp staged map entries (int32) per cell.
-inline size_t pipe_smem_bytes(int CPB, int bp, int sp, int elem) {
-  return size_t(2) * CPB * 4 * 8 + size_t(CPB) * 4 * 8 + size_t(2) * CPB * sp * 4 + size_t(3) * CPB * bp * elem +
-         size_t(2) * CPB * sp * elem;
+// per-cell flux scales (4 doubles), nbuf work buffers of bp elements per cell (3, or 1 for the
+// even-odd kernel, whose fluxes live in registers), two stages of sp staged modes per cell and
+// two stages of sp staged map entries (int32) per cell.
+inline size_t pipe_smem_bytes(int CPB, int bp, int sp, int elem, int nbuf) {
+  return size_t(2) * CPB * 4 * 8 + size_t(CPB) * 4 * 8 + size_t(2) * CPB * sp * 4 +
+         size_t(nbuf) * CPB * bp * elem + size_t(2) * CPB * sp * elem;
 }
 
 // Even-odd form of the 1-D contractions.  Gauss points are mirrored (xi_{Q-1-q} = -xi_q), the
@@ -381,11 +392,15 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB, Q))
   constexpr int Q3 = Q * Q * Q;
   constexpr int NB = N * N * N;
   const int BP = lanes.bp, SP = lanes.sp;
+  // work buffers per cell and the z-plane pitch of a cell's point box in them: the even-odd
+  // kernel keeps one buffer per cell (its fluxes live in registers) at the searched pitch
+  constexpr int CM = EO ? 1 : 3;
+  const int PZ = EO ? lanes.pz : Q2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* hst = reinterpret_cast<double*>(smem_raw);   // [2][CPB][4] staged cell sizes
   double* scl = hst + 2 * CPB * 4;                      // [CPB][4] detJ sx^2, detJ sy^2, detJ sz^2, detJ
-  T* work = reinterpret_cast<T*>(scl + CPB * 4);        // [CPB][3][BP]
-  T* stage = work + 3 * CPB * BP;                       // [2][CPB][SP]
+  T* work = reinterpret_cast<T*>(scl + CPB * 4);        // [CPB][CM][BP]
+  T* stage = work + CM * CPB * BP;                      // [2][CPB][SP]
   int* smap = reinterpret_cast<int*>(stage + 2 * CPB * SP);  // [2][CPB][SP] staged map entries
   const int tid = threadIdx.x;
   x += blockIdx.y * n_vec;
@@ -406,9 +421,9 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB, Q))
     la[s] = (v >> 7) & 15;
     lb[s] = (v >> 11) & 15;
   }
-  const int baseX = keep_reg(3 * lc[kLineX] * BP + Q * la[kLineX] + Q2 * lb[kLineX]);  // x-line (y, z)
-  const int baseY = keep_reg(3 * lc[kLineY] * BP + la[kLineY] + Q2 * lb[kLineY]);      // y-line (x, z)
-  const int baseZ = keep_reg(3 * lc[kLineZ] * BP + la[kLineZ] + Q * lb[kLineZ]);       // z-line (x, y)
+  const int baseX = keep_reg(CM * lc[kLineX] * BP + Q * la[kLineX] + PZ * lb[kLineX]);  // x-line (y, z)
+  const int baseY = keep_reg(CM * lc[kLineY] * BP + la[kLineY] + PZ * lb[kLineY]);      // y-line (x, z)
+  const int baseZ = keep_reg(CM * lc[kLineZ] * BP + la[kLineZ] + Q * lb[kLineZ]);       // z-line (x, y)
   const int stZ = keep_reg(lc[kLineZ] * SP + la[kLineZ] + N * lb[kLineZ]);
   const int cX = keep_reg(lc[kLineX]), cY = keep_reg(lc[kLineY]), cZ = keep_reg(lc[kLineZ]);
   const int pZ = keep_reg(la[kLineZ] + Q * lb[kLineZ]);   // z-line's point offset in the cell box
@@ -482,14 +497,14 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB, Q))
       if constexpr (EO) {
         eo_interp(eo, in, out);
 #pragma unroll
-        for (int q = 0; q < Q; ++q) work[baseZ + Q2 * q] = out[q];
+        for (int q = 0; q < Q; ++q) work[baseZ + PZ * q] = out[q];
       } else {
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
           T v = T(0);
 #pragma unroll
           for (int k = 0; k < N; ++k) v += tab.B[k * Q + q] * in[k];
-          work[baseZ + Q2 * q] = v;
+          work[baseZ + PZ * q] = v;
         }
       }
     }
@@ -580,7 +595,7 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB, Q))
       const T kz = wZ * kappa * T(sc[2]);    // W_a W_b kappa detJ sz^2
       T u[Q], dz[Q];
 #pragma unroll
-      for (int l = 0; l < Q; ++l) u[l] = work[baseZ + Q2 * l];
+      for (int l = 0; l < Q; ++l) u[l] = work[baseZ + PZ * l];
       if constexpr (EO) {
         eo_deriv<Q>(eo.DS, eo.DD, u, dz);
       } else {
@@ -611,14 +626,14 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB, Q))
       if constexpr (EO) {
         eo_deriv<Q>(eo.TS, eo.TD, dz, out);
 #pragma unroll
-        for (int l = 0; l < Q; ++l) work[baseZ + Q2 * l] = u[l] + out[l];
+        for (int l = 0; l < Q; ++l) work[baseZ + PZ * l] = u[l] + out[l];
       } else {
 #pragma unroll
         for (int l = 0; l < Q; ++l) {
           T v = u[l];
 #pragma unroll
           for (int q = 0; q < Q; ++q) v += tab.D[q * Q + l] * dz[q];
-          work[baseZ + Q2 * l] = v;
+          work[baseZ + PZ * l] = v;
         }
       }
     }
@@ -702,7 +717,7 @@ __global__ void __launch_bounds__(Q* Q* CPB, pipe_min_blocks(Q* Q* CPB, Q))
     if (zmodes) {
       const int* sm = smap + s * CPB * SP + stZ;
 #pragma unroll
-      for (int q = 0; q < Q; ++q) line[q] = work[baseZ + Q2 * q];
+      for (int q = 0; q < Q; ++q) line[q] = work[baseZ + PZ * q];
       if constexpr (EO) {
         T m[N];
         eo_interp_t(eo, line, m);

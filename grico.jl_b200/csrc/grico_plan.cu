@@ -142,16 +142,16 @@ Tables1D<N, Q, T> make_tables(const DevBatch& b) {
 // Default 3-D kernel variant by points per axis.  A sweep of all variants on uniform
 // 16-million-dof grids (B200, one apply, degrees 1..7 with q = p + 1) found the pipelined kernel
 // fastest at every q (p = 4: 0.367 vs 0.495 ms for the one-block-per-group kernel; p = 3: 0.374
-// vs 0.710 ms; p = 7: 0.500 vs 0.843 ms).  A second sweep (4-million-dof grids, q = p + 1 and
-// p + 2, ms per apply) compared its even-odd form (fluxes kept in registers) with the direct
-// one: even-odd wins at every shape, by 9-12 % at p = 1..4 and 1.3-1.7x at p = 6..8 in FP64
-// (p = 4, q = 5: 0.091 vs 0.102 ms; FP32 0.064 vs 0.073), and in FP32 it also beats the
-// one-block-per-group kernel at q = 2 (0.150 vs 0.159 ms).  Group sizes: half size (3) except
-// default size (4) for FP64 q = 4, 8 and FP32 q >= 6.
+// vs 0.710 ms; p = 7: 0.500 vs 0.843 ms).  Later sweeps (4-million-dof grids, q = p + 1 and
+// p + 2, ms per apply) compared its even-odd form (fluxes in registers, one work buffer per cell
+// at a searched plane pitch) with the direct one: even-odd wins at every shape, by 10-25 % at
+// p = 1..4 and 1.3-1.9x at p = 6..8 in FP64 (p = 4, q = 5: 0.088 vs 0.102 ms; FP32 0.062 vs
+// 0.073), and in FP32 it also beats the one-block-per-group kernel at q = 2.  Group sizes: half
+// size (3) except default size (4) for FP64 q = 7 and FP32 q = 6, 7, 9.
 int default_tile_3d(int q, bool fp32) {
-  if (q <= 5) return (q == 4 && !fp32) ? 4 : 3;
-  if (fp32) return 4;
-  return q == 8 ? 4 : 3;
+  if (q <= 5) return 3;
+  if (fp32) return q == 8 ? 3 : 4;
+  return q == 7 ? 4 : 3;
 }
 
 int sm_count() {
@@ -200,8 +200,8 @@ bool launch_fused(int dim, const DevBatch& bt, const BatchView& v, const T* x, T
   {                                                                                                            \
     constexpr int CPB = CPB_;                                                                                  \
     constexpr int NT = QQ * QQ * CPB;                                                                          \
-    static const LaneLines<NT> lanes = make_lane_lines<NT>(NN, QQ, CPB, int(sizeof(T)));                      \
-    static const size_t smem = pipe_smem_bytes(CPB, lanes.bp, lanes.sp, int(sizeof(T)));                      \
+    static const LaneLines<NT> lanes = make_lane_lines<NT>(NN, QQ, CPB, int(sizeof(T)), EO_);                 \
+    static const size_t smem = pipe_smem_bytes(CPB, lanes.bp, lanes.sp, int(sizeof(T)), EO_ ? 1 : 3);         \
     auto kern = cell_apply_3d_pipe<NN, QQ, CPB, T, EO_>;                                                      \
     static const int per_sm = persistent_blocks_per_sm(reinterpret_cast<const void*>(kern), NT, smem);        \
     if (per_sm > 0) {                                                                                          \
