@@ -658,7 +658,11 @@ def main():
         if os.path.exists(tpath):
             for line in open(tpath):
                 if line.startswith("traffic_bytes_per_full_apply:") and not args.fp32:
-                    traffic = float(line.split(":", 1)[1])
+                    field = line.split(":", 1)[1].split()
+                    try:  # a summary without a capture of this launch says "null (why)"
+                        traffic = float(field[0]) if field else None
+                    except ValueError:
+                        traffic = None
         cpu = None
         if not args.no_cpu_baseline and world == 1 and not fcm:
             value, sec, threads, sample = cpu_reference_run(3, 1, budget_s=15.0)
