@@ -99,6 +99,30 @@ __global__ void copy_scalars(double* __restrict__ dst, const double* __restrict_
     if (active[s]) dst[s] = src[s];
 }
 
+// End of a lockstep iteration: count it for every active system and freeze the systems that met
+// ||r||^2 <= tol2 or broke down (the stopping test of solve.jl:407-421 and the direction check
+// of :414-416), on the device, so that several iterations run between two host reads.
+__global__ void multi_check(const double* __restrict__ pap, const double* __restrict__ rr,
+                            const double* __restrict__ tol2, int* __restrict__ active, int* __restrict__ iters,
+                            int* __restrict__ status, int nrhs) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nrhs || !active[s]) return;
+  iters[s] += 1;
+  const double a = pap[s];
+  if (!(a > 0.0)) {
+    status[s] = isfinite(a) ? GRICO_ERR_BREAKDOWN : GRICO_ERR_NONFINITE;
+    active[s] = 0;
+    return;
+  }
+  const double v = rr[s];
+  if (!isfinite(v)) {
+    status[s] = GRICO_ERR_NONFINITE;
+    active[s] = 0;
+  } else if (v <= tol2[s]) {
+    active[s] = 0;
+  }
+}
+
 template <typename S, typename D>
 __global__ void cast_copy(const S* __restrict__ x, D* __restrict__ y, int64_t n) {
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
@@ -132,10 +156,11 @@ int multi_cg(GricoPlan* P, const T* b, T* x, int nrhs, const std::vector<double>
              bool graph, cudaStream_t st, MultiResult& res) {
   const int64_t n = P->n_red;
   const int64_t nn = n * nrhs;
-  DevBuf rb, zb, pb, qb, sc, part, act;
+  DevBuf rb, zb, pb, qb, sc, part, act, tolb, itb, stb;
   if (!rb.alloc(sizeof(T) * nn) || !zb.alloc(sizeof(T) * nn) || !pb.alloc(sizeof(T) * nn) || !qb.alloc(sizeof(T) * nn) ||
       !sc.alloc(sizeof(double) * 4 * nrhs) || !part.alloc(sizeof(double) * nrhs * kMultiBlocks) ||
-      !act.alloc(sizeof(int) * nrhs))
+      !act.alloc(sizeof(int) * nrhs) || !tolb.alloc(sizeof(double) * nrhs) || !itb.alloc(sizeof(int) * nrhs) ||
+      !stb.alloc(sizeof(int) * nrhs))
     return GRICO_ERR_CUDA;
   T *r = rb.get<T>(), *z = zb.get<T>(), *p = pb.get<T>(), *q = qb.get<T>();
   double* rz = sc.get<double>();
@@ -168,6 +193,11 @@ int multi_cg(GricoPlan* P, const T* b, T* x, int nrhs, const std::vector<double>
     n_active += ha[s];
   }
   cudaMemcpyAsync(active, ha.data(), sizeof(int) * nrhs, cudaMemcpyHostToDevice, st);
+  int* d_iters = itb.get<int>();
+  int* d_status = stb.get<int>();
+  cudaMemcpyAsync(tolb.ptr, tol2.data(), sizeof(double) * nrhs, cudaMemcpyHostToDevice, st);
+  cudaMemsetAsync(d_iters, 0, sizeof(int) * nrhs, st);
+  cudaMemsetAsync(d_status, 0, sizeof(int) * nrhs, st);  // GRICO_OK
   auto iteration = [&](cudaStream_t s) -> int {
     int rc = run_apply<T>(P, true, p, q, nrhs, s);
     if (rc) return rc;
@@ -178,6 +208,7 @@ int multi_cg(GricoPlan* P, const T* b, T* x, int nrhs, const std::vector<double>
     dot(r, z, rz_new, s);
     multi_direction<T><<<vg, 256, 0, s>>>(p, z, rz_new, rz, active, n);
     copy_scalars<<<1, 64, 0, s>>>(rz, rz_new, active, nrhs);
+    multi_check<<<(nrhs + 63) / 64, 64, 0, s>>>(pap, rr, tolb.get<double>(), active, d_iters, d_status, nrhs);
     return GRICO_OK;
   };
   cudaGraphExec_t exec = nullptr;
@@ -191,33 +222,36 @@ int multi_cg(GricoPlan* P, const T* b, T* x, int nrhs, const std::vector<double>
     }
     (void)cudaGetLastError();
   }
+  // The device freezes converged systems itself (multi_check), so the host reads the flags only
+  // after a burst of iterations; a burst past the last convergence costs a few frozen
+  // iterations, never a changed result.
+  constexpr int kBurst = 8;
   int rc = GRICO_OK;
-  for (int it = 0; it < maxiter && n_active > 0; ++it) {
-    if (exec) {
-      if (cudaGraphLaunch(exec, st) != cudaSuccess) { rc = GRICO_ERR_CUDA; break; }
-    } else if ((rc = iteration(st)) != GRICO_OK) {
-      break;
-    }
-    cudaMemcpyAsync(h.data(), pap, sizeof(double) * 2 * nrhs, cudaMemcpyDeviceToHost, st);
-    cudaStreamSynchronize(st);
-    bool changed = false;
-    for (int s = 0; s < nrhs; ++s) {
-      if (!ha[s]) continue;
-      res.iters[s] += 1;
-      if (!(h[s] > 0.0)) {
-        res.status[s] = std::isfinite(h[s]) ? GRICO_ERR_BREAKDOWN : GRICO_ERR_NONFINITE;
+  std::vector<double> hrr(nrhs);
+  for (int it = 0; it < maxiter && n_active > 0;) {
+    const int k = std::min(kBurst, maxiter - it);
+    for (int j = 0; j < k && rc == GRICO_OK; ++j) {
+      if (exec) {
+        if (cudaGraphLaunch(exec, st) != cudaSuccess) rc = GRICO_ERR_CUDA;
       } else {
-        res.rr[s] = h[nrhs + s];
-        if (!std::isfinite(res.rr[s])) res.status[s] = GRICO_ERR_NONFINITE;
-        else if (res.rr[s] > tol2[s]) continue;
+        rc = iteration(st);
       }
-      ha[s] = 0;
-      --n_active;
-      changed = true;
     }
-    if (changed) cudaMemcpyAsync(active, ha.data(), sizeof(int) * nrhs, cudaMemcpyHostToDevice, st);
+    if (rc != GRICO_OK) break;
+    it += k;
+    cudaMemcpyAsync(ha.data(), active, sizeof(int) * nrhs, cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    n_active = 0;
+    for (int s = 0; s < nrhs; ++s) n_active += ha[s];
   }
   if (exec) cudaGraphExecDestroy(exec);
+  cudaMemcpyAsync(res.iters.data(), d_iters, sizeof(int) * nrhs, cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(res.status.data(), d_status, sizeof(int) * nrhs, cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(hrr.data(), rr, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(ha.data(), active, sizeof(int) * nrhs, cudaMemcpyDeviceToHost, st);
+  cudaStreamSynchronize(st);
+  for (int s = 0; s < nrhs; ++s)
+    if (res.iters[s] > 0) res.rr[s] = hrr[s];
   for (int s = 0; s < nrhs; ++s)
     if (ha[s] && res.status[s] == GRICO_OK) res.status[s] = GRICO_ERR_NOT_CONVERGED;
   if (!cuda_ok(cudaStreamSynchronize(st), "multi cg")) return GRICO_ERR_CUDA;
