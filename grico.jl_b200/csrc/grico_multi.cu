@@ -102,9 +102,12 @@ __global__ void copy_scalars(double* __restrict__ dst, const double* __restrict_
 // End of a lockstep iteration: count it for every active system and freeze the systems that met
 // ||r||^2 <= tol2 or broke down (the stopping test of solve.jl:407-421 and the direction check
 // of :414-416), on the device, so that several iterations run between two host reads.
+// last_rr keeps the squared residual norm of the last iteration that ended finite and with a
+// positive direction: after a breakdown (p.Ap <= 0) the update used alpha = r.z / p.Ap and rr no
+// longer describes a valid iterate, so the report keeps the value before it
 __global__ void multi_check(const double* __restrict__ pap, const double* __restrict__ rr,
                             const double* __restrict__ tol2, int* __restrict__ active, int* __restrict__ iters,
-                            int* __restrict__ status, int nrhs) {
+                            int* __restrict__ status, double* __restrict__ last_rr, int nrhs) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nrhs || !active[s]) return;
   iters[s] += 1;
@@ -118,9 +121,10 @@ __global__ void multi_check(const double* __restrict__ pap, const double* __rest
   if (!isfinite(v)) {
     status[s] = GRICO_ERR_NONFINITE;
     active[s] = 0;
-  } else if (v <= tol2[s]) {
-    active[s] = 0;
+    return;
   }
+  last_rr[s] = v;
+  if (v <= tol2[s]) active[s] = 0;
 }
 
 template <typename S, typename D>
@@ -158,7 +162,7 @@ int multi_cg(GricoPlan* P, const T* b, T* x, int nrhs, const std::vector<double>
   const int64_t nn = n * nrhs;
   DevBuf rb, zb, pb, qb, sc, part, act, tolb, itb, stb;
   if (!rb.alloc(sizeof(T) * nn) || !zb.alloc(sizeof(T) * nn) || !pb.alloc(sizeof(T) * nn) || !qb.alloc(sizeof(T) * nn) ||
-      !sc.alloc(sizeof(double) * 4 * nrhs) || !part.alloc(sizeof(double) * nrhs * kMultiBlocks) ||
+      !sc.alloc(sizeof(double) * 5 * nrhs) || !part.alloc(sizeof(double) * nrhs * kMultiBlocks) ||
       !act.alloc(sizeof(int) * nrhs) || !tolb.alloc(sizeof(double) * nrhs) || !itb.alloc(sizeof(int) * nrhs) ||
       !stb.alloc(sizeof(int) * nrhs))
     return GRICO_ERR_CUDA;
@@ -167,6 +171,7 @@ int multi_cg(GricoPlan* P, const T* b, T* x, int nrhs, const std::vector<double>
   double* rz_new = rz + nrhs;
   double* pap = rz + 2 * nrhs;
   double* rr = rz + 3 * nrhs;
+  double* last_rr = rz + 4 * nrhs;
   double* partial = part.get<double>();
   int* active = act.get<int>();
   const dim3 vg(gblocks(n), nrhs);
@@ -180,6 +185,7 @@ int multi_cg(GricoPlan* P, const T* b, T* x, int nrhs, const std::vector<double>
   cudaMemcpyAsync(p, z, sizeof(T) * nn, cudaMemcpyDeviceToDevice, st);
   dot(r, z, rz, st);
   dot(r, r, rr, st);
+  cudaMemcpyAsync(last_rr, rr, sizeof(double) * nrhs, cudaMemcpyDeviceToDevice, st);
   std::vector<double> h(2 * nrhs);
   std::vector<int> ha(nrhs, 1);
   cudaMemcpyAsync(h.data() + nrhs, rr, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st);
@@ -208,7 +214,8 @@ int multi_cg(GricoPlan* P, const T* b, T* x, int nrhs, const std::vector<double>
     dot(r, z, rz_new, s);
     multi_direction<T><<<vg, 256, 0, s>>>(p, z, rz_new, rz, active, n);
     copy_scalars<<<1, 64, 0, s>>>(rz, rz_new, active, nrhs);
-    multi_check<<<(nrhs + 63) / 64, 64, 0, s>>>(pap, rr, tolb.get<double>(), active, d_iters, d_status, nrhs);
+    multi_check<<<(nrhs + 63) / 64, 64, 0, s>>>(pap, rr, tolb.get<double>(), active, d_iters, d_status, last_rr,
+                                                 nrhs);
     return GRICO_OK;
   };
   cudaGraphExec_t exec = nullptr;
@@ -247,7 +254,7 @@ int multi_cg(GricoPlan* P, const T* b, T* x, int nrhs, const std::vector<double>
   if (exec) cudaGraphExecDestroy(exec);
   cudaMemcpyAsync(res.iters.data(), d_iters, sizeof(int) * nrhs, cudaMemcpyDeviceToHost, st);
   cudaMemcpyAsync(res.status.data(), d_status, sizeof(int) * nrhs, cudaMemcpyDeviceToHost, st);
-  cudaMemcpyAsync(hrr.data(), rr, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(hrr.data(), last_rr, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st);
   cudaMemcpyAsync(ha.data(), active, sizeof(int) * nrhs, cudaMemcpyDeviceToHost, st);
   cudaStreamSynchronize(st);
   for (int s = 0; s < nrhs; ++s)

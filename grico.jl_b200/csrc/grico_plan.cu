@@ -661,6 +661,8 @@ template <typename T>
 int run_apply(GricoPlan* P, bool reduced, const T* x, T* y, int nrhs, cudaStream_t st) {
   const int64_t n = reduced ? P->n_red : P->n_full;
   if (nrhs < 1) return GRICO_ERR_INVALID;
+  // the final check covers this call's launches only, not an error an earlier call left pending
+  (void)cudaGetLastError();
   cudaMemsetAsync(y, 0, sizeof(T) * n * nrhs, st);
   // several batches: round-robin over the branch streams (not while timing batches, whose
   // event pairs need one stream)
@@ -1439,6 +1441,8 @@ extern "C" int grico_reduced_rhs_static(GricoPlan* P, const double* const* sourc
               " full-layout dofs; the static scratch holds at most " + std::to_string(GRICO_STATIC_RHS_MAX_DOFS));
     return GRICO_ERR_INVALID;
   }
+  // a launch error left pending by an earlier, unrelated call would otherwise be reported below
+  (void)cudaGetLastError();
   double* scratch = nullptr;
   if (int rc = static_rhs_scratch(&scratch)) return rc;
   cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : P->stream;

@@ -233,6 +233,11 @@ class Multigrid:
     def level_sizes(self):
         return [p.n_reduced for p in self.plans]
 
+    def lambda_max(self, level):
+        """Power-iteration estimate of lambda_max(D^-1 A) on `level` (0 = coarsest) used by the
+        Chebyshev smoother; 0 when the smoother is not Chebyshev."""
+        return float(L.lib().grico_mg_lambda_max(self.handle, int(level)))
+
     def vcycle(self, r):
         r = np.ascontiguousarray(r, dtype=np.float64)
         z = np.zeros_like(r)

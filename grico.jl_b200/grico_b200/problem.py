@@ -508,19 +508,41 @@ class AssemblyPlan:
         self._build_interface_items(problem)
         # --- Dirichlet: fixed dofs are the dofs with a trace on a selected boundary face ---
         self._compile_dirichlet(problem)
-        # --- reduced map ---
+        # --- reduced map u_full = shift + P u_red (assembly.jl:112-314): free dofs are neither
+        # fixed nor relation pivots, numbered in dof order; a pivot's row expands its relation
+        # (whose dofs are free: fixed dofs were substituted before the relations were formed) ---
         free = np.ones(n_full, dtype=bool)
         free[self.fixed_dofs] = False
+        for (pivot, _, _, _) in self.relations:
+            free[pivot] = False
         self.solve_dofs = np.nonzero(free)[0]
         self.n_reduced = int(self.solve_dofs.size)
         reduced_index = np.full(n_full, -1, dtype=np.int64)
         reduced_index[self.solve_dofs] = np.arange(self.n_reduced)
         self.reduced_index = reduced_index
-        self.red_offsets = np.concatenate([[0], np.cumsum(free.astype(np.int64))]).astype(np.int64)
-        self.red_index = np.arange(self.n_reduced, dtype=np.int64)
-        self.red_coef = np.ones(self.n_reduced)
         self.shift = np.zeros(n_full)
         self.shift[self.fixed_dofs] = self.fixed_values
+        counts = free.astype(np.int64)
+        extra = {}
+        for (pivot, idx, co, rhs) in self.relations:
+            if np.any(reduced_index[idx] < 0):
+                raise ValueError("a Dirichlet relation couples to a constrained dof")
+            extra[pivot] = (reduced_index[idx], co)
+            counts[pivot] = idx.size
+            self.shift[pivot] = rhs
+        self.red_offsets = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+        if extra:
+            self.red_index = np.zeros(int(self.red_offsets[-1]), dtype=np.int64)
+            self.red_coef = np.ones(int(self.red_offsets[-1]))
+            self.red_index[self.red_offsets[self.solve_dofs]] = np.arange(self.n_reduced)
+            for pivot, (ri, co) in extra.items():
+                lo = self.red_offsets[pivot]
+                order = np.argsort(ri, kind="stable")
+                self.red_index[lo:lo + ri.size] = ri[order]
+                self.red_coef[lo:lo + ri.size] = co[order]
+        else:
+            self.red_index = np.arange(self.n_reduced, dtype=np.int64)
+            self.red_coef = np.ones(self.n_reduced)
         self.handle = None
         if device:
             self._create_device_plan()
@@ -760,14 +782,24 @@ class AssemblyPlan:
         return center[:, None, :] + ref[None, :, :] * half[:, None, :]
 
     def _compile_dirichlet(self, problem):
-        """Fixed dofs: every dof with a term on a mode of a selected boundary face; a vertex mode
-        with a single term takes the constraint's value (the last face in enumeration order wins
-        where faces with different values meet), every other fixed dof 0 (plans.jl:486-972 for
-        constant data).  Vectorised per (degrees, axis, side) group of boundary faces."""
+        """Dirichlet data as fixed dofs and affine relation rows (plans.jl:486-972).
+
+        The reference projects the data onto the trace space in L2: a Gram system over every
+        dof with a term on a selected boundary face, its rank from an eigen decomposition, pivot
+        dofs from QR with column pivoting and, for pivots that couple to free dofs, relation
+        rows x_p - sum c_j x_j = rhs (plans.jl:884-943).  Its row space is that of the trace
+        rows: one row per trace mode of each selected face, sum_t c_t x_{d_t} = target (the
+        constant on vertex modes, 0 on the others: a constant is exact in the trace basis).
+        Here a row with one term fixes its dof (target / coefficient; where faces with
+        different constants meet, the last face in enumeration order wins); rows with several
+        terms (hanging-node expansions on a Dirichlet face) have their fixed dofs substituted
+        and are solved per connected component by the reference's steps (`_dirichlet_system`).
+        Vectorised per (degrees, axis, side) group of boundary faces."""
         space = self.space
         D = self.D
         self.fixed_dofs = np.zeros(0, dtype=np.int64)
         self.fixed_values = np.zeros(0, dtype=np.float64)
+        self.relations = []
         if not problem.dirichlet:
             return
         b_leaf, b_axis, b_side = space.boundary_faces
@@ -781,7 +813,9 @@ class AssemblyPlan:
         b_axis = np.asarray(b_axis, dtype=np.int64)
         b_side = np.asarray(b_side, dtype=np.int64)
         face_ids = np.arange(len(b_leaf), dtype=np.int64)
-        dof_parts, val_parts, set_parts, order_parts = [], [], [], []
+        t_entry, t_dof, t_coef = [], [], []          # per term: row, dof, coefficient
+        e_target, e_cnt, e_order = [], [], []        # per row (face trace mode)
+        base = 0
         matched = set()
         degs = space.degrees[b_leaf] if len(b_leaf) else np.zeros((0, D), dtype=np.int64)
         for (ax, sd), val in sel.items():
@@ -803,33 +837,57 @@ class AssemblyPlan:
                 cnt = space.term_offsets[e + 1] - lo
                 rep = np.repeat(np.arange(e.size), cnt)
                 t = np.repeat(lo - np.concatenate([[0], np.cumsum(cnt)[:-1]]), cnt) + np.arange(int(cnt.sum()))
-                dof_parts.append(space.term_index[t].astype(np.int64))
-                single_vertex = np.tile(vertex, len(g))[rep] & (cnt[rep] == 1)
-                set_parts.append(single_vertex & (val != 0.0))
-                val_parts.append(np.full(rep.size, float(val)))
-                # enumeration order: boundary face, then mode, then term
-                face_of = np.repeat(g, len(modes))[rep]
-                order_parts.append(face_of * (1 << 32) + np.arange(rep.size, dtype=np.int64) % (1 << 32))
+                t_entry.append(base + rep)
+                t_dof.append(space.term_index[t].astype(np.int64))
+                t_coef.append(np.asarray(space.term_coef[t], dtype=np.float64))
+                e_target.append(np.where(np.tile(vertex, len(g)), float(val), 0.0))
+                e_cnt.append(cnt.astype(np.int64))
+                # enumeration order: boundary face, then mode
+                e_order.append(np.repeat(g, len(modes)) * (1 << 32) + np.tile(np.arange(len(modes)), len(g)))
+                base += e.size
         for key in sel:
             if key not in matched:
                 raise ValueError("Dirichlet constraint does not match any boundary face")
-        if not dof_parts:
+        if base == 0:
             return
-        dofs = np.concatenate(dof_parts)
-        setv = np.concatenate(set_parts)
-        vals = np.concatenate(val_parts)
-        order = np.concatenate(order_parts)
-        fixed = np.unique(dofs)
+        t_entry, t_dof, t_coef = np.concatenate(t_entry), np.concatenate(t_dof), np.concatenate(t_coef)
+        e_target, e_cnt, e_order = np.concatenate(e_target), np.concatenate(e_cnt), np.concatenate(e_order)
+        single_t = e_cnt[t_entry] == 1
+        fixed = np.unique(t_dof[single_t])
         values = np.zeros(fixed.size)
-        if setv.any():
-            sd_, sv, so = dofs[setv], vals[setv], order[setv]
+        sv_t = single_t & (e_target[t_entry] != 0.0)
+        if sv_t.any():
+            sd_ = t_dof[sv_t]
+            sv = e_target[t_entry[sv_t]] / t_coef[sv_t]
+            so = e_order[t_entry[sv_t]]
             last = np.lexsort((so, sd_))          # by dof, then enumeration order
             sd_, sv = sd_[last], sv[last]
             keep = np.ones(sd_.size, dtype=bool)
             keep[:-1] = sd_[1:] != sd_[:-1]        # last assignment per dof
             values[np.searchsorted(fixed, sd_[keep])] = sv[keep]
+        multi_t = ~single_t
+        rel = []
+        if multi_t.any():
+            fixed_val = np.zeros(self.n_full)
+            is_fixed = np.zeros(self.n_full, dtype=bool)
+            is_fixed[fixed] = True
+            fixed_val[fixed] = values
+            me, md, mc = t_entry[multi_t], t_dof[multi_t], t_coef[multi_t]
+            target = e_target.copy()
+            np.subtract.at(target, me[is_fixed[md]], mc[is_fixed[md]] * fixed_val[md[is_fixed[md]]])
+            keep = ~is_fixed[md]
+            me, md, mc = me[keep], md[keep], mc[keep]
+            if me.size:
+                n_involved = int(np.unique(np.concatenate([t_dof, md])).size)
+                fx, fv, rel = _dirichlet_components(me, md, mc, target, n_involved)
+                if fx.size:
+                    fixed = np.concatenate([fixed, fx])
+                    values = np.concatenate([values, fv])
+                    order = np.argsort(fixed, kind="stable")
+                    fixed, values = fixed[order], values[order]
         self.fixed_dofs = fixed.astype(np.int64)
         self.fixed_values = values
+        self.relations = sorted(rel, key=lambda r: r[0])
 
     def _create_device_plan(self):
         descs = (L.GricoCellBatchDesc * len(self.batches))()
@@ -894,7 +952,19 @@ class AssemblyPlan:
         pd.n_fixed = len(self.fixed_dofs)
         pd.fixed_dofs = L.ptr(self.fixed_dofs, C.c_int64)
         pd.fixed_values = L.ptr(self.fixed_values, C.c_double)
-        pd.n_relations = 0
+        rels = self.relations
+        pd.n_relations = len(rels)
+        if rels:
+            self._rel_pivot = np.array([r[0] for r in rels], dtype=np.int64)
+            self._rel_offsets = np.concatenate([[0], np.cumsum([r[1].size for r in rels])]).astype(np.int64)
+            self._rel_index = np.ascontiguousarray(np.concatenate([r[1] for r in rels]), dtype=np.int64)
+            self._rel_coef = np.ascontiguousarray(np.concatenate([r[2] for r in rels]), dtype=np.float64)
+            self._rel_rhs = np.array([r[3] for r in rels], dtype=np.float64)
+            pd.rel_pivot = L.ptr(self._rel_pivot, C.c_int64)
+            pd.rel_offsets = L.ptr(self._rel_offsets, C.c_int64)
+            pd.rel_index = L.ptr(self._rel_index, C.c_int64)
+            pd.rel_coef = L.ptr(self._rel_coef, C.c_double)
+            pd.rel_rhs = L.ptr(self._rel_rhs, C.c_double)
         pd.n_reduced = self.n_reduced
         pd.red_offsets = L.ptr(self.red_offsets, C.c_int64)
         pd.red_index = L.ptr(self.red_index, C.c_int64)
@@ -984,6 +1054,76 @@ def apply_(y, plan, x, nrhs=1):
 def reduced_apply(plan, x, nrhs=1):
     """_reduced_apply! (assembly.jl:905-915)."""
     return _vector_call(L.lib().grico_reduced_apply, plan, x, None, plan.n_reduced, nrhs)
+
+
+def _dirichlet_components(entry, dof, coef, target, n_involved):
+    """Fixed dofs and relation rows from the multi-term trace rows left after substituting the
+    fixed dofs: per connected component of the row-dof graph, the reference's steps on the
+    component's Gram matrix A^T A (same row space as its face-mass Gram matrix):
+    `_dirichlet_constraint_system` (plans.jl:951-972: symmetric eigen decomposition, rank with
+    tolerance 1000 eps max|lambda| n, consistency of the data, targets in the eigenbasis) and
+    `_dirichlet_relations` (plans.jl:884-943: QR with column pivoting picks the pivot dofs,
+    coupling -P^-1 C_free with entries above the tolerance; a pivot without coupling is fixed).
+    `n_involved` is the number of dofs of the whole projection system (the reference's
+    tolerance scales with it).  Returns (fixed dofs, values, [(pivot, dofs, coefs, rhs)])."""
+    import scipy.linalg as sla
+    from scipy.sparse import coo_matrix
+    from scipy.sparse.csgraph import connected_components
+
+    rows_u, row_inv = np.unique(entry, return_inverse=True)
+    dofs_u, dof_inv = np.unique(dof, return_inverse=True)
+    nr, nd = rows_u.size, dofs_u.size
+    graph = coo_matrix((np.ones(row_inv.size), (row_inv, nr + dof_inv)), shape=(nr + nd, nr + nd))
+    _, label = connected_components(graph, directed=False)
+    eps = np.finfo(np.float64).eps
+    fixed, values, rel = [], [], []
+    row_lab, dof_lab = label[:nr], label[nr:]
+    term_lab = row_lab[row_inv]
+    for comp in np.unique(dof_lab):
+        r_idx = np.nonzero(row_lab == comp)[0]
+        d_idx = np.nonzero(dof_lab == comp)[0]          # ascending dof order
+        rpos = np.full(nr, -1, dtype=np.int64)
+        rpos[r_idx] = np.arange(r_idx.size)
+        dpos = np.full(nd, -1, dtype=np.int64)
+        dpos[d_idx] = np.arange(d_idx.size)
+        sel = term_lab == comp
+        A = np.zeros((r_idx.size, d_idx.size))
+        np.add.at(A, (rpos[row_inv[sel]], dpos[dof_inv[sel]]), coef[sel])
+        b = target[rows_u[r_idx]]
+        G = A.T @ A
+        rhs = A.T @ b
+        evals, evecs = sla.eigh(G, driver="evr")
+        order = np.argsort(-evals, kind="stable")
+        evals, evecs = evals[order], evecs[:, order]
+        scale = float(np.max(np.abs(evals))) if evals.size else 0.0
+        tol = 0.0 if scale == 0.0 else 1000.0 * eps * scale * max(n_involved, 1)
+        count = int(np.sum(evals > tol))
+        transformed = evecs.T @ rhs
+        if np.any(np.abs(transformed[count:]) > tol * max(float(np.linalg.norm(rhs)), 1.0)):
+            raise ValueError("Dirichlet data is inconsistent on the selected boundary faces")
+        if count == 0:
+            continue
+        C = evecs[:, :count].T.copy()
+        targets = transformed[:count] / evals[:count]
+        _, _, perm = sla.qr(C, pivoting=True, mode="economic")
+        piv = perm[:count]
+        pmask = np.zeros(d_idx.size, dtype=bool)
+        pmask[piv] = True
+        free = np.nonzero(~pmask)[0]
+        P = C[:, piv]
+        shift = np.linalg.solve(P, targets)
+        coupling = -np.linalg.solve(P, C[:, free]) if free.size else np.zeros((count, 0))
+        gdofs = dofs_u[d_idx]
+        for k in range(count):
+            big = np.abs(coupling[k]) > tol
+            pivot = int(gdofs[piv[k]])
+            if not big.any():
+                fixed.append(pivot)
+                values.append(float(shift[k]))
+            else:
+                rel.append((pivot, gdofs[free[big]].astype(np.int64), coupling[k][big].astype(np.float64),
+                            float(shift[k])))
+    return np.array(fixed, dtype=np.int64), np.array(values, dtype=np.float64), rel
 
 
 def _source_points(plan, problem=None):

@@ -112,6 +112,9 @@ class ShardPlan:
     def __init__(self, plan, rank, parts, device=True, cell_rank=None):
         if plan.point_batches:
             raise L.GricoError(L.GRICO_ERR_UNSUPPORTED_FORM, "sharded plans support tensor cells only")
+        if getattr(plan, "relations", None):
+            raise L.GricoError(L.GRICO_ERR_UNSUPPORTED_FORM,
+                               "sharded plans need Dirichlet data that fixes single dofs (no relation rows)")
         if not 0 <= rank < parts:
             raise ValueError("rank out of range")
         self.rank, self.parts = int(rank), int(parts)

@@ -281,11 +281,17 @@ class Snapshot:
                 by_lower[a].setdefault(self.lower[l][a], []).append(l)
         self.boundary = []  # (leaf, axis(1-based), side)
         self.interfaces = []  # (minus, plus, axis(1-based))
+        # tree lookup over the active leaves and all their ancestors (topology.jl:1547-1566)
+        self.tree = {}
+        for l in self.leaves:
+            cur = l
+            while cur != NONE:
+                self.tree[(tuple(grid.level(cur, a) for a in range(D)), tuple(grid.coord(cur, a) for a in range(D)))] = cur
+                cur = grid.parent[cur]
         for l in self.leaves:
             for a in range(D):
                 for side in (LOWER, UPPER):
-                    coord = self.lower[l][a] if side == LOWER else self.upper[l][a]
-                    if coord == 0 or coord == self.extent[a]:
+                    if self.covering_neighbor(l, a, side) == NONE:
                         self.boundary.append((l, a + 1, side))
         for l in self.leaves:
             for a in range(D):
@@ -303,6 +309,31 @@ class Snapshot:
                 partners.sort(key=lambda o: tuple(0 if b == a else self.lower[o][b] for b in range(D)))
                 for o in partners:
                     self.interfaces.append((l, o, a + 1))
+
+
+    def covering_neighbor(self, cell, a, side):
+        """`_snapshot_covering_neighbor` (topology.jl:1590-1608, 1670-1677): the tree cell of the
+        same level tuple next to `cell` across side `side` of axis `a` (0-based) if the lookup
+        holds it; otherwise retry from the parent while `cell` touches the parent's boundary on
+        that side (always when the parent was split along another axis).  NONE: no covering
+        neighbour, so the face is a boundary face."""
+        grid = self.grid
+        D = grid.D
+        cur = cell
+        while True:
+            lev = tuple(grid.level(cur, b) for b in range(D))
+            crd = [grid.coord(cur, b) for b in range(D)]
+            crd[a] += -1 if side == LOWER else 1
+            if 0 <= crd[a] < (grid.root_counts[a] << lev[a]):
+                cand = self.tree.get((lev, tuple(crd)), NONE)
+                if cand != NONE:
+                    return cand
+            par = grid.parent[cur]
+            if par == NONE:
+                return NONE
+            if grid.split_axis[par] == a + 1 and (grid.coord(cur, a) & 1) != (0 if side == LOWER else 1):
+                return NONE
+            cur = par
 
 
 class Domain:
@@ -1269,6 +1300,126 @@ def cg_solve(apply_fn, b, precond=None, rtol=1e-10, atol=0.0, maxiter=10000):
     raise ValueError("CG did not converge")
 
 
+def fgmres_solve(apply_fn, b, precond=None, restart=30, rtol=1e-10, atol=0.0, maxiter=10000):
+    """Right-preconditioned flexible GMRES(restart) with modified Gram-Schmidt, restated from
+    `_fgmres_solve` (solve.jl:433-542): Givens rotations on each new Hessenberg column
+    (`_apply_previous_givens_rotations!`, `_givens_rotation`, `_apply_givens_rotation!`,
+    solve.jl:544-576), the cycle ends when |g[j+1]| <= tol or the Arnoldi norm is zero, and
+    `_finish_fgmres_cycle!` (solve.jl:578-589) back-substitutes (`_upper_triangular_solve!`,
+    solve.jl:591-614), adds Z y to x and recomputes the true residual b - A x.
+    Returns (x, total inner iterations)."""
+    n = len(b)
+    x = np.zeros(n)
+    r = np.array(b, dtype=np.float64, copy=True)
+    bnorm = math.sqrt(float(np.dot(b, b)))
+    tol = max(atol, rtol * bnorm)
+    if math.sqrt(float(np.dot(r, r))) <= tol:
+        return x, 0
+    m = min(restart, n)
+    total = 0
+
+    def finish(H, g, Z, count):
+        y = np.zeros(count)
+        for row in range(count - 1, -1, -1):
+            v = g[row]
+            for col in range(row + 1, count):
+                v -= H[row, col] * y[col]
+            d = H[row, row]
+            if not math.isfinite(d):
+                raise ValueError("FGMRES encountered a non-finite Krylov least-squares diagonal")
+            if d == 0.0:
+                raise ValueError("FGMRES encountered a singular Krylov least-squares problem")
+            y[row] = v / d
+        xn = x
+        for col in range(count):
+            if y[col] != 0.0:
+                xn = xn + y[col] * Z[:, col]
+        return xn, b - apply_fn(xn)
+
+    while total < maxiter:
+        V = np.zeros((n, m + 1))
+        Z = np.zeros((n, m))
+        H = np.zeros((m + 1, m))
+        g = np.zeros(m + 1)
+        cs = np.zeros(m)
+        sn = np.zeros(m)
+        beta = math.sqrt(float(np.dot(r, r)))
+        if beta <= tol:
+            return x, total
+        V[:, 0] = r / beta
+        g[0] = beta
+        inner_limit = min(m, maxiter - total)
+        inner = 0
+        updated = False
+        for j in range(inner_limit):
+            total += 1
+            inner = j + 1
+            Z[:, j] = precond(V[:, j]) if precond else V[:, j]
+            w = apply_fn(Z[:, j])
+            for i in range(j + 1):
+                H[i, j] = float(np.dot(w, V[:, i]))
+                w = w - H[i, j] * V[:, i]
+            nrm = math.sqrt(float(np.dot(w, w)))
+            H[j + 1, j] = nrm
+            if nrm > 0.0:
+                V[:, j + 1] = w / nrm
+            for i in range(j):
+                a, c = H[i, j], H[i + 1, j]
+                H[i, j] = cs[i] * a + sn[i] * c
+                H[i + 1, j] = -sn[i] * a + cs[i] * c
+            scale = math.hypot(H[j, j], H[j + 1, j])
+            cs[j], sn[j] = (1.0, 0.0) if scale == 0.0 else (H[j, j] / scale, H[j + 1, j] / scale)
+            a, c = H[j, j], H[j + 1, j]
+            H[j, j] = cs[j] * a + sn[j] * c
+            H[j + 1, j] = -sn[j] * a + cs[j] * c
+            a, c = g[j], g[j + 1]
+            g[j] = cs[j] * a + sn[j] * c
+            g[j + 1] = -sn[j] * a + cs[j] * c
+            if abs(g[j + 1]) <= tol or nrm == 0.0:
+                x, r = finish(H, g, Z, j + 1)
+                if math.sqrt(float(np.dot(r, r))) <= tol:
+                    return x, total
+                updated = True
+                break
+        if inner == 0:
+            raise ValueError("FGMRES failed to build a Krylov update")
+        if not updated:
+            x, r = finish(H, g, Z, inner)
+        if math.sqrt(float(np.dot(r, r))) <= tol:
+            return x, total
+    raise ValueError("FGMRES did not converge")
+
+
+def power_iteration_start(n, level):
+    """Start vector of the lambda_max(D^-1 A) estimate used for the Chebyshev smoother: a
+    xorshift64 stream seeded with 0x9e3779b97f4a7c15 + level, v_i = 0.5 + (s mod 1000003) /
+    1000003.  Project-defined (the reference has no Chebyshev smoother)."""
+    mask = (1 << 64) - 1
+    s = (0x9E3779B97F4A7C15 + level) & mask
+    v = np.empty(n)
+    for i in range(n):
+        s ^= (s << 13) & mask
+        s ^= s >> 7
+        s ^= (s << 17) & mask
+        v[i] = 0.5 + float(s % 1000003) / 1000003.0
+    return v
+
+
+def estimate_lambda_max(apply_fn, dinv, level, iterations=20):
+    """Power iteration on D^-1 A: x_0 from `power_iteration_start`, t = D^-1 A x,
+    lambda = ||t|| / ||x||, x = t / ||t||; 20 steps.  Project-defined estimate."""
+    x = power_iteration_start(len(dinv), level)
+    lam = 0.0
+    for _ in range(iterations):
+        t = dinv * apply_fn(x)
+        tn, xn = math.sqrt(float(np.dot(t, t))), math.sqrt(float(np.dot(x, x)))
+        if not (tn > 0.0 and xn > 0.0):
+            break
+        lam = tn / xn
+        x = t / tn
+    return lam
+
+
 def bratu_residual(plan: Plan, x_full, lam, source=None):
     """Full-layout residual of the accumulator of examples/nonlinear_bratu/driver.jl:39-45:
     value channel lam exp(u) - f, gradient channel kappa grad u, on every cell rule; constraint
@@ -1467,13 +1618,19 @@ def multigrid_transfer(coarse: Plan, fine: Plan):
 
 class Multigrid:
     """V-cycle with damped Jacobi smoothing and a dense Cholesky coarse solve
-    (multigrid.jl:858-956, common.jl:272-330)."""
+    (multigrid.jl:858-956, common.jl:272-330).  `smoother="chebyshev"` adds the project's
+    Chebyshev-Jacobi smoother (no reference counterpart): `chebyshev_degree` steps of the
+    Chebyshev semi-iteration for D^-1 A (Y. Saad, Iterative Methods for Sparse Linear Systems,
+    2nd ed., Algorithm 12.1) on [lambda_max / chebyshev_range, 1.2 lambda_max], lambda_max from
+    `estimate_lambda_max` on every level above the coarsest."""
 
-    def __init__(self, plans, pre=2, post=2, omega=0.8, smoother="jacobi", restart=8):
+    def __init__(self, plans, pre=2, post=2, omega=0.8, smoother="jacobi", restart=8, chebyshev_degree=2,
+                 chebyshev_range=15.0):
         self.plans = plans
         self.pre, self.post, self.omega = pre, post, omega
-        if smoother not in ("jacobi", "gmres"):
-            raise ValueError("smoother must be jacobi or gmres")
+        if smoother not in ("jacobi", "gmres", "chebyshev"):
+            raise ValueError("smoother must be jacobi, gmres or chebyshev")
+        self.chebyshev_degree, self.chebyshev_lower = chebyshev_degree, 1.0 / chebyshev_range
         if smoother == "gmres" and max(pre, post) > restart:
             raise ValueError("GMRES smoother requires restart >= max(pre, post)")  # multigrid.jl:352-358
         self.smoother, self.restart = smoother, restart
@@ -1493,11 +1650,40 @@ class Multigrid:
             e[j] = 1.0
             A0[:, j] = c.reduced_apply(e)
         self.L0 = np.linalg.cholesky(A0)
+        self.lmax = [0.0] * len(plans)
+        if smoother == "chebyshev":
+            for lv in range(1, len(plans)):
+                self.lmax[lv] = estimate_lambda_max(plans[lv].reduced_apply, self.dinv[lv], lv)
+
+    def smooth_chebyshev(self, level, x, b, steps):
+        """Saad's Algorithm 12.1 with the Jacobi preconditioner: theta, delta the centre and
+        half width of [lmin, lmax]; d_0 = D^-1 r / theta, d_k = rho_k rho_{k-1} d_{k-1} +
+        (2 rho_k / delta) D^-1 r, rho_k = 1 / (2 theta/delta - rho_{k-1}); x += d_k."""
+        p = self.plans[level]
+        lmax = 1.2 * self.lmax[level]
+        lmin = lmax * self.chebyshev_lower
+        theta, delta = 0.5 * (lmax + lmin), 0.5 * (lmax - lmin)
+        sigma = theta / delta
+        d = np.zeros_like(x)
+        for _ in range(steps):
+            rho_old = 1.0 / sigma
+            for k in range(self.chebyshev_degree):
+                z = self.dinv[level] * (b - p.reduced_apply(x))
+                if k == 0:
+                    d = (1.0 / theta) * z
+                else:
+                    rho = 1.0 / (2.0 * sigma - rho_old)
+                    d = (rho * rho_old) * d + (2.0 * rho / delta) * z
+                    rho_old = rho
+                x = x + d
+        return x
 
     def smooth(self, level, x, b, steps):
         p = self.plans[level]
         if self.smoother == "gmres":
             return self.smooth_gmres(level, x, b, steps)
+        if self.smoother == "chebyshev":
+            return self.smooth_chebyshev(level, x, b, steps)
         for _ in range(steps):
             r = b - p.reduced_apply(x)
             x = x + self.omega * self.dinv[level] * r

@@ -1,0 +1,76 @@
+"""Krylov solvers and smoothers on the device against the oracle's restatements.
+
+* FGMRES (`_fgmres_solve`, solve.jl:433-614) with Jacobi and with the hp-GMG V-cycle, with a
+  restart short enough to cycle: the device solve takes the oracle's iteration count (within
+  one, for stopping-test rounding) and reaches the same solution within 1e-9.
+* Chebyshev-Jacobi smoothing (no reference counterpart; the oracle restates Saad's Algorithm
+  12.1 with the same eigenvalue bounds): the device's lambda_max estimates equal the oracle's
+  power iteration and its V-cycles match the oracle's to 1e-11."""
+import numpy as np
+import pytest
+
+import grico_oracle as go
+import grico_b200 as gb
+from grico_b200.multigrid import GeometricMultigridPreconditioner, build_multigrid
+from cases import CASES, build, rel_err
+from test_gpu_multigrid import _pair
+from test_multigrid_host import CASES as MG_CASES
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name,restart", [("2d_p4", 30), ("2d_p4", 4), ("3d_p2_hanging", 6), ("3d_p4", 30)])
+def test_fgmres_jacobi_matches_oracle(cuda, name, restart):
+    D = len(CASES[name][0])
+    src = lambda x: np.prod(np.sin(np.pi * x), axis=1) * D * np.pi ** 2 + 0.25 * x[:, 0]
+    oplan, prob = build(name, mu=0.2, source=src)
+    plan = gb.compile(prob)
+    state = gb.solve(plan, solver=gb.FGMRESSolver(gb.JacobiPreconditioner(), restart=restart),
+                     relative_tolerance=1e-11)
+    diag = oplan.jacobi_diagonal()
+    xr, iters = go.fgmres_solve(oplan.reduced_apply, oplan.reduced_rhs(), precond=lambda r: r / diag,
+                                restart=restart, rtol=1e-11)
+    assert abs(state.report.iterations - iters) <= 1, (state.report.iterations, iters)
+    assert rel_err(state.coefficients, oplan.expand(xr, include_shift=True)) <= 1e-9
+
+
+@pytest.mark.parametrize("name", ["2d_p4", "3d_p2"])
+def test_fgmres_gmg_matches_oracle(cuda, name):
+    D = len(MG_CASES[name][0])
+    src = lambda x: np.prod(np.sin(np.pi * x), axis=1) * (1.0 + D * np.pi ** 2)
+    oplans, plan = _pair(name, source=src)
+    state = gb.solve(plan, solver=gb.FGMRESSolver(GeometricMultigridPreconditioner(), restart=5),
+                     relative_tolerance=1e-11)
+    omg = go.Multigrid(oplans)
+    fine = oplans[-1]
+    fine.source = lambda x: float(src(np.array([x]))[0])
+    xr, iters = go.fgmres_solve(fine.reduced_apply, fine.reduced_rhs(), precond=omg.apply, restart=5, rtol=1e-11)
+    assert abs(state.report.iterations - iters) <= 1, (state.report.iterations, iters)
+    assert rel_err(state.coefficients, fine.expand(xr, include_shift=True)) <= 1e-9
+
+
+@pytest.mark.parametrize("name", sorted(MG_CASES))
+@pytest.mark.parametrize("degree,steps", [(2, 2), (3, 1)])
+def test_chebyshev_vcycle_matches_oracle(cuda, name, degree, steps):
+    oplans, plan = _pair(name)
+    opts = GeometricMultigridPreconditioner(smoother="chebyshev", chebyshev_degree=degree,
+                                            pre_smoothing_steps=steps, post_smoothing_steps=steps)
+    mg = build_multigrid(plan, opts)
+    omg = go.Multigrid(oplans, pre=steps, post=steps, smoother="chebyshev", chebyshev_degree=degree)
+    for lv in range(1, len(oplans)):
+        assert abs(mg.lambda_max(lv) - omg.lmax[lv]) <= 1e-10 * omg.lmax[lv]
+    r = np.random.default_rng(11).standard_normal(plan.n_reduced)
+    assert rel_err(mg.vcycle(r), omg.apply(r)) <= 1e-11
+
+
+def test_cg_chebyshev_gmg_matches_oracle(cuda):
+    src = lambda x: np.prod(np.sin(np.pi * x), axis=1) * (1.0 + 3 * np.pi ** 2)
+    oplans, plan = _pair("3d_p2", source=src)
+    state = gb.solve(plan, solver=gb.CGSolver(GeometricMultigridPreconditioner(smoother="chebyshev")),
+                     relative_tolerance=1e-11)
+    omg = go.Multigrid(oplans, smoother="chebyshev")
+    fine = oplans[-1]
+    fine.source = lambda x: float(src(np.array([x]))[0])
+    xr, iters = go.cg_solve(fine.reduced_apply, fine.reduced_rhs(), precond=omg.apply, rtol=1e-11)
+    assert abs(state.report.iterations - iters) <= 1
+    assert rel_err(state.coefficients, fine.expand(xr, include_shift=True)) <= 1e-9

@@ -11,7 +11,7 @@ import pytest
 
 import grico_b200 as gb
 from grico_b200 import _lib as L
-from cases import build, rel_err
+from cases import CASES, build, rel_err
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-12
@@ -41,6 +41,35 @@ def test_static_rhs_matches_allocating_entry_point(cuda, name):
     arrays = gb.problem._source_points(plan)
     first = _static_rhs(plan, arrays)
     second = _static_rhs(plan, arrays)  # the scratch keeps the first call's contents
+    assert rel_err(first, ref) <= TOL
+    assert rel_err(second, ref) <= TOL
+
+
+@pytest.mark.parametrize("name", ["3d_p2_hanging", "2d_p4"])
+def test_static_rhs_with_dirichlet_shift(cuda, name):
+    """Non-zero Dirichlet values make the reduced right-hand side subtract A * shift, which the
+    entry point computes in the second half of the static array; two calls in a row also show
+    that the second call does not pick up the first call's leftovers there."""
+    origin, extent, roots, refine, p, basis, qx, faces = CASES[name]
+    D = len(origin)
+    src = lambda x: np.prod(np.sin(np.pi * x), axis=1) * D * np.pi ** 2 + 0.5 * x[:, 0]
+    d = gb.Domain(origin, extent, roots)
+    if refine:
+        refine(d.grid)
+    s = gb.HpSpace(d, gb.SpaceOptions(basis=gb.FullTensorBasis(), degree=gb.UniformDegree(p)))
+    u = gb.ScalarField(s)
+    prob = gb.AffineProblem(u)
+    gb.add_cell_accumulator(prob, u, u, gb.MassDiffusion(0.5, 1.5))
+    gb.add_cell_accumulator(prob, u, gb.Load(src))
+    for k, (a, side) in enumerate(faces):
+        gb.add_constraint(prob, gb.Dirichlet(u, gb.BoundaryFace(a, side), 1.0 + 0.5 * k))
+    plan = gb.compile(prob)
+    ref = gb.reduced_rhs(plan)
+    arrays = gb.problem._source_points(plan)
+    homogeneous = _static_rhs(plan, [None] * len(arrays))
+    assert np.max(np.abs(homogeneous)) > 0.0  # the shift alone contributes
+    first = _static_rhs(plan, arrays)
+    second = _static_rhs(plan, arrays)
     assert rel_err(first, ref) <= TOL
     assert rel_err(second, ref) <= TOL
 
