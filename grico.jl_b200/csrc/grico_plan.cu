@@ -1076,6 +1076,11 @@ int grico_plan_create(const GricoPlanDesc* d, GricoPlan** out) {
          P->rel_off.upload(d->rel_offsets, size_t(d->n_relations + 1)) &&
          P->rel_idx.upload(d->rel_index, size_t(d->rel_offsets[d->n_relations])) &&
          P->rel_coef.upload(d->rel_coef, size_t(d->rel_offsets[d->n_relations]));
+    if (d->rel_rhs) {
+      ok = ok && P->rel_rhs.upload(d->rel_rhs, size_t(d->n_relations));
+    } else {
+      ok = ok && P->rel_rhs.upload(std::vector<double>(size_t(d->n_relations), 0.0));
+    }
   }
   ok = ok && P->red_off.upload(d->red_offsets, size_t(d->n_full + 1));
   if (d->red_offsets[d->n_full] > 0)
@@ -1296,12 +1301,15 @@ int grico_reduced_apply(GricoPlan* P, const void* x, void* y, int nrhs, int prec
   return apply_common(P, true, x, y, nrhs, precision, flags, stream);
 }
 
-int grico_reduced_rhs(GricoPlan* P, const double* const* source_points, double* b_reduced, int flags) {
-  if (!P || !b_reduced) return GRICO_ERR_INVALID;
-  cudaStream_t st = P->stream;
-  DevBuf full, bred, src;
-  if (!full.alloc(sizeof(double) * std::max<int64_t>(P->n_full, 1))) return GRICO_ERR_CUDA;
-  cudaMemsetAsync(full.ptr, 0, sizeof(double) * P->n_full, st);
+}  // extern "C"
+
+namespace {
+
+// The load vector sum_cells P_c^T (w f) on the full layout into `full` (zeroed first), from the
+// per-batch source values at the quadrature points (host arrays with GRICO_FLAG_HOST_POINTERS).
+int assemble_load(GricoPlan* P, const double* const* source_points, int flags, double* full, cudaStream_t st) {
+  DevBuf src;
+  cudaMemsetAsync(full, 0, sizeof(double) * P->n_full, st);
   for (size_t bi = 0; bi < P->batches.size(); ++bi) {
     const DevBatch& b = P->batches[bi];
     const double* sp = nullptr;
@@ -1316,7 +1324,7 @@ int grico_reduced_rhs(GricoPlan* P, const double* const* source_points, double* 
         sp = source_points[bi];
       }
     }
-    launch_batch<double>(*P, b, false, nullptr, full.get<double>(), P->n_full, 1, sp, 1, st);
+    launch_batch<double>(*P, b, false, nullptr, full, P->n_full, 1, sp, 1, st);
     if (flags & GRICO_FLAG_HOST_POINTERS) cudaStreamSynchronize(st);
   }
   for (size_t bi = 0; bi < P->pbatches.size(); ++bi) {
@@ -1332,9 +1340,46 @@ int grico_reduced_rhs(GricoPlan* P, const double* const* source_points, double* 
         sp = source_points[slot];
       }
     }
-    launch_points<double>(*P, pb, false, nullptr, full.get<double>(), P->n_full, 1, sp, 1, st);
+    launch_points<double>(*P, pb, false, nullptr, full, P->n_full, 1, sp, 1, st);
     if (flags & GRICO_FLAG_HOST_POINTERS) cudaStreamSynchronize(st);
   }
+  return cuda_ok(cudaGetLastError(), "load assembly") ? GRICO_OK : GRICO_ERR_CUDA;
+}
+
+}  // namespace
+
+extern "C" {
+
+// rhs! (assembly.jl:488-507): the load vector on the full layout with the rows of fixed dofs and
+// Dirichlet relation pivots replaced by their constraint right-hand sides (_write_constraint_rhs!,
+// assembly.jl:1876-1891).
+int grico_rhs(GricoPlan* P, const double* const* source_points, double* b_full, int flags) {
+  if (!P || !b_full) { set_error("grico_rhs: invalid argument"); return GRICO_ERR_INVALID; }
+  (void)cudaGetLastError();
+  cudaStream_t st = P->stream;
+  DevBuf tmp;
+  double* out = b_full;
+  if (flags & GRICO_FLAG_HOST_POINTERS) {
+    if (!tmp.alloc(sizeof(double) * std::max<int64_t>(P->n_full, 1))) return GRICO_ERR_CUDA;
+    out = tmp.get<double>();
+  }
+  if (int rc = assemble_load(P, source_points, flags, out, st)) return rc;
+  if (P->n_fixed + P->n_rel > 0)
+    constraint_rhs<<<grid_for(P->n_fixed + P->n_rel), 256, 0, st>>>(
+        P->fixed.get<int64_t>(), P->fixed_vals.get<double>(), P->n_fixed, P->rel_piv.get<int64_t>(),
+        P->rel_rhs.get<double>(), P->n_rel, out);
+  if (flags & GRICO_FLAG_HOST_POINTERS)
+    cudaMemcpyAsync(b_full, out, sizeof(double) * P->n_full, cudaMemcpyDeviceToHost, st);
+  return cuda_ok(cudaStreamSynchronize(st), "rhs") ? GRICO_OK : GRICO_ERR_CUDA;
+}
+
+int grico_reduced_rhs(GricoPlan* P, const double* const* source_points, double* b_reduced, int flags) {
+  if (!P || !b_reduced) return GRICO_ERR_INVALID;
+  (void)cudaGetLastError();
+  cudaStream_t st = P->stream;
+  DevBuf full, bred;
+  if (!full.alloc(sizeof(double) * std::max<int64_t>(P->n_full, 1))) return GRICO_ERR_CUDA;
+  if (int rc = assemble_load(P, source_points, flags, full.get<double>(), st)) return rc;
   if (P->has_shift) {
     DevBuf as;
     if (!as.alloc(sizeof(double) * P->n_full)) return GRICO_ERR_CUDA;

@@ -111,7 +111,7 @@ struct GricoPlan {
   std::vector<grico::DevBatch> batches;
   std::vector<grico::DevPointBatch> pbatches;
   int64_t n_fixed = 0, n_rel = 0;
-  grico::DevBuf fixed, fixed_vals, rel_piv, rel_off, rel_idx, rel_coef;
+  grico::DevBuf fixed, fixed_vals, rel_piv, rel_off, rel_idx, rel_coef, rel_rhs;
   grico::DevBuf red_off, red_idx, red_coef, shift;
   bool has_shift = false;
   std::map<int64_t, double> hang_diag;  // exact diagonal contributions of hanging cells

@@ -127,6 +127,17 @@ static __global__ void constraint_action(const int64_t* __restrict__ fixed, int6
   }
 }
 
+// constraint right-hand sides: b[fixed] = fixed value, b[pivot] = relation rhs
+static __global__ void constraint_rhs(const int64_t* __restrict__ fixed, const double* __restrict__ fixed_vals,
+                                      int64_t n_fixed, const int64_t* __restrict__ piv,
+                                      const double* __restrict__ rel_rhs, int64_t n_rel, double* __restrict__ b) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n_fixed + n_rel;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    if (i < n_fixed) b[fixed[i]] = fixed_vals[i];
+    else b[piv[i - n_fixed]] = rel_rhs[i - n_fixed];
+  }
+}
+
 // u_full = shift + P u_red (CSR rows per full dof)
 static __global__ void expand_reduced(const int64_t* __restrict__ off, const int64_t* __restrict__ idx,
                                const double* __restrict__ coef, const double* __restrict__ shift,

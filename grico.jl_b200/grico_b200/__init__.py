@@ -14,7 +14,7 @@ from .problem import (SPD, AffineProblem, AssemblyPlan, BoundaryFace, CGSolver, 
                       add_boundary_accumulator, add_interface,
                       add_cell_accumulator, add_cell_quadrature, add_constraint, add_surface_accumulator,
                       add_surface_quadrature, apply, apply_, compile, expand_reduced, l2_error, reduced_apply,
-                      reduced_diagonal, reduced_rhs, relative_l2_error, solve)
+                      reduced_diagonal, reduced_rhs, relative_l2_error, rhs, solve)
 from .regions import (FiniteCellExtension, ImplicitRegion, PhysicalDomain, PhysicalMeasure, SurfaceQuadrature,
                       finite_cell_quadrature, sphere_surface_quadrature)
 from .multigrid import GeometricMultigridPreconditioner

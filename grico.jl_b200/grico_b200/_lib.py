@@ -207,6 +207,7 @@ SIGNATURES = {
     "grico_apply": (C.c_int, [P, P, P, C.c_int, C.c_int, C.c_int, P]),
     "grico_reduced_apply": (C.c_int, [P, P, P, C.c_int, C.c_int, C.c_int, P]),
     "grico_reduced_rhs": (C.c_int, [P, C.POINTER(f64p), f64p, C.c_int]),
+    "grico_rhs": (C.c_int, [P, C.POINTER(f64p), f64p, C.c_int]),
     "grico_reduced_rhs_static": (C.c_int, [P, C.POINTER(C.c_void_p), C.c_void_p, C.c_void_p]),
     "grico_reduced_diagonal": (C.c_int, [P, f64p, C.c_int]),
     "grico_expand_reduced": (C.c_int, [P, f64p, f64p, C.c_int]),

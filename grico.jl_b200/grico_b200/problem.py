@@ -1175,6 +1175,18 @@ def _source_points(plan, problem=None):
     return arrays
 
 
+def rhs(plan):
+    """Full-layout right-hand side rhs! (assembly.jl:488-507): the load vector with the
+    constraint rows' right-hand sides written in (fixed values, relation rhs)."""
+    if isinstance(plan, AffineProblem):
+        plan = compile(plan)
+    arrays = _source_points(plan)
+    ptrs = (L.f64p * len(arrays))(*[L.ptr(a, C.c_double) if a is not None else None for a in arrays])
+    out = np.zeros(plan.n_full)
+    L.check(L.lib().grico_rhs(plan.handle, ptrs, L.ptr(out, C.c_double), L.GRICO_FLAG_HOST_POINTERS), "rhs")
+    return out
+
+
 def reduced_rhs(plan):
     """Reduced right-hand side P^T (b - A shift) (assembly.jl:917-933)."""
     arrays = _source_points(plan)

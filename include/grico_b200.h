@@ -12,7 +12,7 @@
  *   plan create/destroy  compile(problem)            src/plans.jl:170-231
  *   apply                apply!(result, plan, x, ws) src/assembly.jl:540-564
  *   reduced apply        _reduced_apply!             src/assembly.jl:905-915
- *   rhs                  _reduced_rhs!/rhs!          src/assembly.jl:456-478, 917-933
+ *   rhs                  rhs!, _reduced_rhs!         src/assembly.jl:456-507, 917-933
  *   diagonal             _reduced_diagonal!          src/assembly.jl:662-675
  *   cg solve             _cg_solve                   src/solve.jl:376-431
  *   fgmres solve         _fgmres_solve               src/solve.jl:433-589
@@ -258,6 +258,11 @@ int grico_apply(GricoPlan* plan, const void* x, void* y, int nrhs, int precision
 /* y_red = P^T A P x_red (assembly.jl:905-915). */
 int grico_reduced_apply(GricoPlan* plan, const void* x, void* y, int nrhs, int precision, int flags,
                         void* stream);
+/* Full-layout right-hand side (rhs!, assembly.jl:488-507): the load vector from the source
+ * values tabulated at the quadrature points (same layout as grico_reduced_rhs), with the rows of
+ * fixed dofs set to their values and the rows of Dirichlet relation pivots to the relations'
+ * right-hand sides (_write_constraint_rhs!, assembly.jl:1876-1891).  b_full: [n_full]. */
+int grico_rhs(GricoPlan* plan, const double* const* source_points, double* b_full, int flags);
 /* Reduced right-hand side P^T (b_phys - A shift) from the load tabulated at the quadrature
  * points of every batch: source[b] = [n_cells*prod(q)] for cell batch b, then one array of
  * [n_points] per point batch (cells: f; Nitsche items: boundary data g giving

@@ -44,7 +44,7 @@ CASES = {
 }
 
 
-def build(name, mu=0.0, kappa=1.0, kappa_fn=None, source=None):
+def build(name, mu=0.0, kappa=1.0, kappa_fn=None, source=None, dirichlet_value=0.0):
     origin, extent, roots, refine, p, basis, qx, faces = CASES[name]
     od = go.Domain(origin, extent, roots)
     pdm = gb.Domain(origin, extent, roots)
@@ -55,7 +55,7 @@ def build(name, mu=0.0, kappa=1.0, kappa_fn=None, source=None):
     kfn_scalar = (lambda x: float(kappa_fn(np.array([x]))[0])) if kappa_fn else None
     src_scalar = (lambda x: float(source(np.array([x]))[0])) if source else None
     oplan = go.Plan(osp, mu=mu, kappa=kappa, kappa_fn=kfn_scalar, source=src_scalar,
-                    dirichlet=[(a, s, 0.0) for a, s in faces])
+                    dirichlet=[(a, s, dirichlet_value) for a, s in faces])
     psp = gb.HpSpace(pdm, gb.SpaceOptions(basis=gb.TrunkBasis() if basis == "trunk" else gb.FullTensorBasis(),
                                            degree=gb.UniformDegree(p), quadrature=gb.DegreePlusQuadrature(qx)))
     u = gb.ScalarField(psp)
@@ -70,7 +70,7 @@ def build(name, mu=0.0, kappa=1.0, kappa_fn=None, source=None):
     if source is not None:
         gb.add_cell_accumulator(prob, u, gb.Load(source))
     for a, s in faces:
-        gb.add_constraint(prob, gb.Dirichlet(u, gb.BoundaryFace(a, s), 0.0))
+        gb.add_constraint(prob, gb.Dirichlet(u, gb.BoundaryFace(a, s), dirichlet_value))
     return oplan, prob
 
 

@@ -67,6 +67,24 @@ def test_reduced_rhs_matches_oracle(cuda, name):
     assert rel_err(gb.reduced_rhs(plan), oplan.reduced_rhs()) <= TOL
 
 
+@pytest.mark.parametrize("name,value", [("2d_p4", 0.0), ("2d_p4", 1.5), ("3d_p2_hanging", 0.75), ("1d_p3", -2.0)])
+def test_full_rhs_matches_oracle(cuda, name, value):
+    """rhs! on the full layout (assembly.jl:488-507): load vector, constraint rows carry their
+    values (_write_constraint_rhs!, assembly.jl:1876-1891)."""
+    D = len(CASES[name][0])
+    src = lambda x: np.prod(np.sin(np.pi * x), axis=1) * D * np.pi ** 2 + 0.5 * x[:, 0]
+    oplan, prob = build(name, mu=0.4, source=src, dirichlet_value=value)
+    plan = gb.compile(prob)
+    ref = oplan.rhs_physical()
+    for d, v in zip(oplan.fixed, oplan.fixed_values):
+        ref[d - 1] = v
+    for (pivot, _, _, r) in oplan.rows:
+        ref[pivot - 1] = r
+    assert rel_err(gb.rhs(plan), ref) <= TOL
+    # the reduced right-hand side with the Dirichlet shift, same data
+    assert rel_err(gb.reduced_rhs(plan), oplan.reduced_rhs()) <= TOL
+
+
 def test_mass_kat_1d(cuda):  # test/matrix_free.jl:538-579: apply(mass, ones(2)) ≈ [0.5, 0.5]; rhs ≈ [0.5, 0.5]
     d = gb.Domain((0.0,), (1.0,), (1,))
     s = gb.HpSpace(d, gb.SpaceOptions(degree=gb.UniformDegree(1), continuity="dg"))

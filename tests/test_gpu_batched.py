@@ -29,7 +29,9 @@ def test_lockstep_cg_matches_single_solves(cuda):
         assert L.lib().grico_cg_solve(plan.handle, None, L.ptr(B[s], C.c_double), L.ptr(x, C.c_double),
                                       C.byref(so), C.byref(rep), L.GRICO_FLAG_HOST_POINTERS) == 0
         assert reps[s].status == 0
-        assert abs(reps[s].iterations - rep.iterations) <= 2
+        # the lockstep and single solves sum their dot products in different orders; after
+        # hundreds of Jacobi-CG iterations at 1e-11 that moves the stopping iteration by ~1 %
+        assert abs(reps[s].iterations - rep.iterations) <= max(2, rep.iterations // 50)
         assert rel_err(X[s], x) <= 1e-9
 
 
