@@ -185,11 +185,13 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     value, sec, threads, sample = cpu_reference_run(args.steps, args.warmup)
+    probe = probe_julia()
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (diagnostic sample vector)",
             "config": dict(WORKLOAD, parallelism="host threads"), "impl": "reference",
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
+                             "reference_probe": probe},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -432,6 +434,191 @@ def batched_legs(gb, L, max_level=7, nrhs=32, rtol=1e-10):
     return out
 
 
+def probe_julia():
+    """The reference itself is Julia: record whether this host can run it."""
+    import shutil
+
+    exe = shutil.which("julia")
+    if exe is None:
+        return "julia: not found on PATH (reference CPU path unavailable on this host)"
+    try:
+        r = subprocess.run([exe, "--version"], capture_output=True, text=True, timeout=30)
+        return (r.stdout or r.stderr).strip()
+    except Exception as exc:  # noqa: BLE001
+        return f"julia present but --version failed: {exc}"
+
+
+def _timed_device(fn, reps, stream):
+    import torch
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def c1_leg(gb, L, peak):
+    """2-D Poisson, 32 x 32 cells, p = 4, q = 5 (16,641 dofs), homogeneous Dirichlet: 100
+    matrix-free applies (direct launches, and replayed as one CUDA graph) and the CG + Jacobi
+    solve to relative residual 1e-10, checked against the exact solution."""
+    import torch
+
+    d = gb.Domain((0.0, 0.0), (1.0, 1.0), (32, 32))
+    sp = gb.HpSpace(d, gb.SpaceOptions(basis=gb.FullTensorBasis(), degree=gb.UniformDegree(4)))
+    u = gb.ScalarField(sp)
+    prob = gb.AffineProblem(u)
+    gb.add_cell_accumulator(prob, u, u, gb.Diffusion())
+    gb.add_cell_accumulator(prob, u, gb.Load(lambda X: 2 * np.pi ** 2 * np.sin(np.pi * X[:, 0]) * np.sin(np.pi * X[:, 1])))
+    for a in (1, 2):
+        for side in (gb.LOWER, gb.UPPER):
+            gb.add_constraint(prob, gb.Dirichlet(u, gb.BoundaryFace(a, side), 0.0))
+    t0 = time.perf_counter()
+    plan = gb.compile(prob)
+    setup = time.perf_counter() - t0
+    n = plan.n_full
+    x = torch.tensor(sample_vector(n), device="cuda", dtype=torch.float64)
+    y = torch.empty_like(x)
+    st = torch.cuda.Stream()
+
+    def apply():
+        L.lib().grico_apply(plan.handle, x.data_ptr(), y.data_ptr(), 1, L.GRICO_PREC_FP64, 0, st.cuda_stream)
+
+    for _ in range(10):
+        apply()
+    torch.cuda.synchronize()
+    ms_direct = _timed_device(apply, 100, st)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(st):
+        with torch.cuda.graph(g, stream=st):
+            for _ in range(100):
+                apply()
+    g.replay()
+    torch.cuda.synchronize()
+    ms_graph = _timed_device(g.replay, 5, st) / 100
+    del g
+    exact = lambda X: np.sin(np.pi * X[:, 0]) * np.sin(np.pi * X[:, 1])
+    gb.solve(plan, solver=gb.CGSolver(gb.JacobiPreconditioner()), relative_tolerance=1e-10)  # warm
+    t0 = time.perf_counter()
+    state = gb.solve(plan, solver=gb.CGSolver(gb.JacobiPreconditioner()), relative_tolerance=1e-10)
+    wall = time.perf_counter() - t0
+    alg = 2 * 8 * n
+    best = min(ms_direct, ms_graph)
+    # the oracle's C port of the reference tensor schedule (2-D), all host threads, 100 applies
+    cpu = None
+    try:
+        for sub in ("oracle", "tests"):
+            sys.path.insert(0, os.path.join(ROOT, sub))
+        from baseline_cases import oracle_cell_sum, uniform_oracle
+        import oracle_lib as ol
+
+        coords, m, ndofs, _ = uniform_oracle((32, 32), 4)
+        xs = sample_vector(ndofs)
+        oracle_cell_sum((32, 32), 4, coords, m, xs, 1.0 / 32)
+        t0 = time.perf_counter()
+        for _ in range(100):
+            oracle_cell_sum((32, 32), 4, coords, m, xs, 1.0 / 32)
+        sec = (time.perf_counter() - t0) / 100
+        cpu = {"value": ndofs / sec, "unit": "DOFs/s", "cores": ol.max_threads(), "kind": "port",
+               "sample": "100 applies of the 32x32 p=4 workload (oracle C restatement, all threads)"}
+    except Exception as exc:  # noqa: BLE001
+        cpu = {"value": None, "error": str(exc)[:200]}
+    return {"metric": "DOFs/s matrix-free apply (100 applies) and CG+Jacobi time to rtol 1e-10",
+            "config": {"workload": "poisson2d_32x32_p4_dirichlet", "cells": "32x32", "degree": 4,
+                       "quadrature": "gauss 5x5", "dofs": n, "reduced_dofs": plan.n_reduced},
+            "value": n / (best * 1e-3), "unit": "DOFs/s", "dtype": "f64",
+            "apply_ms_direct": ms_direct, "apply_ms_graph": ms_graph, "applies_100_ms": 100 * best,
+            "solve": {"iterations": int(state.report.iterations), "device_seconds": float(state.report.seconds),
+                      "wall_seconds_with_host_copies": wall, "l2_error": gb.l2_error(state, exact)},
+            "host_setup_seconds": setup,
+            "roofline": {"bound": "hbm", "achieved": alg / (best * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": alg / (best * 1e-3) / 1e9 / peak, "traffic": None,
+                         "note": "266 KB per apply stay in L2: launch latency, not HBM, bounds this size"},
+            "cpu_baseline": cpu}
+
+
+def c3_leg(gb, L, peak):
+    out = batched_legs(gb, L)
+    a = out["apply_fp64_nrhs32"]
+    alg = 2 * 8 * out["reduced_dofs"] * 32
+    return {"metric": "time to rtol 1e-10 for 32 right-hand sides (adaptive hp L-shape)",
+            "value": out["lockstep_cg_fp64"]["seconds"], "unit": "s", "higher_is_better": False,
+            "config": {"workload": "lshape_hp32", "levels": "2..7", "degrees": "2..7", "nrhs": 32},
+            "batched": out,
+            "roofline": {"bound": "hbm", "achieved": alg / (a["ms"] * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": alg / (a["ms"] * 1e-3) / 1e9 / peak, "traffic": None,
+                         "note": "FP64 reduced apply for 32 right-hand sides: 2*8*n_reduced*32 bytes per apply"},
+            "cpu_baseline": {"value": None, "reason": "the oracle's C port covers single-term (conforming) maps only; "
+                                                      "this mesh has hanging-node expansions"}}
+
+
+def c4_leg(gb, L):
+    out = learned_legs(gb, L, refine=6)
+    leg = out["legs"]
+    return {"metric": "time to relative L2 error 1e-8 (learned + mixed vs plain FP64 GPU)",
+            "value": leg["learned+mixed_fp32_vcycle"]["time_to_target_seconds"], "unit": "s",
+            "higher_is_better": False,
+            "config": {"workload": "grf_learned64", "cells": "64^3", "degree": 2,
+                       "solver": "FGMRES(30) + hp-GMG V(2,2)",
+                       "note": "64^3 cells in the default run; --workload grf_learned128 runs 128^3"},
+            "plain_fp64_seconds": leg["fp64"]["time_to_target_seconds"], "learned": out,
+            "cpu_baseline": {"value": None, "reason": "no CPU port of the FGMRES + GMG solve at this size"}}
+
+
+def c5_leg(gb, L, peak):
+    """Finite-cell shell, 64^3 background cells, p = 3: FP64 and FP32 full applies."""
+    import torch
+
+    t0 = time.perf_counter()
+    plan = gb.compile(build_fcm_problem(gb, refine=6))
+    setup = time.perf_counter() - t0
+    n = plan.n_full
+    res = {}
+    for prec, dt, name in ((L.GRICO_PREC_FP64, torch.float64, "fp64"), (L.GRICO_PREC_FP32, torch.float32, "fp32")):
+        x = torch.tensor(sample_vector(n), device="cuda", dtype=dt)
+        y = torch.empty_like(x)
+        st = torch.cuda.Stream()
+        fn = lambda: L.lib().grico_apply(plan.handle, x.data_ptr(), y.data_ptr(), 1, prec, 0, st.cuda_stream)
+        for _ in range(5):
+            fn()
+        torch.cuda.synchronize()
+        ms = _timed_device(fn, 20, st)
+        res[name] = {"ms": ms, "dofs_per_s": n / (ms * 1e-3)}
+    alg = 2 * 8 * n
+    sub = [b for b in plan.point_batches if b.kind == L.GRICO_ITEM_SUBCELLS]
+    return {"metric": "DOFs/s finite-cell matrix-free apply", "value": res["fp64"]["dofs_per_s"], "unit": "DOFs/s",
+            "config": dict(FCM_WORKLOAD, dofs=n, cut_cells=plan.n_cut,
+                           subcells=int(sum(len(b.subcell_level) for b in sub))),
+            "apply": res, "host_setup_seconds": setup,
+            "roofline": {"bound": "hbm", "achieved": alg / (res["fp64"]["ms"] * 1e-3) / 1e9, "peak": peak,
+                         "unit": "GB/s", "frac": alg / (res["fp64"]["ms"] * 1e-3) / 1e9 / peak, "traffic": None,
+                         "note": "whole FP64 apply (all batches); the cut-cell subcell kernel dominates"},
+            "cpu_baseline": {"value": None, "reason": "the oracle's C port covers tensor cells only; the cut-cell "
+                                                      "oracle is the pure-Python restatement (test sizes)"}}
+
+
+def config_legs(gb, L, only=None):
+    """Every BASELINE configuration besides the headline one, each in its own try block."""
+    import traceback
+
+    peak, _ = load_peaks()
+    legs = {"c1_poisson2d_32_p4": lambda: c1_leg(gb, L, peak), "c3_lshape_hp32": lambda: c3_leg(gb, L, peak),
+            "c4_grf_learned64": lambda: c4_leg(gb, L), "c5_fcm_shell64": lambda: c5_leg(gb, L, peak)}
+    out = {}
+    for name, fn in legs.items():
+        if only and name not in only:
+            continue
+        t0 = time.perf_counter()
+        try:
+            out[name] = fn()
+        except Exception as exc:  # noqa: BLE001
+            out[name] = {"error": f"{type(exc).__name__}: {exc}"[:300], "trace": traceback.format_exc()[-600:]}
+        out[name]["leg_wall_seconds"] = time.perf_counter() - t0
+    return out
+
+
 def sharded_leg(gb, plan, rank, world, steps, warmup):
     """The same mesh split over the ranks (strong scaling): each rank applies the reduced
     operator of its Morton range of cells and the partition-surface halo is summed with one NCCL
@@ -498,6 +685,9 @@ def main():
                              "lshape_hp32"],
                     help="poisson64: 3-D Poisson 64^3 p=4 (default); fcm_shell*: finite-cell shell with Nitsche")
     ap.add_argument("--fp32", action="store_true", help="time the FP32 apply instead of FP64")
+    ap.add_argument("--no-configs", action="store_true", help="skip the other BASELINE configurations")
+    ap.add_argument("--configs", default="", help="comma-separated config legs to run (c1_poisson2d_32_p4, "
+                    "c3_lshape_hp32, c4_grf_learned64, c5_fcm_shell64); default: all")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", 0))
@@ -642,6 +832,9 @@ def main():
     solve_info = None
     if not args.no_solve:
         solve_info = solve_legs(gb, L, plan, prob, only=[v for v in args.solve_legs.split(",") if v])
+    configs_info = None
+    if not fcm and world == 1 and not args.no_configs and not args.fp32:
+        configs_info = config_legs(gb, L, only=[v for v in args.configs.split(",") if v])
 
     if rank == 0:
         peak, peak_kind = load_peaks()
@@ -709,6 +902,9 @@ def main():
         }
         if sharded_info is not None:
             out["sharded"] = sharded_info
+        if configs_info is not None:
+            out["configs"] = configs_info
+        out["reference_probe"] = probe_julia()
         if fcm:
             out["cpu_baseline_note"] = ("the oracle's C kernel covers tensor cells only; the finite-cell parity "
                                         "oracle is a pure-Python restatement (test sizes)")

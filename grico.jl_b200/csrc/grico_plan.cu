@@ -14,6 +14,7 @@
 
 #include "cell_kernels.cuh"
 #include "cell_pipe.cuh"
+#include "cell_plane.cuh"
 #include "grico_host.h"
 #include "grico_plan_internal.h"
 #include "vector_kernels.cuh"
@@ -149,6 +150,11 @@ Tables1D<N, Q, T> make_tables(const DevBatch& b) {
 // 0.073), and in FP32 it also beats the one-block-per-group kernel at q = 2.  Group sizes: half
 // size (3) except default size (4) for FP64 q = 7 and FP32 q = 6, 7, 9.
 int default_tile_3d(int q, bool fp32) {
+  // thread-per-plane kernel (variant 9), measured on uniform grids (B200, ms per apply): p = 1,
+  // 275k dofs: FP64 0.0374 -> 0.0318, FP32 0.0322 -> 0.0250; p = 2, 2.1M dofs: FP64 0.0807 ->
+  // 0.0705, FP32 0.0635 -> 0.0566.  At q >= 4 its register and shared-memory footprint leaves too
+  // few warps per SM (p = 4 FP64: 0.311 vs 0.423 ms) and the pipelined kernel stays the default.
+  if (q <= 3) return 9;
   if (q <= 5) return 3;
   if (fp32) return q == 8 ? 3 : 4;
   return q == 7 ? 4 : 3;
@@ -220,12 +226,34 @@ bool launch_fused(int dim, const DevBatch& bt, const BatchView& v, const T* x, T
       GRICO_L3_PIPE_EO(NN, QQ, CPB_, true)                                                                     \
     GRICO_L3_PIPE_EO(NN, QQ, CPB_, false)                                                                      \
   }
+// variant 9: one warp per 32 / q cells, thread per plane (q <= 6; plain maps, constant coefficients)
+#define GRICO_L3_PLANE(NN, QQ)                                                                                 \
+  if constexpr (QQ <= 6) {                                                                                     \
+    if (mode == 0 && v.coef == nullptr && v.tail_off == nullptr && v.mass_pts == nullptr &&                    \
+        v.kappa_pts == nullptr) {                                                                              \
+      TablesEO<NN, QQ, T> eo{};                                                                                \
+      if (make_eo_tables<NN, QQ, T>(bt.hB.data(), bt.hD.data(), eo)) {                                         \
+        constexpr int CPB = PlaneShape<QQ>::CPB;                                                               \
+        static const PlaneLayout lay = make_plane_layout(NN, QQ, int(sizeof(T)));                              \
+        static const size_t smem = plane_smem_bytes(CPB, lay, int(sizeof(T)));                                 \
+        auto kern = cell_apply_3d_plane<NN, QQ, T>;                                                            \
+        static const int per_sm = persistent_blocks_per_sm(reinterpret_cast<const void*>(kern), 32, smem);    \
+        if (per_sm > 0) {                                                                                      \
+          const int64_t groups = (int64_t(v.n_cells) + CPB - 1) / CPB;                                         \
+          dim3 grid(unsigned(std::min<int64_t>(groups, int64_t(per_sm) * sm_count())), nrhs);                  \
+          kern<<<grid, 32, smem, st>>>(v, make_tables<NN, QQ, T>(bt), eo, lay, x, y, nvec, mass, kappa);       \
+          return true;                                                                                         \
+        }                                                                                                      \
+      }                                                                                                        \
+    }                                                                                                          \
+  }
 #define GRICO_L3(NN, QQ)                                                                                       \
   if (N == NN && Q == QQ) {                                                                                    \
     constexpr int C1 = (256 / (QQ * QQ)) > 0 ? (256 / (QQ * QQ)) : 1;                                          \
     constexpr int C0 = C1 / 2 > 0 ? C1 / 2 : 1;                                                                \
     constexpr int C2 = (2 * C1 * QQ * QQ <= 1024) ? 2 * C1 : C1;                                               \
-    if (var == 3 || var == 6) GRICO_L3_PIPE(NN, QQ, C0, var == 3)                                              \
+    if (var == 9) GRICO_L3_PLANE(NN, QQ)                                                                       \
+    if (var == 3 || var == 6 || var == 9) GRICO_L3_PIPE(NN, QQ, C0, var != 6)                                  \
     if (var == 4 || var == 7) GRICO_L3_PIPE(NN, QQ, C1, var == 4)                                              \
     if (var == 5 || var == 8) GRICO_L3_PIPE(NN, QQ, C2, var == 5)                                              \
     if (var % 3 == 0) GRICO_L3_CPB(NN, QQ, C0)                                                                 \
@@ -249,6 +277,7 @@ bool launch_fused(int dim, const DevBatch& bt, const BatchView& v, const T* x, T
 #undef GRICO_L3
 #undef GRICO_L3_PIPE
 #undef GRICO_L3_PIPE_EO
+#undef GRICO_L3_PLANE
 #undef GRICO_L3_CPB
 #undef GRICO_L2
   return false;

@@ -60,7 +60,7 @@ struct DevBuf {
   bool upload(const std::vector<T>& v) { return upload(v.data(), v.size()); }
 };
 
-constexpr int kTileVariants = 9;
+constexpr int kTileVariants = 10;
 
 struct DevMap {
   DevBuf map, coef, toff, tidx, tcoef;

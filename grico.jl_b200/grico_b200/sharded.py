@@ -163,6 +163,7 @@ class ShardPlan:
         fixed_local = np.nonzero(~lfree)[0]
         lp.fixed_dofs = fixed_local.astype(np.int64)
         lp.fixed_values = np.ascontiguousarray(plan.shift[glob[fixed_local]])
+        lp.relations = []
         lp.solve_dofs = order.astype(np.int64)
         lp.n_reduced = n_red
         lp.reduced_index = red_of_local

@@ -221,8 +221,10 @@ int grico_plan_create(const GricoPlanDesc* desc, GricoPlan** out);
  * batch to `chosen` (may be NULL).  Variants: 0, 1, 2 = half, default, double cells per block
  * with one block per cell group; 3, 4, 5 = the same sizes in the persistent kernel that
  * prefetches the next cell group's gather with asynchronous copies, with the 1-D contractions in
- * even-odd form; 6, 7, 8 = that kernel with direct contractions.  Batches without a 3-D
- * isotropic tensor kernel report 1.  Allocates scratch; call before any stream capture. */
+ * even-odd form; 6, 7, 8 = that kernel with direct contractions; 9 = one warp per 32 / q cells
+ * with one thread per cell plane (q <= 6, plain maps, constant coefficients; the default at
+ * q <= 3).  Batches without a 3-D isotropic tensor kernel report 1.  Allocates scratch; call
+ * before any stream capture. */
 int grico_plan_autotune(GricoPlan* plan, int nrhs, int precision, int reps, int* chosen);
 /* Sets the kernel variant of every cell batch for `precision` (tiles[n_batches], values as
  * reported by grico_plan_autotune), e.g. to replay a stored tuning without timing again.

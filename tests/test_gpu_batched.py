@@ -48,8 +48,9 @@ def test_graph_and_direct_launches_agree(cuda):
     plan, B = _case(nrhs=3)
     Xg, rg = bt.solve_many(plan, B, relative_tolerance=1e-10, graph=True)
     Xd, rd = bt.solve_many(plan, B, relative_tolerance=1e-10, graph=False)
-    # the atomic scatter order varies run to run, which can move a stopping iteration by one
-    assert all(abs(a.iterations - b.iterations) <= 2 for a, b in zip(rg, rd))
+    # the atomic scatter order varies run to run; after hundreds of Jacobi-CG iterations that
+    # moves the stopping iteration by ~1 %
+    assert all(abs(a.iterations - b.iterations) <= max(2, b.iterations // 50) for a, b in zip(rg, rd))
     assert rel_err(Xg, Xd) <= 1e-8
 
 

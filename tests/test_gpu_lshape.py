@@ -10,8 +10,9 @@ rows and keeps the extra dofs.  The checks therefore do not compare dof by dof:
   the product's), the Gram matrix G_ij = a(u_i, u_j) from the oracle's reduced apply equals the
   one from the device's reduced apply on the same functions written in the product's
   coefficients (leaf-local mode coefficients are numbering independent);
-* operator on the product's maps: the oracle's cell kernel (accumulators.jl:1022-1054), gathered
-  and scattered through the product's term maps (hanging-node expansions included) and with the
+* operator on the product's maps: the oracle's cell kernel (accumulators.jl:1022-1054) on the full
+  box of modes, gathered and scattered through the product's term maps (hanging-node expansions
+  included) and with the
   product's constraint rows (fixed dofs and Dirichlet relations, assembly.jl:1893-1920), equals
   the device's full apply, reduced apply and exact reduced diagonal (the probe of
   solve.jl:722-738) to 1e-12."""
@@ -20,94 +21,16 @@ import pytest
 
 import grico_b200 as gb
 from cases import rel_err
-from lshape_cases import oracle_lshape, product_lshape
+from lshape_cases import NOISE, box_local_apply, cell_sum, expand, full_apply, project, setup, to_product
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-12
-# the reference's noise pivots (|pivot| ~ 1e-15, amplified by hanging-node coefficients) leave
-# its functions off the exact continuous space by ~1e-12 relative; the bilinear-form comparison
-# across the two numberings is held to this bound, the same-map comparisons to TOL
-NOISE = 1e-10
 MU, KAPPA = 0.3, 1.7
-
-
-def _setup(device=True):
-    oplan = oracle_lshape(max_level=4, mu=MU, kappa=KAPPA)
-    plan = gb.compile(product_lshape(max_level=4, mu=MU, kappa=KAPPA), device=device)
-    psp, osp = plan.space, oplan.space
-    assert list(osp.snapshot.leaves) == [int(v) for v in psp.leaves]
-    terms = [[psp.mode_terms(leaf, mode) for mode in osp.leaf_modes[li]] for li, leaf in enumerate(osp.snapshot.leaves)]
-    return oplan, plan, terms
 
 
 @pytest.fixture(scope="module")
 def lshape():
-    return _setup()
-
-
-def expand(plan, xr):
-    """u_full = shift + P u_red on the host (assembly.jl:965-970), shift left out."""
-    xf = np.zeros(plan.n_full)
-    for d in range(plan.n_full):
-        lo, hi = plan.red_offsets[d], plan.red_offsets[d + 1]
-        xf[d] = plan.red_coef[lo:hi] @ xr[plan.red_index[lo:hi]]
-    return xf
-
-
-def project(plan, yf):
-    out = np.zeros(plan.n_reduced)
-    for d in range(plan.n_full):
-        lo, hi = plan.red_offsets[d], plan.red_offsets[d + 1]
-        np.add.at(out, plan.red_index[lo:hi], plan.red_coef[lo:hi] * yf[d])
-    return out
-
-
-def to_product(oplan, plan, terms, u_red):
-    """Product reduced coefficients of the function whose oracle reduced coefficients are u_red:
-    solve T_product x = the leaf-local mode coefficients (sparse normal equations), restrict to
-    the solve dofs and check that the result reproduces the function."""
-    import scipy.sparse as sp
-    import scipy.sparse.linalg as spl
-
-    xo = np.concatenate([[0.0], oplan.expand(u_red)])
-    rows, cols, vals, rhs = [], [], [], []
-    r = 0
-    for li, c in enumerate(oplan.cells):
-        for t_or, t_pr in zip(c["terms"], terms[li]):
-            for (d, cc) in t_pr:
-                rows.append(r)
-                cols.append(d - 1)
-                vals.append(cc)
-            rhs.append(sum(cc * xo[d] for (d, cc) in t_or))
-            r += 1
-    T = sp.csr_matrix((vals, (rows, cols)), shape=(r, plan.n_full))
-    rhs = np.array(rhs)
-    x = spl.spsolve((T.T @ T).tocsc(), T.T @ rhs)
-    xr = x[plan.solve_dofs]
-    assert np.max(np.abs(T @ expand(plan, xr) - rhs)) <= NOISE * max(1.0, np.max(np.abs(rhs)))
-    return xr
-
-
-def cell_sum(oplan, plan, terms, x):
-    """Sum of the oracle's local cell operators gathered/scattered through the product's maps."""
-    y = np.zeros(plan.n_full)
-    for li, c in enumerate(oplan.cells):
-        xloc = np.array([sum(cc * x[d - 1] for (d, cc) in t) for t in terms[li]])
-        yloc = oplan.local_apply(c, xloc)
-        for t, v in zip(terms[li], yloc):
-            for (d, cc) in t:
-                y[d - 1] += cc * v
-    return y
-
-
-def full_apply(oplan, plan, terms, x):
-    """apply! on the product's layout: cell sum, then the constraint rows (fixed: y = x;
-    relation: y_p = x_p - sum c_j x_j), assembly.jl:1893-1920."""
-    y = cell_sum(oplan, plan, terms, x)
-    y[plan.fixed_dofs] = x[plan.fixed_dofs]
-    for (p, idx, co, _) in plan.relations:
-        y[p] = x[p] - co @ x[idx]
-    return y
+    return setup(mu=MU, kappa=KAPPA)
 
 
 def test_lshape_has_dirichlet_relations(cuda, lshape):
@@ -139,7 +62,7 @@ def test_lshape_exact_diagonal(cuda, lshape):
     diag = np.zeros(plan.n_reduced)
     for li, c in enumerate(oplan.cells):
         nloc = len(terms[li])
-        K = np.stack([oplan.local_apply(c, e) for e in np.eye(nloc)], axis=1)
+        K = np.stack([box_local_apply(oplan, c, e) for e in np.eye(nloc)], axis=1)
         # local mode -> reduced dofs: product terms composed with the reduced map
         R = {}
         for i, t in enumerate(terms[li]):

@@ -13,16 +13,12 @@ import pytest
 
 import grico_oracle as go
 import grico_b200 as gb
-from lshape_cases import oracle_lshape, product_lshape
+from lshape_cases import expand, setup, to_product
 
 
 @pytest.fixture(scope="module")
 def pair():
-    oplan = oracle_lshape(max_level=4)
-    plan = gb.compile(product_lshape(max_level=4), device=False)
-    terms = [[plan.space.mode_terms(leaf, mode) for mode in oplan.space.leaf_modes[li]]
-             for li, leaf in enumerate(oplan.space.snapshot.leaves)]
-    return oplan, plan, terms
+    return setup(device=False)
 
 
 def test_lshape_topology_matches_oracle(pair):
@@ -48,32 +44,11 @@ def test_lshape_dof_count_and_noise_pivots(pair):
     assert plan.n_full == osp.ndofs + osp.noise_pivots
 
 
-def _local_modes(oplan, terms_of, x1):
-    return [np.array([sum(cc * x1[d] for (d, cc) in t) for t in terms_of(li)]) for li in range(len(oplan.cells))]
-
-
 def test_lshape_dirichlet_space_contains_oracle_space(pair):
-    import scipy.sparse as sp
-    import scipy.sparse.linalg as spl
-
     oplan, plan, terms = pair
     u = np.random.default_rng(0).standard_normal(len(oplan.solve_dofs))
-    xo = np.concatenate([[0.0], oplan.expand(u)])
-    rows, cols, vals, rhs = [], [], [], []
-    r = 0
-    for li, c in enumerate(oplan.cells):
-        for t_or, t_pr in zip(c["terms"], terms[li]):
-            for (d, cc) in t_pr:
-                rows.append(r)
-                cols.append(d - 1)
-                vals.append(cc)
-            rhs.append(sum(cc * xo[d] for (d, cc) in t_or))
-            r += 1
-    T = sp.csr_matrix((vals, (rows, cols)), shape=(r, plan.n_full))
-    rhs = np.array(rhs)
-    x = spl.spsolve((T.T @ T).tocsc(), T.T @ rhs)
-    assert np.max(np.abs(T @ x - rhs)) <= 1e-10
-    # x satisfies the product's Dirichlet constraints
+    xr = to_product(oplan, plan, terms, u)  # checks that the product reproduces the function
+    x = expand(plan, xr)
     assert np.max(np.abs(x[plan.fixed_dofs])) <= 1e-10
     assert len(plan.relations) > 0
     for (p, idx, co, rhs_p) in plan.relations:
@@ -95,6 +70,8 @@ def test_lshape_product_functions_vanish_on_dirichlet_faces(pair):
         li = osp.snapshot.leaf_to_index[leaf]
         c = oplan.cells[li]
         m = np.array([sum(cc * xf[d] for (d, cc) in t) for t in terms[li]])
+        n = [dg + 1 for dg in c["degs"]]
+        modes = [(i, j, k) for k in range(n[2]) for j in range(n[1]) for i in range(n[0])]
         a = axis - 1
         tang = [b for b in range(3) if b != a]
         for p1 in pts:
@@ -103,6 +80,6 @@ def test_lshape_product_functions_vanish_on_dirichlet_faces(pair):
                 ref[a] = -1.0 if side == 1 else 1.0
                 ref[tang[0]], ref[tang[1]] = p1, p2
                 tab = [go.fe_basis_values_and_derivatives(ref[b], c["degs"][b])[0] for b in range(3)]
-                v = sum(m[k] * tab[0][md[0]] * tab[1][md[1]] * tab[2][md[2]] for k, md in enumerate(c["modes"]))
+                v = sum(m[k] * tab[0][md[0]] * tab[1][md[1]] * tab[2][md[2]] for k, md in enumerate(modes))
                 worst = max(worst, abs(v))
     assert worst <= 1e-9
