@@ -643,9 +643,20 @@ void compile_continuity(Space& s) {
           double left = 0.0;
           for (double c : row.coefs) left = std::max(left, std::fabs(c));
           if (left <= 256.0 * 2.220446049250313e-16 * seen) { ++s.noise_rows; continue; }
-          size_t pidx = 0;
-          for (size_t i = 1; i < row.vars.size(); ++i)
-            if (row.vars[i] > row.vars[pidx]) pidx = i;
+          // Pivot: the largest variable id (continuity.jl:995-998) among the terms whose
+          // coefficient is at least kPivotFloor of the row's largest.  Restriction coefficients
+          // of high modes onto half faces are ~2^-p; pivoting on one divides the row by it, and on
+          // deep hp meshes such steps chain (the 3-D L-shape graded to level 7, degrees 2..7:
+          // expansion coefficients up to 9.8e5 with the plain rule, 25 with the floor, and Jacobi
+          // CG stalls on the former).  Where every coefficient is within the floor of the
+          // largest, which covers the meshes the maps are pinned on, the choice is the
+          // reference's.
+          constexpr double kPivotFloor = 0.1;
+          size_t pidx = row.vars.size();
+          for (size_t i = 0; i < row.vars.size(); ++i)
+            if (std::fabs(row.coefs[i]) >= kPivotFloor * left &&
+                (pidx == row.vars.size() || row.vars[i] > row.vars[pidx]))
+              pidx = i;
           int64_t pivot = row.vars[pidx];
           double pcoef = row.coefs[pidx];
           row.remove_at(pidx);
