@@ -5,9 +5,11 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <string>
 
 #include "cnn_kernels.cuh"
+#include "cnn_tc.cuh"
 #include "grico_host.h"
 #include "vector_kernels.cuh"
 
@@ -34,6 +36,59 @@ int launch_status(const char* what) {
     return GRICO_ERR_CUDA;
   }
   return GRICO_OK;
+}
+
+}  // namespace
+
+// error flag of the tensor-core convolution (an mbarrier wait that gave up); one per device,
+// its address resolved on the first call on that device
+static __device__ int g_conv_tc_err;
+
+namespace {
+
+std::mutex g_conv_tc_mutex;
+int* g_conv_tc_err_ptr[64] = {nullptr};
+
+int conv_tc_err_ptr(int** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    set_error("tensor-core convolution: no current CUDA device");
+    return GRICO_ERR_CUDA;
+  }
+  std::lock_guard<std::mutex> lock(g_conv_tc_mutex);
+  if (!g_conv_tc_err_ptr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_conv_tc_err) != cudaSuccess) {
+      set_error(std::string("tensor-core convolution: ") + cudaGetErrorString(cudaGetLastError()));
+      return GRICO_ERR_CUDA;
+    }
+    g_conv_tc_err_ptr[dev] = static_cast<int*>(p);
+  }
+  *out = g_conv_tc_err_ptr[dev];
+  return GRICO_OK;
+}
+
+template <typename TIn, typename TOut>
+int launch_conv_tc(const void* x, const float* w, const float* bias, void* y, int B, int Ci, int Co, int Z, int Y,
+                   int X, int relu, cudaStream_t st) {
+  int* err = nullptr;
+  if (int rc = conv_tc_err_ptr(&err)) return rc;
+  auto kern = tc::conv3d_fwd_tc<TIn, TOut>;
+  const size_t smem = tc::conv_tc_smem_bytes(Ci, Co);
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
+    return launch_status("grico_conv3d_forward_tc");
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, tc::kThreads, smem) != cudaSuccess || per_sm < 1)
+    return launch_status("grico_conv3d_forward_tc");
+  int dev = 0, sms = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t tiles = int64_t(B) * Z * ((Y + tc::kTY - 1) / tc::kTY) * ((X + tc::kTX - 1) / tc::kTX);
+  const int grid = int(std::min<int64_t>(tiles, int64_t(per_sm) * sms));
+  kern<<<grid, tc::kThreads, smem, st>>>(static_cast<const TIn*>(x), w, bias, static_cast<TOut*>(y), B, Ci, Co, Z, Y,
+                                         X, relu, err);
+  return launch_status("grico_conv3d_forward_tc");
 }
 
 }  // namespace
@@ -142,6 +197,43 @@ int grico_weighted_residual(const float* r, const float* ar, const float* w, flo
   weighted_residual<float><<<kRedBlocks, 256, 0, st>>>(r, ar, w, out, n, partial);
   reduce_final<<<1, kRedThreads, 0, st>>>(partial, kRedBlocks, sum);
   return launch_status("grico_weighted_residual");
+}
+
+// Tensor-core forward convolution (tcgen05.mma, BF16 operands rounded from the inputs and
+// weights, FP32 accumulation): same arguments and layout as grico_conv3d_forward, for
+// Ci a multiple of 16 and Co a multiple of 32 up to 128.
+int grico_conv3d_forward_tc(const void* x, int x_bf16, const float* w, const float* bias, void* y, int y_bf16, int B,
+                            int Ci, int Co, int Z, int Y, int X, int relu, void* stream) {
+  if (!x || !w || !y || !conv_args_ok(B, Ci, Co, Z, Y, X) || !tc::conv_tc_supported(Ci, Co)) {
+    set_error("grico_conv3d_forward_tc: invalid argument (Ci must be a multiple of 16, Co a multiple of 32 up to 128)");
+    return GRICO_ERR_INVALID;
+  }
+  cudaStream_t st = as_stream(stream);
+  if (!x_bf16 && !y_bf16) return launch_conv_tc<float, float>(x, w, bias, y, B, Ci, Co, Z, Y, X, relu, st);
+  if (!x_bf16 && y_bf16) return launch_conv_tc<float, __nv_bfloat16>(x, w, bias, y, B, Ci, Co, Z, Y, X, relu, st);
+  if (x_bf16 && y_bf16)
+    return launch_conv_tc<__nv_bfloat16, __nv_bfloat16>(x, w, bias, y, B, Ci, Co, Z, Y, X, relu, st);
+  return launch_conv_tc<__nv_bfloat16, float>(x, w, bias, y, B, Ci, Co, Z, Y, X, relu, st);
+}
+
+// Synchronises `stream` and reports (then clears) a bounded wait of the tensor-core convolution
+// that gave up on this device: GRICO_ERR_TIMEOUT, else GRICO_OK.
+int grico_conv_tc_status(void* stream) {
+  int* err = nullptr;
+  if (int rc = conv_tc_err_ptr(&err)) return rc;
+  cudaStream_t st = as_stream(stream);
+  int h = 0;
+  if (cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return launch_status("grico_conv_tc_status");
+  if (h) {
+    const int zero = 0;
+    cudaMemcpyAsync(err, &zero, sizeof(int), cudaMemcpyHostToDevice, st);
+    cudaStreamSynchronize(st);
+    set_error("grico_conv3d_forward_tc: a tensor-core wait gave up");
+    return GRICO_ERR_TIMEOUT;
+  }
+  return GRICO_OK;
 }
 
 }  // extern "C"

@@ -227,6 +227,9 @@ SIGNATURES = {
     "grico_mg_learned_stats": (C.c_int, [P, i64p, i64p]),
     "grico_conv3d_forward": (C.c_int, [P, C.c_int, P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                        C.c_int, C.c_int, P]),
+    "grico_conv3d_forward_tc": (C.c_int, [P, C.c_int, P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                          C.c_int, C.c_int, P]),
+    "grico_conv_tc_status": (C.c_int, [P]),
     "grico_conv3d_backward_data": (C.c_int, [P, P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P]),
     "grico_conv3d_backward_weight": (C.c_int, [P, P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P]),
     "grico_relu_backward": (C.c_int, [P, P, C.c_int64, P]),

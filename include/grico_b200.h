@@ -419,6 +419,14 @@ int grico_mg_learned_stats(GricoMultigrid* mg, int64_t* sweeps, int64_t* accepte
  * [out][in][27] FP32; activations FP32 or BF16 (x_bf16 / y_bf16), FP32 arithmetic. */
 int grico_conv3d_forward(const void* x, int x_bf16, const float* w, const float* bias, void* y, int y_bf16, int B,
                          int Ci, int Co, int Z, int Y, int X, int relu, void* stream);
+/* The same convolution on the tensor cores (tcgen05.mma, BF16 operands: x and w rounded to BF16,
+ * FP32 accumulation in tensor memory), for Ci a multiple of 16 and Co a multiple of 32 up to 128
+ * (the 32-channel layers of the network); other shapes are rejected with GRICO_ERR_INVALID. */
+int grico_conv3d_forward_tc(const void* x, int x_bf16, const float* w, const float* bias, void* y, int y_bf16, int B,
+                            int Ci, int Co, int Z, int Y, int X, int relu, void* stream);
+/* Synchronises `stream`; GRICO_ERR_TIMEOUT (and the flag cleared) if a bounded wait of the
+ * tensor-core convolution gave up on the current device since the last call, else GRICO_OK. */
+int grico_conv_tc_status(void* stream);
 /* gx = transposed convolution of gy; wt: scratch of Co*Ci*27 floats */
 int grico_conv3d_backward_data(const float* gy, const float* w, float* wt, float* gx, int B, int Ci, int Co, int Z,
                                int Y, int X, void* stream);
