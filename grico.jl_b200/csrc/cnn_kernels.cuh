@@ -187,6 +187,18 @@ __global__ void grid_gather(const int64_t* __restrict__ idx, int64_t n_grid, con
   }
 }
 
+// the same into channel 0 of a channels-last grid: dst[g * stride]
+template <typename TS, typename TD>
+__global__ void grid_gather_strided(const int64_t* __restrict__ idx, int64_t n_grid, const TS* __restrict__ src,
+                                    float scale, const double* __restrict__ scale_dev, TD* __restrict__ dst,
+                                    int stride) {
+  const float s = scale * (scale_dev ? float(*scale_dev) : 1.0f);
+  for (int64_t g = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; g < n_grid; g += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t i = idx[g];
+    dst[g * stride] = from_f<TD>(i >= 0 ? float(src[i]) * s : 0.0f);
+  }
+}
+
 // dst[idx[g]] += src[g] * scale * (scale_dev ? *scale_dev : 1) (each dof appears once in the grid)
 template <typename TS, typename TD>
 __global__ void grid_scatter_add(const int64_t* __restrict__ idx, int64_t n_grid, const TS* __restrict__ src,

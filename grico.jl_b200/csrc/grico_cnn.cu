@@ -11,6 +11,7 @@
 #include "cnn_kernels.cuh"
 #include "cnn_tc.cuh"
 #include "grico_host.h"
+#include "grico_mg_internal.h"
 #include "vector_kernels.cuh"
 
 using namespace grico;
@@ -69,27 +70,54 @@ int conv_tc_err_ptr(int** out) {
   return GRICO_OK;
 }
 
-template <typename TIn, typename TOut>
-int launch_conv_tc(const void* x, const float* w, const float* bias, void* y, int B, int Ci, int Co, int Z, int Y,
-                   int X, int relu, cudaStream_t st) {
+}  // namespace
+
+namespace grico {
+
+int conv_tc_forward(const void* x, const void* wp, const float* bias, void* y, int out_cf, int B, int Ci, int Co,
+                    int Z, int Y, int X, int relu, cudaStream_t st) {
   int* err = nullptr;
   if (int rc = conv_tc_err_ptr(&err)) return rc;
-  auto kern = tc::conv3d_fwd_tc<TIn, TOut>;
+  void (*kern)(const __nv_bfloat16*, const __nv_bfloat16*, const float*, void*, int, int, int, int, int, int, int,
+               int, int*) = nullptr;
+  switch (Ci) {
+    case 16: kern = tc::conv3d_cl_tc<2>; break;
+    case 32: kern = tc::conv3d_cl_tc<4>; break;
+    case 48: kern = tc::conv3d_cl_tc<6>; break;
+    case 64: kern = tc::conv3d_cl_tc<8>; break;
+    default: set_error("grico_conv3d_forward_tc: Ci must be 16, 32, 48 or 64"); return GRICO_ERR_INVALID;
+  }
   const size_t smem = tc::conv_tc_smem_bytes(Ci, Co);
-  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess ||
+      cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100) != cudaSuccess)
     return launch_status("grico_conv3d_forward_tc");
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, tc::kThreads, smem) != cudaSuccess || per_sm < 1)
     return launch_status("grico_conv3d_forward_tc");
+  per_sm = std::min<int>(per_sm, int(512 / tc::conv_tc_tmem_cols(Co)));  // TMEM: 512 columns per SM
   int dev = 0, sms = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int64_t tiles = int64_t(B) * Z * ((Y + tc::kTY - 1) / tc::kTY) * ((X + tc::kTX - 1) / tc::kTX);
-  const int grid = int(std::min<int64_t>(tiles, int64_t(per_sm) * sms));
-  kern<<<grid, tc::kThreads, smem, st>>>(static_cast<const TIn*>(x), w, bias, static_cast<TOut*>(y), B, Ci, Co, Z, Y,
-                                         X, relu, err);
+  const int ctas = per_sm * sms;
+  const int seglen = tc::conv_tc_seglen(B, Z, Y, X, ctas);
+  const int64_t items = int64_t(B) * ((Y + tc::kTY - 1) / tc::kTY) * ((X + tc::kTX - 1) / tc::kTX) *
+                        ((Z + seglen - 1) / seglen);
+  const int grid = int(std::min<int64_t>(items, ctas));
+  kern<<<grid, tc::kThreads, smem, st>>>(static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(wp),
+                                         bias, y, out_cf, B, Co, Z, Y, X, seglen, relu, err);
   return launch_status("grico_conv3d_forward_tc");
 }
+
+int conv_tc_pack(const float* w, int Ci, int Co, void* wp, cudaStream_t st) {
+  const int n = 27 * Ci * tc::conv_tc_npad(Co);
+  tc::conv_tc_pack_weights<<<std::min((n + 255) / 256, 1024), 256, 0, st>>>(w, static_cast<__nv_bfloat16*>(wp), Ci,
+                                                                             Co, tc::conv_tc_npad(Co));
+  return launch_status("grico_conv3d_pack_weights_tc");
+}
+
+}  // namespace grico
+
+namespace {
 
 }  // namespace
 
@@ -199,21 +227,35 @@ int grico_weighted_residual(const float* r, const float* ar, const float* w, flo
   return launch_status("grico_weighted_residual");
 }
 
-// Tensor-core forward convolution (tcgen05.mma, BF16 operands rounded from the inputs and
-// weights, FP32 accumulation): same arguments and layout as grico_conv3d_forward, for
-// Ci a multiple of 16 and Co a multiple of 32 up to 128.
-int grico_conv3d_forward_tc(const void* x, int x_bf16, const float* w, const float* bias, void* y, int y_bf16, int B,
-                            int Ci, int Co, int Z, int Y, int X, int relu, void* stream) {
-  if (!x || !w || !y || !conv_args_ok(B, Ci, Co, Z, Y, X) || !tc::conv_tc_supported(Ci, Co)) {
-    set_error("grico_conv3d_forward_tc: invalid argument (Ci must be a multiple of 16, Co a multiple of 32 up to 128)");
+// Bytes of the packed BF16 weights of the tensor-core convolution (Ci, Co), or -1 when the
+// shape is not served.
+int64_t grico_conv_tc_weight_bytes(int Ci, int Co) {
+  return tc::conv_tc_supported(Ci, Co) ? int64_t(tc::conv_tc_weight_bytes(Ci, Co)) : -1;
+}
+
+// FP32 weights [Co][Ci][27] -> packed BF16 weights (grico_conv_tc_weight_bytes bytes at wp).
+int grico_conv3d_pack_weights_tc(const float* w, int Ci, int Co, void* wp, void* stream) {
+  if (!w || !wp || !tc::conv_tc_supported(Ci, Co)) {
+    set_error("grico_conv3d_pack_weights_tc: invalid argument (Ci a multiple of 16, Co up to 128)");
     return GRICO_ERR_INVALID;
   }
-  cudaStream_t st = as_stream(stream);
-  if (!x_bf16 && !y_bf16) return launch_conv_tc<float, float>(x, w, bias, y, B, Ci, Co, Z, Y, X, relu, st);
-  if (!x_bf16 && y_bf16) return launch_conv_tc<float, __nv_bfloat16>(x, w, bias, y, B, Ci, Co, Z, Y, X, relu, st);
-  if (x_bf16 && y_bf16)
-    return launch_conv_tc<__nv_bfloat16, __nv_bfloat16>(x, w, bias, y, B, Ci, Co, Z, Y, X, relu, st);
-  return launch_conv_tc<__nv_bfloat16, float>(x, w, bias, y, B, Ci, Co, Z, Y, X, relu, st);
+  return conv_tc_pack(w, Ci, Co, wp, as_stream(stream));
+}
+
+// Tensor-core forward convolution (tcgen05.mma, BF16 operands, FP32 accumulation): x BF16
+// channels-last [B][Z][Y][X][Ci], wp packed weights, y BF16 channels-last [B][Z][Y][X][Co]
+// (y_layout 0) or FP32 [B][Co][Z][Y][X] (y_layout 1).
+int grico_conv3d_forward_tc(const void* x, const void* wp, const float* bias, void* y, int y_layout, int B, int Ci,
+                            int Co, int Z, int Y, int X, int relu, void* stream) {
+  const bool aligned = (reinterpret_cast<uintptr_t>(x) % 16 == 0) && (reinterpret_cast<uintptr_t>(wp) % 16 == 0) &&
+                       (y_layout == 1 || reinterpret_cast<uintptr_t>(y) % 16 == 0);
+  if (!x || !wp || !y || !aligned || (y_layout != 0 && y_layout != 1) || !conv_args_ok(B, Ci, Co, Z, Y, X) ||
+      !tc::conv_tc_supported(Ci, Co) || (y_layout == 0 && Co % 8 != 0)) {
+    set_error("grico_conv3d_forward_tc: invalid argument (Ci a multiple of 16, Co up to 128 and a multiple of 8 for "
+              "channels-last output, 16-byte aligned buffers)");
+    return GRICO_ERR_INVALID;
+  }
+  return conv_tc_forward(x, wp, bias, y, y_layout, B, Ci, Co, Z, Y, X, relu, as_stream(stream));
 }
 
 // Synchronises `stream` and reports (then clears) a bounded wait of the tensor-core convolution

@@ -30,6 +30,9 @@
 #include "vector_kernels.cuh"
 #include "cnn_kernels.cuh"
 
+// input channels of the tensor-core network: the 2 inputs padded to one K = 16 step
+constexpr int kTcIn = 16;
+
 struct GricoMultigrid {
   struct Transfer {
     int64_t nf = 0, nc = 0;
@@ -63,6 +66,10 @@ struct GricoMultigrid {
     std::vector<grico::DevBuf> w, bias;  // FP32 weights [co][ci][27] and biases per layer
     grico::DevBuf idx;                   // grid point -> reduced dof (or -1)
     grico::DevBuf in, act0, act1;        // BF16 network input (channel 1: log coefficient) and activations
+    // tensor-core path (every layer served by tcgen05): channels-last activations, the input
+    // padded to kTcIn channels (0: residual, 1: log coefficient, others zero), packed weights
+    bool tc = false;
+    std::vector<grico::DevBuf> wp;
     grico::DevBuf out;                   // FP32 network output grid
     grico::DevBuf xn, tn, z;             // candidate iterate, its operator image, D^-1 r (level precision)
     grico::DevBuf stats;                 // [sweeps, accepted sweeps]
@@ -438,22 +445,36 @@ void learned_sweep(GricoMultigrid* mg, int l, T* x, const T* b, cudaStream_t st)
   residual_scale<<<1, 1, 0, st>>>(sc, n);
   const int gb = int(std::min<int64_t>((L.n_grid + 255) / 256, 148 * 16));
   __nv_bfloat16* in = L.in.get<__nv_bfloat16>();
-  grid_gather<T, __nv_bfloat16><<<gb, 256, 0, st>>>(L.idx.get<int64_t>(), L.n_grid, lbuf<T>(L.z), 1.0f, sc + 2, in);
   const int nl = int(L.w.size());
-  const __nv_bfloat16* src = in;
-  for (int k = 0; k < nl; ++k) {
-    const int ci = L.ch[k], co = L.ch[k + 1];
-    const int tiles = ((L.nx + kConvTile - 1) / kConvTile) * ((L.ny + kConvTile - 1) / kConvTile) *
-                      ((L.nz + kConvTile - 1) / kConvTile);
-    const dim3 grid(tiles, (co + kConvCo - 1) / kConvCo, 1);
-    if (k + 1 < nl) {
-      __nv_bfloat16* dst = (k % 2 == 0) ? L.act0.get<__nv_bfloat16>() : L.act1.get<__nv_bfloat16>();
-      conv3d_fwd<__nv_bfloat16, __nv_bfloat16><<<grid, 512, 0, st>>>(src, L.w[k].get<float>(), L.bias[k].get<float>(),
-                                                                     dst, ci, co, L.nz, L.ny, L.nx, 1);
+  if (L.tc) {
+    grid_gather_strided<T, __nv_bfloat16><<<gb, 256, 0, st>>>(L.idx.get<int64_t>(), L.n_grid, lbuf<T>(L.z), 1.0f,
+                                                               sc + 2, in, kTcIn);
+    const void* src = in;
+    for (int k = 0; k < nl; ++k) {
+      const int ci = k == 0 ? kTcIn : L.ch[k], co = L.ch[k + 1];
+      const bool last = k + 1 == nl;
+      void* dst = last ? L.out.ptr : ((k % 2 == 0) ? L.act0.ptr : L.act1.ptr);
+      conv_tc_forward(src, L.wp[k].ptr, L.bias[k].get<float>(), dst, last ? 1 : 0, 1, ci, co, L.nz, L.ny, L.nx,
+                      last ? 0 : 1, st);
       src = dst;
-    } else {
-      conv3d_fwd<__nv_bfloat16, float><<<grid, 512, 0, st>>>(src, L.w[k].get<float>(), L.bias[k].get<float>(),
-                                                             L.out.get<float>(), ci, co, L.nz, L.ny, L.nx, 0);
+    }
+  } else {
+    grid_gather<T, __nv_bfloat16><<<gb, 256, 0, st>>>(L.idx.get<int64_t>(), L.n_grid, lbuf<T>(L.z), 1.0f, sc + 2, in);
+    const __nv_bfloat16* src = in;
+    for (int k = 0; k < nl; ++k) {
+      const int ci = L.ch[k], co = L.ch[k + 1];
+      const int tiles = ((L.nx + kConvTile - 1) / kConvTile) * ((L.ny + kConvTile - 1) / kConvTile) *
+                        ((L.nz + kConvTile - 1) / kConvTile);
+      const dim3 grid(tiles, (co + kConvCo - 1) / kConvCo, 1);
+      if (k + 1 < nl) {
+        __nv_bfloat16* dst = (k % 2 == 0) ? L.act0.get<__nv_bfloat16>() : L.act1.get<__nv_bfloat16>();
+        conv3d_fwd<__nv_bfloat16, __nv_bfloat16><<<grid, 512, 0, st>>>(src, L.w[k].get<float>(), L.bias[k].get<float>(),
+                                                                       dst, ci, co, L.nz, L.ny, L.nx, 1);
+        src = dst;
+      } else {
+        conv3d_fwd<__nv_bfloat16, float><<<grid, 512, 0, st>>>(src, L.w[k].get<float>(), L.bias[k].get<float>(),
+                                                               L.out.get<float>(), ci, co, L.nz, L.ny, L.nx, 0);
+      }
     }
   }
   T* xn = lbuf<T>(L.xn);
@@ -807,16 +828,43 @@ int grico_mg_set_learned(GricoMultigrid* mg, const GricoLearnedDesc* d) {
   L.bias.resize(d->n_layers);
   for (int k = 0; k < d->n_layers && ok; ++k)
     ok = L.w[k].upload(d->weights[k], size_t(L.ch[k + 1]) * L.ch[k] * 27) && L.bias[k].upload(d->biases[k], size_t(L.ch[k + 1]));
-  std::vector<__nv_bfloat16> coef(ng);
-  for (int64_t g = 0; g < ng; ++g) coef[g] = __float2bfloat16(d->grid_log_coefficient[g]);
+  // every layer on the tensor cores when the shapes allow: hidden widths multiples of 16 up to 128
+  L.tc = true;
+  for (int k = 0; k < d->n_layers; ++k) {
+    const int ci = k == 0 ? kTcIn : L.ch[k], co = L.ch[k + 1];
+    if (grico_conv_tc_weight_bytes(ci, co) < 0 || (k + 1 < d->n_layers && co % 16 != 0)) L.tc = false;
+  }
+  if (L.tc) {
+    L.wp.resize(d->n_layers);
+    for (int k = 0; k < d->n_layers && ok; ++k) {
+      const int ci = k == 0 ? kTcIn : L.ch[k], co = L.ch[k + 1];
+      grico::DevBuf padded;  // first layer: [co][kTcIn][27] with zero weights on the padding channels
+      const float* wsrc = L.w[k].get<float>();
+      if (k == 0) {
+        std::vector<float> wpad(size_t(co) * kTcIn * 27, 0.0f);
+        for (int o = 0; o < co; ++o)
+          for (int i = 0; i < L.ch[0]; ++i)
+            for (int t = 0; t < 27; ++t) wpad[(size_t(o) * kTcIn + i) * 27 + t] = d->weights[0][(size_t(o) * L.ch[0] + i) * 27 + t];
+        ok = padded.upload(wpad.data(), wpad.size());
+        wsrc = padded.get<float>();
+      }
+      ok = ok && L.wp[k].alloc(size_t(grico_conv_tc_weight_bytes(ci, co))) &&
+           grico::conv_tc_pack(wsrc, ci, co, L.wp[k].ptr, mg->stream) == GRICO_OK &&
+           cuda_ok(cudaStreamSynchronize(mg->stream), "pack learned weights");
+    }
+  }
+  const int in_ch = L.tc ? kTcIn : 2;
+  std::vector<__nv_bfloat16> coef(size_t(in_ch) * ng, __float2bfloat16(0.0f));
+  // channel 1 of the input: channel-first [2][grid] or channels-last [grid][kTcIn]
+  for (int64_t g = 0; g < ng; ++g)
+    coef[L.tc ? g * kTcIn + 1 : ng + g] = __float2bfloat16(d->grid_log_coefficient[g]);
   const size_t vb = (mg->opts.precision == GRICO_PREC_FP32 ? 4 : 8) * size_t(std::max<int64_t>(n, 1));
-  ok = ok && L.in.alloc(2 * sizeof(__nv_bfloat16) * ng) && L.act0.alloc(sizeof(__nv_bfloat16) * maxc * ng) &&
+  ok = ok && L.in.alloc(size_t(in_ch) * sizeof(__nv_bfloat16) * ng) && L.act0.alloc(sizeof(__nv_bfloat16) * maxc * ng) &&
        L.act1.alloc(sizeof(__nv_bfloat16) * maxc * ng) && L.out.alloc(sizeof(float) * ng) && L.xn.alloc(vb) &&
        L.tn.alloc(vb) && L.z.alloc(vb) && L.stats.alloc(2 * sizeof(unsigned long long));
   if (!ok) return GRICO_ERR_CUDA;
   cudaMemsetAsync(L.stats.ptr, 0, 2 * sizeof(unsigned long long), mg->stream);
-  cudaMemcpyAsync(L.in.get<__nv_bfloat16>() + ng, coef.data(), sizeof(__nv_bfloat16) * ng, cudaMemcpyHostToDevice,
-                  mg->stream);
+  cudaMemcpyAsync(L.in.ptr, coef.data(), sizeof(__nv_bfloat16) * coef.size(), cudaMemcpyHostToDevice, mg->stream);
   if (!cuda_ok(cudaStreamSynchronize(mg->stream), "set learned")) return GRICO_ERR_CUDA;
   mg->learned = std::move(L);
   return GRICO_OK;

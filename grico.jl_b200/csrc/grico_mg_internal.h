@@ -13,4 +13,9 @@ int mg_smoother(const GricoMultigrid* mg);
 uint64_t mg_identity(const GricoMultigrid* mg);
 // sum of the level plans' epochs (changes when a level's kernels or their arguments change)
 uint64_t mg_epoch(const GricoMultigrid* mg);
+// tensor-core convolution (csrc/grico_cnn.cu): packed BF16 weights from FP32 [Co][Ci][27], and
+// the forward pass on channels-last BF16 activations (out_cf: FP32 channel-first output)
+int conv_tc_pack(const float* w, int Ci, int Co, void* wp, cudaStream_t st);
+int conv_tc_forward(const void* x, const void* wp, const float* bias, void* y, int out_cf, int B, int Ci, int Co,
+                    int Z, int Y, int X, int relu, cudaStream_t st);
 }  // namespace grico

@@ -227,8 +227,10 @@ SIGNATURES = {
     "grico_mg_learned_stats": (C.c_int, [P, i64p, i64p]),
     "grico_conv3d_forward": (C.c_int, [P, C.c_int, P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                        C.c_int, C.c_int, P]),
-    "grico_conv3d_forward_tc": (C.c_int, [P, C.c_int, P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
-                                          C.c_int, C.c_int, P]),
+    "grico_conv_tc_weight_bytes": (C.c_int64, [C.c_int, C.c_int]),
+    "grico_conv3d_pack_weights_tc": (C.c_int, [P, C.c_int, C.c_int, P, P]),
+    "grico_conv3d_forward_tc": (C.c_int, [P, P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                          C.c_int, P]),
     "grico_conv_tc_status": (C.c_int, [P]),
     "grico_conv3d_backward_data": (C.c_int, [P, P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P]),
     "grico_conv3d_backward_weight": (C.c_int, [P, P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P]),

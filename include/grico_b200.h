@@ -419,11 +419,15 @@ int grico_mg_learned_stats(GricoMultigrid* mg, int64_t* sweeps, int64_t* accepte
  * [out][in][27] FP32; activations FP32 or BF16 (x_bf16 / y_bf16), FP32 arithmetic. */
 int grico_conv3d_forward(const void* x, int x_bf16, const float* w, const float* bias, void* y, int y_bf16, int B,
                          int Ci, int Co, int Z, int Y, int X, int relu, void* stream);
-/* The same convolution on the tensor cores (tcgen05.mma, BF16 operands: x and w rounded to BF16,
- * FP32 accumulation in tensor memory), for Ci a multiple of 16 and Co a multiple of 32 up to 128
- * (the 32-channel layers of the network); other shapes are rejected with GRICO_ERR_INVALID. */
-int grico_conv3d_forward_tc(const void* x, int x_bf16, const float* w, const float* bias, void* y, int y_bf16, int B,
-                            int Ci, int Co, int Z, int Y, int X, int relu, void* stream);
+/* The convolution on the tensor cores (tcgen05.mma, BF16 operands, FP32 accumulation in tensor
+ * memory) with channels-last activations: x BF16 [batch][z][y][x][Ci], Ci a multiple of 16;
+ * weights packed once by grico_conv3d_pack_weights_tc; y BF16 channels-last [batch][z][y][x][Co]
+ * (y_layout 0, Co a multiple of 8) or FP32 [batch][Co][z][y][x] (y_layout 1); Co up to 128; x,
+ * wp and a channels-last y 16-byte aligned.  Other shapes are rejected with GRICO_ERR_INVALID. */
+int64_t grico_conv_tc_weight_bytes(int Ci, int Co); /* -1: shape not served */
+int grico_conv3d_pack_weights_tc(const float* w, int Ci, int Co, void* wp, void* stream);
+int grico_conv3d_forward_tc(const void* x, const void* wp, const float* bias, void* y, int y_layout, int B, int Ci,
+                            int Co, int Z, int Y, int X, int relu, void* stream);
 /* Synchronises `stream`; GRICO_ERR_TIMEOUT (and the flag cleared) if a bounded wait of the
  * tensor-core convolution gave up on the current device since the last call, else GRICO_OK. */
 int grico_conv_tc_status(void* stream);

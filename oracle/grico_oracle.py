@@ -1300,14 +1300,15 @@ def cg_solve(apply_fn, b, precond=None, rtol=1e-10, atol=0.0, maxiter=10000):
     raise ValueError("CG did not converge")
 
 
-def fgmres_solve(apply_fn, b, precond=None, restart=30, rtol=1e-10, atol=0.0, maxiter=10000):
+def fgmres_solve(apply_fn, b, precond=None, restart=30, rtol=1e-10, atol=0.0, maxiter=10000, raise_unconverged=True):
     """Right-preconditioned flexible GMRES(restart) with modified Gram-Schmidt, restated from
     `_fgmres_solve` (solve.jl:433-542): Givens rotations on each new Hessenberg column
     (`_apply_previous_givens_rotations!`, `_givens_rotation`, `_apply_givens_rotation!`,
     solve.jl:544-576), the cycle ends when |g[j+1]| <= tol or the Arnoldi norm is zero, and
     `_finish_fgmres_cycle!` (solve.jl:578-589) back-substitutes (`_upper_triangular_solve!`,
     solve.jl:591-614), adds Z y to x and recomputes the true residual b - A x.
-    Returns (x, total inner iterations)."""
+    Returns (x, total inner iterations); after maxiter without convergence it raises, as the
+    reference does (solve.jl:541), or with raise_unconverged=False returns the last iterate."""
     n = len(b)
     x = np.zeros(n)
     r = np.array(b, dtype=np.float64, copy=True)
@@ -1387,6 +1388,8 @@ def fgmres_solve(apply_fn, b, precond=None, restart=30, rtol=1e-10, atol=0.0, ma
             x, r = finish(H, g, Z, inner)
         if math.sqrt(float(np.dot(r, r))) <= tol:
             return x, total
+    if not raise_unconverged:
+        return x, total
     raise ValueError("FGMRES did not converge")
 
 

@@ -11,7 +11,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def declared_functions():
     text = open(os.path.join(ROOT, "include", "grico_b200.h")).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"^\s*(?:int|double|const char\*)\s+(grico_\w+)\s*\(", text, flags=re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|int64_t|double|const char\*)\s+(grico_\w+)\s*\(", text, flags=re.M)))
 
 
 def test_every_declared_symbol_is_exported():
@@ -66,3 +66,14 @@ def test_descriptor_validation_runs_before_cuda():
     desc.batches = batch
     assert L.lib().grico_plan_create(ctypes.byref(desc), ctypes.byref(handle)) == L.GRICO_ERR_INVALID
     assert b"out of range" in L.lib().grico_last_error()
+
+
+def test_conv_tc_weight_bytes():
+    """Packed tensor-core weights: 27 taps x Ci/8 chunks x N rows x 16 bytes, N = Co rounded up to
+    a multiple of 32; shapes the kernel does not serve report -1 (host-only, no device needed)."""
+    lib = L.lib()
+    assert lib.grico_conv_tc_weight_bytes(32, 32) == 27 * 4 * 32 * 16
+    assert lib.grico_conv_tc_weight_bytes(32, 1) == 27 * 4 * 32 * 16
+    assert lib.grico_conv_tc_weight_bytes(16, 40) == 27 * 2 * 64 * 16
+    assert lib.grico_conv_tc_weight_bytes(2, 32) == -1
+    assert lib.grico_conv_tc_weight_bytes(64, 128) == -1  # shared memory over 227 KB

