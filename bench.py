@@ -356,24 +356,33 @@ def learned_legs(gb, L, refine=7, train_refine=5, train_fields=6, train_steps=20
                 entry["learned_sweeps"], entry["learned_kept"] = lr.learned_stats(mg)
             results[name] = entry
             del mg
-    # the reference's method on the GPU: FP64, damped Jacobi (omega 0.8) V(2,2)
+    # the reference's method on the GPU: FP64, damped Jacobi (omega 0.8) V(2,2), without and with
+    # the learned sweep (the same V-cycle; the sweep replaces the last pre-smoothing step)
     opts = GeometricMultigridPreconditioner()
-    mg = Multigrid(*build_hierarchy(plan, opts), opts)
-    tries, hit = [], None
-    for rtol in (1e-4, 1e-5, 1e-6, 1e-7, 1e-8, 1e-9):
-        rc, rep, x = fgmres(mg, rtol, 3000)
-        diff = gb.State(plan, gb.expand_reduced(plan, x - ref), rep)
-        err = gb.l2_error(diff, lambda X: np.zeros(X.shape[0])) / ref_norm
-        tries.append({"rtol": rtol, "status": int(rc), "iterations": int(rep.iterations),
-                      "solve_seconds": float(rep.seconds), "relative_l2_error": err})
-        if rc == 0 and err <= target:
-            hit = tries[-1]
-            break
-        if rc != 0:
-            break
-    results["fp64_reference_jacobi_v22"] = {"time_to_target_seconds": hit["solve_seconds"] if hit else None,
-                                            "iterations": hit["iterations"] if hit else None, "tries": tries}
-    del mg
+    plans, transfers = build_hierarchy(plan, opts)
+    for learned in (False, True):
+        mg = Multigrid(plans, transfers, opts)
+        level = len(plans) - 2
+        if learned:
+            lr.attach(mg, plans[level], level, net, lr.level_log_coefficient(plans[level], field))
+        tries, hit = [], None
+        for rtol in (1e-4, 1e-5, 1e-6, 1e-7, 1e-8, 1e-9):
+            rc, rep, x = fgmres(mg, rtol, 3000)
+            diff = gb.State(plan, gb.expand_reduced(plan, x - ref), rep)
+            err = gb.l2_error(diff, lambda X: np.zeros(X.shape[0])) / ref_norm
+            tries.append({"rtol": rtol, "status": int(rc), "iterations": int(rep.iterations),
+                          "solve_seconds": float(rep.seconds), "relative_l2_error": err})
+            if rc == 0 and err <= target:
+                hit = tries[-1]
+                break
+            if rc != 0:
+                break
+        name = ("learned+" if learned else "") + "fp64_reference_jacobi_v22"
+        results[name] = {"time_to_target_seconds": hit["solve_seconds"] if hit else None,
+                         "iterations": hit["iterations"] if hit else None, "tries": tries}
+        if learned:
+            results[name]["learned_sweeps"], results[name]["learned_kept"] = lr.learned_stats(mg)
+        del mg
     return {"dofs": plan.n_full, "levels": len(plans), "train": {
         "fields": train_fields, "field_cells": f"{2 ** train_refine}^3 (degree 1)", "residual_grids":
         sum(len(s.residuals) for s in samples), "steps": train_steps, "train_seconds": train_s,

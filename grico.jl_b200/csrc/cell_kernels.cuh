@@ -39,6 +39,11 @@ struct BatchView {
   const double* G;           // [n*q]   reference derivative table psi_i'(xi_p)
   const uint8_t* skip;       // nullable: cells excluded from the diagonal kernel
   const double* mass_pts;    // nullable [n_cells*nq]: pointwise mass added to the constant mass
+  // long tails, operator apply: the expansions are summed by tail_gather before the cell kernel
+  // (tail_x[rhs * n_tail + k]) and spread by tail_scatter after it (the kernel stores tail_y)
+  const void* tail_x = nullptr;
+  void* tail_y = nullptr;
+  int64_t n_tail = 0;
 };
 
 template <typename T>
@@ -47,6 +52,7 @@ __device__ __forceinline__ T gather_entry(const BatchView& b, int64_t e, const T
   if (v >= 0) return b.coef ? T(__ldg(b.coef + e)) * x[v] : x[v];
   if (v == -1) return T(0);
   int64_t k = -(int64_t(v) + 2);
+  if (b.tail_x) return static_cast<const T*>(b.tail_x)[blockIdx.y * b.n_tail + k];
   T s = T(0);
   for (int64_t t = b.tail_off[k]; t < b.tail_off[k + 1]; ++t) s += T(b.tail_coef[t]) * x[b.tail_idx[t]];
   return s;
@@ -61,7 +67,45 @@ __device__ __forceinline__ void scatter_entry(const BatchView& b, int64_t e, T v
   }
   if (v == -1) return;
   int64_t k = -(int64_t(v) + 2);
+  if (b.tail_y) {
+    static_cast<T*>(b.tail_y)[blockIdx.y * b.n_tail + k] = val;  // each tail belongs to one entry
+    return;
+  }
   for (int64_t t = b.tail_off[k]; t < b.tail_off[k + 1]; ++t) atomicAdd(y + b.tail_idx[t], T(b.tail_coef[t]) * val);
+}
+
+// xt[r * n_tail + k] = sum_t coef[t] x[r * n_vec + idx[t]] over the terms of tail k (rhs r =
+// blockIdx.y): one warp per tail, lanes over its terms, a shuffle reduction
+template <typename T>
+__global__ void tail_gather(const int64_t* __restrict__ off, const int32_t* __restrict__ idx,
+                            const double* __restrict__ coef, int64_t n_tail, const T* __restrict__ x, int64_t n_vec,
+                            T* __restrict__ xt) {
+  const int lane = threadIdx.x % 32;
+  const int64_t nw = int64_t(gridDim.x) * blockDim.x / 32;
+  x += blockIdx.y * n_vec;
+  xt += blockIdx.y * n_tail;
+  for (int64_t k = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) / 32; k < n_tail; k += nw) {
+    T s = T(0);
+    for (int64_t t = off[k] + lane; t < off[k + 1]; t += 32) s += T(coef[t]) * x[idx[t]];
+#pragma unroll
+    for (int d = 16; d > 0; d /= 2) s += __shfl_down_sync(0xffffffffu, s, d);
+    if (lane == 0) xt[k] = s;
+  }
+}
+
+// y[r * n_vec + idx[t]] += coef[t] yt[r * n_tail + k] over the terms of tail k: one warp per tail
+template <typename T>
+__global__ void tail_scatter(const int64_t* __restrict__ off, const int32_t* __restrict__ idx,
+                             const double* __restrict__ coef, int64_t n_tail, const T* __restrict__ yt, T* __restrict__ y,
+                             int64_t n_vec) {
+  const int lane = threadIdx.x % 32;
+  const int64_t nw = int64_t(gridDim.x) * blockDim.x / 32;
+  y += blockIdx.y * n_vec;
+  yt += blockIdx.y * n_tail;
+  for (int64_t k = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) / 32; k < n_tail; k += nw) {
+    const T v = yt[k];
+    for (int64_t t = off[k] + lane; t < off[k + 1]; t += 32) atomicAdd(y + idx[t], T(coef[t]) * v);
+  }
 }
 
 // 1-D tables of one (n, q) signature, passed by value so that fully unrolled contractions read

@@ -283,11 +283,59 @@ bool launch_fused(int dim, const DevBatch& bt, const BatchView& v, const T* x, T
   return false;
 }
 
+// Tail buffers of one batch map (DevMap::n_tail): only when the longest expansion has at least
+// kTailBufferMin terms and every tail belongs to a single map entry (the cell kernel stores one
+// value per tail).
+bool setup_tail_buffer(DevMap& m, const int32_t* map, int64_t ne, const int64_t* off, int64_t n_tail) {
+  m.n_tail = 0;
+  if (n_tail <= 0) return true;
+  int64_t longest = 0;
+  for (int64_t k = 0; k < n_tail; ++k) longest = std::max(longest, off[k + 1] - off[k]);
+  if (longest < kTailBufferMin) return true;
+  std::vector<uint8_t> seen(size_t(n_tail), 0);
+  for (int64_t e = 0; e < ne; ++e) {
+    if (map[e] > -2) continue;
+    const int64_t k = -(int64_t(map[e]) + 2);
+    if (k >= n_tail || seen[size_t(k)]) return true;
+    seen[size_t(k)] = 1;
+  }
+  if (!m.tx.alloc(sizeof(double) * size_t(n_tail) * kTailRhs) || !m.ty.alloc(sizeof(double) * size_t(n_tail) * kTailRhs))
+    return false;
+  m.n_tail = n_tail;
+  return true;
+}
+
+template <typename T>
+void launch_batch_cells(const GricoPlan& P, const DevBatch& b, BatchView& v, const T* x, T* y, int64_t nvec, int mode,
+                        const double* src, int nrhs, cudaStream_t st);
+
+// One cell batch.  Operator applies of a map with buffered tails run in three launches: the
+// tail sums (one warp per expansion), the cell kernel (tails read from and written to the
+// buffers), the tail scatter; long expansions no longer serialise one thread of the cell kernel.
 template <typename T>
 void launch_batch(const GricoPlan& P, const DevBatch& b, bool reduced, const T* x, T* y, int64_t nvec, int mode,
                   const double* src, int nrhs, cudaStream_t st) {
   BatchView v;
   fill_view(v, b, reduced);
+  const DevMap& m = reduced ? b.red : b.full;
+  const bool buffered = mode == 0 && x && m.n_tail > 0 && nrhs <= kTailRhs;
+  const dim3 tg(int(std::min<int64_t>((m.n_tail * 32 + 255) / 256, 148 * 16)), unsigned(nrhs));
+  if (buffered) {
+    tail_gather<T><<<tg, 256, 0, st>>>(m.toff.get<int64_t>(), m.tidx.get<int32_t>(), m.tcoef.get<double>(), m.n_tail,
+                                       x, nvec, m.tx.get<T>());
+    v.tail_x = m.tx.ptr;
+    v.tail_y = m.ty.ptr;
+    v.n_tail = m.n_tail;
+  }
+  launch_batch_cells<T>(P, b, v, x, y, nvec, mode, src, nrhs, st);
+  if (buffered)
+    tail_scatter<T><<<tg, 256, 0, st>>>(m.toff.get<int64_t>(), m.tidx.get<int32_t>(), m.tcoef.get<double>(), m.n_tail,
+                                        m.ty.get<T>(), y, nvec);
+}
+
+template <typename T>
+void launch_batch_cells(const GricoPlan& P, const DevBatch& b, BatchView& v, const T* x, T* y, int64_t nvec, int mode,
+                        const double* src, int nrhs, cudaStream_t st) {
   const int dim = P.dim;
   if (mode != 3 && mode != 4 && b.isotropic && b.q[0] >= b.n[0] &&
       launch_fused<T>(dim, b, v, x, y, nvec, T(P.mass), T(P.kappa), mode, src, nrhs, st))
@@ -967,6 +1015,7 @@ int grico_plan_create(const GricoPlanDesc* d, GricoPlan** out) {
       ok = ok && b.full.toff.upload(bd.tail_offsets, size_t(bd.n_tail + 1));
       ok = ok && b.full.tidx.upload(bd.tail_index, size_t(bd.tail_offsets[bd.n_tail]));
       ok = ok && b.full.tcoef.upload(bd.tail_coef, size_t(bd.tail_offsets[bd.n_tail]));
+      ok = ok && setup_tail_buffer(b.full, bd.map_index, ne, bd.tail_offsets, bd.n_tail);
     }
     // reduced-layout map
     std::vector<int32_t> rmap, tidx;
@@ -976,7 +1025,9 @@ int grico_plan_create(const GricoPlanDesc* d, GricoPlan** out) {
     compose_reduced(bd, nb, *d, rmap, rcoef, need_coef, toff, tidx, tcoef);
     ok = ok && b.red.map.upload(rmap);
     if (need_coef) ok = ok && b.red.coef.upload(rcoef);
-    if (toff.size() > 1) ok = ok && b.red.toff.upload(toff) && b.red.tidx.upload(tidx) && b.red.tcoef.upload(tcoef);
+    if (toff.size() > 1)
+      ok = ok && b.red.toff.upload(toff) && b.red.tidx.upload(tidx) && b.red.tcoef.upload(tcoef) &&
+           setup_tail_buffer(b.red, rmap.data(), int64_t(rmap.size()), toff.data(), int64_t(toff.size()) - 1);
     b.red_multiterm = toff.size() > 1;
     // Cells whose reduced map couples several local modes to one reduced dof (hanging-node
     // expansions) need off-diagonal local entries for the exact Jacobi diagonal; the reference

@@ -64,7 +64,15 @@ constexpr int kTileVariants = 10;
 
 struct DevMap {
   DevBuf map, coef, toff, tidx, tcoef;
+  // buffered tails (operator apply with long hanging-node expansions): the number of tails
+  // (0: the cell kernels walk the expansions themselves) and their per-right-hand-side sums
+  int64_t n_tail = 0;
+  DevBuf tx, ty;
 };
+// right-hand sides the tail buffers hold; more fall back to the unbuffered walk
+constexpr int kTailRhs = 32;
+// buffer the tails of a map whose longest expansion has at least this many terms
+constexpr int64_t kTailBufferMin = 8;
 
 struct DevBatch {
   int32_t n_cells = 0;

@@ -74,3 +74,35 @@ def test_lshape_exact_diagonal(cuda, lshape):
         for k, ent in R.items():
             diag[k] += sum(ci * K[i, j] * cj for i, ci in ent.items() for j, cj in ent.items())
     assert rel_err(gb.reduced_diagonal(plan), diag) <= TOL
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_buffered_tails_match_the_per_thread_walk(cuda, precision):
+    """Level-5 L-shape (hanging-node expansions up to 72 terms, buffered): the reduced apply of 32
+    right-hand sides (tails summed by one warp each before the cell kernel and spread after it)
+    equals the apply of 33 (above the buffer's width: each cell-kernel thread walks its own
+    expansions) on the same columns, and the single-column apply equals column 0."""
+    import ctypes as C
+
+    import torch
+
+    from grico_b200 import _lib as L
+    from grico_b200 import batched as bt
+    from grico_b200.problem import torch_stream_handle
+
+    plan = gb.compile(bt.lshape_problem(max_level=5))
+    n = plan.n_reduced
+    dt, prec = (torch.float64, L.GRICO_PREC_FP64) if precision == "fp64" else (torch.float32, L.GRICO_PREC_FP32)
+    rng = np.random.default_rng(3)
+    X = torch.tensor(rng.standard_normal((33, n)), dtype=dt, device="cuda")
+    Y = {}
+    for k in (1, 32, 33):
+        y = torch.empty((k, n), dtype=dt, device="cuda")
+        # torch's stream as the library reads it (a NULL stream would mean the plan's own stream)
+        L.check(L.lib().grico_reduced_apply(plan.handle, C.c_void_p(X.data_ptr()), C.c_void_p(y.data_ptr()), k, prec, 0,
+                                            C.c_void_p(torch_stream_handle())), "apply")
+        Y[k] = y.double().cpu().numpy()
+    tol = 1e-12 if precision == "fp64" else 2e-5
+    scale = np.max(np.abs(Y[33]))
+    assert np.max(np.abs(Y[32] - Y[33][:32])) <= tol * scale
+    assert np.max(np.abs(Y[1][0] - Y[33][0])) <= tol * scale
