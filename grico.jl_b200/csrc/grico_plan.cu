@@ -319,18 +319,27 @@ void launch_batch(const GricoPlan& P, const DevBatch& b, bool reduced, const T* 
   fill_view(v, b, reduced);
   const DevMap& m = reduced ? b.red : b.full;
   const bool buffered = mode == 0 && x && m.n_tail > 0 && nrhs <= kTailRhs;
-  const dim3 tg(int(std::min<int64_t>((m.n_tail * 32 + 255) / 256, 148 * 16)), unsigned(nrhs));
+  // several right-hand sides: lanes over the columns (kTailLaneRhs or more), else lanes over terms
+  const bool lanes_rhs = nrhs >= kTailLaneRhs;
+  const dim3 tg(int(std::min<int64_t>((m.n_tail * 32 + 255) / 256, 148 * 16)), lanes_rhs ? 1u : unsigned(nrhs));
   if (buffered) {
-    tail_gather<T><<<tg, 256, 0, st>>>(m.toff.get<int64_t>(), m.tidx.get<int32_t>(), m.tcoef.get<double>(), m.n_tail,
-                                       x, nvec, m.tx.get<T>());
+    if (lanes_rhs)
+      tail_gather_rhs<T><<<tg, 256, 0, st>>>(m.toff.get<int64_t>(), m.tidx.get<int32_t>(), m.tcoef.get<double>(),
+                                             m.n_tail, x, nvec, m.tx.get<T>(), nrhs);
+    else
+      tail_gather<T><<<tg, 256, 0, st>>>(m.toff.get<int64_t>(), m.tidx.get<int32_t>(), m.tcoef.get<double>(),
+                                         m.n_tail, x, nvec, m.tx.get<T>());
     v.tail_x = m.tx.ptr;
     v.tail_y = m.ty.ptr;
     v.n_tail = m.n_tail;
   }
   launch_batch_cells<T>(P, b, v, x, y, nvec, mode, src, nrhs, st);
-  if (buffered)
-    tail_scatter<T><<<tg, 256, 0, st>>>(m.toff.get<int64_t>(), m.tidx.get<int32_t>(), m.tcoef.get<double>(), m.n_tail,
-                                        m.ty.get<T>(), y, nvec);
+  if (buffered && lanes_rhs)
+    tail_scatter_rhs<T><<<tg, 256, 0, st>>>(m.toff.get<int64_t>(), m.tidx.get<int32_t>(), m.tcoef.get<double>(),
+                                            m.n_tail, m.ty.get<T>(), y, nvec, nrhs);
+  else if (buffered)
+    tail_scatter<T><<<tg, 256, 0, st>>>(m.toff.get<int64_t>(), m.tidx.get<int32_t>(), m.tcoef.get<double>(),
+                                        m.n_tail, m.ty.get<T>(), y, nvec);
 }
 
 template <typename T>

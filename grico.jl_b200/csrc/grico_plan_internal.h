@@ -71,6 +71,8 @@ struct DevMap {
 };
 // right-hand sides the tail buffers hold; more fall back to the unbuffered walk
 constexpr int kTailRhs = 32;
+// right-hand sides from which the tail kernels put the columns on the lanes of a warp
+constexpr int kTailLaneRhs = 8;
 // buffer the tails of a map whose longest expansion has at least this many terms
 constexpr int64_t kTailBufferMin = 8;
 
