@@ -45,6 +45,15 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
+def load_bf16_peak():
+    """Measured dense BF16 TFLOP/s (burst, cuBLAS) of this pool's B200s, else the fallback 1590."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return float(json.load(f).get("bf16_tflops", 1590.0))
+    return 1590.0
+
+
 def sample_vector(n):
     """_diagnostic_sample_vector (diagnostics.jl:107-121): sin(0.013 i) + 0.25 cos(0.037 i)."""
     i = np.arange(1, n + 1, dtype=np.float64)
@@ -564,6 +573,57 @@ def c3_leg(gb, L, peak):
                                                       "this mesh has hanging-node expansions"}}
 
 
+def conv_legs(L, peak_tf):
+    """The network's 3x3x3 convolutions, CUDA-core kernel (FP32 arithmetic, channel-first) vs the
+    tcgen05 tensor-core kernel (BF16 operands, channels-last): device time per call (CUDA
+    events, 20 calls after 3), on the 65^3 vertex grid of the 64^3-cell learned level and on a
+    batch of four 64^3 grids."""
+    import ctypes as C
+
+    import torch
+
+    lib = L.lib()
+    st = torch.cuda.Stream()
+    out = []
+    P = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
+    for (B, Ci, Co, Z, Y, X) in ((4, 32, 32, 64, 64, 64), (1, 32, 32, 65, 65, 65), (1, 16, 32, 65, 65, 65),
+                                 (1, 32, 1, 65, 65, 65)):
+        g = torch.Generator(device="cuda").manual_seed(B * 100 + Ci + Co)
+        with torch.cuda.stream(st):
+            x = torch.randn(B, Ci, Z, Y, X, device="cuda", generator=g).bfloat16()
+            xcl = x.permute(0, 2, 3, 4, 1).contiguous()
+            w = 0.2 * torch.randn(Co, Ci, 27, device="cuda", generator=g)
+            b = torch.randn(Co, device="cuda", generator=g)
+            y = torch.empty(B, Co, Z, Y, X, device="cuda", dtype=torch.bfloat16)
+            lay = 1 if Co % 8 else 0
+            ytc = (torch.empty(B, Co, Z, Y, X, device="cuda") if lay else
+                   torch.empty(B, Z, Y, X, Co, device="cuda", dtype=torch.bfloat16))
+            wp = torch.empty(lib.grico_conv_tc_weight_bytes(Ci, Co) // 2, device="cuda", dtype=torch.bfloat16)
+        torch.cuda.synchronize()
+        sh = C.c_void_p(st.cuda_stream)
+        L.check(lib.grico_conv3d_pack_weights_tc(P(w), Ci, Co, P(wp), sh), "pack")
+        calls = {"cuda_core_fp32": lambda: lib.grico_conv3d_forward(P(x), 1, P(w), P(b), P(y), 1, B, Ci, Co, Z, Y, X,
+                                                                    1, sh),
+                 "tcgen05_bf16": lambda: lib.grico_conv3d_forward_tc(P(xcl), P(wp), P(b), P(ytc), lay, B, Ci, Co, Z, Y,
+                                                                     X, 1, sh)}
+        row = {"batch": B, "ci": Ci, "co": Co, "grid": [Z, Y, X]}
+        flops = 2.0 * B * Z * Y * X * Co * Ci * 27
+        for name, fn in calls.items():
+            for _ in range(3):
+                L.check(fn(), name)
+            torch.cuda.synchronize()
+            ms = _timed_device(fn, 20, st)
+            row[name] = {"us": ms * 1e3, "tflops": flops / (ms * 1e-3) / 1e12}
+        L.check(lib.grico_conv_tc_status(sh), "conv tc status")
+        ref = y.float()
+        got = ytc.float() if lay else ytc.float().permute(0, 4, 1, 2, 3)
+        row["max_rel_diff"] = float((ref - got).abs().max() / ref.abs().max())
+        row["speedup"] = row["cuda_core_fp32"]["us"] / row["tcgen05_bf16"]["us"]
+        row["tcgen05_frac_of_bf16_peak"] = row["tcgen05_bf16"]["tflops"] / peak_tf
+        out.append(row)
+    return out
+
+
 def c4_leg(gb, L):
     out = learned_legs(gb, L, refine=6)
     leg = out["legs"]
@@ -574,6 +634,7 @@ def c4_leg(gb, L):
                        "solver": "FGMRES(30) + hp-GMG V(2,2)",
                        "note": "64^3 cells in the default run; --workload grf_learned128 runs 128^3"},
             "plain_fp64_seconds": leg["fp64"]["time_to_target_seconds"], "learned": out,
+            "network_convolutions": conv_legs(L, load_bf16_peak()),
             "cpu_baseline": {"value": None, "reason": "no CPU port of the FGMRES + GMG solve at this size"}}
 
 
@@ -692,7 +753,7 @@ def main():
                     "(ref_jacobi, fp64_nograph, fp64, mixed2, mixed3); default: all")
     ap.add_argument("--workload", default="poisson64",
                     choices=["poisson64", "fcm_shell64", "fcm_shell32", "grf_learned128", "grf_learned64",
-                             "lshape_hp32"],
+                             "lshape_hp32", "lshape_apply32", "conv_tc"],
                     help="poisson64: 3-D Poisson 64^3 p=4 (default); fcm_shell*: finite-cell shell with Nitsche")
     ap.add_argument("--fp32", action="store_true", help="time the FP32 apply instead of FP64")
     ap.add_argument("--no-configs", action="store_true", help="skip the other BASELINE configurations")
@@ -718,6 +779,38 @@ def main():
     import grico_b200 as gb
     from grico_b200 import _lib as L
 
+    if args.workload == "conv_tc":
+        # the network's convolutions alone (CUDA-core vs tensor-core kernels), for profiling
+        rows = conv_legs(L, load_bf16_peak())
+        if rank == 0:
+            print(json.dumps({"metric": "3x3x3 convolution device time", "unit": "us", "n_gpus": world,
+                              "higher_is_better": False, "data": "synthetic (seeded normal activations)",
+                              "config": {"workload": "conv_tc"}, "convolutions": rows}), flush=True)
+        return
+    if args.workload == "lshape_apply32":
+        # the hp L-shape's reduced FP64 apply, 1 and 32 right-hand sides, W untimed then K timed
+        import torch
+
+        from grico_b200 import batched as bt
+
+        plan = gb.compile(bt.lshape_problem(max_level=7))
+        res = {}
+        st = torch.cuda.Stream()
+        for k in (1, 32):
+            xv = torch.ones(k * plan.n_reduced, dtype=torch.float64, device="cuda")
+            yv = torch.empty_like(xv)
+            fn = lambda: L.lib().grico_reduced_apply(plan.handle, xv.data_ptr(), yv.data_ptr(), k, L.GRICO_PREC_FP64,
+                                                     0, st.cuda_stream)
+            for _ in range(args.warmup):
+                fn()
+            torch.cuda.synchronize()
+            res[f"nrhs{k}_ms"] = _timed_device(fn, args.steps, st)
+        if rank == 0:
+            print(json.dumps({"metric": "reduced FP64 apply device time (adaptive hp L-shape)", "unit": "ms",
+                              "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+                              "data": "synthetic", "config": {"workload": "lshape_apply32", "dofs": plan.n_full,
+                                                               "reduced_dofs": plan.n_reduced}, **res}), flush=True)
+        return
     if args.workload == "lshape_hp32":
         out = batched_legs(gb, L)
         if rank == 0:

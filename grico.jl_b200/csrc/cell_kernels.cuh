@@ -93,45 +93,52 @@ __global__ void tail_gather(const int64_t* __restrict__ off, const int32_t* __re
   }
 }
 
-// The same sums for nrhs <= 32 right-hand sides at once: one warp per tail, lane r = right-hand
-// side, so each term's index and coefficient are read once for all columns
+// Tail segments of at most kTailSeg terms, for nrhs <= 32 right-hand sides at once: one warp per
+// segment, lane r = right-hand side, so each term's index and coefficient are read once for
+// all columns and a long expansion is spread over many warps.  The gather adds its partial sum
+// to xt (zeroed before); the scatter spreads yt over the segment's terms.
+constexpr int kTailSeg = 16;
+
 template <typename T>
-__global__ void tail_gather_rhs(const int64_t* __restrict__ off, const int32_t* __restrict__ idx,
-                                const double* __restrict__ coef, int64_t n_tail, const T* __restrict__ x, int64_t n_vec,
-                                T* __restrict__ xt, int nrhs) {
+__global__ void tail_gather_seg(const int32_t* __restrict__ seg_k, const int64_t* __restrict__ seg_t, int64_t n_seg,
+                                const int64_t* __restrict__ off, const int32_t* __restrict__ idx,
+                                const double* __restrict__ coef, int64_t n_tail, const T* __restrict__ x,
+                                int64_t n_vec, T* __restrict__ xt, int nrhs) {
   const int lane = threadIdx.x % 32;
   const bool on = lane < nrhs;
   const int64_t nw = int64_t(gridDim.x) * blockDim.x / 32;
   const T* xr = x + (on ? lane : 0) * n_vec;
-  for (int64_t k = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) / 32; k < n_tail; k += nw) {
-    T s0 = T(0), s1 = T(0);
-    const int64_t t1 = off[k + 1];
-    int64_t t = off[k];
-    for (; t + 1 < t1; t += 2) {
-      const int32_t i0 = __ldg(idx + t), i1 = __ldg(idx + t + 1);
-      const T c0 = T(__ldg(coef + t)), c1 = T(__ldg(coef + t + 1));
-      if (on) {
-        s0 += c0 * xr[i0];
-        s1 += c1 * xr[i1];
-      }
+  for (int64_t sg = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) / 32; sg < n_seg; sg += nw) {
+    const int32_t k = seg_k[sg];
+    const int64_t t0 = seg_t[sg], t1 = min(t0 + kTailSeg, off[k + 1]);
+    T acc = T(0);
+#pragma unroll
+    for (int u = 0; u < kTailSeg; ++u) {
+      const int64_t t = t0 + u;
+      if (t < t1 && on) acc += T(__ldg(coef + t)) * xr[__ldg(idx + t)];
     }
-    if (t < t1 && on) s0 += T(__ldg(coef + t)) * xr[__ldg(idx + t)];
-    if (on) xt[lane * n_tail + k] = s0 + s1;
+    if (on) atomicAdd(xt + lane * n_tail + k, acc);
   }
 }
 
 template <typename T>
-__global__ void tail_scatter_rhs(const int64_t* __restrict__ off, const int32_t* __restrict__ idx,
+__global__ void tail_scatter_seg(const int32_t* __restrict__ seg_k, const int64_t* __restrict__ seg_t, int64_t n_seg,
+                                 const int64_t* __restrict__ off, const int32_t* __restrict__ idx,
                                  const double* __restrict__ coef, int64_t n_tail, const T* __restrict__ yt,
                                  T* __restrict__ y, int64_t n_vec, int nrhs) {
   const int lane = threadIdx.x % 32;
   const bool on = lane < nrhs;
   const int64_t nw = int64_t(gridDim.x) * blockDim.x / 32;
   T* yr = y + (on ? lane : 0) * n_vec;
-  for (int64_t k = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) / 32; k < n_tail; k += nw) {
+  for (int64_t sg = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) / 32; sg < n_seg; sg += nw) {
+    const int32_t k = seg_k[sg];
+    const int64_t t0 = seg_t[sg], t1 = min(t0 + kTailSeg, off[k + 1]);
     const T v = on ? yt[lane * n_tail + k] : T(0);
-    for (int64_t t = off[k]; t < off[k + 1]; ++t)
-      if (on) atomicAdd(yr + __ldg(idx + t), T(__ldg(coef + t)) * v);
+#pragma unroll
+    for (int u = 0; u < kTailSeg; ++u) {
+      const int64_t t = t0 + u;
+      if (t < t1 && on) atomicAdd(yr + __ldg(idx + t), T(__ldg(coef + t)) * v);
+    }
   }
 }
 

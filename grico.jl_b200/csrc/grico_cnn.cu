@@ -74,6 +74,8 @@ int conv_tc_err_ptr(int** out) {
 
 namespace grico {
 
+int tc_error_flag(int** out) { return conv_tc_err_ptr(out); }
+
 int conv_tc_forward(const void* x, const void* wp, const float* bias, void* y, int out_cf, int B, int Ci, int Co,
                     int Z, int Y, int X, int relu, cudaStream_t st) {
   int* err = nullptr;
@@ -94,10 +96,20 @@ int conv_tc_forward(const void* x, const void* wp, const float* bias, void* y, i
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, tc::kThreads, smem) != cudaSuccess || per_sm < 1)
     return launch_status("grico_conv3d_forward_tc");
-  per_sm = std::min<int>(per_sm, int(512 / tc::conv_tc_tmem_cols(Co)));  // TMEM: 512 columns per SM
-  int dev = 0, sms = 1;
+  int dev = 0, sms = 1, smem_sm = 0, regs_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+  cudaFuncAttributes fa{};
+  if (cudaFuncGetAttributes(&fa, kern) == cudaSuccess && fa.numRegs > 0) {
+    // the occupancy query can answer 1 for two CTAs that fit (the carveout it assumes); the
+    // persistent grid does not rely on co-residency, so take the larger of the two estimates
+    const int by_smem = smem_sm / int(smem + fa.sharedSizeBytes + 1024);
+    const int by_regs = regs_sm / (fa.numRegs * tc::kThreads);
+    per_sm = std::max(per_sm, std::min({by_smem, by_regs, 2048 / tc::kThreads}));
+  }
+  per_sm = std::max(1, std::min<int>(per_sm, int(512 / tc::conv_tc_tmem_cols(Co))));  // TMEM: 512 columns per SM
   const int ctas = per_sm * sms;
   const int seglen = tc::conv_tc_seglen(B, Z, Y, X, ctas);
   const int64_t items = int64_t(B) * ((Y + tc::kTY - 1) / tc::kTY) * ((X + tc::kTX - 1) / tc::kTX) *
@@ -258,9 +270,10 @@ int grico_conv3d_forward_tc(const void* x, const void* wp, const float* bias, vo
   return conv_tc_forward(x, wp, bias, y, y_layout, B, Ci, Co, Z, Y, X, relu, as_stream(stream));
 }
 
-// Synchronises `stream` and reports (then clears) a bounded wait of the tensor-core convolution
-// that gave up on this device: GRICO_ERR_TIMEOUT, else GRICO_OK.
-int grico_conv_tc_status(void* stream) {
+// Synchronises `stream` and reports (then clears) a bounded wait of a tensor-core kernel (the
+// convolutions and the FP32 apply of uniform batches) that gave up on this device:
+// GRICO_ERR_TIMEOUT, else GRICO_OK.
+int grico_tc_status(void* stream) {
   int* err = nullptr;
   if (int rc = conv_tc_err_ptr(&err)) return rc;
   cudaStream_t st = as_stream(stream);
@@ -272,10 +285,12 @@ int grico_conv_tc_status(void* stream) {
     const int zero = 0;
     cudaMemcpyAsync(err, &zero, sizeof(int), cudaMemcpyHostToDevice, st);
     cudaStreamSynchronize(st);
-    set_error("grico_conv3d_forward_tc: a tensor-core wait gave up");
+    set_error("a tensor-core kernel's bounded wait gave up");
     return GRICO_ERR_TIMEOUT;
   }
   return GRICO_OK;
 }
+
+int grico_conv_tc_status(void* stream) { return grico_tc_status(stream); }
 
 }  // extern "C"

@@ -10,11 +10,13 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "cell_kernels.cuh"
 #include "cell_pipe.cuh"
 #include "cell_plane.cuh"
+#include "cell_dense_tc.cuh"
 #include "grico_host.h"
 #include "grico_plan_internal.h"
 #include "vector_kernels.cuh"
@@ -186,12 +188,34 @@ int persistent_blocks_per_sm(const void* kern, int threads, size_t smem) {
   return n;
 }
 
+// FP32 apply of a uniform batch on the tensor cores (cell_dense_tc.cuh): persistent CTAs, one
+// per SM (192 KB of shared memory each), gridDim.y = right-hand sides
+bool launch_dense(const DevBatch& bt, const BatchView& v, const float* x, float* y, int64_t nvec, int nrhs,
+                  cudaStream_t st) {
+  int* err = nullptr;
+  if (tc_error_flag(&err) != GRICO_OK) return false;
+  static const bool attr = cudaFuncSetAttribute(dense::cell_apply_dense_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                int(dense::kSmem)) == cudaSuccess;
+  if (!attr) return false;
+  const int64_t tiles = (int64_t(v.n_cells) + dense::kM - 1) / dense::kM;
+  const dim3 grid(unsigned(std::min<int64_t>(tiles, sm_count())), unsigned(nrhs));
+  dense::cell_apply_dense_tc<<<grid, dense::kThreads, dense::kSmem, st>>>(
+      v.map, v.n_cells, bt.n[0] * bt.n[1] * bt.n[2], bt.dense.get<__nv_bfloat16>(), x, y, nvec, err);
+  return true;
+}
+
 template <typename T>
 bool launch_fused(int dim, const DevBatch& bt, const BatchView& v, const T* x, T* y, int64_t nvec, T mass, T kappa,
                   int mode, const double* src, int nrhs, cudaStream_t st) {
   if (v.n_cells == 0) return true;
   const int N = bt.n[0], Q = bt.q[0];
   const int var = bt.tile[sizeof(T) == 4 ? 1 : 0];
+  // variant 10, FP32: uniform batch with a plain map on the tensor cores
+  if constexpr (std::is_same<T, float>::value) {
+    if (dim == 3 && var == kDenseVariant && mode == 0 && bt.dense_ok && v.coef == nullptr && v.tail_off == nullptr &&
+        v.mass_pts == nullptr && v.kappa_pts == nullptr && launch_dense(bt, v, x, y, nvec, nrhs, st))
+      return true;
+  }
 #define GRICO_L3_CPB(NN, QQ, CPB_)                                                                             \
   {                                                                                                            \
     constexpr int CPB = CPB_;                                                                                  \
@@ -301,6 +325,15 @@ bool setup_tail_buffer(DevMap& m, const int32_t* map, int64_t ne, const int64_t*
   }
   if (!m.tx.alloc(sizeof(double) * size_t(n_tail) * kTailRhs) || !m.ty.alloc(sizeof(double) * size_t(n_tail) * kTailRhs))
     return false;
+  std::vector<int32_t> sk;
+  std::vector<int64_t> st;
+  for (int64_t k = 0; k < n_tail; ++k)
+    for (int64_t t = off[k]; t < off[k + 1]; t += kTailSeg) {
+      sk.push_back(int32_t(k));
+      st.push_back(t);
+    }
+  if (!m.seg_k.upload(sk) || !m.seg_t.upload(st)) return false;
+  m.n_seg = int64_t(sk.size());
   m.n_tail = n_tail;
   return true;
 }
@@ -319,14 +352,18 @@ void launch_batch(const GricoPlan& P, const DevBatch& b, bool reduced, const T* 
   fill_view(v, b, reduced);
   const DevMap& m = reduced ? b.red : b.full;
   const bool buffered = mode == 0 && x && m.n_tail > 0 && nrhs <= kTailRhs;
-  // several right-hand sides: lanes over the columns (kTailLaneRhs or more), else lanes over terms
+  // several right-hand sides: segments with the columns on the lanes (kTailLaneRhs or more),
+  // else one warp per tail with the lanes over its terms
   const bool lanes_rhs = nrhs >= kTailLaneRhs;
-  const dim3 tg(int(std::min<int64_t>((m.n_tail * 32 + 255) / 256, 148 * 16)), lanes_rhs ? 1u : unsigned(nrhs));
+  const dim3 tg(int(std::min<int64_t>(((lanes_rhs ? m.n_seg : m.n_tail) * 32 + 255) / 256, 148 * 16)),
+                lanes_rhs ? 1u : unsigned(nrhs));
   if (buffered) {
-    if (lanes_rhs)
-      tail_gather_rhs<T><<<tg, 256, 0, st>>>(m.toff.get<int64_t>(), m.tidx.get<int32_t>(), m.tcoef.get<double>(),
+    if (lanes_rhs) {
+      cudaMemsetAsync(m.tx.ptr, 0, sizeof(T) * size_t(m.n_tail) * nrhs, st);
+      tail_gather_seg<T><<<tg, 256, 0, st>>>(m.seg_k.get<int32_t>(), m.seg_t.get<int64_t>(), m.n_seg,
+                                             m.toff.get<int64_t>(), m.tidx.get<int32_t>(), m.tcoef.get<double>(),
                                              m.n_tail, x, nvec, m.tx.get<T>(), nrhs);
-    else
+    } else
       tail_gather<T><<<tg, 256, 0, st>>>(m.toff.get<int64_t>(), m.tidx.get<int32_t>(), m.tcoef.get<double>(),
                                          m.n_tail, x, nvec, m.tx.get<T>());
     v.tail_x = m.tx.ptr;
@@ -335,7 +372,8 @@ void launch_batch(const GricoPlan& P, const DevBatch& b, bool reduced, const T* 
   }
   launch_batch_cells<T>(P, b, v, x, y, nvec, mode, src, nrhs, st);
   if (buffered && lanes_rhs)
-    tail_scatter_rhs<T><<<tg, 256, 0, st>>>(m.toff.get<int64_t>(), m.tidx.get<int32_t>(), m.tcoef.get<double>(),
+    tail_scatter_seg<T><<<tg, 256, 0, st>>>(m.seg_k.get<int32_t>(), m.seg_t.get<int64_t>(), m.n_seg,
+                                            m.toff.get<int64_t>(), m.tidx.get<int32_t>(), m.tcoef.get<double>(),
                                             m.n_tail, m.ty.get<T>(), y, nvec, nrhs);
   else if (buffered)
     tail_scatter<T><<<tg, 256, 0, st>>>(m.toff.get<int64_t>(), m.tidx.get<int32_t>(), m.tcoef.get<double>(),
@@ -1012,6 +1050,44 @@ int grico_plan_create(const GricoPlanDesc* d, GricoPlan** out) {
     b.hW.assign(W.begin(), W.begin() + b.q[0]);
     bool ok = b.B.upload(B) && b.G.upload(G) && b.W.upload(W) && b.D.upload(Dm);
     ok = ok && b.h.upload(bd.cell_size, size_t(bd.n_cells) * d->dim);
+    // uniform batch: the element matrix of the sum-factorised kernel, once, for the FP32
+    // tensor-core apply (K_e = det J [mass M (x) M (x) M + kappa sum_a (2 / h_a)^2 (1-D
+    // stiffness on axis a, mass on the others)], 1-D mass M = B W B^T, stiffness S = G W G^T)
+    b.dense_ok = false;
+    if (d->dim == 3 && b.isotropic && b.q[0] >= b.n[0] && nb <= dense::kK && !bd.kappa_points && bd.n_cells > 0) {
+      bool uniform = true;
+      for (int64_t c = 1; c < bd.n_cells && uniform; ++c)
+        for (int a = 0; a < 3; ++a) uniform = uniform && bd.cell_size[c * 3 + a] == bd.cell_size[a];
+      if (uniform) {
+        const int n = b.n[0], q = b.q[0];
+        std::vector<double> M1(size_t(n) * n, 0.0), S1(size_t(n) * n, 0.0);
+        for (int i = 0; i < n; ++i)
+          for (int j = 0; j < n; ++j)
+            for (int p = 0; p < q; ++p) {
+              M1[i * n + j] += W[p] * B[i * q + p] * B[j * q + p];
+              S1[i * n + j] += W[p] * G[i * q + p] * G[j * q + p];
+            }
+        const double* h = bd.cell_size;
+        const double detJ = h[0] * h[1] * h[2] * 0.125;
+        const double s0 = 4.0 / (h[0] * h[0]), s1 = 4.0 / (h[1] * h[1]), s2 = 4.0 / (h[2] * h[2]);
+        std::vector<double> Ke(size_t(nb) * nb);
+        for (int iz = 0; iz < n; ++iz)
+          for (int iy = 0; iy < n; ++iy)
+            for (int ix = 0; ix < n; ++ix)
+              for (int jz = 0; jz < n; ++jz)
+                for (int jy = 0; jy < n; ++jy)
+                  for (int jx = 0; jx < n; ++jx) {
+                    const double mx = M1[ix * n + jx], my = M1[iy * n + jy], mz = M1[iz * n + jz];
+                    const double sx = S1[ix * n + jx], sy = S1[iy * n + jy], sz = S1[iz * n + jz];
+                    Ke[size_t(ix + n * (iy + n * iz)) * nb + (jx + n * (jy + n * jz))] =
+                        detJ * (P->mass * mx * my * mz + P->kappa * (s0 * sx * my * mz + s1 * mx * sy * mz + s2 * mx * my * sz));
+                  }
+        std::vector<__nv_bfloat16> wp(2 * size_t(dense::kPiece) / sizeof(__nv_bfloat16));
+        dense::pack_element_matrix(Ke.data(), int(nb), wp.data());
+        ok = ok && b.dense.upload(wp);
+        b.dense_ok = true;  // selectable (grico_plan_set_tiles, the autotuner); not the default
+      }
+    }
     if (bd.kappa_points) {
       int64_t nq = 1;
       for (int a = 0; a < d->dim; ++a) nq *= b.q[a];

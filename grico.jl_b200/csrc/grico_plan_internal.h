@@ -60,7 +60,7 @@ struct DevBuf {
   bool upload(const std::vector<T>& v) { return upload(v.data(), v.size()); }
 };
 
-constexpr int kTileVariants = 10;
+constexpr int kTileVariants = 11;
 
 struct DevMap {
   DevBuf map, coef, toff, tidx, tcoef;
@@ -68,7 +68,15 @@ struct DevMap {
   // (0: the cell kernels walk the expansions themselves) and their per-right-hand-side sums
   int64_t n_tail = 0;
   DevBuf tx, ty;
+  // the tails cut into segments of at most kTailSeg terms: tail index and first term
+  int64_t n_seg = 0;
+  DevBuf seg_k, seg_t;
 };
+// tile variant of the FP32 tensor-core apply of uniform batches
+constexpr int kDenseVariant = 10;
+// error flag of the tensor-core kernels on the current device (a bounded wait that gave up);
+// defined with the convolutions in csrc/grico_cnn.cu
+int tc_error_flag(int** out);
 // right-hand sides the tail buffers hold; more fall back to the unbuffered walk
 constexpr int kTailRhs = 32;
 // right-hand sides from which the tail kernels put the columns on the lanes of a warp
@@ -87,6 +95,10 @@ struct DevBatch {
   DevBuf skip;  // uint8 per cell: hanging cells whose diagonal is added from the host
   DevBuf mass_pts;  // optional pointwise mass [n_cells * nq] added to the form's mass (grico_plan_set_mass_points)
   std::vector<double> hB, hD, hW;  // axis-0 tables on the host (kernel parameters)
+  // uniform batch (3-D, one cell size, constant coefficients, degree <= 4): the element matrix
+  // as BF16 hi/lo pieces for the FP32 tensor-core apply (csrc/cell_dense_tc.cuh)
+  bool dense_ok = false;
+  DevBuf dense;
   int tile[2] = {1, 1};  // 3-D tensor-kernel variant per precision (0: FP64, 1: FP32): cells per block
                          // half (0), default (1) or double (2) the default, one block per cell group;
                          // 3..5 the same sizes in the persistent cp.async-pipelined apply kernel

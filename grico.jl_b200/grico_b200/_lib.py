@@ -36,7 +36,7 @@ SUBCELL_SHAPES = {3: {(2, 2), (2, 3), (3, 3), (2, 4), (3, 4), (4, 4)},
 GRICO_PREC_FP64 = 0
 GRICO_PREC_FP32 = 1
 # 3-D tensor-kernel variants accepted by grico_plan_set_tiles (0..TILE_VARIANTS-1)
-TILE_VARIANTS = 10
+TILE_VARIANTS = 11
 GRICO_FLAG_HOST_POINTERS = 1
 GRICO_FLAG_NO_GRAPH = 2
 GRICO_FLAG_MIXED = 4
@@ -232,6 +232,7 @@ SIGNATURES = {
     "grico_conv3d_forward_tc": (C.c_int, [P, P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                           C.c_int, P]),
     "grico_conv_tc_status": (C.c_int, [P]),
+    "grico_tc_status": (C.c_int, [P]),
     "grico_conv3d_backward_data": (C.c_int, [P, P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P]),
     "grico_conv3d_backward_weight": (C.c_int, [P, P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P]),
     "grico_relu_backward": (C.c_int, [P, P, C.c_int64, P]),

@@ -19,7 +19,9 @@ def autotune(plan, nrhs=1, precision="fp64", reps=5):
     """Per cell batch: 0 = half, 1 = default, 2 = double cells per block (one block per cell
     group); 3, 4, 5 = the same sizes in the persistent pipelined apply kernel (even-odd
     contractions), 6, 7, 8 = with direct contractions; 9 = one warp per 32 / q cells with one
-    thread per cell plane."""
+    thread per cell plane; 10 = FP32 only, uniform batches of degree <= 4: one element matrix on
+    the tensor cores (tcgen05, BF16 hi/lo pieces, FP32 accumulation; measured slower than 3..9,
+    never the default)."""
     chosen = np.zeros(max(len(plan.batches), 1), dtype=np.int32)
     prec = L.GRICO_PREC_FP64 if precision == "fp64" else L.GRICO_PREC_FP32
     L.check(L.lib().grico_plan_autotune(plan.handle, int(nrhs), prec, int(reps), L.ptr(chosen, C.c_int32)), "autotune")

@@ -223,8 +223,12 @@ int grico_plan_create(const GricoPlanDesc* desc, GricoPlan** out);
  * prefetches the next cell group's gather with asynchronous copies, with the 1-D contractions in
  * even-odd form; 6, 7, 8 = that kernel with direct contractions; 9 = one warp per 32 / q cells
  * with one thread per cell plane (q <= 6, plain maps, constant coefficients; the default at
- * q <= 3).  Batches without a 3-D isotropic tensor kernel report 1.  Allocates scratch; call
- * before any stream capture. */
+ * q <= 3); 10 = FP32 only, uniform batches (one cell size, constant coefficients, plain maps,
+ * degree <= 4): one element matrix on the tensor cores (tcgen05, BF16 hi/lo pieces of x and of
+ * the matrix, FP32 accumulation; measured slower than 3..9 on B200, so never the default; other
+ * batches treat 10 as 1;
+ * a bounded wait that gave up is reported by grico_tc_status).  Batches without a 3-D
+ * isotropic tensor kernel report 1.  Allocates scratch; call before any stream capture. */
 int grico_plan_autotune(GricoPlan* plan, int nrhs, int precision, int reps, int* chosen);
 /* Sets the kernel variant of every cell batch for `precision` (tiles[n_batches], values as
  * reported by grico_plan_autotune), e.g. to replay a stored tuning without timing again.
@@ -428,8 +432,10 @@ int64_t grico_conv_tc_weight_bytes(int Ci, int Co); /* -1: shape not served */
 int grico_conv3d_pack_weights_tc(const float* w, int Ci, int Co, void* wp, void* stream);
 int grico_conv3d_forward_tc(const void* x, const void* wp, const float* bias, void* y, int y_layout, int B, int Ci,
                             int Co, int Z, int Y, int X, int relu, void* stream);
-/* Synchronises `stream`; GRICO_ERR_TIMEOUT (and the flag cleared) if a bounded wait of the
- * tensor-core convolution gave up on the current device since the last call, else GRICO_OK. */
+/* Synchronises `stream`; GRICO_ERR_TIMEOUT (and the flag cleared) if a bounded wait of a
+ * tensor-core kernel (the convolutions, the FP32 apply of uniform batches) gave up on the current
+ * device since the last call, else GRICO_OK.  grico_conv_tc_status is the same call. */
+int grico_tc_status(void* stream);
 int grico_conv_tc_status(void* stream);
 /* gx = transposed convolution of gy; wt: scratch of Co*Ci*27 floats */
 int grico_conv3d_backward_data(const float* gy, const float* w, float* wt, float* gx, int B, int Ci, int Co, int Z,
