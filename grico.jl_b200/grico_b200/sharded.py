@@ -330,12 +330,19 @@ class ShardedReport:
         self.final_residual = final_residual
 
 
-def sharded_cg(op, bs, relative_tolerance=None, absolute_tolerance=0.0, maxiter=1000, jacobi=True):
+def sharded_cg(op, bs, relative_tolerance=None, absolute_tolerance=0.0, maxiter=1000, jacobi=True,
+               preconditioner=None):
     """Preconditioned CG on the sharded reduced system (solve.jl:376-431: stop when
-    ||r|| <= max(atol, rtol ||b||), Jacobi or identity preconditioner).  `bs`: consistent local
-    right-hand sides (ShardedOperator.rhs).  Returns (local solutions, report)."""
+    ||r|| <= max(atol, rtol ||b||), Jacobi or identity preconditioner, or `preconditioner`, an
+    object whose apply(r) returns the consistent local z, e.g. ShardedMultigrid; one shard per
+    process then).  `bs`: consistent local right-hand sides (ShardedOperator.rhs).  Returns
+    (local solutions, report)."""
     o = op.ops
     shards = op.shards
+    if preconditioner is not None:
+        if len(shards) != 1:
+            raise ValueError("a V-cycle preconditioner needs one shard per process")
+        jacobi = False
     rtol = math.sqrt(np.finfo(np.float64).eps) if relative_tolerance is None else float(relative_tolerance)
     n = [s.n_reduced for s in shards]
     no = [s.n_owned for s in shards]
@@ -347,10 +354,19 @@ def sharded_cg(op, bs, relative_tolerance=None, absolute_tolerance=0.0, maxiter=
     qs = [o.vector(k) for k in n]
     ss = [o.vector(8) for _ in shards]      # rz, pAp, rr, rz_new, bb
     part = [o.vector(592) for _ in shards]
+
+    def precondition(k):
+        if preconditioner is None:
+            o.precondition(n[k], no[k], dinv[k], rs[k], zs[k], ss[k], part[k])
+            return
+        z = preconditioner.apply(rs[k])
+        zs[k][: n[k]] = z[: n[k]]
+        o.dot(no[k], rs[k], zs[k], ss[k], 3, part[k])
+
     for k in range(len(shards)):
         o.copy(bs[k], rs[k])
         o.dot(no[k], bs[k], bs[k], ss[k], 4, part[k])
-        o.precondition(n[k], no[k], dinv[k], rs[k], zs[k], ss[k], part[k])  # s3 = r.z
+        precondition(k)                                                      # s3 = r.z
         o.copy(zs[k], ps[k])
     op.group.allreduce([s[3:5] for s in ss])                                  # r.z, b.b
     for s in ss:
@@ -372,7 +388,7 @@ def sharded_cg(op, bs, relative_tolerance=None, absolute_tolerance=0.0, maxiter=
         op.group.allreduce([s[1:2] for s in ss])                               # p.Ap
         for k in range(len(shards)):
             o.update_xr(n[k], no[k], xs[k], rs[k], ps[k], qs[k], ss[k], part[k])
-            o.precondition(n[k], no[k], dinv[k], rs[k], zs[k], ss[k], part[k])
+            precondition(k)
         op.group.allreduce([s[2:4] for s in ss])                               # r.r, r.z
         h = o.host(ss[0])
         pap, rr = h[1], h[2]
@@ -400,3 +416,120 @@ def gather_reduced(shards, xs, n_reduced, ops=None):
         hx = ops.host(x) if ops is not None else np.asarray(x)
         out[s.global_reduced[: s.n_owned]] = hx[: s.n_owned]
     return out
+
+
+class ShardedMultigrid:
+    """hp-multigrid V-cycle over sharded levels: `_vcycle!` (multigrid.jl:858-889) with damped
+    Jacobi smoothing (`_smooth_jacobi!`, multigrid.jl:943-956) and the dense coarse solve
+    (multigrid.jl:891-924, common.jl:272-330).
+
+    Every level of the hierarchy (`build_hierarchy`: the same h/p coarsening as the one-GPU
+    V-cycle) is split over the ranks by its own Morton ranges (`ShardPlan`, one shard per
+    process), so a level apply is the sharded apply with its halo sum.  The transfers between
+    levels use global vectors: restriction sums P^T over each rank's owned fine rows into a
+    global coarse vector (one all-reduce of the coarse length), prolongation gathers the coarse
+    correction from the owned entries of all ranks (one all-reduce) and applies the rows of P of
+    the rank's fine dofs.  The coarsest level is solved redundantly on every rank from the same
+    gathered right-hand side (Cholesky of the coarse matrix, assembled at set-up from sharded
+    applies of unit vectors).  Vectors stay consistent on shared dofs throughout, so the
+    V-cycle is that of the unsharded hierarchy up to the order of floating-point sums."""
+
+    def __init__(self, plan, rank, parts, opts=None, group=None, ops=None, device=True):
+        import torch
+
+        from .multigrid import GeometricMultigridPreconditioner, build_hierarchy, resolved_smoother
+
+        self.opts = opts or GeometricMultigridPreconditioner()
+        if resolved_smoother(self.opts, plan.problem) != "jacobi":
+            raise L.GricoError(L.GRICO_ERR_INVALID, "the sharded V-cycle smooths with damped Jacobi")
+        self.torch = torch
+        self.group = group or ShardGroup()
+        self.ops = ops or _DeviceOps()
+        plans, transfers = build_hierarchy(plan, self.opts, device=device)
+        self.shards = [ShardPlan(p, rank, parts, device=device) for p in plans]
+        self.levels = [ShardedOperator([s], group=self.group, ops=self.ops) for s in self.shards]
+        self.n_global = [p.n_reduced for p in plans]
+        self.dinv = [None] + [lv.inverse_diagonal()[0] for lv in self.levels[1:]]
+        dev = self.dinv[-1].device if len(self.dinv) > 1 else torch.device("cpu")
+        self.device = dev
+        self._owned = [torch.as_tensor(s.global_reduced[: s.n_owned].astype(np.int64), device=dev) for s in self.shards]
+        self._local = [torch.as_tensor(s.global_reduced.astype(np.int64), device=dev) for s in self.shards]
+        # prolongation rows of this rank's fine dofs as (local row, global column, value) triples;
+        # restriction sums P^T over the rows of its owned fine dofs (a prefix of the local rows)
+        self._P = []
+        for i, (off, col, val) in enumerate(transfers):
+            rows = np.asarray(self.shards[i + 1].global_reduced, dtype=np.int64)
+            cnt = off[rows + 1] - off[rows]
+            take = np.concatenate([np.arange(off[g], off[g + 1]) for g in rows]) if rows.size else np.zeros(0, np.int64)
+            loc = np.repeat(np.arange(rows.size, dtype=np.int64), cnt)
+            self._P.append((torch.as_tensor(loc, device=dev), torch.as_tensor(col[take].astype(np.int64), device=dev),
+                            torch.as_tensor(val[take].astype(np.float64), device=dev)))
+        # coarse matrix from sharded applies of unit vectors (the same sequence on every rank)
+        n0 = self.n_global[0]
+        A0 = np.zeros((n0, n0))
+        e = np.zeros(n0)
+        for j in range(n0):
+            e[j] = 1.0
+            x = self._upload(e[self.shards[0].global_reduced])
+            y = self.ops.vector(self.shards[0].n_reduced)
+            self.levels[0].apply([x], [y])
+            A0[:, j] = self._gather(0, y).cpu().numpy()
+            e[j] = 0.0
+        self.coarse_factor = np.linalg.cholesky(0.5 * (A0 + A0.T)) if n0 else np.zeros((0, 0))
+
+    def _upload(self, a):
+        return self.torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=self.device)
+
+    def _gather(self, level, x):
+        """Global vector of `level` from the owned entries of every rank (one all-reduce)."""
+        g = self.torch.zeros(max(self.n_global[level], 1), dtype=self.torch.float64, device=self.device)
+        no = self.shards[level].n_owned
+        g.index_copy_(0, self._owned[level], x[:no])
+        self.group.allreduce([g])
+        return g[: self.n_global[level]]
+
+    def _apply(self, level, x):
+        y = self.ops.vector(self.shards[level].n_reduced)
+        self.levels[level].apply([x], [y])
+        return y
+
+    def _smooth(self, level, x, b, steps):
+        n = self.shards[level].n_reduced
+        w = self.opts.smoother_damping
+        for _ in range(steps):
+            y = self._apply(level, x)
+            x[:n] += w * self.dinv[level][:n] * (b[:n] - y[:n])
+        return x
+
+    def vcycle(self, level, b):
+        """Local correction of `level` for the consistent local right-hand side b."""
+        n = self.shards[level].n_reduced
+        if level == 0:
+            bg = self._gather(0, b).cpu().numpy()
+            xg = np.linalg.solve(self.coarse_factor.T, np.linalg.solve(self.coarse_factor, bg)) if bg.size else bg
+            x = self.ops.vector(n)
+            if n:
+                x[:n] = self._upload(xg[self.shards[0].global_reduced])
+            return x
+        x = self._smooth(level, self.ops.vector(n), b, self.opts.pre_smoothing_steps)
+        r = self.ops.vector(n)
+        r[:n] = b[:n] - self._apply(level, x)[:n]
+        nc = self.shards[level - 1].n_reduced
+        fo = self.shards[level].n_owned
+        loc, col, val = self._P[level - 1]
+        own = loc < fo
+        rc = self.torch.zeros(max(self.n_global[level - 1], 1), dtype=self.torch.float64, device=self.device)
+        rc.index_add_(0, col[own], val[own] * r[loc[own]])
+        self.group.allreduce([rc])
+        bc = self.ops.vector(nc)
+        if nc:
+            bc[:nc] = rc[self._local[level - 1]]
+        xc = self.vcycle(level - 1, bc)
+        xg = self._gather(level - 1, xc)
+        if n:
+            x.index_add_(0, loc, val * xg[col])
+        return self._smooth(level, x, b, self.opts.post_smoothing_steps)
+
+    def apply(self, r):
+        """z = V-cycle(r) on the finest level (local, consistent)."""
+        return self.vcycle(len(self.shards) - 1, r)

@@ -70,3 +70,33 @@ def test_sharded_cg_matches_unsharded_cg(cuda, jacobi):
     assert np.linalg.norm(x - xr) <= 1e-8 * np.linalg.norm(xr)
     for s, xv in zip(shards, xs):
         assert np.max(np.abs(xv.cpu().numpy()[: s.n_reduced] - x[s.global_reduced])) <= 1e-13 * np.abs(x).max()
+
+
+def test_sharded_multigrid_on_the_device_matches_the_device_vcycle(cuda):
+    """The sharded V-cycle with the library's device calls (one shard, device ops) against the
+    one-GPU device V-cycle of the same hierarchy (damped Jacobi V(2,2)), and CG preconditioned
+    by it against the device CG + GMG solve."""
+    import torch
+
+    from grico_b200.multigrid import GeometricMultigridPreconditioner, build_multigrid
+    from grico_b200.sharded import ShardedMultigrid
+
+    plan = gb.compile(_problem("3d_p4", source=lambda x: np.prod(np.sin(np.pi * x), axis=1)))
+    opts = GeometricMultigridPreconditioner()
+    smg = ShardedMultigrid(plan, 0, 1, opts=opts)
+    dmg = build_multigrid(plan, opts)
+    r = np.random.default_rng(4).standard_normal(plan.n_reduced)
+    fine = smg.shards[-1]
+    z = smg.apply(smg.ops.upload(fine.scatter(r)))
+    zs = gather_reduced([fine], [z], plan.n_reduced, ops=smg.ops)
+    zd = dmg.vcycle(r)
+    assert np.linalg.norm(zs - zd) <= 1e-11 * np.linalg.norm(zd)
+    op = ShardedOperator([fine])
+    bs = op.rhs()
+    xs, rep = sharded_cg(op, bs, 1e-10, preconditioner=smg)
+    st = gb.solve(plan, solver=gb.CGSolver(GeometricMultigridPreconditioner()), relative_tolerance=1e-10)
+    assert rep.status == 0 and abs(rep.iterations - st.report.iterations) <= max(1, st.report.iterations // 8)
+    xg = gather_reduced([fine], xs, plan.n_reduced, ops=op.ops)
+    full = gb.expand_reduced(plan, xg)
+    assert np.linalg.norm(full - st.coefficients) <= 1e-8 * np.linalg.norm(st.coefficients)
+    torch.cuda.synchronize()
