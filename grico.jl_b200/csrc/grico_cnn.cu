@@ -248,7 +248,7 @@ int64_t grico_conv_tc_weight_bytes(int Ci, int Co) {
 // FP32 weights [Co][Ci][27] -> packed BF16 weights (grico_conv_tc_weight_bytes bytes at wp).
 int grico_conv3d_pack_weights_tc(const float* w, int Ci, int Co, void* wp, void* stream) {
   if (!w || !wp || !tc::conv_tc_supported(Ci, Co)) {
-    set_error("grico_conv3d_pack_weights_tc: invalid argument (Ci a multiple of 16, Co up to 128)");
+    set_error("grico_conv3d_pack_weights_tc: invalid argument (Ci 16, 32, 48 or 64, Co up to 128)");
     return GRICO_ERR_INVALID;
   }
   return conv_tc_pack(w, Ci, Co, wp, as_stream(stream));
@@ -263,7 +263,7 @@ int grico_conv3d_forward_tc(const void* x, const void* wp, const float* bias, vo
                        (y_layout == 1 || reinterpret_cast<uintptr_t>(y) % 16 == 0);
   if (!x || !wp || !y || !aligned || (y_layout != 0 && y_layout != 1) || !conv_args_ok(B, Ci, Co, Z, Y, X) ||
       !tc::conv_tc_supported(Ci, Co) || (y_layout == 0 && Co % 8 != 0)) {
-    set_error("grico_conv3d_forward_tc: invalid argument (Ci a multiple of 16, Co up to 128 and a multiple of 8 for "
+    set_error("grico_conv3d_forward_tc: invalid argument (Ci 16, 32, 48 or 64, Co up to 128 and a multiple of 8 for "
               "channels-last output, 16-byte aligned buffers)");
     return GRICO_ERR_INVALID;
   }

@@ -424,7 +424,7 @@ int grico_mg_learned_stats(GricoMultigrid* mg, int64_t* sweeps, int64_t* accepte
 int grico_conv3d_forward(const void* x, int x_bf16, const float* w, const float* bias, void* y, int y_bf16, int B,
                          int Ci, int Co, int Z, int Y, int X, int relu, void* stream);
 /* The convolution on the tensor cores (tcgen05.mma, BF16 operands, FP32 accumulation in tensor
- * memory) with channels-last activations: x BF16 [batch][z][y][x][Ci], Ci a multiple of 16;
+ * memory) with channels-last activations: x BF16 [batch][z][y][x][Ci], Ci = 16, 32, 48 or 64;
  * weights packed once by grico_conv3d_pack_weights_tc; y BF16 channels-last [batch][z][y][x][Co]
  * (y_layout 0, Co a multiple of 8) or FP32 [batch][Co][z][y][x] (y_layout 1); Co up to 128; x,
  * wp and a channels-last y 16-byte aligned.  Other shapes are rejected with GRICO_ERR_INVALID. */
