@@ -753,7 +753,7 @@ def main():
                     "(ref_jacobi, fp64_nograph, fp64, mixed2, mixed3); default: all")
     ap.add_argument("--workload", default="poisson64",
                     choices=["poisson64", "fcm_shell64", "fcm_shell32", "grf_learned128", "grf_learned64",
-                             "lshape_hp32", "lshape_apply32", "conv_tc"],
+                             "lshape_hp32", "lshape_apply32", "conv_tc", "sipg3d"],
                     help="poisson64: 3-D Poisson 64^3 p=4 (default); fcm_shell*: finite-cell shell with Nitsche")
     ap.add_argument("--fp32", action="store_true", help="time the FP32 apply instead of FP64")
     ap.add_argument("--no-configs", action="store_true", help="skip the other BASELINE configurations")
@@ -786,6 +786,34 @@ def main():
             print(json.dumps({"metric": "3x3x3 convolution device time", "unit": "us", "n_gpus": world,
                               "higher_is_better": False, "data": "synthetic (seeded normal activations)",
                               "config": {"workload": "conv_tc"}, "convolutions": rows}), flush=True)
+        return
+    if args.workload == "sipg3d":
+        # DG (SIPG) Poisson on the unit cube, 16^3 cells of degree 3: FP64 full apply
+        import torch
+
+        d = gb.Domain((0.0, 0.0, 0.0), (1.0, 1.0, 1.0), (16, 16, 16))
+        sp = gb.HpSpace(d, gb.SpaceOptions(basis=gb.FullTensorBasis(), degree=gb.UniformDegree(3), continuity="dg"))
+        u = gb.ScalarField(sp)
+        prob = gb.AffineProblem(u)
+        gb.add_cell_accumulator(prob, u, u, gb.Diffusion())
+        gb.add_interface(prob, gb.SIPG(10.0))
+        plan = gb.compile(prob)
+        st = torch.cuda.Stream()
+        xv = torch.tensor(sample_vector(plan.n_full), dtype=torch.float64, device="cuda")
+        yv = torch.empty_like(xv)
+        fn = lambda: L.lib().grico_apply(plan.handle, xv.data_ptr(), yv.data_ptr(), 1, L.GRICO_PREC_FP64, 0,
+                                         st.cuda_stream)
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        ms = _timed_device(fn, args.steps, st)
+        if rank == 0:
+            print(json.dumps({"metric": "DG (SIPG) FP64 apply device time", "value": ms, "unit": "ms",
+                              "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+                              "data": "synthetic", "config": {"workload": "sipg3d", "cells": "16^3", "degree": 3,
+                                                               "dofs": plan.n_full,
+                                                               "interfaces": int(sum(len(b.cells) for b in plan.point_batches))},
+                              "checksum": float(yv.double().sum().item())}), flush=True)
         return
     if args.workload == "lshape_apply32":
         # the hp L-shape's reduced FP64 apply, 1 and 32 right-hand sides, W untimed then K timed

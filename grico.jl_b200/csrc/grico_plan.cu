@@ -493,8 +493,19 @@ void launch_points(const GricoPlan& P, const DevPointBatch& pb, bool reduced, co
                     pb.np[0] * (D > 1 ? pb.np[1] : 1) * (D > 2 ? pb.np[2] : 1);
     const int nmax = std::max(std::max(pb.n[0], std::max(D > 1 ? pb.n[1] : 1, D > 2 ? pb.n[2] : 1)),
                               std::max(pb.np[0], std::max(D > 1 ? pb.np[1] : 1, D > 2 ? pb.np[2] : 1)));
-    const size_t smem = sizeof(T) * (size_t(nbi) + 4 * size_t(kPointChunk) * D * nmax + 2 * size_t(kPointChunk));
     dim3 grid(pb.n_items, nrhs);
+    if (mode == 0 && pb.sf_ok && D >= 2) {
+      const size_t sm = interface_sf_smem(nbi, nmax, pb.sf_qmax, int(pb.sf_pmax), sizeof(T));
+      auto go_sf = [&](auto kernel) {
+        if (sm > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
+        kernel<<<grid, kPointThreads, sm, st>>>(v, pb.sf_q.get<int32_t>(), pb.sf_x.get<double>(), pb.sf_stride, x, y,
+                                               nvec);
+      };
+      if (D == 2) go_sf(interface_apply_sf<T, 2>);
+      else go_sf(interface_apply_sf<T, 3>);
+      return;
+    }
+    const size_t smem = sizeof(T) * (size_t(nbi) + 4 * size_t(kPointChunk) * D * nmax + 2 * size_t(kPointChunk));
     auto go = [&](auto kernel) {
       if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
       kernel<<<grid, kPointThreads, smem, st>>>(v, x, y, nvec, mode);
@@ -1189,6 +1200,60 @@ int grico_plan_create(const GricoPlanDesc* d, GricoPlan** out) {
       ok = ok && pb.eta.upload(pd.eta, size_t(pd.n_items)) &&
            pb.ref_p.upload(pd.ref_points_plus, size_t(pb.n_points) * d->dim) &&
            pb.h_p.upload(pd.cell_size_plus, size_t(pd.n_items) * d->dim) && pb.axis.upload(pd.face_axis, size_t(pd.n_items));
+    if (iface && d->dim >= 2 && pd.n_items > 0) {
+      // the sum-factorised kernel applies when every item's points are a tensor grid over the
+      // tangential axes t1 < t2 (t1 fastest) with one normal coordinate per side
+      const int D = d->dim;
+      int64_t pmax = 1;
+      for (int64_t it = 0; it < pd.n_items; ++it)
+        pmax = std::max<int64_t>(pmax, pd.point_offsets[it + 1] - pd.point_offsets[it]);
+      const int stride = 2 * int(pmax + 2);
+      std::vector<int32_t> qv(2 * size_t(pd.n_items));
+      std::vector<double> xv(size_t(pd.n_items) * stride, 0.0);
+      bool sf = true;
+      int qmax = 1;
+      for (int64_t it = 0; it < pd.n_items && sf; ++it) {
+        const int ax = pd.face_axis[it];
+        const int t1 = ax == 0 ? 1 : 0, t2 = D == 3 ? (ax == 2 ? 1 : 2) : -1;
+        const int64_t p0 = pd.point_offsets[it], cnt = pd.point_offsets[it + 1] - p0;
+        if (cnt < 1 || ax < 0 || ax >= D) {
+          sf = false;
+          break;
+        }
+        int64_t q1 = cnt;
+        if (D == 3) {
+          q1 = 1;
+          while (q1 < cnt && pd.ref_points[(p0 + q1) * D + t2] == pd.ref_points[p0 * D + t2]) ++q1;
+        }
+        if (cnt % q1) {
+          sf = false;
+          break;
+        }
+        const int64_t q2 = cnt / q1;
+        for (int side = 0; side < 2 && sf; ++side) {
+          const double* R = side ? pd.ref_points_plus : pd.ref_points;
+          double* c = xv.data() + it * stride + side * (q1 + q2 + 1);
+          for (int64_t p = 0; p < cnt && sf; ++p) {
+            const int64_t p1 = p % q1, p2 = p / q1;
+            const double* r = R + (p0 + p) * D;
+            if (p2 == 0) c[p1] = r[t1];
+            if (p1 == 0) c[q1 + p2] = D == 3 ? r[t2] : 0.0;
+            if (p == 0) c[q1 + q2] = r[ax];
+            sf = r[t1] == c[p1] && (D < 3 || r[t2] == c[q1 + p2]) && r[ax] == c[q1 + q2];
+          }
+        }
+        qv[2 * it] = int32_t(q1);
+        qv[2 * it + 1] = int32_t(q2);
+        qmax = std::max<int>(qmax, int(std::max(q1, q2)));
+      }
+      if (sf) {
+        ok = ok && pb.sf_q.upload(qv) && pb.sf_x.upload(xv);
+        pb.sf_ok = true;
+        pb.sf_stride = stride;
+        pb.sf_qmax = qmax;
+        pb.sf_pmax = pmax;
+      }
+    }
     if (pd.kappa_points) ok = ok && pb.kpts.upload(pd.kappa_points, size_t(pb.n_points));
     std::vector<int32_t> rmap, tidx;
     std::vector<double> rcoef, tcoef;

@@ -121,6 +121,12 @@ struct DevPointBatch {
   // GRICO_ITEM_INTERFACE: plus-side modes per axis, reference points, cell sizes, normal axis
   int np[3] = {1, 1, 1};
   DevBuf ref_p, h_p, axis;
+  // sum-factorised interfaces (interface_apply_sf): every item's points form a tangential tensor
+  // grid; (q1, q2) per item and the 1-D coordinates [side][t1 | t2 | normal] with a fixed stride
+  bool sf_ok = false;
+  int sf_stride = 0, sf_qmax = 1;
+  int64_t sf_pmax = 1;
+  DevBuf sf_q, sf_x;
 };
 
 }  // namespace grico
