@@ -44,6 +44,10 @@ struct BatchView {
   const void* tail_x = nullptr;
   void* tail_y = nullptr;
   int64_t n_tail = 0;
+  // deterministic apply: the kernels store every entry's local result at
+  // local_out[rhs * local_stride + e] instead of adding it into y (det_gather sums them)
+  void* local_out = nullptr;
+  int64_t local_stride = 0;
 };
 
 template <typename T>
@@ -60,6 +64,10 @@ __device__ __forceinline__ T gather_entry(const BatchView& b, int64_t e, const T
 
 template <typename T>
 __device__ __forceinline__ void scatter_entry(const BatchView& b, int64_t e, T val, T* __restrict__ y) {
+  if (b.local_out) {
+    static_cast<T*>(b.local_out)[blockIdx.y * b.local_stride + e] = val;
+    return;
+  }
   int v = __ldg(b.map + e);
   if (v >= 0) {
     atomicAdd(y + v, b.coef ? T(__ldg(b.coef + e)) * val : val);
@@ -154,6 +162,21 @@ __global__ void tail_scatter(const int64_t* __restrict__ off, const int32_t* __r
   for (int64_t k = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) / 32; k < n_tail; k += nw) {
     const T v = yt[k];
     for (int64_t t = off[k] + lane; t < off[k + 1]; t += 32) atomicAdd(y + idx[t], T(coef[t]) * v);
+  }
+}
+
+// Deterministic sum of the stored local results: y[r * n_vec + d] = sum over the row d of the
+// gather CSR (in its fixed order) of coef[k] local[r * stride + pos[k]]
+template <typename T>
+__global__ void det_gather(const int64_t* __restrict__ off, const int32_t* __restrict__ pos,
+                           const double* __restrict__ coef, int64_t n, const T* __restrict__ local, int64_t stride,
+                           T* __restrict__ y, int64_t n_vec) {
+  local += blockIdx.y * stride;
+  y += blockIdx.y * n_vec;
+  for (int64_t d = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; d < n; d += int64_t(gridDim.x) * blockDim.x) {
+    T s = T(0);
+    for (int64_t k = off[d]; k < off[d + 1]; ++k) s += T(coef[k]) * local[pos[k]];
+    y[d] = s;
   }
 }
 
@@ -649,6 +672,8 @@ struct PointView {
   const double* ref_p;     // [n_points*dim]
   const double* h_p;       // [n_items*dim]
   const int32_t* axis;     // [n_items]
+  void* local_out;         // deterministic apply (BatchView::local_out)
+  int64_t local_stride;
 };
 
 constexpr int kPointChunk = 32;
@@ -734,6 +759,8 @@ __global__ void __launch_bounds__(kPointThreads) point_apply(PointView b, const 
   bv.tail_off = b.tail_off;
   bv.tail_idx = b.tail_idx;
   bv.tail_coef = b.tail_coef;
+  bv.local_out = b.local_out;
+  bv.local_stride = b.local_stride;
   if (mode == 0)
     for (int i = threadIdx.x; i < nb; i += blockDim.x) xl[i] = gather_entry<T>(bv, item * nb + i, x);
   T acc[kMaxModes];
@@ -914,6 +941,8 @@ __global__ void __launch_bounds__(kPointThreads) interface_apply(PointView b, co
   bv.tail_off = b.tail_off;
   bv.tail_idx = b.tail_idx;
   bv.tail_coef = b.tail_coef;
+  bv.local_out = b.local_out;
+  bv.local_stride = b.local_stride;
   if (mode == 0)
     for (int i = threadIdx.x; i < nb; i += blockDim.x) xl[i] = gather_entry<T>(bv, item * nb + i, x);
   T acc[kIfaceModes];
@@ -1063,6 +1092,8 @@ __global__ void __launch_bounds__(kPointThreads) interface_apply_sf(PointView b,
   bv.tail_off = b.tail_off;
   bv.tail_idx = b.tail_idx;
   bv.tail_coef = b.tail_coef;
+  bv.local_out = b.local_out;
+  bv.local_stride = b.local_stride;
   for (int i = tid; i < nb; i += nt) xl[i] = gather_entry<T>(bv, item * nb + i, x);
   // 1-D tables: normal values and physical normal derivatives, tangential values
   const double* cx = sf_x + item * int64_t(sf_stride);
@@ -1220,6 +1251,8 @@ struct SubcellView {
   const double* ws;         // [n_sub]: weight factor (2^(-dim*level) times the measure factor)
   const double* kpts;       // [n_sub*Q^dim] or null
   const uint8_t* skip;      // diagonal kernel skips these items (host computes them)
+  void* local_out;          // deterministic apply (BatchView::local_out)
+  int64_t local_stride;
 };
 
 template <int Q, typename T>
@@ -1270,6 +1303,8 @@ __global__ void __launch_bounds__(kSubThreads) subcell_apply(SubcellView b, cons
   bv.tail_off = b.tail_off;
   bv.tail_idx = b.tail_idx;
   bv.tail_coef = b.tail_coef;
+  bv.local_out = b.local_out;
+  bv.local_stride = b.local_stride;
   if (mode == 0)
     for (int i = threadIdx.x; i < S::NB; i += blockDim.x) xl[i] = gather_entry<T>(bv, item * S::NB + i, x);
   for (int i = lane; i < S::NB; i += 32) yl[i] = T(0);

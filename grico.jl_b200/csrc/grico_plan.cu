@@ -209,7 +209,8 @@ bool launch_fused(int dim, const DevBatch& bt, const BatchView& v, const T* x, T
                   int mode, const double* src, int nrhs, cudaStream_t st) {
   if (v.n_cells == 0) return true;
   const int N = bt.n[0], Q = bt.q[0];
-  const int var = bt.tile[sizeof(T) == 4 ? 1 : 0];
+  // deterministic applies store local results: the one-block-per-group kernel (scatter_entry)
+  const int var = v.local_out ? 1 : bt.tile[sizeof(T) == 4 ? 1 : 0];
   // variant 10, FP32: uniform batch with a plain map on the tensor cores
   if constexpr (std::is_same<T, float>::value) {
     if (dim == 3 && var == kDenseVariant && mode == 0 && bt.dense_ok && v.coef == nullptr && v.tail_off == nullptr &&
@@ -347,11 +348,13 @@ void launch_batch_cells(const GricoPlan& P, const DevBatch& b, BatchView& v, con
 // buffers), the tail scatter; long expansions no longer serialise one thread of the cell kernel.
 template <typename T>
 void launch_batch(const GricoPlan& P, const DevBatch& b, bool reduced, const T* x, T* y, int64_t nvec, int mode,
-                  const double* src, int nrhs, cudaStream_t st) {
+                  const double* src, int nrhs, cudaStream_t st, void* local_out = nullptr, int64_t local_stride = 0) {
   BatchView v;
   fill_view(v, b, reduced);
+  v.local_out = local_out;
+  v.local_stride = local_stride;
   const DevMap& m = reduced ? b.red : b.full;
-  const bool buffered = mode == 0 && x && m.n_tail > 0 && nrhs <= kTailRhs;
+  const bool buffered = mode == 0 && x && m.n_tail > 0 && nrhs <= kTailRhs && !local_out;
   // several right-hand sides: segments with the columns on the lanes (kTailLaneRhs or more),
   // else one warp per tail with the lanes over its terms
   const bool lanes_rhs = nrhs >= kTailLaneRhs;
@@ -431,9 +434,12 @@ bool subcell_shape_supported(int dim, int n, int q) {
 
 template <typename T>
 void launch_subcells(const GricoPlan& P, const DevPointBatch& pb, bool reduced, const T* x, T* y, int64_t nvec,
-                     int mode, const double* src, int nrhs, cudaStream_t st) {
+                     int mode, const double* src, int nrhs, cudaStream_t st, void* local_out = nullptr,
+                     int64_t local_stride = 0) {
   SubcellView v;
   v.n_items = pb.n_items;
+  v.local_out = local_out;
+  v.local_stride = local_stride;
   const DevMap& m = reduced ? pb.red : pb.full;
   v.map = m.map.get<int32_t>();
   v.coef = m.coef.get<double>();
@@ -461,11 +467,14 @@ void launch_subcells(const GricoPlan& P, const DevPointBatch& pb, bool reduced, 
 
 template <typename T>
 void launch_points(const GricoPlan& P, const DevPointBatch& pb, bool reduced, const T* x, T* y, int64_t nvec, int mode,
-                   const double* src, int nrhs, cudaStream_t st) {
+                   const double* src, int nrhs, cudaStream_t st, void* local_out = nullptr, int64_t local_stride = 0) {
   if (pb.n_items == 0) return;
-  if (pb.kind == GRICO_ITEM_SUBCELLS) return launch_subcells<T>(P, pb, reduced, x, y, nvec, mode, src, nrhs, st);
+  if (pb.kind == GRICO_ITEM_SUBCELLS)
+    return launch_subcells<T>(P, pb, reduced, x, y, nvec, mode, src, nrhs, st, local_out, local_stride);
   PointView v;
   v.n_items = pb.n_items;
+  v.local_out = local_out;
+  v.local_stride = local_stride;
   v.kind = pb.kind;
   for (int a = 0; a < 3; ++a) v.n[a] = pb.n[a];
   const DevMap& m = reduced ? pb.red : pb.full;
@@ -844,6 +853,123 @@ int run_apply(GricoPlan* P, bool reduced, const T* x, T* y, int nrhs, cudaStream
 
 template int run_apply<double>(GricoPlan*, bool, const double*, double*, int, cudaStream_t);
 template int run_apply<float>(GricoPlan*, bool, const float*, float*, int, cudaStream_t);
+
+namespace {
+
+// Gather CSR of the deterministic apply for one layout, from the device maps of every batch: a
+// map entry e of a batch whose local results start at `base` adds coef * local[base + e] to its
+// dof (a single-term entry) or coef_t * local[base + e] to each term's dof (an expansion).
+bool build_det_map(GricoPlan* P, bool reduced) {
+  auto& D = P->det[reduced ? 1 : 0];
+  if (D.built) return true;
+  const int64_t n = reduced ? P->n_red : P->n_full;
+  struct Src {
+    int64_t base = 0, ne = 0;
+    std::vector<int32_t> map, tidx;
+    std::vector<double> coef, tcoef;
+    std::vector<int64_t> toff;
+  };
+  std::vector<Src> src;
+  int64_t base = 0;
+  auto fetch = [&](const DevMap& m, int64_t ne) {
+    Src s;
+    s.base = base;
+    s.ne = ne;
+    s.map.resize(size_t(ne));
+    bool ok = ne == 0 || cuda_ok(cudaMemcpy(s.map.data(), m.map.ptr, sizeof(int32_t) * ne, cudaMemcpyDeviceToHost), "det map");
+    if (ok && m.coef.ptr) {
+      s.coef.resize(size_t(ne));
+      ok = cuda_ok(cudaMemcpy(s.coef.data(), m.coef.ptr, sizeof(double) * ne, cudaMemcpyDeviceToHost), "det coef");
+    }
+    if (ok && m.toff.ptr && m.toff.bytes >= 2 * sizeof(int64_t)) {
+      s.toff.resize(m.toff.bytes / sizeof(int64_t));
+      ok = cuda_ok(cudaMemcpy(s.toff.data(), m.toff.ptr, m.toff.bytes, cudaMemcpyDeviceToHost), "det tails");
+      const int64_t nt = s.toff.back();
+      s.tidx.resize(size_t(nt));
+      s.tcoef.resize(size_t(nt));
+      ok = ok && (nt == 0 || (cuda_ok(cudaMemcpy(s.tidx.data(), m.tidx.ptr, sizeof(int32_t) * nt, cudaMemcpyDeviceToHost), "det tails") &&
+                              cuda_ok(cudaMemcpy(s.tcoef.data(), m.tcoef.ptr, sizeof(double) * nt, cudaMemcpyDeviceToHost), "det tails")));
+    }
+    src.push_back(std::move(s));
+    base += ne;
+    return ok;
+  };
+  D.cell_base.clear();
+  D.point_base.clear();
+  for (const auto& b : P->batches) {
+    D.cell_base.push_back(base);
+    if (!fetch(reduced ? b.red : b.full, int64_t(b.n_cells) * b.n[0] * b.n[1] * b.n[2])) return false;
+  }
+  for (const auto& pb : P->pbatches) {
+    D.point_base.push_back(base);
+    int64_t nb = int64_t(pb.n[0]) * pb.n[1] * pb.n[2];
+    if (pb.kind == GRICO_ITEM_INTERFACE) nb += int64_t(pb.np[0]) * pb.np[1] * pb.np[2];
+    if (!fetch(reduced ? pb.red : pb.full, int64_t(pb.n_items) * nb)) return false;
+  }
+  // two passes in one traversal order: count the terms of every dof, then place them
+  std::vector<int64_t> off(size_t(n) + 1, 0);
+  auto visit = [&](auto&& emit) {
+    for (const auto& s : src)
+      for (int64_t e = 0; e < s.ne; ++e) {
+        const int32_t v = s.map[size_t(e)];
+        if (v >= 0) {
+          emit(v, s.base + e, s.coef.empty() ? 1.0 : s.coef[size_t(e)]);
+        } else if (v <= -2) {
+          const int64_t k = -(int64_t(v) + 2);
+          for (int64_t t = s.toff[size_t(k)]; t < s.toff[size_t(k) + 1]; ++t)
+            emit(s.tidx[size_t(t)], s.base + e, s.tcoef[size_t(t)]);
+        }
+      }
+  };
+  visit([&](int64_t d, int64_t, double) { ++off[size_t(d) + 1]; });
+  for (int64_t d = 0; d < n; ++d) off[size_t(d) + 1] += off[size_t(d)];
+  const size_t n_terms = static_cast<size_t>(off[static_cast<size_t>(n)]);
+  std::vector<int32_t> pos(n_terms);
+  std::vector<double> coef(n_terms);
+  std::vector<int64_t> fill(off.begin(), off.end() - 1);
+  visit([&](int64_t d, int64_t p, double c) {
+    const int64_t k = fill[size_t(d)]++;
+    pos[size_t(k)] = int32_t(p);
+    coef[size_t(k)] = c;
+  });
+  if (!D.off.upload(off) || !D.pos.upload(pos) || !D.coef.upload(coef)) return false;
+  D.entries = base;
+  D.built = true;
+  return true;
+}
+
+// GRICO_FLAG_DETERMINISTIC: every batch kernel stores its local results (the one-block kernels,
+// no atomics), det_gather sums each dof's terms in the map order, then the constraint rows
+template <typename T>
+int run_apply_det(GricoPlan* P, bool reduced, const T* x, T* y, int nrhs, cudaStream_t st) {
+  const int64_t n = reduced ? P->n_red : P->n_full;
+  if (nrhs < 1) return GRICO_ERR_INVALID;
+  (void)cudaGetLastError();
+  if (!build_det_map(P, reduced)) return GRICO_ERR_CUDA;
+  auto& D = P->det[reduced ? 1 : 0];
+  if (D.entries >= (int64_t(1) << 31)) {
+    set_error("deterministic apply: more than 2^31 local entries");
+    return GRICO_ERR_INVALID;
+  }
+  if (!P->det_local.ensure(sizeof(T) * size_t(std::max<int64_t>(D.entries, 1)) * nrhs)) return GRICO_ERR_CUDA;
+  T* loc = P->det_local.get<T>();
+  for (size_t bi = 0; bi < P->batches.size(); ++bi)
+    launch_batch<T>(*P, P->batches[bi], reduced, x, y, n, 0, nullptr, nrhs, st, loc + D.cell_base[bi], D.entries);
+  for (size_t pi = 0; pi < P->pbatches.size(); ++pi)
+    launch_points<T>(*P, P->pbatches[pi], reduced, x, y, n, 0, nullptr, nrhs, st, loc + D.point_base[pi], D.entries);
+  dim3 grid(grid_for(n), nrhs);
+  det_gather<T><<<grid, 256, 0, st>>>(D.off.get<int64_t>(), D.pos.get<int32_t>(), D.coef.get<double>(), n, loc,
+                                      D.entries, y, n);
+  if (!reduced && (P->n_fixed + P->n_rel) > 0) {
+    dim3 cg(grid_for(P->n_fixed + P->n_rel), nrhs);
+    constraint_action<T><<<cg, 256, 0, st>>>(P->fixed.get<int64_t>(), P->n_fixed, P->rel_piv.get<int64_t>(),
+                                             P->rel_off.get<int64_t>(), P->rel_idx.get<int64_t>(),
+                                             P->rel_coef.get<double>(), P->n_rel, x, y, n);
+  }
+  return cuda_ok(cudaGetLastError(), "deterministic apply launch") ? GRICO_OK : GRICO_ERR_CUDA;
+}
+
+}  // namespace
 
 int reduced_diag_device(GricoPlan* P, double* diag, cudaStream_t st) {
   cudaMemsetAsync(diag, 0, sizeof(double) * P->n_red, st);
@@ -1414,9 +1540,15 @@ static int apply_common(GricoPlan* P, bool reduced, const void* x, void* y, int 
     dy = P->host_y.ptr;
   }
   P->time_batches = (flags & GRICO_FLAG_TIME_BATCHES) != 0;
-  int rc = precision == GRICO_PREC_FP64
-               ? run_apply<double>(P, reduced, static_cast<const double*>(dx), static_cast<double*>(dy), nrhs, st)
-               : run_apply<float>(P, reduced, static_cast<const float*>(dx), static_cast<float*>(dy), nrhs, st);
+  int rc;
+  if (flags & GRICO_FLAG_DETERMINISTIC)
+    rc = precision == GRICO_PREC_FP64
+             ? run_apply_det<double>(P, reduced, static_cast<const double*>(dx), static_cast<double*>(dy), nrhs, st)
+             : run_apply_det<float>(P, reduced, static_cast<const float*>(dx), static_cast<float*>(dy), nrhs, st);
+  else
+    rc = precision == GRICO_PREC_FP64
+             ? run_apply<double>(P, reduced, static_cast<const double*>(dx), static_cast<double*>(dy), nrhs, st)
+             : run_apply<float>(P, reduced, static_cast<const float*>(dx), static_cast<float*>(dy), nrhs, st);
   P->time_batches = false;
   if (rc != GRICO_OK) return rc;
   if (flags & GRICO_FLAG_HOST_POINTERS) {

@@ -152,6 +152,17 @@ struct GricoPlan {
   struct Stage { grico::DevBuf x, y; cudaEvent_t done = nullptr; bool used = false; };
   Stage stage[2];
   int stage_next = 0;
+  // GRICO_FLAG_DETERMINISTIC: per layout (0 full, 1 reduced) the gather CSR of the stored local
+  // results (row = dof; its terms in batch, entry, expansion-term order) and the first entry of
+  // every cell and point batch; built on the first deterministic apply of that layout
+  struct DetMap {
+    bool built = false;
+    int64_t entries = 0;
+    std::vector<int64_t> cell_base, point_base;
+    grico::DevBuf off, pos, coef;
+  };
+  DetMap det[2];
+  grico::DevBuf det_local;
   // GRICO_FLAG_TIME_BATCHES: event pairs around cell-batch launches, (batch, start, stop)
   struct BatchEvent { int batch; cudaEvent_t start, stop; };
   bool time_batches = false;

@@ -42,6 +42,7 @@ GRICO_FLAG_NO_GRAPH = 2
 GRICO_FLAG_MIXED = 4
 GRICO_FLAG_TIME_BATCHES = 8
 GRICO_FLAG_ASYNC = 16
+GRICO_FLAG_DETERMINISTIC = 32
 GRICO_PRECOND_IDENTITY = 0
 GRICO_PRECOND_JACOBI = 1
 GRICO_PRECOND_MULTIGRID = 2

@@ -62,6 +62,12 @@ extern "C" {
                                       return; the caller synchronises the stream before reading y
                                       or changing x.  Two calls may be in flight per plan (two
                                       staging slots; a third waits for the first on the device) */
+#define GRICO_FLAG_DETERMINISTIC 32 /* grico_apply / grico_reduced_apply: no atomic scatter; every
+                                      cell and point kernel stores its local results and one pass
+                                      sums each dof's terms in a fixed (batch, entry, term) order,
+                                      so results are bitwise reproducible run to run, as the
+                                      reference's sum is thread-count independent.  Slower; the
+                                      first call per layout builds the gather table (allocates) */
 
 /* ================================================================================
  * Host space compile (native replacement of the Julia-side HpSpace construction)
