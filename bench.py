@@ -45,6 +45,11 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
+# DRAM bytes of one subcell_apply launch per subcell (ncu, 32^3 shell: 19,729,664 B read, 0 B
+# written, 469,928 subcells)
+FCM_SUBCELL_TRAFFIC_PER_SUBCELL = 19729664.0 / 469928.0
+
+
 def load_bf16_peak():
     """Measured dense BF16 TFLOP/s (burst, cuBLAS) of this pool's B200s, else the fallback 1590."""
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -664,7 +669,10 @@ def c5_leg(gb, L, peak):
                            subcells=int(sum(len(b.subcell_level) for b in sub))),
             "apply": res, "host_setup_seconds": setup,
             "roofline": {"bound": "hbm", "achieved": alg / (res["fp64"]["ms"] * 1e-3) / 1e9, "peak": peak,
-                         "unit": "GB/s", "frac": alg / (res["fp64"]["ms"] * 1e-3) / 1e9 / peak, "traffic": None,
+                         "unit": "GB/s", "frac": alg / (res["fp64"]["ms"] * 1e-3) / 1e9 / peak,
+                         "traffic": FCM_SUBCELL_TRAFFIC_PER_SUBCELL * sum(len(b.subcell_level) for b in sub),
+                         "traffic_note": "subcell kernel DRAM bytes per launch, scaled by the subcells from an ncu "
+                                         "capture on the 32^3 shell (19,729,664 B for 469,928 subcells)",
                          "note": "whole FP64 apply (all batches); the cut-cell subcell kernel dominates"},
             "cpu_baseline": {"value": None, "reason": "the oracle's C port covers tensor cells only; the cut-cell "
                                                       "oracle is the pure-Python restatement (test sizes)"}}
@@ -956,6 +964,23 @@ def main():
     torch.cuda.synchronize()
     assert torch.allclose(hy.cuda(), y, rtol=0, atol=(1e-5 if args.fp32 else 1e-12) * float(y.abs().max()))
 
+    # the same apply with GRICO_FLAG_DETERMINISTIC (stored local results summed per dof in a fixed
+    # order): device time per apply and a bitwise repeat check, outside the timed region
+    det_info = None
+    if world == 1:
+        try:
+            yd1, yd2 = torch.empty_like(y), torch.empty_like(y)
+            det = lambda out: L.check(L.lib().grico_apply(plan.handle, x.data_ptr(), out.data_ptr(), 1, prec,
+                                                          L.GRICO_FLAG_DETERMINISTIC, stream.cuda_stream), "det apply")
+            det(yd1)
+            torch.cuda.synchronize()
+            det_ms = _timed_device(lambda: det(yd2), 5, stream)
+            det_info = {"ms": det_ms, "bitwise_repeatable": bool(torch.equal(yd1, yd2)),
+                        "max_rel_diff_vs_atomic": float((yd1 - y).abs().max() / y.abs().max())}
+            del yd1, yd2
+        except Exception as exc:  # noqa: BLE001
+            det_info = {"error": f"{type(exc).__name__}: {exc}"[:200]}
+
     sharded_info = None
     if world > 1 and not fcm:
         sharded_info = sharded_leg(gb, plan, rank, world, args.steps, args.warmup)
@@ -997,8 +1022,12 @@ def main():
                           cut_cells=plan.n_cut, subcells=int(sum(len(b.subcell_level) for b in sub)),
                           surface_points=int(sum(b.weights.size for b in plan.point_batches
                                                  if b.kind == L.GRICO_ITEM_NITSCHE)))
+            if traffic is None:
+                traffic = FCM_SUBCELL_TRAFFIC_PER_SUBCELL * config["subcells"]
             roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                     "traffic": traffic, "peak_kind": peak_kind,
+                    "traffic_note": "subcell kernel DRAM bytes per launch, scaled by the subcells from an ncu capture "
+                                    "on the 32^3 shell (19,729,664 B for 469,928 subcells)",
                     "kernel_ms": kernel_ms, "kernel_share_of_apply": kernel_ms / ms,
                     "note": "achieved = 2*bytes(value)*n_full / average launch time of the dominant kernel "
                             "(CUDA events around each launch inside the timed region); the cut-cell subcell kernel "
@@ -1031,6 +1060,8 @@ def main():
             "cpu_baseline": cpu,
             "solve": solve_info,
         }
+        if det_info is not None:
+            out["deterministic_apply"] = det_info
         if sharded_info is not None:
             out["sharded"] = sharded_info
         if configs_info is not None:
