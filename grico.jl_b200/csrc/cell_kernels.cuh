@@ -40,7 +40,8 @@ struct BatchView {
   const uint8_t* skip;       // nullable: cells excluded from the diagonal kernel
   const double* mass_pts;    // nullable [n_cells*nq]: pointwise mass added to the constant mass
   // long tails, operator apply: the expansions are summed by tail_gather before the cell kernel
-  // (tail_x[rhs * n_tail + k]) and spread by tail_scatter after it (the kernel stores tail_y)
+  // (tail_x[rhs * n_tail + k]) and spread by tail_scatter after it (the kernel adds into tail_y,
+  // zeroed before; entries with the same expansion share a tail)
   const void* tail_x = nullptr;
   void* tail_y = nullptr;
   int64_t n_tail = 0;
@@ -76,7 +77,7 @@ __device__ __forceinline__ void scatter_entry(const BatchView& b, int64_t e, T v
   if (v == -1) return;
   int64_t k = -(int64_t(v) + 2);
   if (b.tail_y) {
-    static_cast<T*>(b.tail_y)[blockIdx.y * b.n_tail + k] = val;  // each tail belongs to one entry
+    atomicAdd(static_cast<T*>(b.tail_y) + blockIdx.y * b.n_tail + k, val);  // entries may share a tail
     return;
   }
   for (int64_t t = b.tail_off[k]; t < b.tail_off[k + 1]; ++t) atomicAdd(y + b.tail_idx[t], T(b.tail_coef[t]) * val);
@@ -87,17 +88,21 @@ __device__ __forceinline__ void scatter_entry(const BatchView& b, int64_t e, T v
 template <typename T>
 __global__ void tail_gather(const int64_t* __restrict__ off, const int32_t* __restrict__ idx,
                             const double* __restrict__ coef, int64_t n_tail, const T* __restrict__ x, int64_t n_vec,
-                            T* __restrict__ xt) {
+                            T* __restrict__ xt, T* __restrict__ yt) {
   const int lane = threadIdx.x % 32;
   const int64_t nw = int64_t(gridDim.x) * blockDim.x / 32;
   x += blockIdx.y * n_vec;
   xt += blockIdx.y * n_tail;
+  yt += blockIdx.y * n_tail;
   for (int64_t k = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) / 32; k < n_tail; k += nw) {
     T s = T(0);
     for (int64_t t = off[k] + lane; t < off[k + 1]; t += 32) s += T(coef[t]) * x[idx[t]];
 #pragma unroll
     for (int d = 16; d > 0; d /= 2) s += __shfl_down_sync(0xffffffffu, s, d);
-    if (lane == 0) xt[k] = s;
+    if (lane == 0) {
+      xt[k] = s;
+      yt[k] = T(0);  // the cell kernel adds the results of the tail's entries here
+    }
   }
 }
 
@@ -111,7 +116,7 @@ template <typename T>
 __global__ void tail_gather_seg(const int32_t* __restrict__ seg_k, const int64_t* __restrict__ seg_t, int64_t n_seg,
                                 const int64_t* __restrict__ off, const int32_t* __restrict__ idx,
                                 const double* __restrict__ coef, int64_t n_tail, const T* __restrict__ x,
-                                int64_t n_vec, T* __restrict__ xt, int nrhs) {
+                                int64_t n_vec, T* __restrict__ xt, T* __restrict__ yt, int nrhs) {
   const int lane = threadIdx.x % 32;
   const bool on = lane < nrhs;
   const int64_t nw = int64_t(gridDim.x) * blockDim.x / 32;
@@ -125,7 +130,10 @@ __global__ void tail_gather_seg(const int32_t* __restrict__ seg_k, const int64_t
       const int64_t t = t0 + u;
       if (t < t1 && on) acc += T(__ldg(coef + t)) * xr[__ldg(idx + t)];
     }
-    if (on) atomicAdd(xt + lane * n_tail + k, acc);
+    if (on) {
+      atomicAdd(xt + lane * n_tail + k, acc);
+      if (t0 == off[k]) yt[lane * n_tail + k] = T(0);  // the tail's first segment clears its result slot
+    }
   }
 }
 

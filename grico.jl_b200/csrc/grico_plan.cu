@@ -7,6 +7,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -80,6 +81,7 @@ void compose_reduced(const Desc& bd, int64_t nb, const GricoPlanDesc& d,
   tidx.clear();
   tcoef.clear();
   std::vector<std::pair<int64_t, double>> acc;
+  std::map<std::vector<std::pair<int64_t, double>>, int32_t> known;  // expansion (term order kept) -> tail
   auto add = [&](int64_t r, double c) {
     for (auto& t : acc)
       if (t.first == r) { t.second += c; return; }
@@ -105,7 +107,15 @@ void compose_reduced(const Desc& bd, int64_t nb, const GricoPlanDesc& d,
       coef[e] = acc[0].second;
       if (acc[0].second != 1.0) need_coef = true;
     } else {
-      map[e] = -int32_t(toff.size() - 1) - 2;
+      // entries with the same expansion (cells sharing a hanging dof) share one tail
+      auto found = known.find(acc);
+      if (found != known.end()) {
+        map[e] = -found->second - 2;
+        continue;
+      }
+      const int32_t id = int32_t(toff.size() - 1);
+      known.emplace(acc, id);
+      map[e] = -id - 2;
       for (auto& t : acc) {
         tidx.push_back(int32_t(t.first));
         tcoef.push_back(t.second);
@@ -309,21 +319,16 @@ bool launch_fused(int dim, const DevBatch& bt, const BatchView& v, const T* x, T
 }
 
 // Tail buffers of one batch map (DevMap::n_tail): only when the longest expansion has at least
-// kTailBufferMin terms and every tail belongs to a single map entry (the cell kernel stores one
-// value per tail).
+// kTailBufferMin terms.  Several entries may share a tail (the cell kernel adds their results
+// into its slot).
 bool setup_tail_buffer(DevMap& m, const int32_t* map, int64_t ne, const int64_t* off, int64_t n_tail) {
   m.n_tail = 0;
   if (n_tail <= 0) return true;
   int64_t longest = 0;
   for (int64_t k = 0; k < n_tail; ++k) longest = std::max(longest, off[k + 1] - off[k]);
   if (longest < kTailBufferMin) return true;
-  std::vector<uint8_t> seen(size_t(n_tail), 0);
-  for (int64_t e = 0; e < ne; ++e) {
-    if (map[e] > -2) continue;
-    const int64_t k = -(int64_t(map[e]) + 2);
-    if (k >= n_tail || seen[size_t(k)]) return true;
-    seen[size_t(k)] = 1;
-  }
+  for (int64_t e = 0; e < ne; ++e)
+    if (map[e] <= -2 && -(int64_t(map[e]) + 2) >= n_tail) return true;
   if (!m.tx.alloc(sizeof(double) * size_t(n_tail) * kTailRhs) || !m.ty.alloc(sizeof(double) * size_t(n_tail) * kTailRhs))
     return false;
   std::vector<int32_t> sk;
@@ -365,10 +370,10 @@ void launch_batch(const GricoPlan& P, const DevBatch& b, bool reduced, const T* 
       cudaMemsetAsync(m.tx.ptr, 0, sizeof(T) * size_t(m.n_tail) * nrhs, st);
       tail_gather_seg<T><<<tg, 256, 0, st>>>(m.seg_k.get<int32_t>(), m.seg_t.get<int64_t>(), m.n_seg,
                                              m.toff.get<int64_t>(), m.tidx.get<int32_t>(), m.tcoef.get<double>(),
-                                             m.n_tail, x, nvec, m.tx.get<T>(), nrhs);
+                                             m.n_tail, x, nvec, m.tx.get<T>(), m.ty.get<T>(), nrhs);
     } else
       tail_gather<T><<<tg, 256, 0, st>>>(m.toff.get<int64_t>(), m.tidx.get<int32_t>(), m.tcoef.get<double>(),
-                                         m.n_tail, x, nvec, m.tx.get<T>());
+                                         m.n_tail, x, nvec, m.tx.get<T>(), m.ty.get<T>());
     v.tail_x = m.tx.ptr;
     v.tail_y = m.ty.ptr;
     v.n_tail = m.n_tail;

@@ -179,8 +179,9 @@ struct GricoPlan {
   uint64_t epoch = 1;
   // The cell and point batches of one apply run concurrently on these streams, forked from and
   // joined back to the launching stream (the scatter is atomic, so their order is free); made
-  // when the plan has more than one batch
-  static constexpr int kBranches = 4;
+  // when the plan has more than one batch; eight, so that each batch of an hp mesh (up to
+  // eight degrees) with its tail passes forms its own chain
+  static constexpr int kBranches = 8;
   int n_branches = 0;
   cudaStream_t branch[kBranches] = {};
   cudaEvent_t fork_ev = nullptr, join_ev[kBranches] = {};
