@@ -344,6 +344,49 @@ bool setup_tail_buffer(DevMap& m, const int32_t* map, int64_t ne, const int64_t*
   return true;
 }
 
+// One numbering of the buffered tails of every cell batch of a layout (GricoPlan::TailAll),
+// from the batches' device maps; segments of kTailSeg terms as in setup_tail_buffer.
+bool build_tail_all(GricoPlan* P, int layout) {
+  auto& A = P->tails[layout];
+  A.base.assign(P->batches.size(), -1);
+  std::vector<int64_t> toff{0};
+  std::vector<int32_t> tidx;
+  std::vector<double> tcoef;
+  int64_t n_tail = 0;
+  for (size_t bi = 0; bi < P->batches.size(); ++bi) {
+    const DevMap& m = layout ? P->batches[bi].red : P->batches[bi].full;
+    if (m.n_tail <= 0) continue;
+    std::vector<int64_t> off(static_cast<size_t>(m.n_tail) + 1);
+    if (!cuda_ok(cudaMemcpy(off.data(), m.toff.ptr, sizeof(int64_t) * off.size(), cudaMemcpyDeviceToHost), "tails"))
+      return false;
+    const int64_t nt = off.back();
+    std::vector<int32_t> idx(static_cast<size_t>(nt));
+    std::vector<double> co(static_cast<size_t>(nt));
+    if (nt > 0 && (!cuda_ok(cudaMemcpy(idx.data(), m.tidx.ptr, sizeof(int32_t) * nt, cudaMemcpyDeviceToHost), "tails") ||
+                   !cuda_ok(cudaMemcpy(co.data(), m.tcoef.ptr, sizeof(double) * nt, cudaMemcpyDeviceToHost), "tails")))
+      return false;
+    A.base[bi] = n_tail;
+    const int64_t t0 = int64_t(tidx.size());
+    for (int64_t k = 0; k < m.n_tail; ++k) toff.push_back(t0 + off[size_t(k) + 1]);
+    tidx.insert(tidx.end(), idx.begin(), idx.end());
+    tcoef.insert(tcoef.end(), co.begin(), co.end());
+    n_tail += m.n_tail;
+  }
+  A.n_tail = n_tail;
+  if (n_tail == 0) return true;
+  std::vector<int32_t> sk;
+  std::vector<int64_t> st;
+  for (int64_t k = 0; k < n_tail; ++k)
+    for (int64_t t = toff[size_t(k)]; t < toff[size_t(k) + 1]; t += kTailSeg) {
+      sk.push_back(int32_t(k));
+      st.push_back(t);
+    }
+  A.n_seg = int64_t(sk.size());
+  return A.toff.upload(toff) && A.tidx.upload(tidx) && A.tcoef.upload(tcoef) && A.seg_k.upload(sk) &&
+         A.seg_t.upload(st) && A.tx.alloc(sizeof(double) * size_t(n_tail) * kTailRhs) &&
+         A.ty.alloc(sizeof(double) * size_t(n_tail) * kTailRhs);
+}
+
 template <typename T>
 void launch_batch_cells(const GricoPlan& P, const DevBatch& b, BatchView& v, const T* x, T* y, int64_t nvec, int mode,
                         const double* src, int nrhs, cudaStream_t st);
@@ -353,11 +396,20 @@ void launch_batch_cells(const GricoPlan& P, const DevBatch& b, BatchView& v, con
 // buffers), the tail scatter; long expansions no longer serialise one thread of the cell kernel.
 template <typename T>
 void launch_batch(const GricoPlan& P, const DevBatch& b, bool reduced, const T* x, T* y, int64_t nvec, int mode,
-                  const double* src, int nrhs, cudaStream_t st, void* local_out = nullptr, int64_t local_stride = 0) {
+                  const double* src, int nrhs, cudaStream_t st, void* local_out = nullptr, int64_t local_stride = 0,
+                  T* merged_tx = nullptr, T* merged_ty = nullptr, int64_t merged_stride = 0) {
   BatchView v;
   fill_view(v, b, reduced);
   v.local_out = local_out;
   v.local_stride = local_stride;
+  if (merged_tx) {
+    // the tails were summed by the apply's merged pass and are spread by it afterwards
+    v.tail_x = merged_tx;
+    v.tail_y = merged_ty;
+    v.n_tail = merged_stride;
+    launch_batch_cells<T>(P, b, v, x, y, nvec, mode, src, nrhs, st);
+    return;
+  }
   const DevMap& m = reduced ? b.red : b.full;
   const bool buffered = mode == 0 && x && m.n_tail > 0 && nrhs <= kTailRhs && !local_out;
   // several right-hand sides: segments with the columns on the lanes (kTailLaneRhs or more),
@@ -813,6 +865,23 @@ int run_apply(GricoPlan* P, bool reduced, const T* x, T* y, int nrhs, cudaStream
   // the final check covers this call's launches only, not an error an earlier call left pending
   (void)cudaGetLastError();
   cudaMemsetAsync(y, 0, sizeof(T) * n * nrhs, st);
+  // the buffered tails of all batches: one gather pass before the cell kernels
+  const GricoPlan::TailAll& TA = P->tails[reduced ? 1 : 0];
+  const bool merged = TA.n_tail > 0 && nrhs <= kTailRhs;
+  const bool lanes_rhs = nrhs >= kTailLaneRhs;
+  const dim3 tg(int(std::min<int64_t>(((lanes_rhs ? TA.n_seg : TA.n_tail) * 32 + 255) / 256, 148 * 16)),
+                lanes_rhs ? 1u : unsigned(nrhs));
+  if (merged) {
+    if (lanes_rhs) {
+      cudaMemsetAsync(TA.tx.ptr, 0, sizeof(T) * size_t(TA.n_tail) * nrhs, st);
+      tail_gather_seg<T><<<tg, 256, 0, st>>>(TA.seg_k.get<int32_t>(), TA.seg_t.get<int64_t>(), TA.n_seg,
+                                             TA.toff.get<int64_t>(), TA.tidx.get<int32_t>(), TA.tcoef.get<double>(),
+                                             TA.n_tail, x, n, TA.tx.get<T>(), TA.ty.get<T>(), nrhs);
+    } else {
+      tail_gather<T><<<tg, 256, 0, st>>>(TA.toff.get<int64_t>(), TA.tidx.get<int32_t>(), TA.tcoef.get<double>(),
+                                         TA.n_tail, x, n, TA.tx.get<T>(), TA.ty.get<T>());
+    }
+  }
   // several batches: round-robin over the branch streams (not while timing batches, whose
   // event pairs need one stream)
   const bool fork = P->n_branches > 1 && !P->time_batches;
@@ -826,7 +895,11 @@ int run_apply(GricoPlan* P, bool reduced, const T* x, T* y, int nrhs, cudaStream
     GricoPlan::BatchEvent ev{int(bi), nullptr, nullptr};
     if (P->time_batches && cudaEventCreate(&ev.start) == cudaSuccess && cudaEventCreate(&ev.stop) == cudaSuccess)
       cudaEventRecord(ev.start, st);
-    launch_batch<T>(*P, P->batches[bi], reduced, x, y, n, 0, nullptr, nrhs, stream_for());
+    if (merged && TA.base[bi] >= 0)
+      launch_batch<T>(*P, P->batches[bi], reduced, x, y, n, 0, nullptr, nrhs, stream_for(), nullptr, 0,
+                      TA.tx.get<T>() + TA.base[bi], TA.ty.get<T>() + TA.base[bi], TA.n_tail);
+    else
+      launch_batch<T>(*P, P->batches[bi], reduced, x, y, n, 0, nullptr, nrhs, stream_for());
     if (ev.stop) {
       cudaEventRecord(ev.stop, st);
       P->batch_events.push_back(ev);
@@ -847,6 +920,15 @@ int run_apply(GricoPlan* P, bool reduced, const T* x, T* y, int nrhs, cudaStream
       cudaEventRecord(P->join_ev[k], P->branch[k]);
       cudaStreamWaitEvent(st, P->join_ev[k], 0);
     }
+  if (merged) {
+    if (lanes_rhs)
+      tail_scatter_seg<T><<<tg, 256, 0, st>>>(TA.seg_k.get<int32_t>(), TA.seg_t.get<int64_t>(), TA.n_seg,
+                                              TA.toff.get<int64_t>(), TA.tidx.get<int32_t>(), TA.tcoef.get<double>(),
+                                              TA.n_tail, TA.ty.get<T>(), y, n, nrhs);
+    else
+      tail_scatter<T><<<tg, 256, 0, st>>>(TA.toff.get<int64_t>(), TA.tidx.get<int32_t>(), TA.tcoef.get<double>(),
+                                          TA.n_tail, TA.ty.get<T>(), y, n);
+  }
   if (!reduced && (P->n_fixed + P->n_rel) > 0) {
     dim3 grid(grid_for(P->n_fixed + P->n_rel), nrhs);
     constraint_action<T><<<grid, 256, 0, st>>>(P->fixed.get<int64_t>(), P->n_fixed, P->rel_piv.get<int64_t>(),
@@ -1455,6 +1537,7 @@ int grico_plan_create(const GricoPlanDesc* d, GricoPlan** out) {
   ok = ok && P->partial.alloc(sizeof(double) * (kRedBlocks + 8)) && P->scalars.alloc(sizeof(double) * 16);
   if (!ok) return GRICO_ERR_CUDA;
   if (!cuda_ok(cudaStreamSynchronize(P->stream), "plan upload")) return GRICO_ERR_CUDA;
+  if (!build_tail_all(P.get(), 0) || !build_tail_all(P.get(), 1)) return GRICO_ERR_CUDA;
   const int n_launch = int(P->batches.size() + P->pbatches.size());
   if (n_launch > 1) {
     const int nbr = std::min(n_launch, int(GricoPlan::kBranches));

@@ -163,6 +163,15 @@ struct GricoPlan {
   };
   DetMap det[2];
   grico::DevBuf det_local;
+  // The buffered tails of every cell batch of one layout (0 full, 1 reduced) in one numbering,
+  // so that an apply sums and spreads all of them in one launch each: batch b's tails are
+  // base[b] .. base[b] + its n_tail; buffers [rhs][n_tail] (kTailRhs columns)
+  struct TailAll {
+    int64_t n_tail = 0, n_seg = 0;
+    std::vector<int64_t> base;  // per cell batch; -1: not buffered
+    grico::DevBuf toff, tidx, tcoef, seg_k, seg_t, tx, ty;
+  };
+  TailAll tails[2];
   // GRICO_FLAG_TIME_BATCHES: event pairs around cell-batch launches, (batch, start, stop)
   struct BatchEvent { int batch; cudaEvent_t start, stop; };
   bool time_batches = false;
