@@ -1271,8 +1271,10 @@ class Plan:
         return self.project(b)
 
 
-def cg_solve(apply_fn, b, precond=None, rtol=1e-10, atol=0.0, maxiter=10000):
-    """PCG with the unpreconditioned stop rule (solve.jl:376-431)."""
+def cg_solve(apply_fn, b, precond=None, rtol=1e-10, atol=0.0, maxiter=10000, raise_unconverged=True):
+    """PCG with the unpreconditioned stop rule (solve.jl:376-431).  After maxiter iterations
+    without convergence it raises, as the reference does (solve.jl:430), or with
+    raise_unconverged=False returns the last iterate."""
     n = len(b)
     x = np.zeros(n)
     r = b.copy()
@@ -1297,6 +1299,8 @@ def cg_solve(apply_fn, b, precond=None, rtol=1e-10, atol=0.0, maxiter=10000):
         beta = rz_new / rz
         p = z + beta * p
         rz = rz_new
+    if not raise_unconverged:
+        return x, maxiter
     raise ValueError("CG did not converge")
 
 

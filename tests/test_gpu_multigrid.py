@@ -209,3 +209,45 @@ def test_kept_cg_graph_replays_across_solves(cuda):
         xd, id_ = run(b, L.GRICO_FLAG_NO_GRAPH)
         assert ig == id_
         assert rel_err(xg, xd) <= 1e-12
+
+
+def test_reference_method_at_8cube_p4_matches_oracle_fixture(cuda):
+    """The reference's own solver at an intermediate size (8^3 cells, degree 4, mass + diffusion,
+    six Dirichlet faces; hp hierarchy p 4 -> 2 -> 1 -> h-merges; damped-Jacobi V(2,2)): level
+    sizes, the V-cycle of a seeded vector (1e-11) and CG with it stopped after 5, 10, 20 and 40
+    iterations (solve.jl:430 reports the non-convergence) against the oracle's iterates in
+    tests/golden/reference_gmg_8cube_p4.npz (tests/golden/make_reference_gmg.py)."""
+    import ctypes as C
+    import os
+
+    from grico_b200 import _lib as L
+    from test_multigrid_host import _refine_uniform
+
+    fx = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_gmg_8cube_p4.npz"))
+    d = gb.Domain((0.0, 0.0, 0.0), (1.0, 1.0, 1.0), (4, 4, 4))
+    _refine_uniform(d.grid, 1)
+    s = gb.HpSpace(d, gb.SpaceOptions(basis=gb.FullTensorBasis(), degree=gb.UniformDegree(4)))
+    u = gb.ScalarField(s)
+    prob = gb.AffineProblem(u)
+    gb.add_cell_accumulator(prob, u, u, gb.MassDiffusion(1.0, 1.0))
+    for a in (1, 2, 3):
+        for side in (gb.LOWER, gb.UPPER):
+            gb.add_constraint(prob, gb.Dirichlet(u, gb.BoundaryFace(a, side), 0.0))
+    plan = gb.compile(prob)
+    mg = build_multigrid(plan, GeometricMultigridPreconditioner())
+    assert mg.level_sizes() == fx["level_sizes"].tolist()
+    b = np.random.default_rng(7).standard_normal(plan.n_reduced)
+    assert abs(b.sum() - fx["b_sum"][0]) <= 1e-9 * abs(fx["b_sum"][0])
+    assert rel_err(mg.vcycle(b), fx["vcycle"]) <= 1e-11
+    # the method diverges on this basis (residual 3.5 ||b|| after 40 iterations), so rounding
+    # differences grow with the iteration count: bounds per stop
+    errs = {}
+    for k, tol in zip(fx["cg_iterations"].tolist(), (1e-10, 1e-9, 1e-7, 1e-5)):
+        x = np.zeros(plan.n_reduced)
+        opts = L.GricoSolveOptions(1e-14, 0.0, k, L.GRICO_PRECOND_MULTIGRID, 30, 0)
+        rep = L.GricoSolveReport()
+        rc = L.lib().grico_cg_solve(plan.handle, mg.handle, L.ptr(b, C.c_double), L.ptr(x, C.c_double),
+                                    C.byref(opts), C.byref(rep), L.GRICO_FLAG_HOST_POINTERS)
+        assert rc == L.GRICO_ERR_NOT_CONVERGED and rep.iterations == k
+        errs[k] = rel_err(x[::7], fx[f"cg_iterate_{k}"])  # the fixture keeps every 7th dof
+        assert errs[k] <= tol, errs

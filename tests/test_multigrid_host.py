@@ -135,3 +135,19 @@ def test_oracle_gmres_smoother_reduces_residual():
         rg = np.linalg.norm(b - fine.reduced_apply(xg))
         assert rg <= np.linalg.norm(b - fine.reduced_apply(xj)) * (1 + 1e-12)
         assert rg < np.linalg.norm(b)
+
+
+def test_reference_gmg_fixture_matches_the_product_hierarchy():
+    """tests/golden/reference_gmg_8cube_p4.npz (the oracle's reference-method solve at 8^3 cells,
+    p = 4): its hierarchy has the level sizes the product builds for the same problem."""
+    import os
+
+    fx = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_gmg_8cube_p4.npz"))
+    d = gb.Domain((0.0, 0.0, 0.0), (1.0, 1.0, 1.0), (4, 4, 4))
+    _refine_uniform(d.grid, 1)
+    plans, _ = build_hierarchy(_product_plan(d, 4, faces=[(a, s) for a in (1, 2, 3) for s in (1, 2)]),
+                               GeometricMultigridPreconditioner(), device=False)
+    assert [p.n_reduced for p in plans] == fx["level_sizes"].tolist()
+    assert fx["vcycle"].size == plans[-1].n_reduced
+    for k in fx["cg_iterations"]:
+        assert fx[f"cg_iterate_{k}"].size == (plans[-1].n_reduced + 6) // 7  # every 7th dof
