@@ -541,7 +541,7 @@ def c1_leg(gb, L, peak):
     try:
         for sub in ("oracle", "tests"):
             sys.path.insert(0, os.path.join(ROOT, sub))
-        from baseline_cases import oracle_cell_sum, uniform_oracle
+        from full_size_cases import oracle_cell_sum, uniform_oracle
         import oracle_lib as ol
 
         coords, m, ndofs, _ = uniform_oracle((32, 32), 4)
@@ -685,7 +685,7 @@ def c5_leg(gb, L, peak):
 
 
 def config_legs(gb, L, only=None):
-    """Every BASELINE configuration besides the headline one, each in its own try block."""
+    """Every benchmark configuration besides the headline one, each in its own try block."""
     import traceback
 
     peak, _ = load_peaks()
@@ -770,7 +770,7 @@ def main():
                              "lshape_hp32", "lshape_apply32", "conv_tc", "sipg3d"],
                     help="poisson64: 3-D Poisson 64^3 p=4 (default); fcm_shell*: finite-cell shell with Nitsche")
     ap.add_argument("--fp32", action="store_true", help="time the FP32 apply instead of FP64")
-    ap.add_argument("--no-configs", action="store_true", help="skip the other BASELINE configurations")
+    ap.add_argument("--no-configs", action="store_true", help="skip the other benchmark configurations")
     ap.add_argument("--configs", default="", help="comma-separated config legs to run (c1_poisson2d_32_p4, "
                     "c3_lshape_hp32, c4_grf_learned64, c5_fcm_shell64); default: all")
     args = ap.parse_args()

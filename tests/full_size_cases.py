@@ -1,4 +1,4 @@
-"""The BASELINE workloads at full size, built through the product's public API, and the
+"""The benchmark workloads at full size, built through the product's public API, and the
 oracle-side data that checks them (uniform numbering, the reference's tensor schedule in C)."""
 import math
 

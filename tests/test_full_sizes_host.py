@@ -4,7 +4,7 @@ literal restatement of continuity.jl in test_oracle_kat.py)."""
 import numpy as np
 
 import grico_b200 as gb
-from baseline_cases import poisson3d_64, uniform_oracle
+from full_size_cases import poisson3d_64, uniform_oracle
 
 
 def test_poisson64_maps_and_fixed_set_bit_exact():

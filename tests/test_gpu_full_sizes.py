@@ -1,4 +1,4 @@
-"""GPU parity at the BASELINE sizes.
+"""GPU parity at the benchmark workloads' full sizes.
 
 * 64^3 cells, p = 4 (16,974,593 dofs): the device's full apply! and reduced apply against the
   oracle's C restatement of the reference's tensor schedule (D + D^2 contractions per cell,
@@ -13,7 +13,7 @@ import pytest
 
 import grico_oracle as go
 import grico_b200 as gb
-from baseline_cases import (diagnostic_sample_vector, oracle_cell_sum, poisson2d_32, poisson3d_64,
+from full_size_cases import (diagnostic_sample_vector, oracle_cell_sum, poisson2d_32, poisson3d_64,
                             uniform_oracle)
 from cases import rel_err
 
