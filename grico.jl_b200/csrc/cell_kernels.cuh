@@ -1052,13 +1052,21 @@ __global__ void __launch_bounds__(kPointThreads) interface_apply(PointView b, co
 // the points, the flux w (sigma J - {du/dn}) and -w J / 2 (J = u- - u+) is formed per point,
 // and the transposed contractions project it back: O(n^3 + n^2 q + n q^2) per side instead of
 // q^2 n^3 mode evaluations.
-template <typename T, int D>
+template <typename T, int D, int G>
 __global__ void __launch_bounds__(kPointThreads) interface_apply_sf(PointView b, const int32_t* __restrict__ sf_q,
                                                                     const double* __restrict__ sf_x, int sf_stride,
                                                                     const T* __restrict__ x, T* __restrict__ y,
-                                                                    int64_t n_vec) {
+                                                                    int64_t n_vec, int64_t item_elems) {
+  // G threads per interface: a warp (32, kPointThreads / 32 interfaces per block, warp barriers)
+  // or the whole block (kPointThreads)
+  static_assert(G == 32 || G == kPointThreads, "one warp or one block per interface");
   extern __shared__ unsigned char smem_raw[];
-  const int64_t item = blockIdx.x;
+  const int64_t item = int64_t(blockIdx.x) * (kPointThreads / G) + threadIdx.x / G;
+  if (item >= b.n_items) return;  // only warp barriers follow when G == 32
+  auto sync = [] {
+    if constexpr (G == 32) __syncwarp();
+    else __syncthreads();
+  };
   x += blockIdx.y * n_vec;
   y += blockIdx.y * n_vec;
   const int ax = b.axis[item];
@@ -1077,7 +1085,7 @@ __global__ void __launch_bounds__(kPointThreads) interface_apply_sf(PointView b,
   const int P = q1 * q2;
   // shared memory (T): local modes; per side Vn, Dn [nmax], V1 [nmax x Qm], V2 [nmax x Qm],
   // U/Dv [nmax x nmax], W/WD [Qm x nmax]; traces at the points u[2][P], d[2][P]; flux F0, F1 [P]
-  T* xl = reinterpret_cast<T*>(smem_raw);
+  T* xl = reinterpret_cast<T*>(smem_raw) + (threadIdx.x / G) * item_elems;
   T* base = xl + nb;
   const int per_side = 2 * nmax + 2 * nmax * Qm + 2 * nmax * nmax + 2 * Qm * nmax;
   auto Vn = [&](int s) { return base + s * per_side; };
@@ -1091,7 +1099,7 @@ __global__ void __launch_bounds__(kPointThreads) interface_apply_sf(PointView b,
   T* tr = base + 2 * per_side;  // u[s][p] at tr + s * P, d[s][p] at tr + (2 + s) * P
   T* F0 = tr + 4 * P;
   T* F1 = F0 + P;
-  const int tid = threadIdx.x, nt = blockDim.x;
+  const int tid = threadIdx.x % G, nt = G;
 
   BatchView bv;
   bv.n_cells = b.n_items;
@@ -1128,7 +1136,7 @@ __global__ void __launch_bounds__(kPointThreads) interface_apply_sf(PointView b,
       for (int i = 0; i <= deg; ++i) V2(s)[i * Qm + (r - 1 - q1)] = v[i];
     }
   }
-  __syncthreads();
+  sync();
   auto box = [&](int s, int ia, int i1, int i2) {
     int mi[3] = {0, 0, 0};
     mi[ax] = ia;
@@ -1150,7 +1158,7 @@ __global__ void __launch_bounds__(kPointThreads) interface_apply_sf(PointView b,
     U0(s)[i1 * nmax + i2] = u;
     UD(s)[i1 * nmax + i2] = du;
   }
-  __syncthreads();
+  sync();
   // B: t1 contraction -> W0, WD [p1 * nmax + i2]
   for (int t = tid; t < 2 * q1 * nmax; t += nt) {
     const int s = t / (q1 * nmax), p1 = (t / nmax) % q1, i2 = t % nmax;
@@ -1164,7 +1172,7 @@ __global__ void __launch_bounds__(kPointThreads) interface_apply_sf(PointView b,
     W0(s)[p1 * nmax + i2] = u;
     WD(s)[p1 * nmax + i2] = du;
   }
-  __syncthreads();
+  sync();
   // C: t2 contraction -> traces at the points p = p1 + q1 p2
   for (int t = tid; t < 2 * P; t += nt) {
     const int s = t / P, p = t % P, p1 = p % q1, p2 = p / q1;
@@ -1177,7 +1185,7 @@ __global__ void __launch_bounds__(kPointThreads) interface_apply_sf(PointView b,
     tr[s * P + p] = u;
     tr[(2 + s) * P + p] = du;
   }
-  __syncthreads();
+  sync();
   const T sigma = T(b.eta[item]);
   const int64_t p0 = b.pt_off[item];
   for (int p = tid; p < P; p += nt) {
@@ -1187,7 +1195,7 @@ __global__ void __launch_bounds__(kPointThreads) interface_apply_sf(PointView b,
     F0[p] = w * (sigma * jump - avg);
     F1[p] = -T(0.5) * w * jump;
   }
-  __syncthreads();
+  sync();
   // C^T: sum over p2 -> W0 (F0 with the side's sign), WD (F1)
   for (int t = tid; t < 2 * q1 * nmax; t += nt) {
     const int s = t / (q1 * nmax), p1 = (t / nmax) % q1, i2 = t % nmax;
@@ -1201,7 +1209,7 @@ __global__ void __launch_bounds__(kPointThreads) interface_apply_sf(PointView b,
     W0(s)[p1 * nmax + i2] = s ? -g0 : g0;
     WD(s)[p1 * nmax + i2] = g1;
   }
-  __syncthreads();
+  sync();
   // B^T: sum over p1 -> U0, UD
   for (int t = tid; t < 2 * nmax * nmax; t += nt) {
     const int s = t / (nmax * nmax), i1 = (t / nmax) % nmax, i2 = t % nmax;
@@ -1215,7 +1223,7 @@ __global__ void __launch_bounds__(kPointThreads) interface_apply_sf(PointView b,
     U0(s)[i1 * nmax + i2] = h0;
     UD(s)[i1 * nmax + i2] = h1;
   }
-  __syncthreads();
+  sync();
   // A^T and scatter: y_i = Vn[ia] H0[i1, i2] + Dn[ia] H1[i1, i2]
   for (int i = tid; i < nb; i += nt) {
     const int s = i >= nbm ? 1 : 0, li = s ? i - nbm : i;

@@ -561,14 +561,18 @@ void launch_points(const GricoPlan& P, const DevPointBatch& pb, bool reduced, co
                               std::max(pb.np[0], std::max(D > 1 ? pb.np[1] : 1, D > 2 ? pb.np[2] : 1)));
     dim3 grid(pb.n_items, nrhs);
     if (mode == 0 && pb.sf_ok && D >= 2) {
-      const size_t sm = interface_sf_smem(nbi, nmax, pb.sf_qmax, int(pb.sf_pmax), sizeof(T));
+      // one warp per interface, kPointThreads / 32 interfaces per block
+      const size_t item_bytes = interface_sf_smem(nbi, nmax, pb.sf_qmax, int(pb.sf_pmax), sizeof(T));
+      const int per_block = kPointThreads / 32;
+      const size_t sm = item_bytes * per_block;
+      const dim3 gsf(unsigned((pb.n_items + per_block - 1) / per_block), unsigned(nrhs));
       auto go_sf = [&](auto kernel) {
         if (sm > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
-        kernel<<<grid, kPointThreads, sm, st>>>(v, pb.sf_q.get<int32_t>(), pb.sf_x.get<double>(), pb.sf_stride, x, y,
-                                               nvec);
+        kernel<<<gsf, kPointThreads, sm, st>>>(v, pb.sf_q.get<int32_t>(), pb.sf_x.get<double>(), pb.sf_stride, x, y,
+                                              nvec, int64_t(item_bytes / sizeof(T)));
       };
-      if (D == 2) go_sf(interface_apply_sf<T, 2>);
-      else go_sf(interface_apply_sf<T, 3>);
+      if (D == 2) go_sf(interface_apply_sf<T, 2, 32>);
+      else go_sf(interface_apply_sf<T, 3, 32>);
       return;
     }
     const size_t smem = sizeof(T) * (size_t(nbi) + 4 * size_t(kPointChunk) * D * nmax + 2 * size_t(kPointChunk));
