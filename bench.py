@@ -767,7 +767,7 @@ def main():
                     "(ref_jacobi, fp64_nograph, fp64, mixed2, mixed3); default: all")
     ap.add_argument("--workload", default="poisson64",
                     choices=["poisson64", "fcm_shell64", "fcm_shell32", "grf_learned128", "grf_learned64",
-                             "lshape_hp32", "lshape_apply32", "conv_tc", "sipg3d"],
+                             "lshape_hp32", "lshape_apply32", "conv_tc", "sipg3d", "dense_tc64"],
                     help="poisson64: 3-D Poisson 64^3 p=4 (default); fcm_shell*: finite-cell shell with Nitsche")
     ap.add_argument("--fp32", action="store_true", help="time the FP32 apply instead of FP64")
     ap.add_argument("--no-configs", action="store_true", help="skip the other benchmark configurations")
@@ -828,6 +828,43 @@ def main():
                                                                "dofs": plan.n_full,
                                                                "interfaces": int(sum(len(b.cells) for b in plan.point_batches))},
                               "checksum": float(yv.double().sum().item())}), flush=True)
+        return
+    if args.workload == "dense_tc64":
+        # the 64^3 p = 4 reduced FP32 apply with every 3-D kernel variant, the tensor-core
+        # element-matrix variant (10) among them, against the FP64 apply
+        import torch
+
+        from grico_b200 import batched as bt
+
+        prob = build_problem(gb)
+        plan = gb.compile(prob)
+        st = torch.cuda.Stream()
+        nr = plan.n_reduced
+        x64 = torch.tensor(sample_vector(nr), dtype=torch.float64, device="cuda")
+        y64 = torch.empty_like(x64)
+        x32, y32 = x64.float(), torch.empty(nr, dtype=torch.float32, device="cuda")
+        f64 = lambda: L.lib().grico_reduced_apply(plan.handle, x64.data_ptr(), y64.data_ptr(), 1, L.GRICO_PREC_FP64, 0,
+                                                  st.cuda_stream)
+        for _ in range(args.warmup):
+            f64()
+        torch.cuda.synchronize()
+        res = {"fp64_ms": _timed_device(f64, args.steps, st)}
+        ref = y64.double()
+        f32 = lambda: L.lib().grico_reduced_apply(plan.handle, x32.data_ptr(), y32.data_ptr(), 1, L.GRICO_PREC_FP32, 0,
+                                                  st.cuda_stream)
+        for var in (10, 3, 9, 1):
+            bt.set_tiles(plan, [var] * len(plan.batches), "fp32")
+            for _ in range(args.warmup):
+                f32()
+            torch.cuda.synchronize()
+            ms = _timed_device(f32, args.steps, st)
+            res[f"fp32_variant{var}"] = {"ms": ms, "rel_err_vs_fp64": float((y32.double() - ref).abs().max() / ref.abs().max())}
+        L.check(L.lib().grico_tc_status(C.c_void_p(st.cuda_stream)), "tensor-core status")
+        if rank == 0:
+            print(json.dumps({"metric": "64^3 p=4 reduced apply device time per kernel variant", "unit": "ms",
+                              "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+                              "data": "synthetic", "config": {"workload": "dense_tc64", "reduced_dofs": nr}, **res}),
+                  flush=True)
         return
     if args.workload == "lshape_apply32":
         # the hp L-shape's reduced FP64 apply, 1 and 32 right-hand sides, W untimed then K timed
