@@ -99,6 +99,15 @@ __global__ void jacobi_smooth(T* __restrict__ x, const T* __restrict__ b, const 
     x[i] += w * dinv[i] * (b[i] - ax[i]);
 }
 
+// First smoothing step from x = 0, whose apply is skipped: A 0 = 0, so b - ax is b and the
+// damped-Jacobi step x += w dinv (b - ax) becomes x = w dinv b (the same values, bit for bit)
+template <typename T>
+__global__ void jacobi_from_zero(T* __restrict__ x, const T* __restrict__ b, const T* __restrict__ dinv, T w,
+                                 int64_t n) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    x[i] = T(0) + w * dinv[i] * b[i];
+}
+
 // d = c1*d + c2*dinv*(b - ax); x += d
 template <typename T>
 __global__ void chebyshev_step(T* __restrict__ x, T* __restrict__ d, const T* __restrict__ b,
@@ -108,6 +117,17 @@ __global__ void chebyshev_step(T* __restrict__ x, T* __restrict__ d, const T* __
     T di = (c1 != T(0) ? c1 * d[i] : T(0)) + c2 * dinv[i] * (b[i] - ax[i]);
     d[i] = di;
     x[i] += di;
+  }
+}
+
+// First Chebyshev step from x = 0 (apply skipped, as for jacobi_from_zero): d = x = c2 dinv b
+template <typename T>
+__global__ void chebyshev_from_zero(T* __restrict__ x, T* __restrict__ d, const T* __restrict__ b,
+                                    const T* __restrict__ dinv, T c2, int64_t n) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    const T di = T(0) + c2 * dinv[i] * b[i];
+    d[i] = di;
+    x[i] = T(0) + di;
   }
 }
 
@@ -201,8 +221,10 @@ void level_apply(GricoMultigrid* mg, int l, const T* x, T* y, cudaStream_t st) {
 template <typename T>
 void smooth_gmres(GricoMultigrid* mg, int l, T* x, const T* b, int steps, cudaStream_t st);
 
+// x_zero: x holds no values yet and is taken as zero (Jacobi and Chebyshev only; the caller
+// zeroes x for the GMRES smoother), so the first step skips its apply of x
 template <typename T>
-void smooth(GricoMultigrid* mg, int l, T* x, const T* b, int steps, cudaStream_t st) {
+void smooth(GricoMultigrid* mg, int l, T* x, const T* b, int steps, cudaStream_t st, bool x_zero = false) {
   using B = LevelBufs<T>;
   const int64_t n = mg->levels[l]->n_red;
   T* t = B::t(mg, l);
@@ -214,6 +236,10 @@ void smooth(GricoMultigrid* mg, int l, T* x, const T* b, int steps, cudaStream_t
   }
   if (mg->opts.smoother == GRICO_SMOOTHER_JACOBI) {
     for (int s = 0; s < steps; ++s) {
+      if (s == 0 && x_zero) {
+        jacobi_from_zero<T><<<blocks(n), 256, 0, st>>>(x, b, dinv, T(mg->opts.jacobi_omega), n);
+        continue;
+      }
       level_apply<T>(mg, l, x, t, st);
       jacobi_smooth<T><<<blocks(n), 256, 0, st>>>(x, b, t, dinv, T(mg->opts.jacobi_omega), n);
     }
@@ -227,6 +253,10 @@ void smooth(GricoMultigrid* mg, int l, T* x, const T* b, int steps, cudaStream_t
   for (int s = 0; s < steps; ++s) {
     double rho_old = 1.0 / sigma;
     for (int k = 0; k < mg->opts.chebyshev_degree; ++k) {
+      if (s == 0 && k == 0 && x_zero) {
+        chebyshev_from_zero<T><<<blocks(n), 256, 0, st>>>(x, d, b, dinv, T(1.0 / theta), n);
+        continue;
+      }
       level_apply<T>(mg, l, x, t, st);
       if (k == 0) {
         chebyshev_step<T><<<blocks(n), 256, 0, st>>>(x, d, b, t, dinv, T(0), T(1.0 / theta), n);
@@ -496,14 +526,15 @@ void vcycle(GricoMultigrid* mg, int l, T* x, const T* b, cudaStream_t st) {
     coarse_solve(mg, x, b, st);
     return;
   }
-  cudaMemsetAsync(x, 0, sizeof(T) * n, st);
-  if (mg->learned.level == l) {
-    // the learned sweep replaces the last pre-smoothing step on its level
-    smooth<T>(mg, l, x, b, std::max(mg->opts.pre_steps - 1, 0), st);
-    learned_sweep<T>(mg, l, x, b, st);
-  } else {
-    smooth<T>(mg, l, x, b, mg->opts.pre_steps, st);
-  }
+  // the learned sweep replaces the last pre-smoothing step on its level
+  const bool learned = mg->learned.level == l;
+  const int pre = learned ? std::max(mg->opts.pre_steps - 1, 0) : mg->opts.pre_steps;
+  // x starts at zero; Jacobi and Chebyshev take that as given in their first step instead of
+  // applying the operator to a zeroed vector
+  const bool from_zero = pre > 0 && mg->opts.smoother != GRICO_SMOOTHER_GMRES;
+  if (!from_zero) cudaMemsetAsync(x, 0, sizeof(T) * n, st);
+  smooth<T>(mg, l, x, b, pre, st, from_zero);
+  if (learned) learned_sweep<T>(mg, l, x, b, st);
   T* t = B::t(mg, l);
   T* r = B::r(mg, l);
   level_apply<T>(mg, l, x, t, st);
