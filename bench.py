@@ -706,52 +706,58 @@ def config_legs(gb, L, only=None):
 
 def sharded_leg(gb, plan, rank, world, steps, warmup):
     """The same mesh split over the ranks (strong scaling): each rank applies the reduced
-    operator of its Morton range of cells and the partition-surface halo is summed with one NCCL
-    all-reduce per apply.  Device time with CUDA events, max over ranks; the result is checked
-    against the unsharded reduced apply on this rank's dofs."""
+    operator of its Morton range of cells and the partition-surface halo is summed, either by
+    point-to-point exchange with the ranks sharing dofs (NCCL send/receive, the default) or by
+    one NCCL all-reduce over every halo slot.  Device time with CUDA events, max over ranks; the
+    result is checked against the unsharded reduced apply on this rank's dofs."""
     import torch
     import torch.distributed as dist
 
-    from grico_b200.sharded import ShardedOperator, ShardPlan
+    from grico_b200.sharded import ShardedOperator, ShardGroup, ShardPlan
 
     t0 = time.perf_counter()
     shard = ShardPlan(plan, rank, world)
     setup = time.perf_counter() - t0
-    op = ShardedOperator([shard])
     xg = sample_vector(plan.n_reduced)
-    x = op.ops.upload(shard.scatter(xg))
-    y = op.ops.vector(shard.n_reduced)
-    yl = op.ops.vector(shard.n_reduced)
-    for _ in range(warmup):
-        op.apply([x], [y])
-    torch.cuda.synchronize()
-    dist.barrier()
-    torch.cuda.synchronize()
+    ref = gb.reduced_apply(plan, xg)[shard.global_reduced]
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(steps):
-        op.apply([x], [y])
-    e1.record()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / steps
-    e0.record()
-    for _ in range(steps):
-        op.ops.apply(shard, x, yl)  # the local apply alone: the halo sum's cost is the difference
-    e1.record()
-    torch.cuda.synchronize()
-    ms_local = e0.elapsed_time(e1) / steps
-    ref = gb.reduced_apply(plan, xg)[shard.global_reduced]
-    err = float(np.max(np.abs(y.cpu().numpy()[: shard.n_reduced] - ref)) / np.max(np.abs(ref)))
-    t = torch.tensor([ms, ms_local, err], device="cuda", dtype=torch.float64)
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        dist.barrier()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    res = []
+    for mode in ("neighbours", "allreduce"):
+        op = ShardedOperator([shard], ShardGroup(halo=mode))
+        x = op.ops.upload(shard.scatter(xg))
+        y = op.ops.vector(shard.n_reduced)
+        for _ in range(warmup):
+            op.apply([x], [y])
+        res.append(timed(lambda: op.apply([x], [y])))
+        res.append(float(np.max(np.abs(y.cpu().numpy()[: shard.n_reduced] - ref)) / np.max(np.abs(ref))))
+    yl = op.ops.vector(shard.n_reduced)
+    res.append(timed(lambda: op.ops.apply(shard, x, yl)))  # the local apply alone
+    t = torch.tensor(res, device="cuda", dtype=torch.float64)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms, ms_local, err = (float(v) for v in t.cpu())
+    ms, err, ms_ar, err_ar, ms_local = (float(v) for v in t.cpu())
     return {"metric": "sharded reduced apply throughput (one 64^3 p=4 mesh split over the GPUs)",
             "value": plan.n_reduced / (ms * 1e-3), "unit": "DOFs/s", "scaling": "strong",
-            "ms_per_apply": ms, "local_apply_ms_max": ms_local, "halo_slots": shard.n_halo,
-            "halo_bytes_per_apply": 8 * shard.n_halo, "cells_rank0": int(sum(len(b.cells) for b in shard.plan.batches)),
-            "partition": "contiguous Morton ranges balanced by (p+1)^3 q^3", "collective": "NCCL all-reduce of the halo",
-            "max_rel_err_vs_unsharded": err, "shard_setup_seconds": setup}
+            "ms_per_apply": ms, "allreduce_halo_ms_per_apply": ms_ar, "local_apply_ms_max": ms_local,
+            "halo_slots": shard.n_halo, "neighbours_rank0": [q for q, _ in shard.neighbours],
+            "halo_bytes_per_apply_rank0": 16 * sum(int(pos.size) for _, pos in shard.neighbours),
+            "cells_rank0": int(sum(len(b.cells) for b in shard.plan.batches)),
+            "partition": "contiguous Morton ranges balanced by (p+1)^3 q^3",
+            "collective": "NCCL send/receive with the neighbouring ranks (ms_per_apply); NCCL all-reduce of every "
+                          "halo slot (allreduce_halo_ms_per_apply)",
+            "max_rel_err_vs_unsharded": max(err, err_ar), "shard_setup_seconds": setup}
 
 
 def main():

@@ -10,10 +10,12 @@ several ranks is shared: the lowest of them owns it, the others hold it as a gho
 reduced vector lists owned dofs first and ghosts after them, so a sum over owned entries (a dot
 product) is a sum over a prefix.
 
-One sharded apply is the local reduced apply followed by the halo sum: each rank packs its
-contributions to the shared dofs into a buffer indexed by global halo slot, the buffers are
-summed over ranks (one all-reduce), and each rank unpacks the sums.  Vectors stay consistent:
-every rank holds the same value of a shared dof.  CG (`solve.jl:376-431`) then needs two more
+One sharded apply is the local reduced apply followed by the halo sum.  With one shard per
+process, each rank sends its contributions to the dofs it shares with a neighbouring rank to
+that rank and receives the neighbour's (point-to-point, `ShardGroup.exchange`), then adds the
+contributions in rank order; otherwise each shard packs its contributions into a buffer indexed
+by global halo slot, the buffers are summed over all shards (one all-reduce), and each shard
+unpacks the sums.  Vectors stay consistent: every rank holds the same value of a shared dof.  CG (`solve.jl:376-431`) then needs two more
 all-reduces per iteration: p.Ap, and (r.r, r.z) together.
 
 `ShardGroup` is the collective: `torch.distributed` across processes (NCCL between GPUs) and,
@@ -107,7 +109,8 @@ class ShardPlan:
     Attributes: `plan` (an AssemblyPlan over the local dofs: apply, rhs and diagonal work on it
     unchanged), `n_owned` (owned reduced dofs: local reduced ids 0..n_owned-1), `global_reduced`
     (global reduced id of every local reduced dof), `halo_local` / `halo_slot` (the local reduced
-    ids of shared dofs and their global halo slots) and `n_halo` (global halo slots)."""
+    ids of shared dofs and their global halo slots), `n_halo` (global halo slots) and
+    `neighbours` (a list of (rank, positions in the halo list of the dofs shared with it))."""
 
     def __init__(self, plan, rank, parts, device=True, cell_rank=None):
         if plan.point_batches:
@@ -123,14 +126,17 @@ class ShardPlan:
         # ranks touching every full dof: how many, and the lowest
         count = np.zeros(plan.n_full, dtype=np.int32)
         first = np.full(plan.n_full, -1, dtype=np.int32)
-        mine = None
+        free = plan.reduced_index >= 0
+        mine = _touched(plan, cr, rank)
+        common = []   # (rank q, full ids of the free dofs both ranks touch, ascending)
         for r in range(parts):
-            t = _touched(plan, cr, r)
+            t = mine if r == rank else _touched(plan, cr, r)
             count += t
             first[(first < 0) & t] = r
-            if r == rank:
-                mine = t
-        free = plan.reduced_index >= 0
+            if r != rank:
+                both = np.nonzero(mine & t & free)[0]
+                if both.size:
+                    common.append((r, both))
         shared = free & (count >= 2)
         halo_global = np.nonzero(shared)[0]                      # full ids, sorted: slot order
         self.n_halo = int(halo_global.size)
@@ -149,6 +155,12 @@ class ShardPlan:
         sh = shared[glob[order]]
         self.halo_local = np.ascontiguousarray(np.nonzero(sh)[0].astype(np.int32))
         self.halo_slot = np.ascontiguousarray(np.searchsorted(halo_global, glob[order][sh]).astype(np.int32))
+        # neighbours: every rank sharing a dof with this one, with the positions of the shared
+        # dofs in this rank's halo list, in ascending global order (the order both sides use)
+        halo_full = glob[order][sh]
+        by_full = np.argsort(halo_full, kind="stable")
+        self.neighbours = [(q, np.ascontiguousarray(by_full[np.searchsorted(halo_full[by_full], ids)].astype(np.int64)))
+                           for q, ids in common]
         # the local plan: same problem and form, local cells and dofs
         lp = object.__new__(AssemblyPlan)
         lp.problem, lp.form, lp.space, lp.D = plan.problem, plan.form, plan.space, plan.D
@@ -188,13 +200,37 @@ class ShardPlan:
 class ShardGroup:
     """Sum over all shards of a job: first over the shards this process holds (a list; one in a
     job with one process per GPU), then across processes with torch.distributed (`group`, or
-    the default group when it is initialised with more than one rank)."""
+    the default group when it is initialised with more than one rank).
 
-    def __init__(self, group=None):
+    `halo`: how a job with one shard per process sums the halo of an apply.  "neighbours"
+    (default): each rank exchanges its contributions with the ranks it shares dofs with
+    (point-to-point, one send and one receive per neighbour) and adds them in rank order;
+    "allreduce": one all-reduce over every halo slot of the job."""
+
+    def __init__(self, group=None, halo="neighbours"):
         import torch.distributed as dist
 
+        if halo not in ("neighbours", "allreduce"):
+            raise ValueError("halo must be 'neighbours' or 'allreduce'")
         self.group = group
+        self.halo = halo
         self.dist = dist if dist.is_available() and dist.is_initialized() and dist.get_world_size(group) > 1 else None
+
+    def peer(self, q):
+        """Global rank of rank q of the group."""
+        return q if self.group is None else self.dist.get_global_rank(self.group, q)
+
+    def exchange(self, sends, recvs):
+        """Point-to-point: sends[k] = (rank, tensor) goes to that rank, recvs[k] = (rank, tensor)
+        is filled from it; returns when all have completed."""
+        d = self.dist
+        ops = []
+        for (q, sb), (q2, rb) in zip(sends, recvs):
+            ops.append(d.P2POp(d.isend, sb, self.peer(q), self.group))
+            ops.append(d.P2POp(d.irecv, rb, self.peer(q2), self.group))
+        if ops:
+            for w in d.batch_isend_irecv(ops):
+                w.wait()
 
     def allreduce(self, views):
         """Sum the same-shaped tensors `views` (one per local shard) over every shard of the job;
@@ -285,11 +321,55 @@ class ShardedOperator:
         self.ops = ops or _DeviceOps()
         o = self.ops
         self._idx = [(o.index(s.halo_local), o.index(s.halo_slot)) for s in self.shards]
-        self._buf = [o.vector(s.n_halo) for s in self.shards]
+        self._nbr = None
+        if self.group.dist is not None and self.group.halo == "neighbours" and len(self.shards) == 1:
+            self._setup_neighbours(o.vector(1).device)
+        else:
+            self._buf = [o.vector(s.n_halo) for s in self.shards]
+
+    def _setup_neighbours(self, device):
+        import torch
+
+        s = self.shards[0]
+        h = int(s.halo_local.size)
+        rows = sorted([s.rank] + [q for q, _ in s.neighbours])
+        self._loc = torch.as_tensor(s.halo_local.astype(np.int64), device=device)
+        self._rows = torch.zeros((len(rows), max(h, 1)), dtype=torch.float64, device=device)
+        self._me = rows.index(s.rank)
+        self._nbr = [(q, rows.index(q), torch.as_tensor(pos, device=device),
+                      torch.zeros(pos.size, dtype=torch.float64, device=device),
+                      torch.zeros(pos.size, dtype=torch.float64, device=device)) for q, pos in s.neighbours]
+        # a first collective over the whole group, so that the point-to-point calls that follow
+        # only ever involve neighbours
+        self.group.dist.all_reduce(torch.zeros(1, dtype=torch.float64, device=device), group=self.group.group)
+
+    def _halo_neighbours(self, y):
+        """Neighbour halo sum: this rank's contributions to its shared dofs go to the ranks that
+        share them, theirs come back into one row per rank, and the rows are added in rank order,
+        so every rank forms the same sum, bit for bit, for a dof it shares."""
+        h = int(self.shards[0].halo_local.size)
+        if h == 0:
+            return
+        rows = self._rows[:, :h]
+        rows.zero_()
+        mine = rows[self._me]
+        mine.copy_(y.index_select(0, self._loc))
+        for _, _, pos, sb, _ in self._nbr:
+            sb.copy_(mine.index_select(0, pos))
+        self.group.exchange([(q, sb) for q, _, _, sb, _ in self._nbr], [(q, rb) for q, _, _, _, rb in self._nbr])
+        for _, row, pos, _, rb in self._nbr:
+            rows[row].index_copy_(0, pos, rb)
+        acc = rows[0].clone()
+        for i in range(1, rows.shape[0]):
+            acc.add_(rows[i])
+        y.index_copy_(0, self._loc, acc)
 
     def halo_sum(self, ys):
         """Sum the shards' contributions to every shared dof; each shard's entries become the sums."""
         o = self.ops
+        if self._nbr is not None:
+            self._halo_neighbours(ys[0])
+            return
         if self.shards[0].n_halo == 0:
             return
         for s, idx, y, buf in zip(self.shards, self._idx, ys, self._buf):

@@ -171,3 +171,63 @@ def test_sharded_plan_rejects_point_items():
     assert plan.point_batches
     with pytest.raises(gb.GricoError):
         ShardPlan(plan, 0, 2, device=False)
+
+
+@pytest.mark.parametrize("D,roots,p,parts", [(2, (4, 4), 3, 4), (3, (2, 2, 2), 2, 3)])
+def test_neighbour_lists_are_symmetric(D, roots, p, parts):
+    """Rank r lists rank q with the dofs they share exactly when q lists r with the same dofs,
+    in the same (ascending global) order; every shared dof of a rank is listed with each other
+    rank that touches it."""
+    plan = _plan(D, roots, p, rounds=1)
+    shards = [ShardPlan(plan, r, parts, device=False) for r in range(parts)]
+    shared = {}
+    for s in shards:
+        g = s.global_reduced[s.halo_local]
+        for q, pos in s.neighbours:
+            assert q != s.rank and np.all(np.diff(g[pos]) > 0)
+            shared[(s.rank, q)] = g[pos]
+        listed = np.concatenate([g[pos] for _, pos in s.neighbours]) if s.neighbours else np.zeros(0)
+        assert set(listed.tolist()) == set(g.tolist())
+    for (r, q), ids in shared.items():
+        assert np.array_equal(shared[(q, r)], ids)
+    assert any(len(s.neighbours) >= 2 for s in shards)
+
+
+def _gloo_halo_rank(rank, world, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        plan = _plan(2, (4, 4), 3, rounds=1, mass=0.5)
+        x = np.random.default_rng(3).standard_normal(plan.n_reduced)
+        shard = ShardPlan(plan, rank, world, device=False)
+        ops = HostOps()
+        for mode in ("neighbours", "allreduce"):
+            op = ShardedOperator([shard], ShardGroup(halo=mode), ops)
+            y = ops.vector(shard.n_reduced)
+            op.apply([ops.upload(shard.scatter(x))], [y])
+            np.save(os.path.join(out, f"y_{mode}{rank}.npy"), y.numpy()[: shard.n_reduced])
+        np.save(os.path.join(out, f"g{rank}.npy"), shard.global_reduced)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_neighbour_halo_exchange_four_gloo_ranks(tmp_path):
+    """world_size 4 over gloo (ranks with two and three neighbours): the point-to-point halo sum
+    gives the unsharded apply, every rank holds the same bits for a dof it shares, and it agrees
+    with the all-reduce halo to rounding."""
+    world = 4
+    mp.start_processes(_gloo_halo_rank, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    plan = _plan(2, (4, 4), 3, rounds=1, mass=0.5)
+    x = np.random.default_rng(3).standard_normal(plan.n_reduced)
+    ref = reduced_apply(plan, x)
+    scale = np.max(np.abs(ref))
+    seen = {}
+    for r in range(world):
+        g = np.load(tmp_path / f"g{r}.npy")
+        yn = np.load(tmp_path / f"y_neighbours{r}.npy")
+        ya = np.load(tmp_path / f"y_allreduce{r}.npy")
+        assert np.max(np.abs(yn - ref[g])) <= 1e-13 * scale
+        assert np.max(np.abs(yn - ya)) <= 1e-14 * scale
+        for gi, v in zip(g.tolist(), yn.tolist()):
+            assert seen.setdefault(gi, v) == v   # bitwise the same on every rank holding it
