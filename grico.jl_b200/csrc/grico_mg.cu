@@ -92,50 +92,61 @@ __global__ void csr_gather(const int64_t* __restrict__ off, const int64_t* __res
 }
 
 // x += w * dinv * (b - ax)
+// The smoothing kernels below read the level's operator product ax once; with `clear` they
+// leave zeros in its place, so the next apply into that buffer need not zero it first.
 template <typename T>
-__global__ void jacobi_smooth(T* __restrict__ x, const T* __restrict__ b, const T* __restrict__ ax,
-                              const T* __restrict__ dinv, T w, int64_t n) {
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+__global__ void jacobi_smooth(T* __restrict__ x, const T* __restrict__ b, T* __restrict__ ax,
+                              const T* __restrict__ dinv, T w, int64_t n, bool clear) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
     x[i] += w * dinv[i] * (b[i] - ax[i]);
+    if (clear) ax[i] = T(0);
+  }
 }
 
 // First smoothing step from x = 0, whose apply is skipped: A 0 = 0, so b - ax is b and the
 // damped-Jacobi step x += w dinv (b - ax) becomes x = w dinv b (the same values, bit for bit)
 template <typename T>
 __global__ void jacobi_from_zero(T* __restrict__ x, const T* __restrict__ b, const T* __restrict__ dinv, T w,
-                                 int64_t n) {
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+                                 T* __restrict__ clear, int64_t n) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
     x[i] = T(0) + w * dinv[i] * b[i];
+    if (clear) clear[i] = T(0);
+  }
 }
 
 // d = c1*d + c2*dinv*(b - ax); x += d
 template <typename T>
 __global__ void chebyshev_step(T* __restrict__ x, T* __restrict__ d, const T* __restrict__ b,
-                               const T* __restrict__ ax, const T* __restrict__ dinv, T c1, T c2, int64_t n) {
+                               T* __restrict__ ax, const T* __restrict__ dinv, T c1, T c2, int64_t n, bool clear) {
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
     // the first step must not read d: fresh device memory may hold NaN bit patterns
     T di = (c1 != T(0) ? c1 * d[i] : T(0)) + c2 * dinv[i] * (b[i] - ax[i]);
     d[i] = di;
     x[i] += di;
+    if (clear) ax[i] = T(0);
   }
 }
 
 // First Chebyshev step from x = 0 (apply skipped, as for jacobi_from_zero): d = x = c2 dinv b
 template <typename T>
 __global__ void chebyshev_from_zero(T* __restrict__ x, T* __restrict__ d, const T* __restrict__ b,
-                                    const T* __restrict__ dinv, T c2, int64_t n) {
+                                    const T* __restrict__ dinv, T c2, T* __restrict__ clear, int64_t n) {
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
     const T di = T(0) + c2 * dinv[i] * b[i];
     d[i] = di;
     x[i] = T(0) + di;
+    if (clear) clear[i] = T(0);
   }
 }
 
-// r = b - ax
+// r = b - ax (ax cleared after the read with `clear`)
 template <typename T>
-__global__ void residual_kernel(T* __restrict__ r, const T* __restrict__ b, const T* __restrict__ ax, int64_t n) {
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+__global__ void residual_kernel(T* __restrict__ r, const T* __restrict__ b, T* __restrict__ ax, int64_t n,
+                                bool clear = false) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
     r[i] = b[i] - ax[i];
+    if (clear) ax[i] = T(0);
+  }
 }
 
 template <typename S, typename D>
@@ -214,17 +225,20 @@ struct LevelBufs<float> {
 };
 
 template <typename T>
-void level_apply(GricoMultigrid* mg, int l, const T* x, T* y, cudaStream_t st) {
-  run_apply<T>(mg->levels[l], true, x, y, 1, st);
+void level_apply(GricoMultigrid* mg, int l, const T* x, T* y, cudaStream_t st, bool y_zero = false) {
+  run_apply<T>(mg->levels[l], true, x, y, 1, st, y_zero);
 }
 
 template <typename T>
 void smooth_gmres(GricoMultigrid* mg, int l, T* x, const T* b, int steps, cudaStream_t st);
 
 // x_zero: x holds no values yet and is taken as zero (Jacobi and Chebyshev only; the caller
-// zeroes x for the GMRES smoother), so the first step skips its apply of x
+// zeroes x for the GMRES smoother), so the first step skips its apply of x.
+// t_zero (optional): whether the level's product buffer t holds zeros, kept up to date; the
+// Jacobi and Chebyshev steps then clear t as they read it, and the next apply skips zeroing it.
 template <typename T>
-void smooth(GricoMultigrid* mg, int l, T* x, const T* b, int steps, cudaStream_t st, bool x_zero = false) {
+void smooth(GricoMultigrid* mg, int l, T* x, const T* b, int steps, cudaStream_t st, bool x_zero = false,
+            bool* t_zero = nullptr) {
   using B = LevelBufs<T>;
   const int64_t n = mg->levels[l]->n_red;
   T* t = B::t(mg, l);
@@ -232,16 +246,24 @@ void smooth(GricoMultigrid* mg, int l, T* x, const T* b, int steps, cudaStream_t
   if (steps <= 0) return;
   if (mg->opts.smoother == GRICO_SMOOTHER_GMRES) {
     smooth_gmres<T>(mg, l, x, b, steps, st);
+    if (t_zero) *t_zero = false;
     return;
   }
+  const bool clear = t_zero != nullptr;
+  auto apply_t = [&]() {
+    level_apply<T>(mg, l, x, t, st, clear && *t_zero);
+    if (clear) *t_zero = false;
+  };
   if (mg->opts.smoother == GRICO_SMOOTHER_JACOBI) {
     for (int s = 0; s < steps; ++s) {
       if (s == 0 && x_zero) {
-        jacobi_from_zero<T><<<blocks(n), 256, 0, st>>>(x, b, dinv, T(mg->opts.jacobi_omega), n);
-        continue;
+        jacobi_from_zero<T><<<blocks(n), 256, 0, st>>>(x, b, dinv, T(mg->opts.jacobi_omega),
+                                                       clear && !*t_zero ? t : nullptr, n);
+      } else {
+        apply_t();
+        jacobi_smooth<T><<<blocks(n), 256, 0, st>>>(x, b, t, dinv, T(mg->opts.jacobi_omega), n, clear);
       }
-      level_apply<T>(mg, l, x, t, st);
-      jacobi_smooth<T><<<blocks(n), 256, 0, st>>>(x, b, t, dinv, T(mg->opts.jacobi_omega), n);
+      if (clear) *t_zero = true;
     }
     return;
   }
@@ -254,17 +276,21 @@ void smooth(GricoMultigrid* mg, int l, T* x, const T* b, int steps, cudaStream_t
     double rho_old = 1.0 / sigma;
     for (int k = 0; k < mg->opts.chebyshev_degree; ++k) {
       if (s == 0 && k == 0 && x_zero) {
-        chebyshev_from_zero<T><<<blocks(n), 256, 0, st>>>(x, d, b, dinv, T(1.0 / theta), n);
+        chebyshev_from_zero<T><<<blocks(n), 256, 0, st>>>(x, d, b, dinv, T(1.0 / theta),
+                                                          clear && !*t_zero ? t : nullptr, n);
+        if (clear) *t_zero = true;
         continue;
       }
-      level_apply<T>(mg, l, x, t, st);
+      apply_t();
       if (k == 0) {
-        chebyshev_step<T><<<blocks(n), 256, 0, st>>>(x, d, b, t, dinv, T(0), T(1.0 / theta), n);
+        chebyshev_step<T><<<blocks(n), 256, 0, st>>>(x, d, b, t, dinv, T(0), T(1.0 / theta), n, clear);
       } else {
         const double rho = 1.0 / (2.0 * sigma - rho_old);
-        chebyshev_step<T><<<blocks(n), 256, 0, st>>>(x, d, b, t, dinv, T(rho * rho_old), T(2.0 * rho / delta), n);
+        chebyshev_step<T><<<blocks(n), 256, 0, st>>>(x, d, b, t, dinv, T(rho * rho_old), T(2.0 * rho / delta), n,
+                                                     clear);
         rho_old = rho;
       }
+      if (clear) *t_zero = true;
     }
   }
 }
@@ -533,19 +559,26 @@ void vcycle(GricoMultigrid* mg, int l, T* x, const T* b, cudaStream_t st) {
   // applying the operator to a zeroed vector
   const bool from_zero = pre > 0 && mg->opts.smoother != GRICO_SMOOTHER_GMRES;
   if (!from_zero) cudaMemsetAsync(x, 0, sizeof(T) * n, st);
-  smooth<T>(mg, l, x, b, pre, st, from_zero);
-  if (learned) learned_sweep<T>(mg, l, x, b, st);
+  // t (the level's product buffer) is cleared by the passes that read it, from the first
+  // smoothing step on, so the applies of this level skip zeroing it
+  bool t_zero = false;
+  smooth<T>(mg, l, x, b, pre, st, from_zero, &t_zero);
+  if (learned) {
+    learned_sweep<T>(mg, l, x, b, st);
+    t_zero = false;
+  }
   T* t = B::t(mg, l);
   T* r = B::r(mg, l);
-  level_apply<T>(mg, l, x, t, st);
-  residual_kernel<T><<<blocks(n), 256, 0, st>>>(r, b, t, n);
+  level_apply<T>(mg, l, x, t, st, t_zero);
+  residual_kernel<T><<<blocks(n), 256, 0, st>>>(r, b, t, n, true);
+  t_zero = true;
   auto& X = mg->xfer[l - 1];
   T* bc = B::b(mg, l - 1);
   T* xc = B::x(mg, l - 1);
   csr_gather<T><<<blocks(X.nc), 256, 0, st>>>(X.r_off.get<int64_t>(), X.r_idx.get<int64_t>(), B::rval(X), r, bc, X.nc, 0);
   vcycle<T>(mg, l - 1, xc, bc, st);
   csr_gather<T><<<blocks(X.nf), 256, 0, st>>>(X.p_off.get<int64_t>(), X.p_idx.get<int64_t>(), B::pval(X), xc, x, X.nf, 1);
-  smooth<T>(mg, l, x, b, mg->opts.post_steps, st);
+  smooth<T>(mg, l, x, b, mg->opts.post_steps, st, false, &t_zero);
 }
 
 }  // namespace

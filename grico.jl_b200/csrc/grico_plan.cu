@@ -863,12 +863,12 @@ void accumulate_hanging_diagonal(const GricoPlanDesc& d, const GricoCellBatchDes
 }
 
 template <typename T>
-int run_apply(GricoPlan* P, bool reduced, const T* x, T* y, int nrhs, cudaStream_t st) {
+int run_apply(GricoPlan* P, bool reduced, const T* x, T* y, int nrhs, cudaStream_t st, bool y_zero) {
   const int64_t n = reduced ? P->n_red : P->n_full;
   if (nrhs < 1) return GRICO_ERR_INVALID;
   // the final check covers this call's launches only, not an error an earlier call left pending
   (void)cudaGetLastError();
-  cudaMemsetAsync(y, 0, sizeof(T) * n * nrhs, st);
+  if (!y_zero) cudaMemsetAsync(y, 0, sizeof(T) * n * nrhs, st);
   // the buffered tails of all batches: one gather pass before the cell kernels
   const GricoPlan::TailAll& TA = P->tails[reduced ? 1 : 0];
   const bool merged = TA.n_tail > 0 && nrhs <= kTailRhs;
@@ -942,8 +942,8 @@ int run_apply(GricoPlan* P, bool reduced, const T* x, T* y, int nrhs, cudaStream
   return cuda_ok(cudaGetLastError(), "apply launch") ? GRICO_OK : GRICO_ERR_CUDA;
 }
 
-template int run_apply<double>(GricoPlan*, bool, const double*, double*, int, cudaStream_t);
-template int run_apply<float>(GricoPlan*, bool, const float*, float*, int, cudaStream_t);
+template int run_apply<double>(GricoPlan*, bool, const double*, double*, int, cudaStream_t, bool);
+template int run_apply<float>(GricoPlan*, bool, const float*, float*, int, cudaStream_t, bool);
 
 namespace {
 

@@ -199,8 +199,10 @@ struct GricoPlan {
 };
 
 namespace grico {
+// y_zero: y already holds zeros (the caller cleared it in its last pass over it), so the apply
+// skips zeroing it
 template <typename T>
-int run_apply(GricoPlan* P, bool reduced, const T* x, T* y, int nrhs, cudaStream_t st);
+int run_apply(GricoPlan* P, bool reduced, const T* x, T* y, int nrhs, cudaStream_t st, bool y_zero = false);
 int reduced_diag_device(GricoPlan* P, double* diag, cudaStream_t st);
 int grid_blocks(int64_t n);
 }  // namespace grico
