@@ -433,14 +433,16 @@ def batched_legs(gb, L, max_level=7, nrhs=32, rtol=1e-10):
            "batches": [[int(b.degree[0]), len(b.cells)] for b in plan.batches], "nrhs": nrhs, "rtol": rtol,
            "host_setup_seconds": setup, "tiles": tiles,
            "single_cg_fp64": {"seconds": single_s, "iterations_max": max(single_it)}}
-    # three repeats of each lockstep solve (the first also captures the iteration graph): the
-    # median is the leg's time, all repeats are reported
+    # three repeats of each lockstep solve (each captures its iteration graph; the first call on
+    # the plan also allocates the solver's work buffers): the median is the leg's time, all
+    # repeats are reported with their iteration counts
     for name, mixed in (("lockstep_cg_fp64", False), ("lockstep_cg_fp32_in_fp64_refinement", True)):
-        times = []
+        times, its = [], []
         for _ in range(3):
             X, reps = bt.solve_many(plan, B, relative_tolerance=rtol, mixed=mixed)
             times.append(float(reps[0].seconds))
-        out[name] = {"seconds": float(np.median(times)), "repeats_seconds": times,
+            its.append(int(max(r.iterations for r in reps)))
+        out[name] = {"seconds": float(np.median(times)), "repeats_seconds": times, "repeats_iterations_max": its,
                      "iterations_max": max(r.iterations for r in reps),
                      "status": sorted({int(r.status) for r in reps})}
     # operator throughput, 1 vs nrhs right-hand sides (FP64 and FP32)

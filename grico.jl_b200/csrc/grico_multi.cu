@@ -153,6 +153,17 @@ struct MultiResult {
   std::vector<double> rr;
 };
 
+// Work buffer `slot` of the plan's lockstep solver, `count` elements of T: kept on the plan and
+// reallocated only to grow, so repeated solves on a plan allocate nothing (nullptr on failure).
+// Slots 0-9: multi_cg; 10-18: grico_cg_solve_multi.
+template <typename T>
+T* solver_ws(GricoPlan* P, int slot, int64_t count) {
+  DevBuf& b = P->solver_ws[slot];
+  const size_t bytes = sizeof(T) * size_t(std::max<int64_t>(count, 1));
+  if ((b.bytes < bytes || !b.ptr) && !b.alloc(bytes)) return nullptr;
+  return b.get<T>();
+}
+
 // Lockstep preconditioned CG on nrhs stacked systems A x_s = b_s from x_s = 0, stopping
 // system s once ||r_s||^2 <= tol2[s].
 template <typename T>
@@ -160,20 +171,18 @@ int multi_cg(GricoPlan* P, const T* b, T* x, int nrhs, const std::vector<double>
              bool graph, cudaStream_t st, MultiResult& res) {
   const int64_t n = P->n_red;
   const int64_t nn = n * nrhs;
-  DevBuf rb, zb, pb, qb, sc, part, act, tolb, itb, stb;
-  if (!rb.alloc(sizeof(T) * nn) || !zb.alloc(sizeof(T) * nn) || !pb.alloc(sizeof(T) * nn) || !qb.alloc(sizeof(T) * nn) ||
-      !sc.alloc(sizeof(double) * 5 * nrhs) || !part.alloc(sizeof(double) * nrhs * kMultiBlocks) ||
-      !act.alloc(sizeof(int) * nrhs) || !tolb.alloc(sizeof(double) * nrhs) || !itb.alloc(sizeof(int) * nrhs) ||
-      !stb.alloc(sizeof(int) * nrhs))
-    return GRICO_ERR_CUDA;
-  T *r = rb.get<T>(), *z = zb.get<T>(), *p = pb.get<T>(), *q = qb.get<T>();
-  double* rz = sc.get<double>();
+  T *r = solver_ws<T>(P, 0, nn), *z = solver_ws<T>(P, 1, nn), *p = solver_ws<T>(P, 2, nn), *q = solver_ws<T>(P, 3, nn);
+  double* rz = solver_ws<double>(P, 4, 5 * int64_t(nrhs));
+  double* partial = solver_ws<double>(P, 5, int64_t(nrhs) * kMultiBlocks);
+  int* active = solver_ws<int>(P, 6, nrhs);
+  double* tolb = solver_ws<double>(P, 7, nrhs);
+  int* d_iters = solver_ws<int>(P, 8, nrhs);
+  int* d_status = solver_ws<int>(P, 9, nrhs);
+  if (!r || !z || !p || !q || !rz || !partial || !active || !tolb || !d_iters || !d_status) return GRICO_ERR_CUDA;
   double* rz_new = rz + nrhs;
   double* pap = rz + 2 * nrhs;
   double* rr = rz + 3 * nrhs;
   double* last_rr = rz + 4 * nrhs;
-  double* partial = part.get<double>();
-  int* active = act.get<int>();
   const dim3 vg(gblocks(n), nrhs);
   auto dot = [&](const T* a, const T* c, double* out, cudaStream_t s) {
     multi_dot<T><<<dim3(kMultiBlocks, nrhs), 256, 0, s>>>(a, c, nullptr, n, partial);
@@ -199,9 +208,7 @@ int multi_cg(GricoPlan* P, const T* b, T* x, int nrhs, const std::vector<double>
     n_active += ha[s];
   }
   cudaMemcpyAsync(active, ha.data(), sizeof(int) * nrhs, cudaMemcpyHostToDevice, st);
-  int* d_iters = itb.get<int>();
-  int* d_status = stb.get<int>();
-  cudaMemcpyAsync(tolb.ptr, tol2.data(), sizeof(double) * nrhs, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(tolb, tol2.data(), sizeof(double) * nrhs, cudaMemcpyHostToDevice, st);
   cudaMemsetAsync(d_iters, 0, sizeof(int) * nrhs, st);
   cudaMemsetAsync(d_status, 0, sizeof(int) * nrhs, st);  // GRICO_OK
   auto iteration = [&](cudaStream_t s) -> int {
@@ -214,7 +221,7 @@ int multi_cg(GricoPlan* P, const T* b, T* x, int nrhs, const std::vector<double>
     dot(r, z, rz_new, s);
     multi_direction<T><<<vg, 256, 0, s>>>(p, z, rz_new, rz, active, n);
     copy_scalars<<<1, 64, 0, s>>>(rz, rz_new, active, nrhs);
-    multi_check<<<(nrhs + 63) / 64, 64, 0, s>>>(pap, rr, tolb.get<double>(), active, d_iters, d_status, last_rr,
+    multi_check<<<(nrhs + 63) / 64, 64, 0, s>>>(pap, rr, tolb, active, d_iters, d_status, last_rr,
                                                  nrhs);
     return GRICO_OK;
   };
@@ -291,15 +298,14 @@ extern "C" int grico_cg_solve_multi(GricoPlan* P, const double* B, double* X, in
   const int64_t nn = n * nrhs;
   const bool graph = !(flags & GRICO_FLAG_NO_GRAPH);
   const bool mixed = (flags & GRICO_FLAG_MIXED) != 0;
-  DevBuf bb, xb, dinv32;
   const double* bd = B;
   double* xd = X;
   if (flags & GRICO_FLAG_HOST_POINTERS) {
-    if (!bb.alloc(sizeof(double) * std::max<int64_t>(nn, 1)) || !xb.alloc(sizeof(double) * std::max<int64_t>(nn, 1)))
-      return GRICO_ERR_CUDA;
-    cudaMemcpyAsync(bb.ptr, B, sizeof(double) * nn, cudaMemcpyHostToDevice, st);
-    bd = bb.get<double>();
-    xd = xb.get<double>();
+    double* bs = solver_ws<double>(P, 10, nn);
+    xd = solver_ws<double>(P, 11, nn);
+    if (!bs || !xd) return GRICO_ERR_CUDA;
+    cudaMemcpyAsync(bs, B, sizeof(double) * nn, cudaMemcpyHostToDevice, st);
+    bd = bs;
   }
   const double* dinv = nullptr;
   if (opts->preconditioner == GRICO_PRECOND_JACOBI) {
@@ -307,12 +313,13 @@ extern "C" int grico_cg_solve_multi(GricoPlan* P, const double* B, double* X, in
     dinv = P->w_dinv.get<double>();
   }
   // tolerances from ||b_s||
-  DevBuf part, bn;
-  if (!part.alloc(sizeof(double) * nrhs * kMultiBlocks) || !bn.alloc(sizeof(double) * nrhs)) return GRICO_ERR_CUDA;
-  multi_dot<double><<<dim3(kMultiBlocks, nrhs), 256, 0, st>>>(bd, bd, nullptr, n, part.get<double>());
-  multi_reduce<<<nrhs, 256, 0, st>>>(part.get<double>(), kMultiBlocks, bn.get<double>());
+  double* part = solver_ws<double>(P, 12, int64_t(nrhs) * kMultiBlocks);
+  double* bn = solver_ws<double>(P, 13, nrhs);
+  if (!part || !bn) return GRICO_ERR_CUDA;
+  multi_dot<double><<<dim3(kMultiBlocks, nrhs), 256, 0, st>>>(bd, bd, nullptr, n, part);
+  multi_reduce<<<nrhs, 256, 0, st>>>(part, kMultiBlocks, bn);
   std::vector<double> bnorm2(nrhs), tol2(nrhs);
-  cudaMemcpyAsync(bnorm2.data(), bn.ptr, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(bnorm2.data(), bn, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st);
   cudaStreamSynchronize(st);
   for (int s = 0; s < nrhs; ++s) {
     const double t = std::max(opts->absolute_tolerance, opts->relative_tolerance * std::sqrt(bnorm2[s]));
@@ -334,19 +341,20 @@ extern "C" int grico_cg_solve_multi(GricoPlan* P, const double* B, double* X, in
   } else {
     // FP64 iterative refinement: r = b - A x in FP64, FP32 inner CG on A e = r to 1e-4
     // relative, x += e; repeat until every system meets its FP64 tolerance.
-    DevBuf r64, r32, e32;
-    if (!r64.alloc(sizeof(double) * nn) || !r32.alloc(sizeof(float) * nn) || !e32.alloc(sizeof(float) * nn) ||
-        (dinv && !dinv32.alloc(sizeof(float) * n)))
-      return GRICO_ERR_CUDA;
-    if (dinv) cast_copy<double, float><<<gblocks(n), 256, 0, st>>>(dinv, dinv32.get<float>(), n);
+    double* r64 = solver_ws<double>(P, 14, nn);
+    float* r32 = solver_ws<float>(P, 15, nn);
+    float* e32 = solver_ws<float>(P, 16, nn);
+    double* ax = solver_ws<double>(P, 17, nn);
+    float* dinv32 = dinv ? solver_ws<float>(P, 18, n) : nullptr;
+    if (!r64 || !r32 || !e32 || !ax || (dinv && !dinv32)) return GRICO_ERR_CUDA;
+    if (dinv) cast_copy<double, float><<<gblocks(n), 256, 0, st>>>(dinv, dinv32, n);
     cudaMemsetAsync(xd, 0, sizeof(double) * nn, st);
-    cudaMemcpyAsync(r64.ptr, bd, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(r64, bd, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st);
     std::vector<int> done(nrhs, 0);
     for (int outer = 0; outer < 60; ++outer) {
-      multi_dot<double><<<dim3(kMultiBlocks, nrhs), 256, 0, st>>>(r64.get<double>(), r64.get<double>(), nullptr, n,
-                                                                  part.get<double>());
-      multi_reduce<<<nrhs, 256, 0, st>>>(part.get<double>(), kMultiBlocks, bn.get<double>());
-      cudaMemcpyAsync(final_rr.data(), bn.ptr, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st);
+      multi_dot<double><<<dim3(kMultiBlocks, nrhs), 256, 0, st>>>(r64, r64, nullptr, n, part);
+      multi_reduce<<<nrhs, 256, 0, st>>>(part, kMultiBlocks, bn);
+      cudaMemcpyAsync(final_rr.data(), bn, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st);
       cudaStreamSynchronize(st);
       bool all = true;
       std::vector<double> inner_tol2(nrhs);
@@ -360,8 +368,8 @@ extern "C" int grico_cg_solve_multi(GricoPlan* P, const double* B, double* X, in
       bool over = false;
       for (int s = 0; s < nrhs; ++s) over = over || (!done[s] && total[s] >= opts->maxiter);
       if (over) break;
-      cast_copy<double, float><<<gblocks(nn), 256, 0, st>>>(r64.get<double>(), r32.get<float>(), nn);
-      rc = multi_cg<float>(P, r32.get<float>(), e32.get<float>(), nrhs, inner_tol2, opts->maxiter, dinv32.get<float>(),
+      cast_copy<double, float><<<gblocks(nn), 256, 0, st>>>(r64, r32, nn);
+      rc = multi_cg<float>(P, r32, e32, nrhs, inner_tol2, opts->maxiter, dinv32,
                            graph, st, res);
       if (rc) break;
       for (int s = 0; s < nrhs; ++s) {
@@ -369,12 +377,10 @@ extern "C" int grico_cg_solve_multi(GricoPlan* P, const double* B, double* X, in
         total[s] += res.iters[s];
         if (res.status[s] != GRICO_OK && res.status[s] != GRICO_ERR_NOT_CONVERGED) status[s] = res.status[s];
       }
-      cast_add<float, double><<<gblocks(nn), 256, 0, st>>>(e32.get<float>(), xd, nn);
-      cudaMemcpyAsync(r64.ptr, bd, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st);
-      DevBuf ax;
-      if (!ax.alloc(sizeof(double) * nn)) return GRICO_ERR_CUDA;
-      run_apply<double>(P, true, xd, ax.get<double>(), nrhs, st);
-      axpby_kernel<double><<<grid_blocks(nn), 256, 0, st>>>(-1.0, ax.get<double>(), 1.0, r64.get<double>(), nn);
+      cast_add<float, double><<<gblocks(nn), 256, 0, st>>>(e32, xd, nn);
+      cudaMemcpyAsync(r64, bd, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st);
+      run_apply<double>(P, true, xd, ax, nrhs, st);
+      axpby_kernel<double><<<grid_blocks(nn), 256, 0, st>>>(-1.0, ax, 1.0, r64, nn);
     }
     for (int s = 0; s < nrhs; ++s)
       if (status[s] == GRICO_OK && final_rr[s] > tol2[s]) status[s] = GRICO_ERR_NOT_CONVERGED;

@@ -190,6 +190,10 @@ struct GricoPlan {
   // joined back to the launching stream (the scatter is atomic, so their order is free); made
   // when the plan has more than one batch; eight, so that each batch of an hp mesh (up to
   // eight degrees) with its tail passes forms its own chain
+  // work buffers of the lockstep solver (grico_cg_solve_multi), kept across calls and grown on
+  // demand; calls on one plan share them, as they share its tail buffers and streams
+  static constexpr int kSolverWs = 20;
+  grico::DevBuf solver_ws[kSolverWs];
   static constexpr int kBranches = 8;
   int n_branches = 0;
   cudaStream_t branch[kBranches] = {};

@@ -357,7 +357,9 @@ int grico_cg_solve(GricoPlan* plan, GricoMultigrid* mg, const double* b, double*
  * for all systems per iteration, identity or Jacobi preconditioning, each with the reference's
  * stopping rule; with GRICO_FLAG_MIXED the CG runs in FP32 inside FP64 iterative refinement
  * (FP64 residuals and updates).  reports: [nrhs] or NULL.  No reference counterpart for the
- * batching. */
+ * batching.  Its work vectors (about 4 + 5 per system of n_reduced values, FP32 and FP64) stay
+ * on the plan for the next call until grico_plan_destroy, so repeated solves allocate nothing;
+ * concurrent calls on one plan share them. */
 int grico_cg_solve_multi(GricoPlan* plan, const double* B, double* X, int nrhs, const GricoSolveOptions* opts,
                          GricoSolveReport* reports, int flags);
 
