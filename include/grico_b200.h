@@ -281,14 +281,12 @@ int grico_rhs(GricoPlan* plan, const double* const* source_points, double* b_ful
  * TestChannels(eta*g, -g*n)); NULL => 0 — assembly.jl:917-933. */
 int grico_reduced_rhs(GricoPlan* plan, const double* const* source_points, double* b_reduced, int flags);
 /* Allocation-free variant of grico_reduced_rhs for callers that cannot allocate GPU memory
- * (code running while a stream is captured into a CUDA graph, host callbacks, services with a
- * fixed GPU memory budget).  No counterpart in the reference.  Its two full-layout temporaries
+ * (host callbacks, services with a fixed GPU memory budget).  No counterpart in the reference.  Its two full-layout temporaries
  * live in a static 16 MiB device array that every GPU loading the library holds until exit, so
  * plans with more than 1,048,576 full-layout dofs are rejected with GRICO_ERR_INVALID.
  * source_points[b] and b_reduced are DEVICE pointers; the work is enqueued on `stream`
  * (NULL = the plan's stream) and the call does not synchronise.  The first call on a device
- * resolves the array's device address (cudaGetSymbolAddress), so make that first call before
- * any stream capture.  All calls share the array: calls whose GPU work overlaps in time (other
+ * resolves the array's device address (cudaGetSymbolAddress).  All calls share the array: calls whose GPU work overlaps in time (other
  * streams, other threads) race on it. */
 int grico_reduced_rhs_static(GricoPlan* plan, const double* const* source_points, double* b_reduced,
                              void* stream);

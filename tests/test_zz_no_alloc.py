@@ -1,9 +1,9 @@
 """grico_reduced_rhs_static: the reduced right-hand side without any GPU allocation.
 
-It exists for callers that cannot allocate GPU memory during the call (work being captured
-into a CUDA graph, host callbacks, services with a fixed memory budget); its temporaries live
-in a static device array instead.  Checked through the C ABI against grico_reduced_rhs on two
-calls in a row, and the size limit is checked.  This file is collected last on purpose."""
+It exists for callers that cannot allocate GPU memory during the call (host callbacks,
+services with a fixed memory budget); its temporaries live in a static device array instead.
+Checked through the C ABI against grico_reduced_rhs on two calls in a row, and the size limit
+is checked.  This file is collected last on purpose."""
 import ctypes as C
 
 import numpy as np
