@@ -778,6 +778,8 @@ def main():
                              "lshape_hp32", "lshape_apply32", "conv_tc", "sipg3d", "dense_tc64"],
                     help="poisson64: 3-D Poisson 64^3 p=4 (default); fcm_shell*: finite-cell shell with Nitsche")
     ap.add_argument("--fp32", action="store_true", help="time the FP32 apply instead of FP64")
+    ap.add_argument("--train-fields", type=int, default=6, help="grf_learned*: training fields (32^3 cells each)")
+    ap.add_argument("--train-steps", type=int, default=200, help="grf_learned*: Adam steps")
     ap.add_argument("--no-configs", action="store_true", help="skip the other benchmark configurations")
     ap.add_argument("--configs", default="", help="comma-separated config legs to run (c1_poisson2d_32_p4, "
                     "c3_lshape_hp32, c4_grf_learned64, c5_fcm_shell64); default: all")
@@ -910,7 +912,8 @@ def main():
                               "batched": out}), flush=True)
         return
     if args.workload.startswith("grf_learned"):
-        out = learned_legs(gb, L, refine=7 if args.workload.endswith("128") else 6)
+        out = learned_legs(gb, L, refine=7 if args.workload.endswith("128") else 6, train_fields=args.train_fields,
+                           train_steps=args.train_steps)
         leg = out["legs"]
         value = leg["learned+mixed_fp32_vcycle"]["time_to_target_seconds"]
         if rank == 0:
