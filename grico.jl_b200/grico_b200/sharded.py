@@ -222,12 +222,11 @@ class ShardGroup:
 
     def exchange(self, sends, recvs):
         """Point-to-point: sends[k] = (rank, tensor) goes to that rank, recvs[k] = (rank, tensor)
-        is filled from it; returns when all have completed."""
+        is filled from it (the two lists may name different ranks); returns when all have
+        completed.  Every pair of ranks must agree on what it exchanges."""
         d = self.dist
-        ops = []
-        for (q, sb), (q2, rb) in zip(sends, recvs):
-            ops.append(d.P2POp(d.isend, sb, self.peer(q), self.group))
-            ops.append(d.P2POp(d.irecv, rb, self.peer(q2), self.group))
+        ops = [d.P2POp(d.isend, sb, self.peer(q), self.group) for q, sb in sends]
+        ops += [d.P2POp(d.irecv, rb, self.peer(q), self.group) for q, rb in recvs]
         if ops:
             for w in d.batch_isend_irecv(ops):
                 w.wait()
@@ -488,6 +487,123 @@ def sharded_cg(op, bs, relative_tolerance=None, absolute_tolerance=0.0, maxiter=
     return xs, ShardedReport(it, status, init, math.sqrt(rr) if math.isfinite(rr) else rr)
 
 
+def _csr_take(off, rows):
+    """Entry positions of the CSR rows `rows`, row by row."""
+    rows = np.asarray(rows, dtype=np.int64)
+    cnt = off[rows + 1] - off[rows]
+    if cnt.sum() == 0:
+        return np.zeros(0, dtype=np.int64)
+    return np.repeat(off[rows] - (np.cumsum(cnt) - cnt), cnt) + np.arange(int(cnt.sum()), dtype=np.int64)
+
+
+def _reduced_sets(plan, cell_rank, parts):
+    """Per rank, the sorted global reduced ids of the free dofs its cells touch (a rank's local
+    reduced dofs), and per reduced dof the lowest rank holding it (its owner)."""
+    sets = []
+    for r in range(parts):
+        g = plan.reduced_index[np.nonzero(_touched(plan, cell_rank, r))[0]]
+        sets.append(np.unique(g[g >= 0]).astype(np.int64))
+    owner = np.full(plan.n_reduced, parts, dtype=np.int64)
+    for r in reversed(range(parts)):
+        owner[sets[r]] = r
+    return sets, owner
+
+
+class _TransferLinks:
+    """Point-to-point restriction and prolongation between a sharded coarse level and the fine
+    level above it, for rank `me`; every list is computed from the global hierarchy on every
+    rank, so both ends of a send agree on it.
+
+    Restriction: this rank sums P^T over its owned fine rows into the coarse dofs they reach
+    (`cols_own`, sorted global ids), keeps the entries it holds and sends the others' share to
+    each rank holding them; every holder adds the contributions in rank order.  Prolongation:
+    the coarse values this rank's fine rows need but it does not hold come from their owners."""
+
+    def __init__(self, me, parts, off, col, coarse_sets, coarse_owner, fine_sets, fine_owner, coarse_local, device):
+        import torch
+
+        self.me = me
+        nc = coarse_owner.size
+        holds = []
+        for r in range(parts):
+            m = np.zeros(nc, dtype=bool)
+            m[coarse_sets[r]] = True
+            holds.append(m)
+        lpos = np.full(nc, -1, dtype=np.int64)
+        lpos[coarse_local] = np.arange(coarse_local.size)
+        cols = [np.unique(col[_csr_take(off, np.nonzero(fine_owner == r)[0])]) for r in range(parts)]
+        need = [np.unique(col[_csr_take(off, fine_sets[r])]) for r in range(parts)]
+        own = cols[me]
+        self.cols_own = own
+        t = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.int64), device=device)
+        f = lambda n: torch.zeros(int(n), dtype=torch.float64, device=device)
+        # restriction
+        mine = holds[me][own]
+        self.r_keep = (t(np.nonzero(mine)[0]), t(lpos[own[mine]]))
+        self.r_send = []
+        for q in range(parts):
+            if q != me:
+                sel = np.nonzero(holds[q][own])[0]
+                if sel.size:
+                    self.r_send.append((q, t(sel), f(sel.size)))
+        self.r_recv = []
+        for q in range(parts):
+            if q != me:
+                ids = cols[q][holds[me][cols[q]]]
+                if ids.size:
+                    self.r_recv.append((q, t(lpos[ids]), f(ids.size)))
+        rows = sorted({me} | {q for q, _, _ in self.r_recv})
+        self.r_rows = f(len(rows) * max(coarse_local.size, 1)).reshape(len(rows), -1)
+        self.r_me = rows.index(me)
+        self.r_row = {q: rows.index(q) for q, _, _ in self.r_recv}
+        # prolongation
+        nd = need[me]
+        here = holds[me][nd]
+        self.need = nd
+        self.p_here = (t(np.nonzero(here)[0]), t(lpos[nd[here]]))
+        self.p_recv = []
+        miss = nd[~here]
+        for q in range(parts):
+            ids = miss[coarse_owner[miss] == q]
+            if q != me and ids.size:
+                self.p_recv.append((q, t(np.searchsorted(nd, ids)), f(ids.size)))
+        self.p_send = []
+        for q in range(parts):
+            if q != me:
+                mq = need[q][~holds[q][need[q]]]
+                ids = mq[coarse_owner[mq] == me]
+                if ids.size:
+                    self.p_send.append((q, t(lpos[ids]), f(ids.size)))
+
+    def restrict(self, group, partial, n_local):
+        """Local coarse right-hand side from this rank's partial sums over `cols_own`."""
+        rows = self.r_rows[:, : max(n_local, 1)]
+        rows.zero_()
+        sel, pos = self.r_keep
+        rows[self.r_me].index_copy_(0, pos, partial.index_select(0, sel))
+        for _, sel, sb in self.r_send:
+            sb.copy_(partial.index_select(0, sel))
+        group.exchange([(q, sb) for q, _, sb in self.r_send], [(q, rb) for q, _, rb in self.r_recv])
+        for q, pos, rb in self.r_recv:
+            rows[self.r_row[q]].index_copy_(0, pos, rb)
+        acc = rows[0].clone()
+        for i in range(1, rows.shape[0]):
+            acc.add_(rows[i])
+        return acc
+
+    def needed_values(self, group, xc, out):
+        """out[k] = the coarse value of global id need[k], from xc (local coarse vector) and the
+        owners of the ones this rank does not hold."""
+        k, pos = self.p_here
+        out.index_copy_(0, k, xc.index_select(0, pos))
+        for _, pos, sb in self.p_send:
+            sb.copy_(xc.index_select(0, pos))
+        group.exchange([(q, sb) for q, _, sb in self.p_send], [(q, rb) for q, _, rb in self.p_recv])
+        for _, k, rb in self.p_recv:
+            out.index_copy_(0, k, rb)
+        return out
+
+
 def gather_reduced(shards, xs, n_reduced, ops=None):
     """Global reduced vector from the owned entries of the shards (host arrays; for one process
     holding every shard, or rank 0 after gathering)."""
@@ -505,11 +621,14 @@ class ShardedMultigrid:
 
     Every level of the hierarchy (`build_hierarchy`: the same h/p coarsening as the one-GPU
     V-cycle) is split over the ranks by its own Morton ranges (`ShardPlan`, one shard per
-    process), so a level apply is the sharded apply with its halo sum.  The transfers between
-    levels use global vectors: restriction sums P^T over each rank's owned fine rows into a
-    global coarse vector (one all-reduce of the coarse length), prolongation gathers the coarse
-    correction from the owned entries of all ranks (one all-reduce) and applies the rows of P of
-    the rank's fine dofs.  The coarsest level is solved redundantly on every rank from the same
+    process), so a level apply is the sharded apply with its halo sum.  Transfers between
+    levels, in a job of several processes with neighbour halos: restriction sums P^T over each
+    rank's owned fine rows and sends each rank holding a reached coarse dof its share, the
+    holders adding the shares in rank order; prolongation fetches the coarse values a rank's fine
+    rows need but it does not hold from their owners, then applies the rank's rows of P
+    (`_TransferLinks`, all point to point).  Otherwise they use global vectors: restriction into
+    a global coarse vector (one all-reduce of the coarse length), prolongation from the owned
+    entries of all ranks (one all-reduce).  The coarsest level is solved redundantly on every rank from the same
     gathered right-hand side (Cholesky of the coarse matrix, assembled at set-up from sharded
     applies of unit vectors).  Vectors stay consistent on shared dofs throughout, so the
     V-cycle is that of the unsharded hierarchy up to the order of floating-point sums."""
@@ -544,6 +663,24 @@ class ShardedMultigrid:
             loc = np.repeat(np.arange(rows.size, dtype=np.int64), cnt)
             self._P.append((torch.as_tensor(loc, device=dev), torch.as_tensor(col[take].astype(np.int64), device=dev),
                             torch.as_tensor(val[take].astype(np.float64), device=dev)))
+        # with one shard per process and neighbour halos, the transfers exchange only the coarse
+        # entries a rank's rows reach or need, point to point (`_TransferLinks`); otherwise they
+        # go through global coarse vectors and all-reduces
+        self._links = None
+        if self.group.dist is not None and self.group.halo == "neighbours":
+            parts = self.shards[0].parts
+            sets = [_reduced_sets(p, s.cell_rank, parts) for p, s in zip(plans, self.shards)]
+            self._links = []
+            for i, (off, col, _) in enumerate(transfers):
+                lk = _TransferLinks(rank, parts, off, col, sets[i][0], sets[i][1], sets[i + 1][0], sets[i + 1][1],
+                                    np.asarray(self.shards[i].global_reduced, dtype=np.int64), dev)
+                loc, colg, v = self._P[i]
+                cg = colg.cpu().numpy()
+                own = (loc < self.shards[i + 1].n_owned).cpu().numpy()
+                lk.pos_need = torch.as_tensor(np.searchsorted(lk.need, cg), device=dev)
+                lk.own = torch.as_tensor(np.nonzero(own)[0], device=dev)
+                lk.pos_own = torch.as_tensor(np.searchsorted(lk.cols_own, cg[own]), device=dev)
+                self._links.append(lk)
         # coarse matrix from sharded applies of unit vectors (the same sequence on every rank)
         n0 = self.n_global[0]
         A0 = np.zeros((n0, n0))
@@ -597,11 +734,24 @@ class ShardedMultigrid:
         nc = self.shards[level - 1].n_reduced
         fo = self.shards[level].n_owned
         loc, col, val = self._P[level - 1]
+        bc = self.ops.vector(nc)
+        if self._links is not None:
+            lk = self._links[level - 1]
+            torch = self.torch
+            pc = torch.zeros(lk.cols_own.size, dtype=torch.float64, device=self.device)
+            pc.index_add_(0, lk.pos_own, val[lk.own] * r[loc[lk.own]])
+            bl = lk.restrict(self.group, pc, nc)
+            if nc:
+                bc[:nc] = bl[:nc]
+            xc = self.vcycle(level - 1, bc)
+            xn = lk.needed_values(self.group, xc, torch.zeros(lk.need.size, dtype=torch.float64, device=self.device))
+            if n:
+                x.index_add_(0, loc, val * xn[lk.pos_need])
+            return self._smooth(level, x, b, self.opts.post_smoothing_steps)
         own = loc < fo
         rc = self.torch.zeros(max(self.n_global[level - 1], 1), dtype=self.torch.float64, device=self.device)
         rc.index_add_(0, col[own], val[own] * r[loc[own]])
         self.group.allreduce([rc])
-        bc = self.ops.vector(nc)
         if nc:
             bc[:nc] = rc[self._local[level - 1]]
         xc = self.vcycle(level - 1, bc)

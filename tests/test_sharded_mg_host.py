@@ -50,6 +50,7 @@ def _gloo_rank(rank, world, port, out, name):
         _, plan = _pair(name)
         ops = HostOps()
         mg = ShardedMultigrid(plan, rank, world, ops=ops, device=False, group=ShardGroup())
+        assert mg._links is not None and len(mg._links) == len(mg.shards) - 1  # point-to-point transfers
         fine = mg.shards[-1]
         r = np.random.default_rng(2).standard_normal(plan.n_reduced)
         z = mg.apply(ops.upload(fine.scatter(r))).numpy()[: fine.n_reduced]
@@ -65,11 +66,12 @@ def _gloo_rank(rank, world, port, out, name):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("name", ["2d_p4", "3d_p2"])
-def test_sharded_vcycle_and_pcg_two_gloo_ranks(tmp_path, name):
-    """world_size 2 over gloo: every level split in two; the V-cycle of a residual and the
-    GMG-preconditioned CG solution match the oracle's; each level's owned dofs partition it."""
-    world = 2
+@pytest.mark.parametrize("name,world", [("2d_p4", 2), ("3d_p2", 2), ("2d_p4", 3)])
+def test_sharded_vcycle_and_pcg_gloo_ranks(tmp_path, name, world):
+    """world_size 2 and 3 over gloo: every level split across the ranks, halos and transfers
+    exchanged point to point between the ranks that share entries; the V-cycle of a residual
+    and the GMG-preconditioned CG solution match the oracle's; each level's owned dofs
+    partition it."""
     mp.start_processes(_gloo_rank, args=(world, _free_port(), str(tmp_path), name), nprocs=world, join=True,
                        start_method="spawn")
     oplans, plan = _pair(name)
