@@ -165,10 +165,13 @@ T* solver_ws(GricoPlan* P, int slot, int64_t count) {
 }
 
 // Lockstep preconditioned CG on nrhs stacked systems A x_s = b_s from x_s = 0, stopping
-// system s once ||r_s||^2 <= tol2[s].
+// system s once ||r_s||^2 <= tol2[s].  keep (optional): the instantiated iteration graph of an
+// earlier call with the same x, dinv and nrhs on this plan (its other buffers are the plan's
+// work vectors), reused instead of a new capture; a newly captured graph is left there for the
+// caller to destroy.
 template <typename T>
 int multi_cg(GricoPlan* P, const T* b, T* x, int nrhs, const std::vector<double>& tol2, int maxiter, const T* dinv,
-             bool graph, cudaStream_t st, MultiResult& res) {
+             bool graph, cudaStream_t st, MultiResult& res, cudaGraphExec_t* keep = nullptr) {
   const int64_t n = P->n_red;
   const int64_t nn = n * nrhs;
   T *r = solver_ws<T>(P, 0, nn), *z = solver_ws<T>(P, 1, nn), *p = solver_ws<T>(P, 2, nn), *q = solver_ws<T>(P, 3, nn);
@@ -225,8 +228,8 @@ int multi_cg(GricoPlan* P, const T* b, T* x, int nrhs, const std::vector<double>
                                                  nrhs);
     return GRICO_OK;
   };
-  cudaGraphExec_t exec = nullptr;
-  if (graph && n_active > 0) {
+  cudaGraphExec_t exec = keep ? *keep : nullptr;
+  if (graph && n_active > 0 && !exec) {
     cudaGraph_t g = nullptr;
     if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
       const int crc = iteration(st);
@@ -258,7 +261,8 @@ int multi_cg(GricoPlan* P, const T* b, T* x, int nrhs, const std::vector<double>
     n_active = 0;
     for (int s = 0; s < nrhs; ++s) n_active += ha[s];
   }
-  if (exec) cudaGraphExecDestroy(exec);
+  if (keep) *keep = exec;
+  else if (exec) cudaGraphExecDestroy(exec);
   cudaMemcpyAsync(res.iters.data(), d_iters, sizeof(int) * nrhs, cudaMemcpyDeviceToHost, st);
   cudaMemcpyAsync(res.status.data(), d_status, sizeof(int) * nrhs, cudaMemcpyDeviceToHost, st);
   cudaMemcpyAsync(hrr.data(), last_rr, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st);
@@ -351,6 +355,7 @@ extern "C" int grico_cg_solve_multi(GricoPlan* P, const double* B, double* X, in
     cudaMemsetAsync(xd, 0, sizeof(double) * nn, st);
     cudaMemcpyAsync(r64, bd, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st);
     std::vector<int> done(nrhs, 0);
+    cudaGraphExec_t inner_graph = nullptr;
     for (int outer = 0; outer < 60; ++outer) {
       multi_dot<double><<<dim3(kMultiBlocks, nrhs), 256, 0, st>>>(r64, r64, nullptr, n, part);
       multi_reduce<<<nrhs, 256, 0, st>>>(part, kMultiBlocks, bn);
@@ -369,8 +374,8 @@ extern "C" int grico_cg_solve_multi(GricoPlan* P, const double* B, double* X, in
       for (int s = 0; s < nrhs; ++s) over = over || (!done[s] && total[s] >= opts->maxiter);
       if (over) break;
       cast_copy<double, float><<<gblocks(nn), 256, 0, st>>>(r64, r32, nn);
-      rc = multi_cg<float>(P, r32, e32, nrhs, inner_tol2, opts->maxiter, dinv32,
-                           graph, st, res);
+      // every refinement step solves into the same buffers: one iteration graph serves them all
+      rc = multi_cg<float>(P, r32, e32, nrhs, inner_tol2, opts->maxiter, dinv32, graph, st, res, &inner_graph);
       if (rc) break;
       for (int s = 0; s < nrhs; ++s) {
         if (done[s]) continue;
@@ -382,6 +387,7 @@ extern "C" int grico_cg_solve_multi(GricoPlan* P, const double* B, double* X, in
       run_apply<double>(P, true, xd, ax, nrhs, st);
       axpby_kernel<double><<<grid_blocks(nn), 256, 0, st>>>(-1.0, ax, 1.0, r64, nn);
     }
+    if (inner_graph) cudaGraphExecDestroy(inner_graph);
     for (int s = 0; s < nrhs; ++s)
       if (status[s] == GRICO_OK && final_rr[s] > tol2[s]) status[s] = GRICO_ERR_NOT_CONVERGED;
   }
