@@ -139,6 +139,24 @@ __global__ void chebyshev_from_zero(T* __restrict__ x, T* __restrict__ d, const 
   }
 }
 
+// Three-term Chebyshev step: nxt = x_k + c1 (x_k - x_{k-1}) + c2 dinv (b - A x_k), with x_k in
+// `cur` and x_{k-1} in `nxt` (overwritten).  cur_zero: x_k = 0 (not read, and ax == nullptr:
+// no apply); prev_zero: x_{k-1} = 0 (not read); c1 == 0 reads no x_{k-1} either.  With `clear`
+// the product ax is zeroed after the read; `clear_t` (when ax is null) is zeroed instead.
+template <typename T>
+__global__ void chebyshev3_step(T* __restrict__ nxt, const T* __restrict__ cur, const T* __restrict__ b,
+                                T* __restrict__ ax, const T* __restrict__ dinv, T c1, T c2, int64_t n,
+                                bool cur_zero, bool prev_zero, bool clear, T* __restrict__ clear_t) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    const T xk = cur_zero ? T(0) : cur[i];
+    const T r = ax ? b[i] - ax[i] : b[i];
+    const T prev = (c1 != T(0) && !prev_zero) ? nxt[i] : T(0);
+    nxt[i] = xk + (c1 != T(0) ? c1 * (xk - prev) : T(0)) + c2 * dinv[i] * r;
+    if (clear && ax) ax[i] = T(0);
+    if (clear_t) clear_t[i] = T(0);
+  }
+}
+
 // r = b - ax (ax cleared after the read with `clear`)
 template <typename T>
 __global__ void residual_kernel(T* __restrict__ r, const T* __restrict__ b, T* __restrict__ ax, int64_t n,
@@ -250,8 +268,8 @@ void smooth(GricoMultigrid* mg, int l, T* x, const T* b, int steps, cudaStream_t
     return;
   }
   const bool clear = t_zero != nullptr;
-  auto apply_t = [&]() {
-    level_apply<T>(mg, l, x, t, st, clear && *t_zero);
+  auto apply_t = [&](const T* v) {
+    level_apply<T>(mg, l, v, t, st, clear && *t_zero);
     if (clear) *t_zero = false;
   };
   if (mg->opts.smoother == GRICO_SMOOTHER_JACOBI) {
@@ -260,7 +278,7 @@ void smooth(GricoMultigrid* mg, int l, T* x, const T* b, int steps, cudaStream_t
         jacobi_from_zero<T><<<blocks(n), 256, 0, st>>>(x, b, dinv, T(mg->opts.jacobi_omega),
                                                        clear && !*t_zero ? t : nullptr, n);
       } else {
-        apply_t();
+        apply_t(x);
         jacobi_smooth<T><<<blocks(n), 256, 0, st>>>(x, b, t, dinv, T(mg->opts.jacobi_omega), n, clear);
       }
       if (clear) *t_zero = true;
@@ -272,16 +290,45 @@ void smooth(GricoMultigrid* mg, int l, T* x, const T* b, int steps, cudaStream_t
   const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin);
   const double sigma = theta / delta;
   T* d = B::d(mg, l);
+  const int degree = mg->opts.chebyshev_degree;
+  if (degree % 2 == 0) {
+    // Even degree: the three-term form x_{k+1} = x_k + c1 (x_k - x_{k-1}) + c2 D^-1 (b - A x_k)
+    // (the same recurrence, d_k = x_{k+1} - x_k), the iterates alternating between x and d, so
+    // each step streams x_k, x_{k-1}, b, A x_k and D^-1 and writes x_{k+1}: one vector fewer
+    // than the update form, and the sweep's last iterate lands in x.
+    for (int s = 0; s < steps; ++s) {
+      double rho_old = 1.0 / sigma;
+      for (int k = 0; k < degree; ++k) {
+        T* cur = (k % 2 == 0) ? x : d;
+        T* nxt = (k % 2 == 0) ? d : x;
+        const bool cur_zero = s == 0 && k == 0 && x_zero;
+        const bool prev_zero = s == 0 && k == 1 && x_zero;
+        if (!cur_zero) apply_t(cur);
+        double c1 = 0.0, c2 = 1.0 / theta;
+        if (k > 0) {
+          const double rho = 1.0 / (2.0 * sigma - rho_old);
+          c1 = rho * rho_old;
+          c2 = 2.0 * rho / delta;
+          rho_old = rho;
+        }
+        chebyshev3_step<T><<<blocks(n), 256, 0, st>>>(nxt, cur, b, cur_zero ? nullptr : t, dinv, T(c1), T(c2), n,
+                                                      cur_zero, prev_zero, clear,
+                                                      cur_zero && clear && !*t_zero ? t : nullptr);
+        if (clear) *t_zero = true;
+      }
+    }
+    return;
+  }
   for (int s = 0; s < steps; ++s) {
     double rho_old = 1.0 / sigma;
-    for (int k = 0; k < mg->opts.chebyshev_degree; ++k) {
+    for (int k = 0; k < degree; ++k) {
       if (s == 0 && k == 0 && x_zero) {
         chebyshev_from_zero<T><<<blocks(n), 256, 0, st>>>(x, d, b, dinv, T(1.0 / theta),
                                                           clear && !*t_zero ? t : nullptr, n);
         if (clear) *t_zero = true;
         continue;
       }
-      apply_t();
+      apply_t(x);
       if (k == 0) {
         chebyshev_step<T><<<blocks(n), 256, 0, st>>>(x, d, b, t, dinv, T(0), T(1.0 / theta), n, clear);
       } else {
