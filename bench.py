@@ -1037,7 +1037,10 @@ def main():
 
     sharded_info = None
     if world > 1 and not fcm:
-        sharded_info = sharded_leg(gb, plan, rank, world, args.steps, args.warmup)
+        try:
+            sharded_info = sharded_leg(gb, plan, rank, world, args.steps, args.warmup)
+        except Exception as exc:  # noqa: BLE001  (the headline line is printed either way)
+            sharded_info = {"error": f"{type(exc).__name__}: {exc}"[:200]}
 
     solve_info = None
     if not args.no_solve:
