@@ -97,3 +97,42 @@ def test_sharded_vcycle_and_pcg_gloo_ranks(tmp_path, name, world):
     # damped Jacobi on the modal basis is a weak smoother (~260 iterations to 1e-10 in 3-D), so
     # the order of the halo sums shifts the stopping iteration by a few percent
     assert len(its) == 1 and abs(its.pop() - iters) <= max(1, iters // 8)
+
+
+@pytest.mark.parametrize("name,parts", [("2d_p4", 3), ("3d_p2", 2)])
+def test_transfer_lists_agree_between_ranks(name, parts):
+    """The point-to-point transfer lists: each rank's local coarse set is its shard's; what rank
+    r sends rank q (restriction shares, prolongation values) is exactly what q expects from r;
+    and the CSR row gather equals a loop over the rows."""
+    from grico_b200.multigrid import GeometricMultigridPreconditioner, build_hierarchy
+    from grico_b200.sharded import ShardPlan, _csr_take, _reduced_sets, _TransferLinks
+
+    _, plan = _pair(name)
+    plans, transfers = build_hierarchy(plan, GeometricMultigridPreconditioner(), device=False)
+    shards = [[ShardPlan(p, r, parts, device=False) for p in plans] for r in range(parts)]
+    sets = [_reduced_sets(p, shards[0][i].cell_rank, parts) for i, p in enumerate(plans)]
+    for i, p in enumerate(plans):
+        for r in range(parts):
+            assert np.array_equal(np.sort(shards[r][i].global_reduced), sets[i][0][r])
+    moved = 0
+    for i, (off, col, _) in enumerate(transfers):
+        rows = np.arange(0, len(off) - 1, 3)
+        assert np.array_equal(_csr_take(off, rows), np.concatenate([np.arange(off[g], off[g + 1]) for g in rows]))
+        links = [_TransferLinks(r, parts, off, col, sets[i][0], sets[i][1], sets[i + 1][0], sets[i + 1][1],
+                                np.asarray(shards[r][i].global_reduced, dtype=np.int64), "cpu") for r in range(parts)]
+        for r, lk in enumerate(links):
+            for q, sel, sb in lk.r_send:
+                ids = lk.cols_own[sel.numpy()]
+                peer = next(x for x in links[q].r_recv if x[0] == r)
+                got = shards[q][i].global_reduced[peer[1].numpy()]
+                assert np.array_equal(ids, got) and sb.numel() == peer[2].numel()
+                moved += ids.size
+            for q, pos, sb in lk.p_send:
+                ids = shards[r][i].global_reduced[pos.numpy()]
+                peer = next(x for x in links[q].p_recv if x[0] == r)
+                assert np.array_equal(ids, links[q].need[peer[1].numpy()])
+                moved += ids.size
+        for r, lk in enumerate(links):  # and every expected receive has its send
+            assert all(any(x[0] == r for x in links[q].r_send) for q, _, _ in lk.r_recv)
+            assert all(any(x[0] == r for x in links[q].p_send) for q, _, _ in lk.p_recv)
+    assert moved > 0
