@@ -92,6 +92,54 @@ def test_chebyshev_recurrence_equals_polynomial(degree):
     assert rel_err(x - np.linalg.solve(A, b), ek) <= 1e-10
 
 
+def _three_term_sweeps(A, dinv, lam, degree, x, b, steps, x_zero):
+    """The device smoother's even-degree form (`chebyshev3_step` in csrc/grico_mg.cu), written
+    out with its two buffers: x_{k+1} = x_k + c1 (x_k - x_{k-1}) + c2 D^-1 (b - A x_k), iterates
+    alternating between `x` and `d`; with x_zero the first iterate is zero and not applied."""
+    lmax = 1.2 * lam
+    lmin = lmax / 15.0
+    theta, delta = 0.5 * (lmax + lmin), 0.5 * (lmax - lmin)
+    sigma = theta / delta
+    bufs = {"x": np.full_like(b, np.nan) if x_zero else x.copy(), "d": np.full_like(b, np.nan)}
+    for s in range(steps):
+        rho_old = 1.0 / sigma
+        for k in range(degree):
+            cur, nxt = ("x", "d") if k % 2 == 0 else ("d", "x")
+            cur_zero = s == 0 and k == 0 and x_zero
+            prev_zero = s == 0 and k == 1 and x_zero
+            xk = np.zeros_like(b) if cur_zero else bufs[cur]
+            r = b if cur_zero else b - A @ xk
+            c1, c2 = 0.0, 1.0 / theta
+            if k > 0:
+                rho = 1.0 / (2.0 * sigma - rho_old)
+                c1, c2 = rho * rho_old, 2.0 * rho / delta
+                rho_old = rho
+            prev = np.zeros_like(b) if (c1 == 0.0 or prev_zero) else bufs[nxt]
+            bufs[nxt] = xk + (c1 * (xk - prev) if c1 != 0.0 else 0.0) + c2 * dinv * r
+    return bufs["x"]
+
+
+@pytest.mark.parametrize("degree,steps,x_zero", [(2, 1, True), (2, 2, True), (4, 2, False), (2, 2, False)])
+def test_three_term_chebyshev_equals_update_form(degree, steps, x_zero):
+    """The even-degree three-term form of the device smoother gives the oracle's update-form
+    Chebyshev sweeps (Saad, Algorithm 12.1), from a zero or a given start, to rounding."""
+    rng = np.random.default_rng(3 + degree)
+    n = 40
+    Q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    A = Q @ np.diag(np.linspace(0.3, 25.0, n)) @ Q.T
+    A = 0.5 * (A + A.T)
+    dinv = 1.0 / np.diag(A)
+    lam = go.estimate_lambda_max(lambda v: A @ v, dinv, 1, iterations=100)
+    fake = types.SimpleNamespace(plans=[None, _dense_level(A)], dinv=[None, dinv], lmax=[0.0, lam],
+                                 chebyshev_lower=1.0 / 15.0, chebyshev_degree=degree)
+    b = rng.standard_normal(n)
+    x0 = np.zeros(n) if x_zero else rng.standard_normal(n)
+    ref = go.Multigrid.smooth_chebyshev(fake, 1, x0.copy(), b, steps)
+    got = _three_term_sweeps(A, dinv, lam, degree, x0, b, steps, x_zero)
+    assert np.all(np.isfinite(got))  # no NaN of the never-written buffers was read
+    assert rel_err(got, ref) <= 1e-13
+
+
 def test_power_iteration_start_is_deterministic():
     v = go.power_iteration_start(5, 3)
     assert np.all((v >= 0.5) & (v < 1.5))
